@@ -1,0 +1,178 @@
+/*
+ * linqt_gpu.h -- C ABI of the B200 Chebyshev-moment engine (liblinqt_gpu.so).
+ *
+ * The library computes LinQT's kernel-polynomial hot path on one NVIDIA B200
+ * (sm_100a): the Chebyshev recursion T_{n+1} = 2 H T_n - T_{n-1} on a rescaled
+ * sparse complex Hamiltonian, the 1D moments mu_n = <r|T_n(H)|r>, the 2D
+ * Kubo-Bastin moments mu_nm = <r|V T_m(H) V T_n(H)|r>, the FFT-based
+ * Bastin/Greenwood reconstruction of Kubo_solver_FFT, and the energy-grid
+ * reconstructions of the *FromChebmom post-processors.
+ *
+ * Conventions
+ *   - Complex numbers are interleaved (re, im) pairs of double.
+ *   - Operators are square CSR matrices, 0-based, int32 indices.  With
+ *     LINQT_STORAGE_HERMITIAN_UPPER (LinQT's convention, include/sparse_matrix.hpp:52-54)
+ *     only entries with col >= row are read, the diagonal counts once and the
+ *     lower triangle is the conjugate of the upper one.
+ *   - States are R consecutive length-N vectors (the `vector` state-file layout,
+ *     include/quantum_states.hpp:155-183).
+ *   - Every function returns LINQT_OK (0) or a negative LINQT_ERR_* code; the
+ *     message of the last error of the calling thread is linqt_last_error().
+ *     No function aborts or throws across the ABI.
+ *   - Host-pointer entry points copy inputs to the device and results back and
+ *     return when the results are on the host.  *_dev entry points take device
+ *     pointers and enqueue work on the session's stream without synchronising.
+ *   - A session (NULL = the calling thread's default session on the current
+ *     device) owns a CUDA stream and a cache of device workspaces; one session
+ *     must not be used by two host threads at once.
+ */
+#ifndef LINQT_GPU_H
+#define LINQT_GPU_H
+
+#include <stddef.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define LINQT_ABI_VERSION 1
+
+enum {
+  LINQT_OK = 0,
+  LINQT_ERR_INVALID = -1,     /* bad argument (size, pointer, CSR structure) */
+  LINQT_ERR_CUDA = -2,        /* a CUDA runtime call failed */
+  LINQT_ERR_NOMEM = -3,       /* device allocation failed or exceeds the session budget */
+  LINQT_ERR_UNSUPPORTED = -4, /* option combination not implemented */
+  LINQT_ERR_INTERNAL = -5,    /* unexpected internal failure */
+  LINQT_ERR_TIMEOUT = -6,     /* a bounded device wait expired */
+  LINQT_ERR_CANCELLED = -7    /* request cancelled (serving) */
+};
+
+enum { LINQT_STORAGE_HERMITIAN_UPPER = 0, LINQT_STORAGE_GENERAL = 1 };
+
+enum {
+  LINQT_PREC_FP64 = 0,  /* FP64 recursion, FP64 moment contraction */
+  LINQT_PREC_MIXED = 1, /* FP32 recursion, split-TF32 tensor-core contraction, FP64 accumulation */
+  LINQT_PREC_FP32 = 2   /* FP32 recursion, FP32 contraction (diagnostic) */
+};
+
+enum { LINQT_KUBO_GREENWOOD = 0, LINQT_KUBO_BASTIN = 1 }; /* chebyshev::formula, include/Kubo_solver_FFT.hpp:17-21 */
+
+enum { LINQT_FORMAT_CSR = 0, LINQT_FORMAT_SELL = 1, LINQT_FORMAT_AUTO = 2 };
+
+typedef struct linqt_op linqt_op;
+typedef struct linqt_session linqt_session;
+
+/* Solver options; zero-initialised = defaults (FP64, CSR, automatic tiling). */
+typedef struct linqt_opts {
+  int precision;    /* LINQT_PREC_* */
+  int format;       /* LINQT_FORMAT_*: sparse format of H in the recursion */
+  int block_width;  /* vector columns per recursion block (0 = all R, or the autotuned chunk) */
+  int doubling;     /* 1D only: 1 = use T_{2n} = 2T_n^2 - T_0 (identity operator only); 0 = direct <r|T_n r> */
+  int use_graphs;   /* 1 = replay the recursion as a captured CUDA graph */
+  int reserved[11];
+} linqt_opts;
+
+/* ---- library / sessions ------------------------------------------------ */
+int linqt_abi_version(void);
+const char *linqt_last_error(void);
+int linqt_session_create(int device, linqt_session **out);
+int linqt_session_destroy(linqt_session *s);
+/* Run the session's work on an externally owned stream (e.g. torch's current stream). */
+int linqt_session_set_stream(linqt_session *s, void *cuda_stream);
+int linqt_session_get_stream(linqt_session *s, void **cuda_stream);
+int linqt_session_synchronize(linqt_session *s);
+/* Release cached device workspaces. */
+int linqt_session_trim(linqt_session *s);
+/* Cumulative device time (ms, CUDA events on the session stream) spent in each
+ * phase since the last reset: [0] recursion, [1] moment contraction, [2] FFT
+ * reconstruction, [3] other; launches[0..3] the kernel launches per phase. */
+int linqt_session_phase_times(linqt_session *s, double ms[4], long launches[4], int reset);
+int linqt_session_enable_timing(linqt_session *s, int on);
+
+/* ---- operators: SparseMatrixType (include/sparse_matrix.hpp:45-88) ------ */
+/* ConvertFromCSR (src/mkl_sparse_matrix.cpp:39-54) + BuildOPFromCSRFile (include/sparse_matrix.hpp:100-108) */
+int linqt_csr_create(linqt_session *s, int n, const int *rowptr, const int *col, const double *val, int storage,
+                     linqt_op **out);
+int linqt_op_destroy(linqt_op *op);
+/* dimension and Hermitian-expanded non-zeros (diagonal included) */
+int linqt_op_info(const linqt_op *op, int *n, long *nnz);
+/* H <- a*H + b*I  -- SparseMatrixType::Rescale (src/mkl_sparse_matrix.cpp:73-97) */
+int linqt_op_rescale(linqt_op *op, const double a[2], const double b[2]);
+/* y <- a*op*x + b*y for ncols column-major vectors of length n (ld = n):
+ * SparseMatrixType::Multiply (src/mkl_sparse_matrix.cpp:56-69) for ncols = 1,
+ * SparseMatrixType::BatchMultiply (src/mkl_sparse_matrix.cpp:102-106) for ncols > 1.  Host pointers. */
+int linqt_op_multiply(linqt_session *s, const linqt_op *op, const double a[2], const double *x, const double b[2],
+                      double *y, int ncols);
+/* Gershgorin bounds of the Hermitian operator in FP64 on the device (replaces
+ * utility::SpectralBounds, src/chebyshev_solver.cpp:8-23, which reads ./BOUNDS). */
+int linqt_spectral_bounds(linqt_session *s, const linqt_op *op, double *lo, double *hi);
+
+/* ---- moment solvers ------------------------------------------------------ */
+/* chebyshev::SpectralMoments (src/chebyshev_solver.cpp:176-199): mu[2*M] =
+ * sum_r (2/R)(1/2)^{[m=0]} <r|T_m(H) OP|r>.  op = NULL is the identity. */
+int linqt_moments1d(linqt_session *s, const linqt_op *H, const linqt_op *op, const double *states, int R, int M,
+                    const linqt_opts *opts, double *mu);
+int linqt_moments1d_dev(linqt_session *s, const linqt_op *H, const linqt_op *op, const double *states_dev, int R,
+                        int M, const linqt_opts *opts, double *mu_dev);
+
+/* chebyshev::CorrelationExpansionMoments (src/chebyshev_solver.cpp:86-172) with the
+ * default BATCH_SIZE: mu[2*M*M] row-major mu(mL, mR), symmetrised and scaled by
+ * (4/R)(1/2)^{[mL=0]}(1/2)^{[mR=0]}.  opl/opr = NULL are identities. */
+int linqt_moments2d(linqt_session *s, const linqt_op *H, const linqt_op *opl, const linqt_op *opr,
+                    const double *states, int R, int M, const linqt_opts *opts, double *mu);
+int linqt_moments2d_dev(linqt_session *s, const linqt_op *H, const linqt_op *opl, const linqt_op *opr,
+                        const double *states_dev, int R, int M, const linqt_opts *opts, double *mu_dev);
+
+/* chebyshev::Kubo_solver_FFT::compute with one section (src/Kubo_solver_FFT.cpp:12-136,
+ * src/Bastin_FFTs.cpp:6-173, src/Greenwood_FFTs.cpp:6-91) and its post-processing
+ * (src/Kubo_solver_FFT_postProcess.cpp:120-397).  nump >= M.  Outputs of length nump,
+ * ascending energy: E (printed as a*E - b by the reference), sigma, integrand (Bastin;
+ * may be NULL).  band_width/band_center are the rescaling of H (a = band_width/2). */
+int linqt_kubo_fft(linqt_session *s, const linqt_op *H, const linqt_op *opl, const linqt_op *opr,
+                   const double *states, int R, int M, int nump, int formula, double band_width, double band_center,
+                   const linqt_opts *opts, double *E, double *sigma, double *integrand);
+int linqt_kubo_fft_dev(linqt_session *s, const linqt_op *H, const linqt_op *opl, const linqt_op *opr,
+                       const double *states_dev, int R, int M, int nump, int formula, double band_width,
+                       double band_center, const linqt_opts *opts, double *out_dev /* 3*nump: E, sigma, integrand */);
+
+/* ---- reconstructions (FP64 on the device) ------------------------------- */
+/* Moments1D::ApplyJacksonKernel (src/chebyshev_moments1D.cpp:68-87) followed by the DOS of
+ * spectralFunctionFromChebmom_FFTgrid (src/spectralFunctionFromChebmom_FFTgrid.cpp:35-75).
+ * mu[2*M] in; E, dos of length *num_out (= truncated M) out. */
+int linqt_dos_from_moments(linqt_session *s, const double *mu, int M, int N, double band_width, double band_center,
+                           double broad_meV, double *E, double *dos, int *num_out);
+/* Moments2D::ApplyJacksonKernel (src/chebyshev_moments2D.cpp:87-117) followed by
+ * kuboBastinFromChebmom (src/kuboBastinFromChebmom.cpp:35-81): num_div energies in
+ * [-xbound, xbound] (num_div <= 0 means 30*M'), *num_out = num_div-1 points written. */
+int linqt_bastin_from_moments(linqt_session *s, const double *mu, int M0, int M1, int N, double band_width,
+                              double band_center, double broad_meV, double xbound, int num_div, double *E,
+                              double *sigma, int *num_out);
+/* Jackson kernels alone (in place on host arrays; returns the truncated sizes). */
+int linqt_jackson1d(double *mu, int M, double band_width, double broad_meV, int *M_out);
+int linqt_jackson2d(double *mu, int M0, int M1, double band_width, double b0, double b1, int *M0_out, int *M1_out);
+
+/* ---- serving (continuous batching of DOS / Kubo-Bastin solves) ----------- */
+typedef struct linqt_server linqt_server;
+enum { LINQT_REQ_DOS = 0, LINQT_REQ_KUBO_BASTIN = 1 };
+typedef struct linqt_request {
+  int kind;              /* LINQT_REQ_* */
+  const linqt_op *H;     /* rescaled Hamiltonian (device resident) */
+  const linqt_op *op;    /* DOS: optional operator; Kubo: velocity used on both sides */
+  const double *states;  /* host, R x N (copied at submit) */
+  int R, M;
+  int precision;         /* LINQT_PREC_* */
+  double *mu_out;        /* host result buffer: 2*M (DOS) or 2*M*M (Kubo) */
+} linqt_request;
+int linqt_server_create(int device, size_t hbm_budget_bytes, int max_active, linqt_server **out);
+int linqt_server_submit(linqt_server *srv, const linqt_request *req, long *ticket);
+/* status: 0 pending, 1 running, 2 done, <0 error code; latency in ms once done */
+int linqt_server_poll(linqt_server *srv, long ticket, int *status, double *latency_ms);
+int linqt_server_wait_all(linqt_server *srv);
+int linqt_server_destroy(linqt_server *srv);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif

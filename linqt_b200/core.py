@@ -1,0 +1,282 @@
+"""Python host API over the C ABI.
+
+Mirrors the reference operations on the hot path:
+
+    Operator.from_csr / Operator.rescale / Operator.multiply   SparseMatrixType (include/sparse_matrix.hpp)
+    moments1d                                                  chebyshev::SpectralMoments
+    moments2d                                                  chebyshev::CorrelationExpansionMoments
+    kubo_fft                                                   chebyshev::Kubo_solver_FFT::compute
+    dos_from_moments                                           spectralFunctionFromChebmom_FFTgrid
+    bastin_from_moments                                        kuboBastinFromChebmom
+
+Host arrays are numpy; *_dev functions take device pointers (ints) or torch CUDA
+tensors and enqueue on the session stream.
+"""
+import ctypes
+
+import numpy as np
+
+from ._lib import Opts, check, load
+
+PREC_FP64, PREC_MIXED, PREC_FP32 = 0, 1, 2
+KUBO_GREENWOOD, KUBO_BASTIN = 0, 1
+STORAGE_HERMITIAN_UPPER, STORAGE_GENERAL = 0, 1
+
+
+def _dp(a):
+    return a.ctypes.data_as(ctypes.POINTER(ctypes.c_double))
+
+
+def _ip(a):
+    return a.ctypes.data_as(ctypes.POINTER(ctypes.c_int))
+
+
+def _c128(a):
+    return np.ascontiguousarray(np.asarray(a, dtype=np.complex128))
+
+
+def _ptr(x):
+    """Device pointer of a torch tensor or an int."""
+    if x is None:
+        return None
+    if isinstance(x, int):
+        return x
+    return x.data_ptr()
+
+
+def make_opts(precision=PREC_FP64, fmt=0, block_width=0, doubling=0, use_graphs=0):
+    o = Opts()
+    o.precision, o.format, o.block_width, o.doubling, o.use_graphs = precision, fmt, block_width, doubling, use_graphs
+    return o
+
+
+class Session:
+    """A CUDA stream plus cached device workspaces on one GPU."""
+
+    def __init__(self, device=0, stream=None):
+        h = ctypes.c_void_p()
+        check(load().linqt_session_create(device, ctypes.byref(h)))
+        self.h = h
+        if stream is not None:
+            self.set_stream(stream)
+
+    def close(self):
+        if getattr(self, "h", None):
+            check(load().linqt_session_destroy(self.h))
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def set_stream(self, stream):
+        """Adopt an external CUDA stream (an int handle or a torch.cuda.Stream)."""
+        ptr = stream if isinstance(stream, int) else stream.cuda_stream
+        check(load().linqt_session_set_stream(self.h, ctypes.c_void_p(ptr)))
+
+    def stream(self):
+        p = ctypes.c_void_p()
+        check(load().linqt_session_get_stream(self.h, ctypes.byref(p)))
+        return p.value or 0
+
+    def synchronize(self):
+        check(load().linqt_session_synchronize(self.h))
+
+    def trim(self):
+        check(load().linqt_session_trim(self.h))
+
+    def enable_timing(self, on=True):
+        check(load().linqt_session_enable_timing(self.h, 1 if on else 0))
+
+    def phase_times(self, reset=False):
+        """(ms[4], launches[4]) for recursion, contraction, FFT, other."""
+        ms = (ctypes.c_double * 4)()
+        ln = (ctypes.c_long * 4)()
+        check(load().linqt_session_phase_times(self.h, ms, ln, 1 if reset else 0))
+        return list(ms), list(ln)
+
+
+def _sh(session):
+    return None if session is None else session.h
+
+
+class Operator:
+    """A sparse operator resident on the GPU (SparseMatrixType)."""
+
+    def __init__(self, handle, session=None):
+        self.h = handle
+        self.session = session
+
+    @classmethod
+    def from_csr(cls, n, rowptr, col, val, storage=STORAGE_HERMITIAN_UPPER, session=None):
+        rowptr = np.ascontiguousarray(rowptr, dtype=np.int32)
+        col = np.ascontiguousarray(col, dtype=np.int32)
+        v = _c128(val).view(np.float64) if np.iscomplexobj(val) else np.ascontiguousarray(val, dtype=np.float64)
+        if len(rowptr) != n + 1:
+            raise ValueError("rowptr must have n+1 entries")
+        h = ctypes.c_void_p()
+        check(load().linqt_csr_create(_sh(session), n, _ip(rowptr), _ip(col), _dp(v), storage, ctypes.byref(h)))
+        return cls(h, session)
+
+    @classmethod
+    def from_file(cls, path, session=None):
+        """Read a LinQT CSR file (src/sparse_matrix.cpp:3-50)."""
+        from .formats import read_csr
+        n, rp, cl, vl = read_csr(path)
+        return cls.from_csr(n, rp, cl, vl, session=session)
+
+    def close(self):
+        if getattr(self, "h", None):
+            check(load().linqt_op_destroy(self.h))
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def info(self):
+        n = ctypes.c_int()
+        nnz = ctypes.c_long()
+        check(load().linqt_op_info(self.h, ctypes.byref(n), ctypes.byref(nnz)))
+        return n.value, nnz.value
+
+    @property
+    def n(self):
+        return self.info()[0]
+
+    @property
+    def nnz(self):
+        return self.info()[1]
+
+    def rescale(self, a, b):
+        """H <- a*H + b*I (SparseMatrixType::Rescale)."""
+        av = np.array([complex(a).real, complex(a).imag])
+        bv = np.array([complex(b).real, complex(b).imag])
+        check(load().linqt_op_rescale(self.h, _dp(av), _dp(bv)))
+        return self
+
+    def rescale_to_chebyshev(self, band_width, band_center):
+        """Moments::Rescale2ChebyshevDomain: H <- H/a - (c/a) I, a = band_width/2."""
+        a = band_width / 2.0
+        return self.rescale(1.0 / a, -band_center / a)
+
+    def multiply(self, x, a=1.0, b=0.0, y=None, session=None):
+        """y <- a*H*x + b*y for one vector (N,) or a column block (N, ncols) (column-major semantics)."""
+        x = _c128(x)
+        single = x.ndim == 1
+        X = x.reshape(-1, 1) if single else x
+        n, ncols = X.shape
+        # the C ABI takes ncols column-major vectors: transpose to (ncols, n) contiguous
+        xt = np.ascontiguousarray(X.T)
+        yt = np.zeros_like(xt) if y is None else np.ascontiguousarray(_c128(y).reshape(n, ncols).T)
+        av = np.array([complex(a).real, complex(a).imag])
+        bv = np.array([complex(b).real, complex(b).imag])
+        check(load().linqt_op_multiply(_sh(session or self.session), self.h, _dp(av), _dp(xt.view(np.float64)),
+                                       _dp(bv), _dp(yt.view(np.float64)), ncols))
+        out = yt.T
+        return out.reshape(-1) if single else np.ascontiguousarray(out)
+
+    def spectral_bounds(self, session=None):
+        lo, hi = ctypes.c_double(), ctypes.c_double()
+        check(load().linqt_spectral_bounds(_sh(session or self.session), self.h, ctypes.byref(lo), ctypes.byref(hi)))
+        return lo.value, hi.value
+
+
+def _oph(op):
+    return None if op is None else op.h
+
+
+def moments1d(H, op, states, M, opts=None, session=None):
+    """mu[M] of chebyshev::SpectralMoments over the R states (rows of `states`)."""
+    st = np.atleast_2d(_c128(states))
+    R = st.shape[0]
+    mu = np.zeros(M, np.complex128)
+    o = opts or make_opts()
+    check(load().linqt_moments1d(_sh(session), H.h, _oph(op), _dp(st.view(np.float64)), R, M, ctypes.byref(o),
+                                 _dp(mu.view(np.float64))))
+    return mu
+
+
+def moments1d_dev(H, op, states_dev, R, M, mu_dev, opts=None, session=None):
+    o = opts or make_opts()
+    check(load().linqt_moments1d_dev(_sh(session), H.h, _oph(op), ctypes.c_void_p(_ptr(states_dev)), R, M,
+                                     ctypes.byref(o), ctypes.c_void_p(_ptr(mu_dev))))
+
+
+def moments2d(H, opl, opr, states, M, opts=None, session=None):
+    """mu[M, M] of chebyshev::CorrelationExpansionMoments (row index follows OPL)."""
+    st = np.atleast_2d(_c128(states))
+    R = st.shape[0]
+    mu = np.zeros((M, M), np.complex128)
+    o = opts or make_opts()
+    check(load().linqt_moments2d(_sh(session), H.h, _oph(opl), _oph(opr), _dp(st.view(np.float64)), R, M,
+                                 ctypes.byref(o), _dp(mu.view(np.float64))))
+    return mu
+
+
+def moments2d_dev(H, opl, opr, states_dev, R, M, mu_dev, opts=None, session=None):
+    o = opts or make_opts()
+    check(load().linqt_moments2d_dev(_sh(session), H.h, _oph(opl), _oph(opr), ctypes.c_void_p(_ptr(states_dev)), R,
+                                     M, ctypes.byref(o), ctypes.c_void_p(_ptr(mu_dev))))
+
+
+def kubo_fft(H, opl, opr, states, M, nump, formula, band_width, band_center, opts=None, session=None):
+    """(E, sigma, integrand) of Kubo_solver_FFT with one section, nump >= M."""
+    st = np.atleast_2d(_c128(states))
+    R = st.shape[0]
+    E, s, integ = np.zeros(nump), np.zeros(nump), np.zeros(nump)
+    o = opts or make_opts()
+    check(load().linqt_kubo_fft(_sh(session), H.h, _oph(opl), _oph(opr), _dp(st.view(np.float64)), R, M, nump,
+                                formula, band_width, band_center, ctypes.byref(o), _dp(E), _dp(s), _dp(integ)))
+    return E, s, integ
+
+
+def kubo_fft_dev(H, opl, opr, states_dev, R, M, nump, formula, band_width, band_center, out_dev, opts=None,
+                 session=None):
+    o = opts or make_opts()
+    check(load().linqt_kubo_fft_dev(_sh(session), H.h, _oph(opl), _oph(opr), ctypes.c_void_p(_ptr(states_dev)), R, M,
+                                    nump, formula, band_width, band_center, ctypes.byref(o),
+                                    ctypes.c_void_p(_ptr(out_dev))))
+
+
+def dos_from_moments(mu, N, band_width, band_center, broad_meV, session=None):
+    """Jackson kernel + DOS on the Chebyshev grid (spectralFunctionFromChebmom_FFTgrid)."""
+    m = _c128(mu)
+    M = len(m)
+    E, d = np.zeros(M), np.zeros(M)
+    n = ctypes.c_int()
+    check(load().linqt_dos_from_moments(_sh(session), _dp(m.view(np.float64)), M, N, band_width, band_center,
+                                        broad_meV, _dp(E), _dp(d), ctypes.byref(n)))
+    return E[: n.value], d[: n.value]
+
+
+def bastin_from_moments(mu, N, band_width, band_center, broad_meV, xbound=0.99, num_div=0, session=None):
+    """Jackson kernel + Kubo-Bastin conductivity (kuboBastinFromChebmom)."""
+    m = _c128(mu)
+    M0, M1 = m.shape
+    nd = num_div if num_div > 0 else 30 * max(M0, M1)
+    E, s = np.zeros(nd), np.zeros(nd)
+    n = ctypes.c_int()
+    check(load().linqt_bastin_from_moments(_sh(session), _dp(m.view(np.float64)), M0, M1, N, band_width,
+                                           band_center, broad_meV, xbound, num_div, _dp(E), _dp(s), ctypes.byref(n)))
+    return E[: n.value], s[: n.value]
+
+
+def jackson1d(mu, band_width, broad_meV):
+    m = _c128(mu).copy()
+    n = ctypes.c_int()
+    check(load().linqt_jackson1d(_dp(m.view(np.float64)), len(m), band_width, broad_meV, ctypes.byref(n)))
+    return m[: n.value]
+
+
+def jackson2d(mu, band_width, b0, b1):
+    m = _c128(mu).copy()
+    M0, M1 = m.shape
+    a, b = ctypes.c_int(), ctypes.c_int()
+    check(load().linqt_jackson2d(_dp(m.view(np.float64)), M0, M1, band_width, b0, b1, ctypes.byref(a),
+                                 ctypes.byref(b)))
+    return m.reshape(-1)[: a.value * b.value].reshape(a.value, b.value)

@@ -1,0 +1,951 @@
+// C ABI of liblinqt_gpu.so: sessions, operators and the solver orchestration.
+//
+// Every entry point catches linqt::Error (and std::exception) and turns it into a
+// negative status plus a thread-local message; nothing aborts across the ABI.
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <memory>
+
+#include "internal.cuh"
+
+namespace linqt {
+
+static thread_local std::string g_last_error;
+
+void set_last_error(const std::string &msg) { g_last_error = msg; }
+
+[[noreturn]] void fail(int code, const std::string &msg) { throw Error(code, msg); }
+
+template <class F>
+static int guarded(F &&f) {
+  try {
+    f();
+    return LINQT_OK;
+  } catch (const Error &e) {
+    set_last_error(e.what());
+    return e.code;
+  } catch (const std::bad_alloc &) {
+    set_last_error("host allocation failed");
+    return LINQT_ERR_NOMEM;
+  } catch (const std::exception &e) {
+    set_last_error(e.what());
+    return LINQT_ERR_INTERNAL;
+  }
+}
+
+// ---------------------------------------------------------------------------
+// sessions
+// ---------------------------------------------------------------------------
+struct EventPair {
+  cudaEvent_t a, b;
+  int phase;
+};
+static thread_local std::vector<EventPair> *g_pending = nullptr;
+
+static void init_session(Session &s, int device) {
+  s.device = device;
+  LQ_CUDA(cudaSetDevice(device));
+  LQ_CUDA(cudaStreamCreateWithFlags(&s.stream, cudaStreamNonBlocking));
+  s.own_stream = true;
+  int sms = 0;
+  LQ_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device));
+  s.sm_count = sms;
+}
+
+void *Session::get(const std::string &name, size_t bytes) {
+  if (bytes == 0) bytes = 16;
+  auto it = ws.find(name);
+  if (it != ws.end() && it->second.second >= bytes) return it->second.first;
+  if (it != ws.end()) {
+    LQ_CUDA(cudaStreamSynchronize(stream));
+    LQ_CUDA(cudaFree(it->second.first));
+    ws.erase(it);
+  }
+  if (hbm_budget) {
+    size_t used = 0;
+    for (auto &kv : ws) used += kv.second.second;
+    if (used + bytes > hbm_budget)
+      fail(LINQT_ERR_NOMEM, "workspace '" + name + "' exceeds the session HBM budget");
+  }
+  void *p = nullptr;
+  cudaError_t e = cudaMalloc(&p, bytes);
+  if (e != cudaSuccess) {
+    cudaGetLastError();
+    fail(LINQT_ERR_NOMEM, "cudaMalloc(" + std::to_string(bytes) + ") for '" + name + "' failed: " +
+                              cudaGetErrorString(e));
+  }
+  // counters used by the last-block reductions must start at zero
+  if (name.find("counter") != std::string::npos) LQ_CUDA(cudaMemsetAsync(p, 0, bytes, stream));
+  ws[name] = {p, bytes};
+  return p;
+}
+
+void Session::trim() {
+  if (stream) cudaStreamSynchronize(stream);
+  for (auto &kv : ws) cudaFree(kv.second.first);
+  ws.clear();
+}
+
+Session::~Session() {
+  int cur = 0;
+  cudaGetDevice(&cur);
+  cudaSetDevice(device);
+  trim();
+  if (own_stream && stream) cudaStreamDestroy(stream);
+  cudaSetDevice(cur);
+}
+
+struct SessionPhaseLog {
+  std::vector<EventPair> pending;
+};
+static std::map<Session *, SessionPhaseLog> &phase_logs() {
+  static std::map<Session *, SessionPhaseLog> m;
+  return m;
+}
+static std::mutex g_log_mu;
+
+PhaseScope::PhaseScope(Session *s_, Phase p) : s(s_), ph(p) {
+  if (!s->timing) return;
+  LQ_CUDA(cudaEventCreate(&a));
+  LQ_CUDA(cudaEventCreate(&b));
+  LQ_CUDA(cudaEventRecord(a, s->stream));
+}
+
+PhaseScope::~PhaseScope() {
+  if (!a) return;
+  cudaEventRecord(b, s->stream);
+  std::lock_guard<std::mutex> g(g_log_mu);
+  phase_logs()[s].pending.push_back({a, b, (int)ph});
+}
+
+static void collect_phases(Session *s) {
+  std::vector<EventPair> v;
+  {
+    std::lock_guard<std::mutex> g(g_log_mu);
+    v.swap(phase_logs()[s].pending);
+  }
+  for (auto &e : v) {
+    cudaEventSynchronize(e.b);
+    float ms = 0.f;
+    cudaEventElapsedTime(&ms, e.a, e.b);
+    s->phase_ms[e.phase] += ms;
+    cudaEventDestroy(e.a);
+    cudaEventDestroy(e.b);
+  }
+}
+
+static std::map<int, std::unique_ptr<linqt_session>> &default_sessions() {
+  static thread_local std::map<int, std::unique_ptr<linqt_session>> m;
+  return m;
+}
+
+Session *default_session() {
+  int dev = 0;
+  LQ_CUDA(cudaGetDevice(&dev));
+  auto &m = default_sessions();
+  auto it = m.find(dev);
+  if (it == m.end()) {
+    std::unique_ptr<linqt_session> s(new linqt_session);
+    init_session(s->s, dev);
+    it = m.emplace(dev, std::move(s)).first;
+  }
+  return &it->second->s;
+}
+
+Session *resolve(linqt_session *s) {
+  Session *r = s ? &s->s : default_session();
+  LQ_CUDA(cudaSetDevice(r->device));
+  return r;
+}
+
+// ---------------------------------------------------------------------------
+// operators
+// ---------------------------------------------------------------------------
+// Hermitian expansion of an upper-stored CSR: entries with col >= row are used,
+// the lower triangle is conj(upper) (include/sparse_matrix.hpp:52-54).  Rows come out
+// sorted by column: the mirrored (lower) entries of row j are appended while
+// scanning rows i < j, before row j's own entries.
+static void expand_hermitian(int n, const std::vector<int> &urp, const std::vector<int> &ucol,
+                             const std::vector<double2> &uval, std::vector<int> &rp, std::vector<int> &col,
+                             std::vector<double2> &val) {
+  std::vector<long> cnt(n + 1, 0);
+  for (int i = 0; i < n; ++i)
+    for (int k = urp[i]; k < urp[i + 1]; ++k) {
+      const int j = ucol[k];
+      cnt[i]++;
+      if (j != i) cnt[j]++;
+    }
+  rp.assign(n + 1, 0);
+  long tot = 0;
+  for (int i = 0; i < n; ++i) {
+    rp[i] = (int)tot;
+    tot += cnt[i];
+    if (tot > 0x7fffffffL) fail(LINQT_ERR_INVALID, "operator has more than 2^31-1 non-zeros");
+  }
+  rp[n] = (int)tot;
+  col.resize(tot);
+  val.resize(tot);
+  std::vector<int> fill(rp.begin(), rp.end() - 1);
+  for (int i = 0; i < n; ++i)
+    for (int k = urp[i]; k < urp[i + 1]; ++k) {
+      const int j = ucol[k];
+      col[fill[i]] = j;
+      val[fill[i]++] = uval[k];
+      if (j != i) {
+        col[fill[j]] = i;
+        val[fill[j]++] = make_double2(uval[k].x, -uval[k].y);
+      }
+    }
+}
+
+void DeviceOp::free_device() {
+  cudaFree(d_rowptr);
+  cudaFree(d_col);
+  cudaFree(d_val64);
+  cudaFree(d_val32);
+  cudaFree(d_sell_off);
+  cudaFree(d_sell_w);
+  cudaFree(d_sell_col);
+  cudaFree(d_sell_val64);
+  cudaFree(d_sell_val32);
+  d_rowptr = d_col = nullptr;
+  d_val64 = nullptr;
+  d_val32 = nullptr;
+  d_sell_off = nullptr;
+  d_sell_w = d_sell_col = nullptr;
+  d_sell_val64 = nullptr;
+  d_sell_val32 = nullptr;
+  sell_C = 0;
+}
+
+void DeviceOp::upload() {
+  if (hermitian)
+    expand_hermitian(n, up_rowptr, up_col, up_val, rowptr, col, val);
+  else {
+    rowptr = up_rowptr;
+    col = up_col;
+    val = up_val;
+  }
+  nnz = rowptr[n];
+  free_device();
+  LQ_CUDA(cudaSetDevice(device));
+  LQ_CUDA(cudaMalloc(&d_rowptr, sizeof(int) * (n + 1)));
+  LQ_CUDA(cudaMalloc(&d_col, sizeof(int) * std::max(1L, nnz)));
+  LQ_CUDA(cudaMalloc(&d_val64, sizeof(double2) * std::max(1L, nnz)));
+  LQ_CUDA(cudaMemcpy(d_rowptr, rowptr.data(), sizeof(int) * (n + 1), cudaMemcpyHostToDevice));
+  if (nnz) {
+    LQ_CUDA(cudaMemcpy(d_col, col.data(), sizeof(int) * nnz, cudaMemcpyHostToDevice));
+    LQ_CUDA(cudaMemcpy(d_val64, val.data(), sizeof(double2) * nnz, cudaMemcpyHostToDevice));
+  }
+  version++;
+}
+
+void DeviceOp::ensure_fp32() {
+  std::lock_guard<std::mutex> g(mu);
+  if (d_val32) return;
+  std::vector<float2> v(std::max(1L, nnz));
+  for (long k = 0; k < nnz; ++k) v[k] = make_float2((float)val[k].x, (float)val[k].y);
+  LQ_CUDA(cudaMalloc(&d_val32, sizeof(float2) * v.size()));
+  LQ_CUDA(cudaMemcpy(d_val32, v.data(), sizeof(float2) * v.size(), cudaMemcpyHostToDevice));
+}
+
+void DeviceOp::ensure_sell(int) { fail(LINQT_ERR_UNSUPPORTED, "SELL-C layout not built in this library"); }
+
+// ---------------------------------------------------------------------------
+// block geometry
+// ---------------------------------------------------------------------------
+static int pow2_at_least(int r) {
+  int p = 1;
+  while (p < r) p <<= 1;
+  return p;
+}
+
+static size_t free_device_bytes() {
+  size_t fr = 0, tot = 0;
+  LQ_CUDA(cudaMemGetInfo(&fr, &tot));
+  return fr;
+}
+
+// states (R x N, device) -> chunk c of width Rc (power of two) as an N x Rc block
+static void chunk_block(Session *s, const double2 *states, int N, int R, int c0, int Rc, void *blk, bool fp32) {
+  const int w = std::min(Rc, R - c0);
+  states_to_block(s, states + (size_t)c0 * N, blk, N, w, Rc, fp32);
+}
+
+static linqt_opts defaults(const linqt_opts *o) {
+  linqt_opts d;
+  std::memset(&d, 0, sizeof(d));
+  if (o) d = *o;
+  return d;
+}
+
+// ---------------------------------------------------------------------------
+// 1D moments: chebyshev::SpectralMoments (src/chebyshev_solver.cpp:176-199)
+// ---------------------------------------------------------------------------
+static void moments1d_dev(Session *s, const DeviceOp &H, const DeviceOp *op, const double2 *states, int R, int M,
+                          const linqt_opts &o, double2 *mu) {
+  LQ_REQUIRE(R > 0 && M > 0, "moments1d: R and M must be positive");
+  LQ_REQUIRE(!op || op->n == H.n, "moments1d: operator dimension mismatch");
+  const int N = H.n;
+  const bool fp32 = o.precision != LINQT_PREC_FP64;
+  if (fp32) {
+    const_cast<DeviceOp &>(H).ensure_fp32();
+    if (op) const_cast<DeviceOp &>(*op).ensure_fp32();
+  }
+  const bool doubling = (o.doubling == 0 && op == nullptr) || o.doubling == 1;
+  LQ_REQUIRE(!(doubling && op), "moments1d: the doubling identities need the identity operator");
+  int Rc = o.block_width > 0 ? o.block_width : std::min(256, pow2_at_least(R));
+  Rc = std::min(256, pow2_at_least(Rc));
+  const int nchunks = (R + Rc - 1) / Rc;
+  const int steps = doubling ? (M + 1) / 2 : M;
+  const size_t esz = fp32 ? sizeof(float2) : sizeof(double2);
+  const size_t blk = esz * (size_t)N * Rc;
+  char *T = (char *)s->get("m1_T", 3 * blk);
+  double2 *dots = (double2 *)s->get("m1_dots", sizeof(double2) * 2 * (size_t)steps * nchunks);
+  LQ_CUDA(cudaMemsetAsync(dots, 0, sizeof(double2) * 2 * (size_t)steps * nchunks, s->stream));
+  PhaseScope ph(s, PH_RECURSION);
+  long launches = 0;
+  for (int c = 0; c < nchunks; ++c) {
+    void *b0 = T, *b1 = T + blk, *b2 = T + 2 * blk;
+    double2 *cd = dots + (size_t)2 * steps * c;
+    void *phi = b2;
+    chunk_block(s, states, N, R, c * Rc, Rc, phi, fp32);
+    launches++;
+    void *x;
+    if (doubling) {
+      x = phi;  // T_0 = phi
+    } else if (op) {
+      spmm(s, *op, make_double2(1, 0), phi, make_double2(0, 0), b0, Rc, fp32);  // T_0 = OP phi
+      launches++;
+      x = b0;
+    } else {
+      LQ_CUDA(cudaMemcpyAsync(b0, phi, blk, cudaMemcpyDeviceToDevice, s->stream));
+      x = b0;
+    }
+    // step 0: T_1 = H T_0
+    void *prev = nullptr, *cur = x;
+    void *next = doubling ? b1 : (x == b0 ? b1 : b0);
+    for (int st = 0; st < steps; ++st) {
+      StepArgs a;
+      a.x = cur;
+      a.yprev = prev;
+      const bool need_y = doubling ? (2 * st + 1 < M) : (st + 1 < M);
+      a.y = need_y ? (prev ? (void *)prev : next) : nullptr;
+      a.phi = phi;
+      a.dot_mode = doubling ? 2 : 1;
+      a.dots = cd + 2 * st;
+      cheb_step(s, H, a, Rc, fp32, o.format);
+      launches++;
+      if (!need_y) break;
+      void *ny = a.y;
+      prev = cur;
+      cur = ny;
+      if (!doubling && st == 0) {
+        // free buffer for the rest: the one that is neither prev nor cur nor phi
+      }
+    }
+  }
+  ph.launches(launches);
+  // assemble (sum chunk dots first)
+  if (nchunks > 1) {
+    // fold chunk c>0 into chunk 0 (fixed order) with a tiny kernel via the GEMM reducer
+    PhaseScope p2(s, PH_OTHER);
+    sum_chunks(s, dots, 2 * steps, nchunks);
+  }
+  PhaseScope p3(s, PH_OTHER);
+  moments1d_from_dots(s, dots, steps, M, R, doubling ? 2 : 1, mu);
+}
+
+// ---------------------------------------------------------------------------
+// L/R Chebyshev vector blocks (shared by the 2D moments and the FFT solver)
+//   L_m = T_m(H) OPL phi  (Moments::SetInitVectors(OP, phi) + Vectors::IterateAll,
+//                          src/chebyshev_moments.cpp:5-22, src/chebyshev_vectors.cpp:4-21)
+//   R_m = OPR T_m(H) phi  (+ Vectors::Multiply, src/chebyshev_vectors.cpp:24-51)
+// Lstore/Rstore: M blocks of N x Rc (site-major) each.
+// ---------------------------------------------------------------------------
+static long lr_vectors(Session *s, const DeviceOp &H, const DeviceOp *opl, const DeviceOp *opr, void *phi, int M,
+                       int Rc, bool fp32, char *Lstore, char *Rstore, char *tmp3, int format) {
+  const size_t esz = fp32 ? sizeof(float2) : sizeof(double2);
+  const size_t blk = esz * (size_t)H.n * Rc;
+  long launches = 0;
+  // ---- L side: the recursion runs in place inside the store
+  if (opl) {
+    spmm(s, *opl, make_double2(1, 0), phi, make_double2(0, 0), Lstore, Rc, fp32);
+  } else {
+    LQ_CUDA(cudaMemcpyAsync(Lstore, phi, blk, cudaMemcpyDeviceToDevice, s->stream));
+  }
+  launches++;
+  for (int m = 0; m + 1 < M; ++m) {
+    StepArgs a;
+    a.x = Lstore + blk * m;
+    a.yprev = m ? Lstore + blk * (m - 1) : nullptr;
+    a.y = Lstore + blk * (m + 1);
+    cheb_step(s, H, a, Rc, fp32, format);
+    launches++;
+  }
+  // ---- R side
+  if (!opr) {
+    LQ_CUDA(cudaMemcpyAsync(Rstore, phi, blk, cudaMemcpyDeviceToDevice, s->stream));
+    for (int m = 0; m + 1 < M; ++m) {
+      StepArgs a;
+      a.x = Rstore + blk * m;
+      a.yprev = m ? Rstore + blk * (m - 1) : nullptr;
+      a.y = Rstore + blk * (m + 1);
+      cheb_step(s, H, a, Rc, fp32, format);
+      launches++;
+    }
+    return launches;
+  }
+  // T_m live in three rotating buffers; each step also writes OPR T_m into Rstore[m]
+  char *buf[3] = {tmp3, tmp3 + blk, tmp3 + 2 * blk};
+  void *prev = nullptr, *cur = phi;
+  int nb = 0;
+  for (int m = 0; m < M; ++m) {
+    StepArgs a;
+    a.x = cur;
+    a.yprev = prev;
+    a.V = opr;
+    a.vout = Rstore + blk * m;
+    if (m + 1 < M) {
+      void *dst = buf[nb % 3];
+      if (dst == cur || dst == prev) dst = buf[(++nb) % 3];
+      if (dst == cur || dst == prev) dst = buf[(++nb) % 3];
+      a.y = dst;
+      nb++;
+    }
+    cheb_step(s, H, a, Rc, fp32, format);
+    launches++;
+    prev = cur;
+    cur = a.y;
+  }
+  return launches;
+}
+
+struct Chunking {
+  int Rc, nchunks;
+};
+
+// pick the vector-chunk width so that 2 stores of M*N*Rc + buffers fit in memory
+static Chunking pick_chunks(Session *s, int N, int R, int M, size_t esz, const linqt_opts &o, size_t extra) {
+  int Rc = o.block_width > 0 ? pow2_at_least(o.block_width) : pow2_at_least(R);
+  Rc = std::min(Rc, 256);
+  size_t avail;
+  if (s->hbm_budget) {
+    // a session with a fixed budget (serving) chunks by the budget alone, so the
+    // result does not depend on what else occupies the device
+    avail = s->hbm_budget;
+  } else {
+    avail = free_device_bytes();
+    // keep what this session already caches for the same buffers
+    for (auto &kv : s->ws) avail += kv.second.second;
+    avail = (size_t)(avail * 0.90);
+  }
+  while (Rc > 1) {
+    const size_t need = esz * (size_t)N * Rc * (2 * (size_t)M + 4) + extra;
+    if (need <= avail) break;
+    Rc >>= 1;
+  }
+  const size_t need = esz * (size_t)N * Rc * (2 * (size_t)M + 4) + extra;
+  if (need > avail)
+    fail(LINQT_ERR_NOMEM, "2D moments: " + std::to_string(need >> 20) + " MiB of Chebyshev blocks exceed the " +
+                              std::to_string(avail >> 20) + " MiB available");
+  return {Rc, (R + Rc - 1) / Rc};
+}
+
+// ---------------------------------------------------------------------------
+// 2D moments: chebyshev::CorrelationExpansionMoments (src/chebyshev_solver.cpp:86-172)
+// ---------------------------------------------------------------------------
+static void moments2d_dev(Session *s, const DeviceOp &H, const DeviceOp *opl, const DeviceOp *opr,
+                          const double2 *states, int R, int M, const linqt_opts &o, double2 *mu) {
+  LQ_REQUIRE(R > 0 && M > 0, "moments2d: R and M must be positive");
+  LQ_REQUIRE((!opl || opl->n == H.n) && (!opr || opr->n == H.n), "moments2d: operator dimension mismatch");
+  if (o.precision != LINQT_PREC_FP64)
+    fail(LINQT_ERR_UNSUPPORTED, "moments2d: mixed precision is provided by the tensor-core build");
+  const int N = H.n;
+  const size_t esz = sizeof(double2);
+  const Chunking ch = pick_chunks(s, N, R, M, esz, o, sizeof(double2) * (size_t)M * M * 64);
+  const size_t blk = esz * (size_t)N * ch.Rc;
+  char *Ls = (char *)s->get("lr_L", blk * M);
+  char *Rs = (char *)s->get("lr_R", blk * M);
+  char *tmp = (char *)s->get("lr_tmp", blk * 4);
+  double2 *raw = (double2 *)s->get("mu_raw", sizeof(double2) * (size_t)M * M);
+  LQ_CUDA(cudaMemsetAsync(raw, 0, sizeof(double2) * (size_t)M * M, s->stream));
+  for (int c = 0; c < ch.nchunks; ++c) {
+    void *phi = tmp + 3 * blk;
+    {
+      PhaseScope ph(s, PH_RECURSION);
+      chunk_block(s, states, N, R, c * ch.Rc, ch.Rc, phi, false);
+      ph.launches(1 + lr_vectors(s, H, opl, opr, phi, M, ch.Rc, false, Ls, Rs, tmp, o.format));
+    }
+    {
+      PhaseScope ph(s, PH_CONTRACT);
+      mu_contract(s, Ls, Rs, M, (long)N * ch.Rc, false, o.precision, raw);
+      ph.launches(2);
+    }
+  }
+  PhaseScope ph(s, PH_OTHER);
+  mu_finalize(s, raw, M, R, mu);
+  ph.launches(1);
+}
+
+// ---------------------------------------------------------------------------
+// Kubo_solver_FFT::compute (src/Kubo_solver_FFT.cpp:12-136)
+// ---------------------------------------------------------------------------
+
+static void kubo_fft_dev(Session *s, const DeviceOp &H, const DeviceOp *opl, const DeviceOp *opr,
+                         const double2 *states, int R, int M, int nump, int formula, double bw, double bc,
+                         const linqt_opts &o, double *out) {
+  LQ_REQUIRE(R > 0 && M > 0, "kubo_fft: R and M must be positive");
+  LQ_REQUIRE(nump >= M, "kubo_fft: nump must be >= M (pre_factors are indexed m < M, src/Bastin_FFTs.cpp:18-21)");
+  LQ_REQUIRE(formula == LINQT_KUBO_BASTIN || formula == LINQT_KUBO_GREENWOOD, "kubo_fft: unknown formula");
+  LQ_REQUIRE(bw > 0, "kubo_fft: band_width must be positive");
+  if (o.precision != LINQT_PREC_FP64) fail(LINQT_ERR_UNSUPPORTED, "kubo_fft: FP64 only");
+  const int N = H.n;
+  const Chunking ch = pick_chunks(s, N, R, M, sizeof(double2), o, sizeof(double2) * 2 * (size_t)nump * 1024);
+  const size_t blk = sizeof(double2) * (size_t)N * ch.Rc;
+  char *Ls = (char *)s->get("lr_L", blk * M);
+  char *Rs = (char *)s->get("lr_R", blk * M);
+  char *tmp = (char *)s->get("lr_tmp", blk * 4);
+  double2 *acc = (double2 *)s->get("kubo_acc", sizeof(double2) * 2 * (size_t)nump);
+  double2 *acc_c = (double2 *)s->get("kubo_acc_c", sizeof(double2) * 2 * (size_t)nump);
+  LQ_CUDA(cudaMemsetAsync(acc, 0, sizeof(double2) * 2 * (size_t)nump, s->stream));
+  for (int c = 0; c < ch.nchunks; ++c) {
+    void *phi = tmp + 3 * blk;
+    {
+      PhaseScope ph(s, PH_RECURSION);
+      chunk_block(s, states, N, R, c * ch.Rc, ch.Rc, phi, false);
+      ph.launches(1 + lr_vectors(s, H, opl, opr, phi, M, ch.Rc, false, Ls, Rs, tmp, o.format));
+    }
+    {
+      PhaseScope ph(s, PH_FFT);
+      kubo_fft_sites(s, Ls, Rs, (long)N * ch.Rc, M, nump, formula, false, acc_c);
+      add_into(s, acc, acc_c, 2 * nump);
+      ph.launches(4);
+    }
+  }
+  PhaseScope ph(s, PH_OTHER);
+  kubo_postprocess(s, acc, R, nump, formula, N, bw, bc, out);
+  ph.launches(1);
+}
+
+void moments1d_for_server(Session *s, const DeviceOp &H, const DeviceOp *op, const double2 *states, int R, int M,
+                          int precision, double2 *mu) {
+  linqt_opts o = defaults(nullptr);
+  o.precision = precision;
+  moments1d_dev(s, H, op, states, R, M, o, mu);
+}
+
+void moments2d_for_server(Session *s, const DeviceOp &H, const DeviceOp *opl, const DeviceOp *opr,
+                          const double2 *states, int R, int M, int precision, double2 *mu) {
+  linqt_opts o = defaults(nullptr);
+  o.precision = precision;
+  moments2d_dev(s, H, opl, opr, states, R, M, o, mu);
+}
+
+// ---------------------------------------------------------------------------
+// host staging helpers
+// ---------------------------------------------------------------------------
+struct DevBuf {
+  void *p = nullptr;
+  explicit DevBuf(size_t bytes) {
+    cudaError_t e = cudaMalloc(&p, std::max<size_t>(bytes, 16));
+    if (e != cudaSuccess) {
+      cudaGetLastError();
+      fail(LINQT_ERR_NOMEM, std::string("cudaMalloc failed: ") + cudaGetErrorString(e));
+    }
+  }
+  ~DevBuf() { cudaFree(p); }
+};
+
+static const DeviceOp *dop(const linqt_op *o) { return o ? &o->op : nullptr; }
+
+static void check_op(const linqt_op *o, const char *what) {
+  if (!o) fail(LINQT_ERR_INVALID, std::string(what) + " is NULL");
+}
+
+}  // namespace linqt
+
+using namespace linqt;
+
+// ===========================================================================
+// C entry points
+// ===========================================================================
+extern "C" {
+
+int linqt_abi_version(void) { return LINQT_ABI_VERSION; }
+
+const char *linqt_last_error(void) { return g_last_error.c_str(); }
+
+int linqt_session_create(int device, linqt_session **out) {
+  return guarded([&] {
+    LQ_REQUIRE(out, "out is NULL");
+    int n = 0;
+    LQ_CUDA(cudaGetDeviceCount(&n));
+    LQ_REQUIRE(device >= 0 && device < n, "no such device");
+    std::unique_ptr<linqt_session> s(new linqt_session);
+    init_session(s->s, device);
+    *out = s.release();
+  });
+}
+
+int linqt_session_destroy(linqt_session *s) {
+  return guarded([&] {
+    if (!s) return;
+    {
+      std::lock_guard<std::mutex> g(g_log_mu);
+      for (auto &e : phase_logs()[&s->s].pending) {
+        cudaEventDestroy(e.a);
+        cudaEventDestroy(e.b);
+      }
+      phase_logs().erase(&s->s);
+    }
+    delete s;
+  });
+}
+
+int linqt_session_set_stream(linqt_session *s, void *stream) {
+  return guarded([&] {
+    Session *r = resolve(s);
+    LQ_CUDA(cudaStreamSynchronize(r->stream));
+    if (r->own_stream) LQ_CUDA(cudaStreamDestroy(r->stream));
+    r->stream = (cudaStream_t)stream;
+    r->own_stream = false;
+  });
+}
+
+int linqt_session_get_stream(linqt_session *s, void **stream) {
+  return guarded([&] {
+    LQ_REQUIRE(stream, "stream is NULL");
+    *stream = (void *)resolve(s)->stream;
+  });
+}
+
+int linqt_session_synchronize(linqt_session *s) {
+  return guarded([&] { LQ_CUDA(cudaStreamSynchronize(resolve(s)->stream)); });
+}
+
+int linqt_session_trim(linqt_session *s) {
+  return guarded([&] { resolve(s)->trim(); });
+}
+
+int linqt_session_enable_timing(linqt_session *s, int on) {
+  return guarded([&] { resolve(s)->timing = on != 0; });
+}
+
+int linqt_session_phase_times(linqt_session *s, double ms[4], long launches[4], int reset) {
+  return guarded([&] {
+    Session *r = resolve(s);
+    collect_phases(r);
+    for (int i = 0; i < 4; ++i) {
+      if (ms) ms[i] = r->phase_ms[i];
+      if (launches) launches[i] = r->phase_launches[i];
+      if (reset) {
+        r->phase_ms[i] = 0;
+        r->phase_launches[i] = 0;
+      }
+    }
+  });
+}
+
+int linqt_csr_create(linqt_session *s, int n, const int *rowptr, const int *col, const double *val, int storage,
+                     linqt_op **out) {
+  return guarded([&] {
+    LQ_REQUIRE(out && rowptr, "NULL argument");
+    LQ_REQUIRE(n > 0, "dimension must be positive");
+    LQ_REQUIRE(rowptr[n] == 0 || (col && val), "NULL col/val with non-zeros");
+    LQ_REQUIRE(storage == LINQT_STORAGE_HERMITIAN_UPPER || storage == LINQT_STORAGE_GENERAL, "unknown storage");
+    LQ_REQUIRE(rowptr[0] == 0, "rowptr[0] must be 0");
+    for (int i = 0; i < n; ++i) LQ_REQUIRE(rowptr[i + 1] >= rowptr[i], "rowptr must be non-decreasing");
+    const long nnz_in = rowptr[n];
+    Session *r = resolve(s);
+    std::unique_ptr<linqt_op> h(new linqt_op);
+    DeviceOp &d = h->op;
+    d.device = r->device;
+    d.n = n;
+    d.hermitian = storage == LINQT_STORAGE_HERMITIAN_UPPER;
+    // keep the stored part the way the library interprets it, rows sorted by column
+    d.up_rowptr.assign(n + 1, 0);
+    std::vector<std::pair<int, double2>> row;
+    for (int i = 0; i < n; ++i) {
+      row.clear();
+      for (long k = rowptr[i]; k < rowptr[i + 1]; ++k) {
+        const int j = col[k];
+        LQ_REQUIRE(j >= 0 && j < n, "column index out of range at row " + std::to_string(i));
+        if (d.hermitian && j < i) continue;  // strictly lower entries are ignored
+        row.push_back({j, make_double2(val[2 * k], val[2 * k + 1])});
+      }
+      std::stable_sort(row.begin(), row.end(),
+                       [](const std::pair<int, double2> &a, const std::pair<int, double2> &b) { return a.first < b.first; });
+      for (auto &e : row) {
+        if (!d.up_col.empty() && (long)d.up_col.size() > d.up_rowptr[i] && d.up_col.back() == e.first) {
+          d.up_val.back().x += e.second.x;  // duplicate entries are summed
+          d.up_val.back().y += e.second.y;
+          continue;
+        }
+        d.up_col.push_back(e.first);
+        d.up_val.push_back(e.second);
+      }
+      d.up_rowptr[i + 1] = (int)d.up_col.size();
+    }
+    (void)nnz_in;
+    d.upload();
+    *out = h.release();
+  });
+}
+
+int linqt_op_destroy(linqt_op *op) {
+  return guarded([&] {
+    if (!op) return;
+    int cur = 0;
+    cudaGetDevice(&cur);
+    cudaSetDevice(op->op.device);
+    cudaDeviceSynchronize();
+    op->op.free_device();
+    cudaSetDevice(cur);
+    delete op;
+  });
+}
+
+int linqt_op_info(const linqt_op *op, int *n, long *nnz) {
+  return guarded([&] {
+    check_op(op, "op");
+    if (n) *n = op->op.n;
+    if (nnz) *nnz = op->op.nnz;
+  });
+}
+
+// SparseMatrixType::Rescale (src/mkl_sparse_matrix.cpp:73-97): C = a*A + b*I on the stored
+// entries (mkl_sparse_z_add); a missing diagonal entry is inserted.
+int linqt_op_rescale(linqt_op *op, const double a[2], const double b[2]) {
+  return guarded([&] {
+    check_op(op, "op");
+    LQ_REQUIRE(a && b, "NULL scale");
+    DeviceOp &d = op->op;
+    std::lock_guard<std::mutex> g(d.mu);
+    LQ_CUDA(cudaSetDevice(d.device));
+    LQ_CUDA(cudaDeviceSynchronize());
+    const double2 A = make_double2(a[0], a[1]), B = make_double2(b[0], b[1]);
+    std::vector<int> rp(d.n + 1, 0), cl;
+    std::vector<double2> vl;
+    cl.reserve(d.up_col.size() + d.n);
+    vl.reserve(d.up_col.size() + d.n);
+    for (int i = 0; i < d.n; ++i) {
+      bool placed = false;
+      for (int k = d.up_rowptr[i]; k < d.up_rowptr[i + 1]; ++k) {
+        const int j = d.up_col[k];
+        if (!placed && j > i) {
+          cl.push_back(i);
+          vl.push_back(B);
+          placed = true;
+        }
+        double2 v = cmul(A, d.up_val[k]);
+        if (j == i) {
+          v = cadd(v, B);
+          placed = true;
+        }
+        cl.push_back(j);
+        vl.push_back(v);
+      }
+      if (!placed) {
+        cl.push_back(i);
+        vl.push_back(B);
+      }
+      rp[i + 1] = (int)cl.size();
+    }
+    d.up_rowptr.swap(rp);
+    d.up_col.swap(cl);
+    d.up_val.swap(vl);
+    d.upload();
+  });
+}
+
+int linqt_op_multiply(linqt_session *s, const linqt_op *op, const double a[2], const double *x, const double b[2],
+                      double *y, int ncols) {
+  return guarded([&] {
+    check_op(op, "op");
+    LQ_REQUIRE(a && b && x && y && ncols > 0, "bad argument");
+    Session *r = resolve(s);
+    const DeviceOp &d = op->op;
+    const int N = d.n;
+    const int Rc = std::min(256, pow2_at_least(ncols));
+    DevBuf st(sizeof(double2) * (size_t)N * ncols), yt(sizeof(double2) * (size_t)N * ncols);
+    DevBuf bx(sizeof(double2) * (size_t)N * Rc), by(sizeof(double2) * (size_t)N * Rc);
+    LQ_CUDA(cudaMemcpyAsync(st.p, x, sizeof(double2) * (size_t)N * ncols, cudaMemcpyHostToDevice, r->stream));
+    LQ_CUDA(cudaMemcpyAsync(yt.p, y, sizeof(double2) * (size_t)N * ncols, cudaMemcpyHostToDevice, r->stream));
+    for (int c0 = 0; c0 < ncols; c0 += Rc) {
+      const int w = std::min(Rc, ncols - c0);
+      states_to_block(r, (const double2 *)st.p + (size_t)c0 * N, bx.p, N, w, Rc, false);
+      states_to_block(r, (const double2 *)yt.p + (size_t)c0 * N, by.p, N, w, Rc, false);
+      spmm(r, d, make_double2(a[0], a[1]), bx.p, make_double2(b[0], b[1]), by.p, Rc, false);
+      block_to_states(r, by.p, (double2 *)yt.p + (size_t)c0 * N, N, w, Rc);
+    }
+    LQ_CUDA(cudaMemcpyAsync(y, yt.p, sizeof(double2) * (size_t)N * ncols, cudaMemcpyDeviceToHost, r->stream));
+    LQ_CUDA(cudaStreamSynchronize(r->stream));
+  });
+}
+
+int linqt_spectral_bounds(linqt_session *s, const linqt_op *op, double *lo, double *hi) {
+  return guarded([&] {
+    check_op(op, "op");
+    LQ_REQUIRE(lo && hi, "NULL output");
+    gershgorin(resolve(s), op->op, lo, hi);
+  });
+}
+
+int linqt_moments1d_dev(linqt_session *s, const linqt_op *H, const linqt_op *op, const double *states_dev, int R,
+                        int M, const linqt_opts *opts, double *mu_dev) {
+  return guarded([&] {
+    check_op(H, "H");
+    LQ_REQUIRE(states_dev && mu_dev, "NULL pointer");
+    moments1d_dev(resolve(s), H->op, dop(op), (const double2 *)states_dev, R, M, defaults(opts), (double2 *)mu_dev);
+  });
+}
+
+int linqt_moments1d(linqt_session *s, const linqt_op *H, const linqt_op *op, const double *states, int R, int M,
+                    const linqt_opts *opts, double *mu) {
+  return guarded([&] {
+    check_op(H, "H");
+    LQ_REQUIRE(states && mu && R > 0 && M > 0, "bad argument");
+    Session *r = resolve(s);
+    const size_t sb = sizeof(double2) * (size_t)R * H->op.n;
+    double2 *d_st = (double2 *)r->get("io_states", sb);
+    double2 *d_mu = (double2 *)r->get("io_mu", sizeof(double2) * (size_t)M);
+    LQ_CUDA(cudaMemcpyAsync(d_st, states, sb, cudaMemcpyHostToDevice, r->stream));
+    moments1d_dev(r, H->op, dop(op), d_st, R, M, defaults(opts), d_mu);
+    LQ_CUDA(cudaMemcpyAsync(mu, d_mu, sizeof(double2) * (size_t)M, cudaMemcpyDeviceToHost, r->stream));
+    LQ_CUDA(cudaStreamSynchronize(r->stream));
+  });
+}
+
+int linqt_moments2d_dev(linqt_session *s, const linqt_op *H, const linqt_op *opl, const linqt_op *opr,
+                        const double *states_dev, int R, int M, const linqt_opts *opts, double *mu_dev) {
+  return guarded([&] {
+    check_op(H, "H");
+    LQ_REQUIRE(states_dev && mu_dev, "NULL pointer");
+    moments2d_dev(resolve(s), H->op, dop(opl), dop(opr), (const double2 *)states_dev, R, M, defaults(opts),
+                  (double2 *)mu_dev);
+  });
+}
+
+int linqt_moments2d(linqt_session *s, const linqt_op *H, const linqt_op *opl, const linqt_op *opr,
+                    const double *states, int R, int M, const linqt_opts *opts, double *mu) {
+  return guarded([&] {
+    check_op(H, "H");
+    LQ_REQUIRE(states && mu && R > 0 && M > 0, "bad argument");
+    Session *r = resolve(s);
+    const size_t sb = sizeof(double2) * (size_t)R * H->op.n;
+    const size_t mb = sizeof(double2) * (size_t)M * M;
+    double2 *d_st = (double2 *)r->get("io_states", sb);
+    double2 *d_mu = (double2 *)r->get("io_mu", mb);
+    LQ_CUDA(cudaMemcpyAsync(d_st, states, sb, cudaMemcpyHostToDevice, r->stream));
+    moments2d_dev(r, H->op, dop(opl), dop(opr), d_st, R, M, defaults(opts), d_mu);
+    LQ_CUDA(cudaMemcpyAsync(mu, d_mu, mb, cudaMemcpyDeviceToHost, r->stream));
+    LQ_CUDA(cudaStreamSynchronize(r->stream));
+  });
+}
+
+int linqt_kubo_fft_dev(linqt_session *s, const linqt_op *H, const linqt_op *opl, const linqt_op *opr,
+                       const double *states_dev, int R, int M, int nump, int formula, double band_width,
+                       double band_center, const linqt_opts *opts, double *out_dev) {
+  return guarded([&] {
+    check_op(H, "H");
+    LQ_REQUIRE(states_dev && out_dev, "NULL pointer");
+    kubo_fft_dev(resolve(s), H->op, dop(opl), dop(opr), (const double2 *)states_dev, R, M, nump, formula,
+                 band_width, band_center, defaults(opts), out_dev);
+  });
+}
+
+int linqt_kubo_fft(linqt_session *s, const linqt_op *H, const linqt_op *opl, const linqt_op *opr,
+                   const double *states, int R, int M, int nump, int formula, double band_width, double band_center,
+                   const linqt_opts *opts, double *E, double *sigma, double *integrand) {
+  return guarded([&] {
+    check_op(H, "H");
+    LQ_REQUIRE(states && E && sigma && R > 0 && M > 0 && nump > 0, "bad argument");
+    Session *r = resolve(s);
+    const size_t sb = sizeof(double2) * (size_t)R * H->op.n;
+    double2 *d_st = (double2 *)r->get("io_states", sb);
+    double *d_out = (double *)r->get("io_kubo", sizeof(double) * 3 * (size_t)nump);
+    LQ_CUDA(cudaMemcpyAsync(d_st, states, sb, cudaMemcpyHostToDevice, r->stream));
+    kubo_fft_dev(r, H->op, dop(opl), dop(opr), d_st, R, M, nump, formula, band_width, band_center, defaults(opts),
+                 d_out);
+    std::vector<double> h(3 * (size_t)nump);
+    LQ_CUDA(cudaMemcpyAsync(h.data(), d_out, sizeof(double) * h.size(), cudaMemcpyDeviceToHost, r->stream));
+    LQ_CUDA(cudaStreamSynchronize(r->stream));
+    std::memcpy(E, h.data(), sizeof(double) * nump);
+    std::memcpy(sigma, h.data() + nump, sizeof(double) * nump);
+    if (integrand) std::memcpy(integrand, h.data() + 2 * (size_t)nump, sizeof(double) * nump);
+  });
+}
+
+int linqt_jackson1d(double *mu, int M, double band_width, double broad_meV, int *M_out) {
+  return guarded([&] {
+    LQ_REQUIRE(mu && M > 0 && band_width > 0 && broad_meV > 0, "bad argument");
+    const int Mt = jackson_cut(M, band_width, broad_meV);
+    for (int m = 0; m < Mt; ++m) {
+      const double g = jackson_factor(m, Mt);
+      mu[2 * m] *= g;
+      mu[2 * m + 1] *= g;
+    }
+    if (M_out) *M_out = Mt;
+  });
+}
+
+int linqt_jackson2d(double *mu, int M0, int M1, double band_width, double b0, double b1, int *M0_out, int *M1_out) {
+  return guarded([&] {
+    LQ_REQUIRE(mu && M0 > 0 && M1 > 0 && band_width > 0 && b0 > 0 && b1 > 0, "bad argument");
+    const int T0 = jackson_cut(M0, band_width, b0), T1 = jackson_cut(M1, band_width, b1);
+    for (int i = 0; i < T0; ++i)
+      for (int j = 0; j < T1; ++j) {
+        const double g = jackson_factor(i, T0) * jackson_factor(j, T1);
+        mu[2 * ((size_t)i * T1 + j)] = mu[2 * ((size_t)i * M1 + j)] * g;
+        mu[2 * ((size_t)i * T1 + j) + 1] = mu[2 * ((size_t)i * M1 + j) + 1] * g;
+      }
+    if (M0_out) *M0_out = T0;
+    if (M1_out) *M1_out = T1;
+  });
+}
+
+int linqt_dos_from_moments(linqt_session *s, const double *mu, int M, int N, double band_width, double band_center,
+                           double broad_meV, double *E, double *dos, int *num_out) {
+  return guarded([&] {
+    LQ_REQUIRE(mu && E && dos && M > 0 && band_width > 0 && broad_meV > 0, "bad argument");
+    Session *r = resolve(s);
+    const int Mt = jackson_cut(M, band_width, broad_meV);
+    double2 *d_mu = (double2 *)r->get("dos_mu", sizeof(double2) * M);
+    double2 *d_muj = (double2 *)r->get("dos_muj", sizeof(double2) * M);
+    double *d_out = (double *)r->get("dos_out", sizeof(double) * 2 * M);
+    LQ_CUDA(cudaMemcpyAsync(d_mu, mu, sizeof(double2) * M, cudaMemcpyHostToDevice, r->stream));
+    jackson2d_dev(r, d_mu, 1, M, 1, Mt, d_muj);  // a 1 x M table: g(0, 1) = 1 on the first axis
+    dos_grid(r, d_muj, Mt, N, band_width, band_center, d_out, d_out + Mt);
+    LQ_CUDA(cudaMemcpyAsync(E, d_out, sizeof(double) * Mt, cudaMemcpyDeviceToHost, r->stream));
+    LQ_CUDA(cudaMemcpyAsync(dos, d_out + Mt, sizeof(double) * Mt, cudaMemcpyDeviceToHost, r->stream));
+    LQ_CUDA(cudaStreamSynchronize(r->stream));
+    if (num_out) *num_out = Mt;
+  });
+}
+
+int linqt_bastin_from_moments(linqt_session *s, const double *mu, int M0, int M1, int N, double band_width,
+                              double band_center, double broad_meV, double xbound, int num_div, double *E,
+                              double *sigma, int *num_out) {
+  return guarded([&] {
+    LQ_REQUIRE(mu && E && sigma && M0 > 0 && M1 > 0 && band_width > 0 && broad_meV > 0, "bad argument");
+    LQ_REQUIRE(xbound > 0 && xbound < 1, "xbound must lie in (0, 1)");
+    Session *r = resolve(s);
+    const int T0 = jackson_cut(M0, band_width, broad_meV), T1 = jackson_cut(M1, band_width, broad_meV);
+    const int nd = num_div > 0 ? num_div : 30 * std::max(T0, T1);
+    LQ_REQUIRE(nd >= 2, "num_div must be >= 2");
+    double2 *d_mu = (double2 *)r->get("bas_mu", sizeof(double2) * (size_t)M0 * M1);
+    double2 *d_muj = (double2 *)r->get("bas_muj", sizeof(double2) * (size_t)T0 * T1);
+    double *d_out = (double *)r->get("bas_out", sizeof(double) * 2 * (size_t)nd);
+    LQ_CUDA(cudaMemcpyAsync(d_mu, mu, sizeof(double2) * (size_t)M0 * M1, cudaMemcpyHostToDevice, r->stream));
+    jackson2d_dev(r, d_mu, M0, M1, T0, T1, d_muj);
+    bastin_grid(r, d_muj, T0, T1, N, band_width, band_center, xbound, nd, d_out, d_out + nd);
+    LQ_CUDA(cudaMemcpyAsync(E, d_out, sizeof(double) * (nd - 1), cudaMemcpyDeviceToHost, r->stream));
+    LQ_CUDA(cudaMemcpyAsync(sigma, d_out + nd, sizeof(double) * (nd - 1), cudaMemcpyDeviceToHost, r->stream));
+    LQ_CUDA(cudaStreamSynchronize(r->stream));
+    if (num_out) *num_out = nd - 1;
+  });
+}
+
+}  // extern "C"

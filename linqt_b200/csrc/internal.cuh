@@ -1,0 +1,246 @@
+// Internal declarations shared by the translation units of liblinqt_gpu.so.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <cstdint>
+#include <map>
+#include <mutex>
+#include <stdexcept>
+#include <string>
+#include <vector>
+
+#include "../../include/linqt_gpu.h"
+
+namespace linqt {
+
+// ---------------------------------------------------------------------------
+// errors: internal code throws linqt::Error; every C entry point catches it
+// ---------------------------------------------------------------------------
+struct Error : std::runtime_error {
+  int code;
+  Error(int c, const std::string &m) : std::runtime_error(m), code(c) {}
+};
+
+[[noreturn]] void fail(int code, const std::string &msg);
+void set_last_error(const std::string &msg);
+
+#define LQ_CUDA(x)                                                                                    \
+  do {                                                                                                \
+    cudaError_t e_ = (x);                                                                             \
+    if (e_ != cudaSuccess)                                                                            \
+      ::linqt::fail(e_ == cudaErrorMemoryAllocation ? LINQT_ERR_NOMEM : LINQT_ERR_CUDA,               \
+                    std::string(#x) + " failed: " + cudaGetErrorString(e_) + " (" + __FILE__ + ":" + \
+                        std::to_string(__LINE__) + ")");                                              \
+  } while (0)
+
+#define LQ_REQUIRE(cond, msg)                                       \
+  do {                                                              \
+    if (!(cond)) ::linqt::fail(LINQT_ERR_INVALID, std::string(msg)); \
+  } while (0)
+
+// after a launch: surface configuration errors immediately
+#define LQ_LAUNCHED() LQ_CUDA(cudaGetLastError())
+
+// ---------------------------------------------------------------------------
+// complex helpers on CUDA vector types
+// ---------------------------------------------------------------------------
+template <class T>
+struct cplx_t;
+template <>
+struct cplx_t<double> {
+  using type = double2;
+};
+template <>
+struct cplx_t<float> {
+  using type = float2;
+};
+
+__host__ __device__ inline double2 mk2(double x, double y) { return make_double2(x, y); }
+__host__ __device__ inline float2 mk2(float x, float y) { return make_float2(x, y); }
+
+// c + a*b
+__device__ __forceinline__ double2 cfma(double2 a, double2 b, double2 c) {
+  c.x = fma(a.x, b.x, c.x);
+  c.x = fma(-a.y, b.y, c.x);
+  c.y = fma(a.x, b.y, c.y);
+  c.y = fma(a.y, b.x, c.y);
+  return c;
+}
+__device__ __forceinline__ float2 cfma(float2 a, float2 b, float2 c) {
+  c.x = fmaf(a.x, b.x, c.x);
+  c.x = fmaf(-a.y, b.y, c.x);
+  c.y = fmaf(a.x, b.y, c.y);
+  c.y = fmaf(a.y, b.x, c.y);
+  return c;
+}
+// c + conj(a)*b
+__device__ __forceinline__ double2 cfma_conj(double2 a, double2 b, double2 c) {
+  c.x = fma(a.x, b.x, c.x);
+  c.x = fma(a.y, b.y, c.x);
+  c.y = fma(a.x, b.y, c.y);
+  c.y = fma(-a.y, b.x, c.y);
+  return c;
+}
+__host__ __device__ __forceinline__ double2 cmul(double2 a, double2 b) {
+  return make_double2(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x);
+}
+__host__ __device__ __forceinline__ double2 cadd(double2 a, double2 b) { return make_double2(a.x + b.x, a.y + b.y); }
+__host__ __device__ __forceinline__ double2 csub(double2 a, double2 b) { return make_double2(a.x - b.x, a.y - b.y); }
+__host__ __device__ __forceinline__ double2 cscale(double2 a, double s) { return make_double2(a.x * s, a.y * s); }
+__host__ __device__ __forceinline__ double2 cconj(double2 a) { return make_double2(a.x, -a.y); }
+
+__device__ __forceinline__ double2 to_d2(double2 a) { return a; }
+__device__ __forceinline__ double2 to_d2(float2 a) { return make_double2(a.x, a.y); }
+
+// ---------------------------------------------------------------------------
+// device operator: Hermitian-expanded CSR (plus optional FP32 copy and SELL-C)
+// ---------------------------------------------------------------------------
+struct SellView {
+  int nslices = 0, C = 0;
+  const long *slice_off = nullptr;  // [nslices+1], in entries
+  const int *slice_w = nullptr;     // [nslices]
+  const int *col = nullptr;         // padded, column-major per slice
+  const void *val = nullptr;        // double2 or float2
+};
+
+struct CsrView {
+  int n = 0;
+  long nnz = 0;
+  const int *rowptr = nullptr;
+  const int *col = nullptr;
+  const void *val = nullptr;  // double2 or float2
+};
+
+struct DeviceOp {
+  int device = 0;
+  int n = 0;
+  // host copy of the operator as LinQT stores it (upper triangle incl. diagonal, sorted
+  // by column); rescale acts here and the expansion is re-uploaded
+  std::vector<int> up_rowptr, up_col;
+  std::vector<double2> up_val;
+  bool hermitian = true;
+  // expanded CSR (host mirror + device)
+  std::vector<int> rowptr, col;
+  std::vector<double2> val;
+  long nnz = 0;
+  int *d_rowptr = nullptr, *d_col = nullptr;
+  double2 *d_val64 = nullptr;
+  float2 *d_val32 = nullptr;  // created on first mixed-precision use
+  // SELL-C layout (created on first use)
+  int sell_C = 0, sell_nslices = 0;
+  long sell_len = 0;
+  long *d_sell_off = nullptr;
+  int *d_sell_w = nullptr, *d_sell_col = nullptr;
+  double2 *d_sell_val64 = nullptr;
+  float2 *d_sell_val32 = nullptr;
+  unsigned version = 0;  // bumped by rescale
+  std::mutex mu;
+
+  CsrView csr64() const { return CsrView{n, nnz, d_rowptr, d_col, d_val64}; }
+  void ensure_fp32();
+  void ensure_sell(int C);
+  void free_device();
+  void upload();
+};
+
+// ---------------------------------------------------------------------------
+// sessions: stream + workspace cache + phase timing
+// ---------------------------------------------------------------------------
+enum Phase { PH_RECURSION = 0, PH_CONTRACT = 1, PH_FFT = 2, PH_OTHER = 3 };
+
+struct Session {
+  int device = 0;
+  cudaStream_t stream = nullptr;
+  bool own_stream = false;
+  std::map<std::string, std::pair<void *, size_t>> ws;
+  bool timing = false;
+  double phase_ms[4] = {0, 0, 0, 0};
+  long phase_launches[4] = {0, 0, 0, 0};
+  int sm_count = 148;
+  size_t hbm_budget = 0;  // 0 = no limit beyond the device
+
+  void *get(const std::string &name, size_t bytes);  // cached device buffer, >= bytes
+  void trim();
+  ~Session();
+};
+
+Session *default_session();
+Session *resolve(linqt_session *s);
+
+// scoped phase timer (CUDA events on the session stream when timing is on)
+struct PhaseScope {
+  Session *s;
+  Phase ph;
+  cudaEvent_t a = nullptr, b = nullptr;
+  PhaseScope(Session *s_, Phase p);
+  ~PhaseScope();
+  void launches(long k) { s->phase_launches[ph] += k; }
+};
+
+// ---------------------------------------------------------------------------
+// kernel launchers (spmm.cu, moments.cu, mu_gemm.cu, kubo_fft.cu, reconstruct.cu)
+// ---------------------------------------------------------------------------
+// y = alpha*A*x + beta*y on a block of R columns in site-major layout (x[i*R + r])
+void spmm(Session *s, const DeviceOp &A, double2 alpha, const void *x, double2 beta, void *y, int R, bool fp32);
+
+// one recursion step on a block: y = 2*H*x - yprev (yprev may alias y),
+// optional fused V*x into vout, optional dot products into dots (see spmm.cu)
+struct StepArgs {
+  const void *x = nullptr;      // T_m
+  const void *yprev = nullptr;  // T_{m-1} (nullptr: first step, y = H x)
+  void *y = nullptr;            // T_{m+1} (nullptr: skip)
+  const DeviceOp *V = nullptr;  // fused second operator
+  void *vout = nullptr;         // V*x
+  const void *phi = nullptr;    // for <phi|x> (direct 1D moments)
+  double2 *dots = nullptr;      // per-step outputs: [0]=<x|x> or <phi|x>, [1]=<y|x>
+  int dot_mode = 0;             // 0 none, 1 <phi|x>, 2 doubling (<x|x>, <y|x>)
+};
+void cheb_step(Session *s, const DeviceOp &H, const StepArgs &a, int R, bool fp32, int format);
+
+// layout conversions between R x N (state-major, double) and N x R (site-major)
+void states_to_block(Session *s, const double2 *states, void *block, int N, int R, int Rpad, bool fp32);
+
+// 1D moments assembly from per-step dots
+void moments1d_from_dots(Session *s, const double2 *dots, int steps, int M, int R, int mode, double2 *mu);
+
+// mu_raw[M x M] += sum_k conj(L[m0][k]) * Rv[m1][k], FP64 (or FP32-input) operands
+// C(i,j) (+)= sum_k conj(A[i][k]) B[j][k], FP64
+void zgemm_cn(Session *s, const double2 *A, int MA, const double2 *B, int MB, long K, double2 *C, bool accumulate);
+void mu_contract(Session *s, const void *L, const void *Rv, int M, long K, bool fp32_inputs, int precision,
+                 double2 *mu_raw);
+void mu_finalize(Session *s, const double2 *mu_raw, int M, int R, double2 *mu);
+
+// FFT path: accumulate p/w over all sites into acc[2*nump] (complex)
+void kubo_fft_sites(Session *s, const void *L, const void *Rv, long nsites, int M, int nump, int formula,
+                    bool fp32_inputs, double2 *acc);
+void kubo_postprocess(Session *s, const double2 *acc, int R, int nump, int formula, int N, double band_width,
+                      double band_center, double *out);
+
+// reconstructions
+void dos_grid(Session *s, const double2 *mu, int M, int N, double band_width, double band_center, double *E,
+              double *dos);
+void bastin_grid(Session *s, const double2 *mu, int M0, int M1, int N, double band_width, double band_center,
+                 double xbound, int num_div, double *E, double *sigma);
+
+// bounds
+void gershgorin(Session *s, const DeviceOp &A, double *lo, double *hi);
+
+// Jackson kernel helpers (reconstruct.cu)
+int jackson_cut(int M, double band_width, double broad);
+double jackson_factor(int m, int Mom);
+void jackson2d_dev(Session *s, const double2 *mu, int M0, int M1, int M0t, int M1t, double2 *out);
+
+// small utilities (util.cu)
+void sum_chunks(Session *s, double2 *d, int len, int nchunks);       // d[0:len] += sum_{c>0} d[c*len : ...]
+void add_into(Session *s, double2 *dst, const double2 *src, int len); // dst += src
+void block_to_states(Session *s, const void *blk, double2 *states, int N, int R, int Rpad);  // N x Rpad -> R x N
+
+}  // namespace linqt
+
+struct linqt_op {
+  linqt::DeviceOp op;
+};
+struct linqt_session {
+  linqt::Session s;
+};

@@ -1,0 +1,483 @@
+// Kubo_solver_FFT on the device: per-site DFTs of the Chebyshev vectors, the
+// Bastin / Greenwood products, the sum over sites and the post-processing.
+//
+// Reference: src/Bastin_FFTs.cpp:6-173, src/Greenwood_FFTs.cpp:6-91,
+// src/Kubo_solver_FFT_postProcess.cpp:8-397, include/Kubo_solver_FFT.hpp:93-107.
+//
+// For every site l (a (site, vector) pair of the block) and m < M the reference
+// forms  pf_m = (2 - [m=0]) g_m exp(i pi m / (2 nump))  (g_m the Jackson factor of
+// Kubo_solver_FFT::Jackson_kernel) and runs FFTW backward DFTs (exponent +1,
+// unnormalised, zero padded to nump) of
+//   pf_m Re(bra_m), pf_m Im(bra_m), pf_m Re(ket_m), pf_m Im(ket_m)
+// and (Bastin) of the same four multiplied by m, with bra_m = L_m[l] (= T_m(H) OPL phi)
+// and ket_m = R_m[l] (= OPR T_m(H) phi).  Products of the transforms are summed over
+// sites into p[k] (and w[k]).
+//
+// Design: one CTA per site at a time (persistent over a contiguous chunk of sites),
+// all 8 (or 4) transforms of the site in shared memory.  nump = 16 * 16 * R3,
+// R3 in {1, 2, 4, 8}: pass 1 does 16-point DFTs in registers straight from the
+// global loads, pass 2 16-point DFTs, pass 3 R3-point DFTs; every pass reads its
+// inputs into registers, synchronises, and writes its outputs back in place
+// (rows padded by one element to spread shared-memory banks).  The product stage
+// then reads all transforms at a fixed set of frequencies per thread and keeps the
+// per-frequency sums in registers across the CTA's sites; CTA partials are summed
+// in a fixed order (deterministic).  Other nump use a direct DFT kernel.
+#include <cmath>
+
+#include "internal.cuh"
+
+namespace linqt {
+
+namespace {
+
+__device__ __forceinline__ double2 mul_i(double2 a) { return make_double2(-a.y, a.x); }
+
+__device__ __forceinline__ void dft2(double2 &a0, double2 &a1) {
+  const double2 t = a0;
+  a0 = cadd(t, a1);
+  a1 = csub(t, a1);
+}
+
+// 4-point DFT with exponent +1 (in place)
+__device__ __forceinline__ void dft4(double2 &a0, double2 &a1, double2 &a2, double2 &a3) {
+  const double2 s02 = cadd(a0, a2), d02 = csub(a0, a2), s13 = cadd(a1, a3), d13 = mul_i(csub(a1, a3));
+  a0 = cadd(s02, s13);
+  a2 = csub(s02, s13);
+  a1 = cadd(d02, d13);
+  a3 = csub(d02, d13);
+}
+
+// exp(+2 pi i j / 16), j = 0..9
+__device__ __forceinline__ double2 w16(int j) {
+  constexpr double c1 = 0.92387953251128675613, s1 = 0.38268343236508977173, h = 0.70710678118654752440;
+  switch (j) {
+    case 0: return make_double2(1.0, 0.0);
+    case 1: return make_double2(c1, s1);
+    case 2: return make_double2(h, h);
+    case 3: return make_double2(s1, c1);
+    case 4: return make_double2(0.0, 1.0);
+    case 5: return make_double2(-s1, c1);
+    case 6: return make_double2(-h, h);
+    case 7: return make_double2(-c1, s1);
+    case 8: return make_double2(-1.0, 0.0);
+    default: return make_double2(-c1, -s1);
+  }
+}
+
+// 16-point DFT, exponent +1.  On return v[4*q1 + q2] holds X[q1 + 4*q2].
+__device__ __forceinline__ void dft16(double2 (&v)[16]) {
+#pragma unroll
+  for (int r2 = 0; r2 < 4; ++r2) dft4(v[r2], v[4 + r2], v[8 + r2], v[12 + r2]);
+  // now v[4*q1 + r2] = Y_{r2}[q1]
+#pragma unroll
+  for (int q1 = 1; q1 < 4; ++q1)
+#pragma unroll
+    for (int r2 = 1; r2 < 4; ++r2) v[4 * q1 + r2] = cmul(v[4 * q1 + r2], w16(q1 * r2));
+#pragma unroll
+  for (int q1 = 0; q1 < 4; ++q1) dft4(v[4 * q1], v[4 * q1 + 1], v[4 * q1 + 2], v[4 * q1 + 3]);
+}
+
+// R-point DFT (R in 1, 2, 4, 8), exponent +1, natural output order
+template <int R>
+__device__ __forceinline__ void dft_small(double2 (&v)[R]) {
+  if constexpr (R == 2) {
+    dft2(v[0], v[1]);
+  } else if constexpr (R == 4) {
+    dft4(v[0], v[1], v[2], v[3]);
+  } else if constexpr (R == 8) {
+    // r = 2 r1 + r2, q = q1 + 4 q2
+    dft4(v[0], v[2], v[4], v[6]);  // Y_0[q1] at v[0], v[2], v[4], v[6]
+    dft4(v[1], v[3], v[5], v[7]);  // Y_1[q1] at v[1], v[3], v[5], v[7]
+    constexpr double h = 0.70710678118654752440;
+    v[3] = cmul(v[3], make_double2(h, h));
+    v[5] = mul_i(v[5]);
+    v[7] = cmul(v[7], make_double2(-h, h));
+    double2 o[8];
+#pragma unroll
+    for (int q1 = 0; q1 < 4; ++q1) {
+      double2 a = v[2 * q1], b = v[2 * q1 + 1];
+      dft2(a, b);
+      o[q1] = a;
+      o[q1 + 4] = b;
+    }
+#pragma unroll
+    for (int q = 0; q < 8; ++q) v[q] = o[q];
+  }
+}
+
+// Sequence s of a site: source (0 bra, 1 ket), part (0 re, 1 im), derivative.
+// Bastin order (src/Bastin_FFTs.cpp:40-52): re_bras, im_bras, re_kets, im_kets, re_D_bras,
+// im_D_bras, re_D_kets, im_D_kets.  Greenwood uses the first four.
+__device__ __forceinline__ double2 seq_input(int s, double2 bra, double2 ket, double2 pf, int m) {
+  const double2 src = (s & 2) ? ket : bra;
+  const double u = (s & 1) ? src.y : src.x;
+  double f = u;
+  if (s >= 4) f *= (double)m;
+  return make_double2(pf.x * f, pf.y * f);
+}
+
+// Bastin products for one frequency (src/Bastin_FFTs.cpp:128-163), accumulated into p, w
+__device__ __forceinline__ void bastin_products(int j, int nump, const double2 *X, int stride, double2 &p,
+                                                double2 &w) {
+  const double2 rb = X[0 * stride], ib = X[1 * stride], rk = X[2 * stride], ik = X[3 * stride];
+  const double2 rDb = X[4 * stride], iDb = X[5 * stride], rDk = X[6 * stride], iDk = X[7 * stride];
+  // Re(rb) - i Re(ib)
+  const double2 ReG_b = make_double2(rb.x, -ib.x);
+  // Re(rk) + i Re(ik)
+  const double2 ReG_k = make_double2(rk.x, ik.x);
+  double2 Gk, Gb, dGb, dGk;
+  if (j < nump / 2) {
+    Gk = cadd(rk, mul_i(ik));                           // rk + i ik
+    Gb = csub(cconj(rb), mul_i(cconj(ib)));             // conj(rb) - i conj(ib)
+    dGb = csub(cconj(rDb), mul_i(cconj(iDb)));          // conj(rDb) - i conj(iDb)
+    dGk = cadd(rDk, mul_i(iDk));                        // rDk + i iDk
+  } else {
+    Gk = cadd(cconj(rk), mul_i(cconj(ik)));             // conj(rk) + i conj(ik)
+    Gb = csub(rb, mul_i(ib));                           // rb - i ib
+    dGb = csub(rDb, mul_i(iDb));                        // rDb - i iDb
+    dGk = cadd(cconj(rDk), mul_i(cconj(iDk)));          // conj(rDk) + i conj(iDk)
+  }
+  p = cadd(p, cadd(cmul(ReG_b, Gk), cmul(Gb, ReG_k)));
+  w = cadd(w, csub(cmul(dGb, ReG_k), cmul(ReG_b, dGk)));
+}
+
+// Greenwood product (src/Greenwood_FFTs.cpp:252-257): Re[(Re rb - i Re ib)(Re rk + i Re ik)]
+__device__ __forceinline__ void greenwood_product(const double2 *X, int stride, double2 &p) {
+  const double2 rb = X[0], ib = X[stride], rk = X[2 * stride], ik = X[3 * stride];
+  p.x += rb.x * rk.x + ib.x * ik.x;
+}
+
+// prefactors pf_m (src/Bastin_FFTs.cpp:20-21, include/Kubo_solver_FFT.hpp:99-107)
+__global__ void k_prefactors(int M, int nump, double2 *__restrict__ pf) {
+  for (int m = blockIdx.x * blockDim.x + threadIdx.x; m < M; m += gridDim.x * blockDim.x) {
+    const double g = 1 / (M + 1.0) *
+                     ((M - m + 1.0) * cos(M_PI * m / (M + 1.0)) + sin(M_PI * m / (M + 1.0)) / tan(M_PI / (M + 1.0)));
+    const double amp = (2 - (m == 0)) * g;
+    double sn, cs;
+    sincos(M_PI * m / (2.0 * nump), &sn, &cs);
+    pf[m] = make_double2(amp * cs, amp * sn);
+  }
+}
+
+constexpr int kFftThreads = 512;
+
+template <int R3, int NSEQ>
+__global__ void __launch_bounds__(kFftThreads)
+    k_kubo_fft(const double2 *__restrict__ L, const double2 *__restrict__ Rv, long K, long chunk, int M,
+               const double2 *__restrict__ pf_g, double2 *__restrict__ part) {
+  constexpr int P = 16 * R3;    // n / 16
+  constexpr int n = 16 * P;     // nump
+  constexpr int ROW = P + 1;    // padded row of the 16 x P arrangement
+  constexpr int SEQ = 16 * ROW; // per-sequence footprint
+  constexpr int KPT = (n + kFftThreads - 1) / kFftThreads;
+  extern __shared__ double2 sm[];
+  double2 *buf = sm;                    // NSEQ * SEQ
+  double2 *tw = sm + NSEQ * SEQ;        // n twiddles exp(2 pi i t / n)
+  double2 *pfs = tw + n;                // M prefactors
+  for (int t = threadIdx.x; t < n; t += blockDim.x) {
+    double sn, cs;
+    sincospi(2.0 * t / n, &sn, &cs);
+    tw[t] = make_double2(cs, sn);
+  }
+  for (int m = threadIdx.x; m < M; m += blockDim.x) pfs[m] = pf_g[m];
+  double2 accp[KPT], accw[KPT];
+#pragma unroll
+  for (int q = 0; q < KPT; ++q) accp[q] = accw[q] = make_double2(0, 0);
+  __syncthreads();
+
+  const long lbeg = (long)blockIdx.x * chunk;
+  const long lend = min(K, lbeg + chunk);
+  for (long l = lbeg; l < lend; ++l) {
+    // ---- pass 1: x_s[m1 + P m2], m2 < 16 -> 16-point DFT over m2, twiddle w_n^{m1 k2}
+    for (int item = threadIdx.x; item < NSEQ * P; item += blockDim.x) {
+      const int s = item / P, m1 = item % P;
+      double2 v[16];
+#pragma unroll
+      for (int m2 = 0; m2 < 16; ++m2) {
+        const int m = m1 + P * m2;
+        if (m < M) {
+          const double2 bra = __ldg(L + (size_t)m * K + l), ket = __ldg(Rv + (size_t)m * K + l);
+          v[m2] = seq_input(s, bra, ket, pfs[m], m);
+        } else {
+          v[m2] = make_double2(0, 0);
+        }
+      }
+      dft16(v);
+      double2 *row = buf + s * SEQ;
+#pragma unroll
+      for (int q1 = 0; q1 < 4; ++q1)
+#pragma unroll
+        for (int q2 = 0; q2 < 4; ++q2) {
+          const int k2 = q1 + 4 * q2;
+          row[k2 * ROW + m1] = cmul(v[4 * q1 + q2], tw[(m1 * k2) % n]);
+        }
+    }
+    __syncthreads();
+    // ---- pass 2: for row k2, m1 = a + R3 b: 16-point DFT over b, twiddle w_P^{a c}
+    {
+      double2 v[16];
+      int s = 0, k2 = 0, a = 0;
+      const int items = NSEQ * 16 * R3;
+      const bool active = threadIdx.x < items;  // items <= kFftThreads for all instantiations
+      if (active) {
+        s = threadIdx.x / (16 * R3);
+        k2 = (threadIdx.x / R3) % 16;
+        a = threadIdx.x % R3;
+        const double2 *row = buf + s * SEQ + k2 * ROW;
+#pragma unroll
+        for (int b = 0; b < 16; ++b) v[b] = row[a + R3 * b];
+      }
+      __syncthreads();
+      if (active) {
+        dft16(v);
+        double2 *row = buf + s * SEQ + k2 * ROW;
+#pragma unroll
+        for (int q1 = 0; q1 < 4; ++q1)
+#pragma unroll
+          for (int q2 = 0; q2 < 4; ++q2) {
+            const int c = q1 + 4 * q2;
+            row[c * R3 + a] = R3 == 1 ? v[4 * q1 + q2] : cmul(v[4 * q1 + q2], tw[(a * c * 16) % n]);
+          }
+      }
+      __syncthreads();
+    }
+    // ---- pass 3: for row k2 and c < 16: R3-point DFT over a -> X[k2 + 16 c + 256 d]
+    if constexpr (R3 > 1) {
+      for (int base = 0; base < NSEQ * 256; base += blockDim.x) {
+        const int item = base + threadIdx.x;
+        double2 v[R3];
+        int s = 0, k2 = 0, c = 0;
+        const bool active = item < NSEQ * 256;
+        if (active) {
+          s = item / 256;
+          k2 = (item / 16) % 16;
+          c = item % 16;
+          const double2 *row = buf + s * SEQ + k2 * ROW;
+#pragma unroll
+          for (int a = 0; a < R3; ++a) v[a] = row[c * R3 + a];
+          dft_small<R3>(v);
+        }
+        __syncthreads();
+        if (active) {
+          double2 *row = buf + s * SEQ + k2 * ROW;
+          // store X[k1 = c + 16 d] at row k2, column k1 (column index < P)
+#pragma unroll
+          for (int d = 0; d < R3; ++d) row[c + 16 * d] = v[d];
+        }
+        __syncthreads();
+      }
+    } else {
+      // R3 == 1: pass 2 wrote X[k2 + 16 c] at row k2, column c already
+    }
+    // ---- products: X_s[k] lives at buf[s*SEQ + (k % 16)*ROW + k / 16]
+#pragma unroll
+    for (int q = 0; q < KPT; ++q) {
+      const int k = threadIdx.x + q * kFftThreads;
+      if (k < n) {
+        const double2 *X = buf + (k % 16) * ROW + k / 16;
+        if constexpr (NSEQ == 8)
+          bastin_products(k, n, X, SEQ, accp[q], accw[q]);
+        else
+          greenwood_product(X, SEQ, accp[q]);
+      }
+    }
+    __syncthreads();
+  }
+  double2 *out = part + (size_t)blockIdx.x * 2 * n;
+#pragma unroll
+  for (int q = 0; q < KPT; ++q) {
+    const int k = threadIdx.x + q * kFftThreads;
+    if (k < n) {
+      out[k] = accp[q];
+      out[k + n] = accw[q];
+    }
+  }
+}
+
+// Direct DFT for any nump: one CTA per site at a time, thread per frequency.
+template <int NSEQ>
+__global__ void __launch_bounds__(256)
+    k_kubo_dft(const double2 *__restrict__ L, const double2 *__restrict__ Rv, long K, long chunk, int M, int nump,
+               const double2 *__restrict__ pf_g, const double2 *__restrict__ twg, double2 *__restrict__ part) {
+  extern __shared__ double2 sm[];
+  double2 *bk = sm;  // bra[M], ket[M]
+  const int kpt = (nump + blockDim.x - 1) / blockDim.x;
+  double2 *acc_g = part + (size_t)blockIdx.x * 2 * nump;
+  for (int q = 0; q < kpt; ++q) {
+    const int k = threadIdx.x + q * blockDim.x;
+    if (k < nump) acc_g[k] = acc_g[k + nump] = make_double2(0, 0);
+  }
+  const long lbeg = (long)blockIdx.x * chunk;
+  const long lend = min(K, lbeg + chunk);
+  for (long l = lbeg; l < lend; ++l) {
+    __syncthreads();
+    for (int m = threadIdx.x; m < M; m += blockDim.x) {
+      bk[m] = L[(size_t)m * K + l];
+      bk[M + m] = Rv[(size_t)m * K + l];
+    }
+    __syncthreads();
+    for (int q = 0; q < kpt; ++q) {
+      const int k = threadIdx.x + q * blockDim.x;
+      if (k >= nump) continue;
+      double2 X[NSEQ];
+#pragma unroll
+      for (int s = 0; s < NSEQ; ++s) X[s] = make_double2(0, 0);
+      for (int m = 0; m < M; ++m) {
+        const double2 c = cmul(__ldg(pf_g + m), __ldg(twg + ((long)m * k) % nump));
+#pragma unroll
+        for (int s = 0; s < NSEQ; ++s) {
+          const double2 src = (s & 2) ? bk[M + m] : bk[m];
+          double u = (s & 1) ? src.y : src.x;
+          if (s >= 4) u *= (double)m;
+          X[s].x = fma(c.x, u, X[s].x);
+          X[s].y = fma(c.y, u, X[s].y);
+        }
+      }
+      double2 p = acc_g[k], w = acc_g[k + nump];
+      if constexpr (NSEQ == 8)
+        bastin_products(k, nump, X, 1, p, w);
+      else
+        greenwood_product(X, 1, p);
+      acc_g[k] = p;
+      acc_g[k + nump] = w;
+    }
+  }
+}
+
+__global__ void k_twiddles(int n, double2 *__restrict__ tw) {
+  for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < n; t += gridDim.x * blockDim.x) {
+    double sn, cs;
+    sincospi(2.0 * t / n, &sn, &cs);
+    tw[t] = make_double2(cs, sn);
+  }
+}
+
+// acc[t] = sum_b part[b][t]  (fixed order)
+__global__ void k_sum_parts(const double2 *__restrict__ part, int nb, int len, double2 *__restrict__ acc) {
+  for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < len; t += gridDim.x * blockDim.x) {
+    double2 s = make_double2(0, 0);
+    for (int b = 0; b < nb; ++b) s = cadd(s, part[(size_t)b * len + t]);
+    acc[t] = s;
+  }
+}
+
+// rearrange_crescent_order (src/Kubo_solver_FFT_postProcess.cpp:98-116)
+__device__ void rearrange(double *x, double *tmp, int n) {
+  for (int k = 0; k < n; ++k) tmp[k] = x[k];
+  for (int k = 0; k < n / 2; ++k) {
+    x[2 * k] = tmp[k];
+    x[2 * k + 1] = tmp[n - k - 1];
+  }
+  for (int k = 0; k < n / 2; ++k) {
+    const double t = x[k];
+    x[k] = x[n - k - 1];
+    x[n - k - 1] = t;
+  }
+}
+
+// Post-processing (single thread, FP64): final_data = acc / R (the running mean of
+// Kubo_solver_FFT::update_data over R states), then Bastin_postProcess
+// (src/Kubo_solver_FFT_postProcess.cpp:120-273) or Greenwood_postProcess (:279-397).
+// out = [E (nump), sigma (nump), integrand (nump)]; scratch = 3*nump doubles.
+__global__ void k_kubo_post(const double2 *__restrict__ acc, double R, int nump, int formula, double N, double a,
+                            double b, double *__restrict__ out, double *__restrict__ scratch) {
+  if (threadIdx.x || blockIdx.x) return;
+  double *E = out, *sig = out + nump, *integ = out + 2 * nump;
+  double *Ek = scratch, *tmp = scratch + nump;
+  const double omega = N / (a * a);
+  for (int k = 0; k < nump; ++k) {
+    Ek[k] = cos(M_PI * (2 * k + 0.5) / nump);
+    E[k] = Ek[k];
+  }
+  rearrange(E, tmp, nump);
+  if (formula == LINQT_KUBO_BASTIN) {
+    for (int k = 0; k < nump; ++k) {
+      const double pr = acc[k].x / R, wi = acc[k + nump].y / R;
+      double v = Ek[k] * pr - (sqrt(1.0 - Ek[k] * Ek[k]) * wi);
+      v *= 1.0 / pow((1.0 - Ek[k] * Ek[k]), 2.0);
+      v *= omega / (M_PI);
+      integ[k] = v;
+    }
+    rearrange(integ, tmp, nump);
+    double s = 0;
+    for (int i = 0; i < nump - 1; ++i) {
+      s += integ[i] * (E[i + 1] - E[i]);
+      sig[i] = s;
+    }
+    sig[nump - 1] = 0.0;
+  } else {
+    for (int k = 0; k < nump; ++k) sig[k] = 2.0 * omega * (acc[k].x / R) / (1.0 - Ek[k] * Ek[k]) / (2 * M_PI);
+    rearrange(sig, tmp, nump);
+    for (int k = 0; k < nump; ++k) integ[k] = 0.0;
+  }
+  for (int k = 0; k < nump; ++k) E[k] = a * E[k] - b;
+}
+
+template <int R3, int NSEQ>
+void launch_fft(Session *s, const double2 *L, const double2 *Rv, long K, int M, const double2 *pf, double2 *acc) {
+  constexpr int n = 256 * R3;
+  const size_t smem = sizeof(double2) * ((size_t)NSEQ * 16 * (16 * R3 + 1) + n + M);
+  if (smem > 227 * 1024) fail(LINQT_ERR_UNSUPPORTED, "kubo_fft: nump too large for the shared-memory FFT");
+  LQ_CUDA(cudaFuncSetAttribute(k_kubo_fft<R3, NSEQ>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  const int nb = (int)std::max(1L, std::min(K, (long)s->sm_count));
+  const long chunk = (K + nb - 1) / nb;
+  double2 *part = (double2 *)s->get("kubo_part", sizeof(double2) * 2 * (size_t)n * nb);
+  k_kubo_fft<R3, NSEQ><<<nb, kFftThreads, smem, s->stream>>>(L, Rv, K, chunk, M, pf, part);
+  LQ_LAUNCHED();
+  k_sum_parts<<<(2 * n + 255) / 256, 256, 0, s->stream>>>(part, nb, 2 * n, acc);
+  LQ_LAUNCHED();
+}
+
+template <int NSEQ>
+void launch_dft(Session *s, const double2 *L, const double2 *Rv, long K, int M, int nump, const double2 *pf,
+                double2 *acc) {
+  double2 *tw = (double2 *)s->get("kubo_tw", sizeof(double2) * nump);
+  k_twiddles<<<(nump + 255) / 256, 256, 0, s->stream>>>(nump, tw);
+  LQ_LAUNCHED();
+  const size_t smem = sizeof(double2) * 2 * (size_t)M;
+  if (smem > 227 * 1024) fail(LINQT_ERR_UNSUPPORTED, "kubo_fft: M too large for the direct DFT");
+  LQ_CUDA(cudaFuncSetAttribute(k_kubo_dft<NSEQ>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  const int nb = (int)std::max(1L, std::min(K, (long)s->sm_count * 4));
+  const long chunk = (K + nb - 1) / nb;
+  double2 *part = (double2 *)s->get("kubo_part", sizeof(double2) * 2 * (size_t)nump * nb);
+  k_kubo_dft<NSEQ><<<nb, 256, smem, s->stream>>>(L, Rv, K, chunk, M, nump, pf, tw, part);
+  LQ_LAUNCHED();
+  k_sum_parts<<<(2 * nump + 255) / 256, 256, 0, s->stream>>>(part, nb, 2 * nump, acc);
+  LQ_LAUNCHED();
+}
+
+}  // namespace
+
+void kubo_fft_sites(Session *s, const void *Lv, const void *Rvv, long nsites, int M, int nump, int formula,
+                    bool fp32_inputs, double2 *acc) {
+  if (fp32_inputs) fail(LINQT_ERR_UNSUPPORTED, "kubo_fft: FP32 Chebyshev vectors are not supported");
+  const double2 *L = (const double2 *)Lv, *Rv = (const double2 *)Rvv;
+  double2 *pf = (double2 *)s->get("kubo_pf", sizeof(double2) * M);
+  k_prefactors<<<(M + 255) / 256, 256, 0, s->stream>>>(M, nump, pf);
+  LQ_LAUNCHED();
+  const bool bastin = formula == LINQT_KUBO_BASTIN;
+  const bool pow2 = nump >= 256 && nump <= 2048 && (nump & (nump - 1)) == 0;
+  const bool fits = pow2 && (bastin ? nump <= 1024 : true);
+  if (fits) {
+    switch (nump) {
+      case 256: bastin ? launch_fft<1, 8>(s, L, Rv, nsites, M, pf, acc) : launch_fft<1, 4>(s, L, Rv, nsites, M, pf, acc); return;
+      case 512: bastin ? launch_fft<2, 8>(s, L, Rv, nsites, M, pf, acc) : launch_fft<2, 4>(s, L, Rv, nsites, M, pf, acc); return;
+      case 1024: bastin ? launch_fft<4, 8>(s, L, Rv, nsites, M, pf, acc) : launch_fft<4, 4>(s, L, Rv, nsites, M, pf, acc); return;
+      case 2048: launch_fft<8, 4>(s, L, Rv, nsites, M, pf, acc); return;
+    }
+  }
+  if (bastin)
+    launch_dft<8>(s, L, Rv, nsites, M, nump, pf, acc);
+  else
+    launch_dft<4>(s, L, Rv, nsites, M, nump, pf, acc);
+}
+
+void kubo_postprocess(Session *s, const double2 *acc, int R, int nump, int formula, int N, double band_width,
+                      double band_center, double *out) {
+  double *scratch = (double *)s->get("kubo_post", sizeof(double) * 3 * (size_t)nump);
+  k_kubo_post<<<1, 32, 0, s->stream>>>(acc, (double)R, nump, formula, (double)N, band_width / 2.0, band_center, out,
+                                       scratch);
+  LQ_LAUNCHED();
+}
+
+}  // namespace linqt

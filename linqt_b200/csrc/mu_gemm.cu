@@ -1,0 +1,199 @@
+// Moment contraction  mu_raw(m0, m1) += sum_k conj(L[m0][k]) * Rv[m1][k].
+//
+// This is ComputeMomTable (src/chebyshev_solver.cpp:26-42: an M x M table of
+// zdotc over the site index) written as the GEMM it is (the unused
+// linalg::batch_vdot, src/mkl_linear_algebra.cpp:68-78, is the same product).
+// Both operands are "K-major": moment m's block T_m is N*R contiguous complex
+// numbers, so K = N*R and the contraction also sums over the R random vectors.
+//
+// FP64 path: CUDA-core DFMA with 64x64 complex output tiles per CTA, 4x4 complex
+// outputs per thread, cp.async double-buffered 16-deep K slices in shared memory,
+// split-K over the long K axis with a fixed-order FP64 reduction (deterministic).
+// (B200 has no FP64 tcgen05 kind; its FP64 tensor rate equals the DFMA rate.)
+#include "internal.cuh"
+
+namespace linqt {
+
+namespace {
+
+constexpr int BM = 64, BN = 64, BK = 16, LDS = BK + 1;  // LDS: padded smem row (double2)
+
+__device__ __forceinline__ void cp_async16(void *smem, const void *gmem, bool valid) {
+  const unsigned s = (unsigned)__cvta_generic_to_shared(smem);
+  const int n = valid ? 16 : 0;
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;\n" ::"r"(s), "l"(gmem), "r"(n));
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::); }
+template <int N>
+__device__ __forceinline__ void cp_async_wait() {
+  asm volatile("cp.async.wait_group %0;\n" ::"n"(N));
+}
+
+// Load a BM x BK tile of rows [row0, row0+BM) and k in [k0, k0+BK) of a K-major matrix.
+__device__ __forceinline__ void load_tile(double2 (*sm)[LDS], const double2 *__restrict__ g, int M, long K, int row0,
+                                          long k0, long kend) {
+  // 256 threads x 4 double2: thread t covers row t>>2, k slots (t&3)*4 .. +3
+  const int t = threadIdx.x;
+  const int r = t >> 2, kq = (t & 3) * 4;
+  const int row = row0 + r;
+#pragma unroll
+  for (int q = 0; q < 4; ++q) {
+    const long k = k0 + kq + q;
+    const bool ok = row < M && k < kend;
+    const double2 *src = ok ? g + (size_t)row * K + k : g;
+    cp_async16(&sm[r][kq + q], src, ok);
+  }
+}
+
+__global__ void __launch_bounds__(256) k_zgemm_cn_f64(const double2 *__restrict__ L, const double2 *__restrict__ Rv,
+                                                      int MA, int MB, long K, long kchunk, double2 *__restrict__ part) {
+  extern __shared__ double2 smem[];
+  double2(*As)[BM][LDS] = reinterpret_cast<double2(*)[BM][LDS]>(smem);
+  double2(*Bs)[BN][LDS] = reinterpret_cast<double2(*)[BN][LDS]>(smem + 2 * BM * LDS);
+  const int tx = threadIdx.x & 15, ty = threadIdx.x >> 4;
+  const int m0 = blockIdx.y * BM, m1 = blockIdx.x * BN;
+  const long kbeg = (long)blockIdx.z * kchunk;
+  const long kend = min(K, kbeg + kchunk);
+  double2 acc[4][4];
+#pragma unroll
+  for (int i = 0; i < 4; ++i)
+#pragma unroll
+    for (int j = 0; j < 4; ++j) acc[i][j] = make_double2(0, 0);
+  if (kbeg < kend) {
+    const int nk = (int)((kend - kbeg + BK - 1) / BK);
+    load_tile(As[0], L, MA, K, m0, kbeg, kend);
+    load_tile(Bs[0], Rv, MB, K, m1, kbeg, kend);
+    cp_async_commit();
+    for (int it = 0; it < nk; ++it) {
+      const int cur = it & 1;
+      if (it + 1 < nk) {
+        load_tile(As[cur ^ 1], L, MA, K, m0, kbeg + (long)(it + 1) * BK, kend);
+        load_tile(Bs[cur ^ 1], Rv, MB, K, m1, kbeg + (long)(it + 1) * BK, kend);
+      }
+      cp_async_commit();
+      cp_async_wait<1>();
+      __syncthreads();
+#pragma unroll
+      for (int kk = 0; kk < BK; ++kk) {
+        double2 a[4], b[4];
+#pragma unroll
+        for (int i = 0; i < 4; ++i) a[i] = As[cur][ty + 16 * i][kk];
+#pragma unroll
+        for (int j = 0; j < 4; ++j) b[j] = Bs[cur][tx + 16 * j][kk];
+#pragma unroll
+        for (int i = 0; i < 4; ++i)
+#pragma unroll
+          for (int j = 0; j < 4; ++j) acc[i][j] = cfma_conj(a[i], b[j], acc[i][j]);
+      }
+      __syncthreads();
+    }
+    cp_async_wait<0>();
+  }
+  double2 *out = part + (size_t)blockIdx.z * MA * MB;
+#pragma unroll
+  for (int i = 0; i < 4; ++i) {
+    const int r = m0 + ty + 16 * i;
+    if (r >= MA) continue;
+#pragma unroll
+    for (int j = 0; j < 4; ++j) {
+      const int c = m1 + tx + 16 * j;
+      if (c < MB) out[(size_t)r * MB + c] = acc[i][j];
+    }
+  }
+}
+
+// mu_raw += sum_z part[z]  (fixed order over z)
+__global__ void k_reduce_parts(const double2 *__restrict__ part, int S, long MM, double2 *__restrict__ mu_raw) {
+  for (long t = blockIdx.x * (long)blockDim.x + threadIdx.x; t < MM; t += (long)gridDim.x * blockDim.x) {
+    double2 s = mu_raw[t];
+    for (int z = 0; z < S; ++z) s = cadd(s, part[(size_t)z * MM + t]);
+    mu_raw[t] = s;
+  }
+}
+
+// Hermitian symmetrisation and scaling of CorrelationExpansionMoments
+// (src/chebyshev_solver.cpp:143-162):
+//   mu(i,j) = s_ij (raw(i,j) + conj(raw(j,i)))/2 for j >= i, mu(j,i) = conj(mu(i,j)),
+//   s_ij = (4/R) (1/2)^{[i=0]} (1/2)^{[j=0]}
+__global__ void k_mu_finalize(const double2 *__restrict__ raw, int M, double R, double2 *__restrict__ mu) {
+  const long MM = (long)M * M;
+  for (long t = blockIdx.x * (long)blockDim.x + threadIdx.x; t < MM; t += (long)gridDim.x * blockDim.x) {
+    const int i = (int)(t / M), j = (int)(t % M);
+    if (j < i) continue;
+    double scal = 4.0 / R;
+    if (i == 0) scal *= 0.5;
+    if (j == 0) scal *= 0.5;
+    const double2 a = raw[(size_t)i * M + j], b = raw[(size_t)j * M + i];
+    const double2 v = make_double2(scal * (a.x + b.x) / 2.0, scal * (a.y - b.y) / 2.0);
+    mu[(size_t)i * M + j] = v;
+    mu[(size_t)j * M + i] = cconj(v);
+  }
+}
+
+// 1D moments from per-step dot products (chebyshev::SpectralMoments scaling,
+// src/chebyshev_solver.cpp:190-195: (2/R)(1/2)^{[m=0]}).
+// mode 1: dots[2m] = <phi|T_m>; mode 2: dots[2s] = <T_s|T_s>, dots[2s+1] = <T_{s+1}|T_s>.
+__global__ void k_moments1d(const double2 *__restrict__ dots, int steps, int M, double R, int mode,
+                            double2 *__restrict__ mu) {
+  for (int m = blockIdx.x * blockDim.x + threadIdx.x; m < M; m += gridDim.x * blockDim.x) {
+    double2 v;
+    if (mode == 1) {
+      v = dots[2 * m];
+    } else {
+      const int s = m >> 1;
+      if (m & 1)
+        v = s == 0 ? dots[1] : csub(cscale(dots[2 * s + 1], 2.0), dots[1]);
+      else
+        v = s == 0 ? dots[0] : csub(cscale(dots[2 * s], 2.0), dots[0]);
+    }
+    double scal = 2.0 / R;
+    if (m == 0) scal *= 0.5;
+    mu[m] = cscale(v, scal);
+  }
+}
+
+}  // namespace
+
+// C(i, j) (+)= sum_k conj(A[i][k]) * B[j][k] for i < MA, j < MB  (FP64, deterministic split-K)
+void zgemm_cn(Session *s, const double2 *A, int MA, const double2 *B, int MB, long K, double2 *C, bool accumulate) {
+  const int tiles = ((MA + BM - 1) / BM) * ((MB + BN - 1) / BN);
+  const long target = (long)s->sm_count * 2 * 2;
+  long S = std::max(1L, (target + tiles - 1) / tiles);
+  const long min_chunk = 512;
+  S = std::max(1L, std::min(std::min(S, 64L), (K + min_chunk - 1) / min_chunk));
+  long kchunk = (K + S - 1) / S;
+  kchunk = (kchunk + BK - 1) / BK * BK;
+  S = (K + kchunk - 1) / kchunk;
+  double2 *part = (double2 *)s->get("zgemm_parts", sizeof(double2) * (size_t)S * MA * MB);
+  const size_t smem = sizeof(double2) * 2 * (BM + BN) * LDS;
+  LQ_CUDA(cudaFuncSetAttribute(k_zgemm_cn_f64, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  dim3 grid((MB + BN - 1) / BN, (MA + BM - 1) / BM, (unsigned)S);
+  k_zgemm_cn_f64<<<grid, 256, smem, s->stream>>>(A, B, MA, MB, K, kchunk, part);
+  LQ_LAUNCHED();
+  const long MM = (long)MA * MB;
+  if (!accumulate) LQ_CUDA(cudaMemsetAsync(C, 0, sizeof(double2) * MM, s->stream));
+  const int g2 = (int)std::max(1L, std::min((MM + 255) / 256, (long)s->sm_count * 8));
+  k_reduce_parts<<<g2, 256, 0, s->stream>>>(part, (int)S, MM, C);
+  LQ_LAUNCHED();
+}
+
+void mu_contract(Session *s, const void *L, const void *Rv, int M, long K, bool fp32_inputs, int precision,
+                 double2 *mu_raw) {
+  if (fp32_inputs) fail(LINQT_ERR_INTERNAL, "mu_contract: FP32 operands take the tensor-core path");
+  (void)precision;
+  zgemm_cn(s, (const double2 *)L, M, (const double2 *)Rv, M, K, mu_raw, true);
+}
+
+void mu_finalize(Session *s, const double2 *mu_raw, int M, int R, double2 *mu) {
+  const long MM = (long)M * M;
+  const int g = (int)std::max(1L, std::min((MM + 255) / 256, (long)s->sm_count * 8));
+  k_mu_finalize<<<g, 256, 0, s->stream>>>(mu_raw, M, (double)R, mu);
+  LQ_LAUNCHED();
+}
+
+void moments1d_from_dots(Session *s, const double2 *dots, int steps, int M, int R, int mode, double2 *mu) {
+  k_moments1d<<<(M + 255) / 256, 256, 0, s->stream>>>(dots, steps, M, (double)R, mode, mu);
+  LQ_LAUNCHED();
+}
+
+}  // namespace linqt
