@@ -27,10 +27,11 @@ def read_csr(path):
 
 
 def write_csr(path, n, rowptr, col, val):
+    """Values are written with 17 significant digits (lossless for doubles)."""
     val = np.asarray(val, dtype=np.complex128)
     with open(path, "w") as f:
         f.write("%d %d\n" % (n, len(col)))
-        f.write(" ".join("%s %s" % (_g(z.real), _g(z.imag)) for z in val) + " \n")
+        f.write(" ".join("%.17g %.17g" % (z.real, z.imag) for z in val) + " \n")
         f.write(" ".join(str(int(c)) for c in col) + " \n")
         f.write(" ".join(str(int(r)) for r in rowptr) + " \n")
 

@@ -1,0 +1,104 @@
+"""Pin the C restatement against the reference's own sources (oracle/_ref).
+
+oracle/_ref holds LinQT's src/*.cpp compiled unmodified against stand-in MKL /
+FFTW / Eigen headers, plus its CLI drivers and ref_harness (an in-process timing
+harness).  These tests feed both the same seeded synthetic operators and states,
+through the reference's own file formats, and compare the results.
+"""
+import os
+import subprocess
+
+import numpy as np
+import pytest
+
+from linqt_b200 import formats, lattices
+
+pytestmark = pytest.mark.skipif(not os.path.exists(os.path.join(os.path.dirname(__file__), "..", "oracle", "_ref",
+                                                                "ref_harness")),
+                                reason="oracle/_ref not built (needs the reference checkout)")
+
+
+def setup_dir(oracle_lib, tmp_path, label, ops, bounds, states):
+    d = tmp_path
+    (d / "operators").mkdir()
+    for name, (n, csr) in ops.items():
+        formats.write_csr(str(d / "operators" / ("%s.%s.CSR" % (label, name))), n, *csr)
+    (d / "BOUNDS").write_text("%.17g %.17g\n" % bounds)
+    formats.write_vector_states(str(d / "states.txt"), states)
+    return str(d)
+
+
+def rel(a, b):
+    return float(np.abs(np.asarray(a) - np.asarray(b)).max() / np.abs(np.asarray(b)).max())
+
+
+def test_spectral_moments_vs_ref(oracle_lib, tmp_path):
+    N, H = lattices.square_lattice(16, t=1.0, W=1.0, seed=11)
+    st = lattices.random_phase_states(N, 2, seed=12)
+    lo, hi = -4.725, 4.725
+    d = setup_dir(oracle_lib, tmp_path, "sq", {"HAM": (N, H)}, (lo, hi), st)
+    out = oracle_lib.run_ref_harness(["spectral", "sq", "1", 64, "states.txt"], d)
+    n, bw, bc, mu_ref = formats.read_chebmom1d(os.path.join(d, out["out"]))
+    assert n == N and bw == hi - lo
+    Ho = oracle_lib.Op(*formats.read_csr(os.path.join(d, "operators", "sq.HAM.CSR"))[1:])
+    Ho.rescale(2 / bw, -bc / (bw / 2))
+    st_file = formats.read_state_file(os.path.join(d, "states.txt"))
+    mu = oracle_lib.moments1d(Ho, None, st_file, 64)
+    assert rel(mu, mu_ref) < 1e-12
+
+
+def test_correlation_moments_vs_ref(oracle_lib, tmp_path):
+    N, H, V = lattices.honeycomb(6, 5, t=-2.7, W=1.0, seed=21)
+    st = lattices.random_phase_states(N, 3, seed=22)
+    lo, hi = lattices.gershgorin_bounds(N, *H)
+    d = setup_dir(oracle_lib, tmp_path, "gr", {"HAM": (N, H), "VX": (N, V)}, (1.05 * lo, 1.05 * hi), st)
+    env = dict(os.environ)
+    env.pop("BATCH_SIZE", None)
+    out = oracle_lib.run_ref_harness(["nonEq", "gr", "VX", "VX", 40, "states.txt"], d)
+    n, bw, bc, mu_ref = formats.read_chebmom2d(os.path.join(d, out["out"]))
+    _, rp, cl, vl = formats.read_csr(os.path.join(d, "operators", "gr.HAM.CSR"))
+    Ho = oracle_lib.Op(rp, cl, vl).rescale(2 / bw, -bc / (bw / 2))
+    _, rp, cl, vl = formats.read_csr(os.path.join(d, "operators", "gr.VX.CSR"))
+    Vo = oracle_lib.Op(rp, cl, vl)
+    mu = oracle_lib.moments2d(Ho, Vo, Vo, formats.read_state_file(os.path.join(d, "states.txt")), 40)
+    assert rel(mu, mu_ref) < 1e-12
+
+
+@pytest.mark.parametrize("formula,nump", [(1, 64), (0, 64), (1, 50)])
+def test_kubo_fft_vs_ref(oracle_lib, tmp_path, formula, nump):
+    N, H, V = lattices.honeycomb(5, 4, t=-2.7, W=1.0, seed=21)
+    st = lattices.random_phase_states(N, 2, seed=23)
+    lo, hi = lattices.gershgorin_bounds(N, *H)
+    d = setup_dir(oracle_lib, tmp_path, "gr", {"HAM": (N, H), "VX": (N, V)}, (1.05 * lo, 1.05 * hi), st)
+    M = 32
+    out = oracle_lib.run_ref_harness(["kuboFFT", "gr", "VX", "VX", M, nump, formula, "states.txt"], d)
+    ref = np.loadtxt(os.path.join(d, out["out"]))
+    bw, bc = 1.05 * (hi - lo), 1.05 * (hi + lo) / 2
+    _, rp, cl, vl = formats.read_csr(os.path.join(d, "operators", "gr.HAM.CSR"))
+    Ho = oracle_lib.Op(rp, cl, vl).rescale(2 / bw, -bc / (bw / 2))
+    _, rp, cl, vl = formats.read_csr(os.path.join(d, "operators", "gr.VX.CSR"))
+    Vo = oracle_lib.Op(rp, cl, vl)
+    E, s, integ, _ = oracle_lib.kubo_fft(Ho, Vo, Vo, formats.read_state_file(os.path.join(d, "states.txt")), M, nump,
+                                         formula, N, bw, bc)
+    # the reference prints with 6 significant digits
+    assert np.abs(E - ref[:, 0]).max() < 1e-5 * np.abs(E).max()
+    assert np.abs(s - ref[:, 1]).max() < 2e-6 * np.abs(s).max() + 1e-300
+    if formula == 1:
+        ri = np.loadtxt(os.path.join(d, out["out"] + "_integrand"))
+        assert np.abs(integ - ri[:, 1]).max() < 2e-6 * np.abs(integ).max()
+
+
+def test_reference_driver_on_golden_chain(tmp_path):
+    """The reference's own inline_compute-kpm-nonEqOp, built here, reproduces the shipped table."""
+    golden = np.load(os.path.join(os.path.dirname(__file__), "golden", "linear_chain.npz"))
+    (tmp_path / "operators").mkdir()
+    for op in ("HAM", "VX"):
+        rp, cl, vl = golden[op + "_rowptr"], golden[op + "_col"], golden[op + "_val"]
+        formats.write_csr(str(tmp_path / "operators" / ("linear_chain.%s.CSR" % op)), len(rp) - 1, rp, cl,
+                          vl[0::2] + 1j * vl[1::2])
+    (tmp_path / "BOUNDS").write_text("-5 5\n")
+    exe = os.path.join(os.path.dirname(__file__), "..", "oracle", "_ref", "inline_compute-kpm-nonEqOp")
+    subprocess.run([exe, "linear_chain", "VX", "VX", "100"], cwd=str(tmp_path), check=True, capture_output=True)
+    n, bw, bc, mu = formats.read_chebmom2d(str(tmp_path / "NonEqOpVX-VXlinear_chainKPM_M100x100_statedefault.chebmom2D"))
+    ref = golden["mu100"][..., 0] + 1j * golden["mu100"][..., 1]
+    assert rel(mu, ref) < 1e-13
