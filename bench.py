@@ -1,0 +1,374 @@
+#!/usr/bin/env python
+"""Benchmark: Chebyshev steps*nnz/s of one Kubo-Bastin sigma_xx(E) solve on a B200.
+
+Workload (one "step" = one solve): honeycomb graphene, 128 x 128 cells (N = 32,768
+sites), t = -2.7 eV, Anderson disorder W = 1.0 eV (seed 21), V_x = i (x_i - x_j) H_ij
+(a = 1.42 A); 8 random-phase vectors (seed 22) as one block; 512 x 512 2D moments
+(CorrelationExpansionMoments) and the FFT Bastin reconstruction at 1024 energies
+(Kubo_solver_FFT), both from one pass of the recursion.  Synthetic, seeded inputs stand
+in for operators read from files.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl linqt|reference]
+                    [--precision fp64|mixed]
+
+metric = (recursion steps per vector column: 2M) x (columns: R) x nnz(H, Hermitian-
+expanded, diagonal included) / seconds.  value: device time of K solves with operators
+and states resident in HBM (CUDA events on the launching stream, max over ranks);
+e2e: the same through the host-pointer C ABI call with the states copied from pinned
+host memory and mu / sigma(E) copied back inside the timed region.  Multi-GPU: one
+independent solve per rank (different random vectors), no collective on the data path.
+"""
+import argparse
+import json
+import os
+import subprocess
+import sys
+import tempfile
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+WORKLOAD = dict(workload="kubo_bastin_graphene_128x128", lattice="honeycomb", Lx=128, Ly=128, t=-2.7, W=1.0, a=1.42,
+                disorder_seed=21, phase_seed=22, R=8, M=512, nump=1024, formula="bastin", bounds_pad=1.05)
+METRIC = "chebyshev_steps_nnz_per_s"
+UNIT = "steps*nnz/s"
+
+
+def build_inputs(rank=0):
+    from linqt_b200 import lattices
+    w = WORKLOAD
+    N, H, V = lattices.honeycomb(w["Lx"], w["Ly"], t=w["t"], W=w["W"], seed=w["disorder_seed"], a=w["a"])
+    lo, hi = lattices.gershgorin_bounds(N, *H)
+    bw = w["bounds_pad"] * (hi - lo)
+    bc = (hi + lo) / 2
+    st = lattices.random_phase_states(N, w["R"], seed=w["phase_seed"] + 1000 * rank)
+    return N, H, V, bw, bc, st
+
+
+def nnz_full(N, H):
+    rp, col, _ = H
+    rows = np.repeat(np.arange(N), np.diff(rp))
+    off = int((col != rows).sum())
+    return N + 2 * off  # diagonal always present after rescaling
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled every 200 ms during the timed region."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device):
+        self.device = device
+        self.f = tempfile.NamedTemporaryFile("w+", suffix=".csv", delete=False)
+        self.p = None
+
+    def __enter__(self):
+        try:
+            self.p = subprocess.Popen(["nvidia-smi", "-i", str(self.device), "--query-gpu=" + self.FIELDS,
+                                       "--format=csv,noheader,nounits", "-lms", "200"], stdout=self.f,
+                                      stderr=subprocess.DEVNULL)
+        except OSError:
+            self.p = None
+        time.sleep(0.3)
+        return self
+
+    def __exit__(self, *a):
+        if self.p:
+            self.p.terminate()
+            self.p.wait()
+
+    def summary(self):
+        self.f.seek(0)
+        rows = [r.split(",") for r in self.f.read().strip().splitlines() if r.strip()]
+        os.unlink(self.f.name)
+        if not rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        sm = [float(r[1]) for r in rows if r[1].strip().replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in rows if r[2].strip().replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for r in rows for i in range(4) if len(r) > 5 + i and "Active" in r[5 + i]
+                          and "Not" not in r[5 + i]})
+        return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "samples": len(rows), "reasons": reasons}
+
+
+def measured_peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        d = json.load(open(p))
+        return d.get("hbm_gbs", 6650.0), d.get("bf16_tflops", 1590.0), "measured"
+    return 6650.0, 1590.0, "fallback"
+
+
+def fp64_peak_tflops(torch, device):
+    """FP64 dense peak measured here with torch.matmul (cuBLAS DGEMM), best of 5."""
+    n = 8192
+    a = torch.randn(n, n, dtype=torch.float64, device=device)
+    b = torch.randn(n, n, dtype=torch.float64, device=device)
+    for _ in range(2):
+        a @ b
+    best = 0.0
+    for _ in range(5):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        a @ b
+        e1.record()
+        e1.synchronize()
+        best = max(best, 2 * n ** 3 / (e0.elapsed_time(e1) * 1e-3) / 1e12)
+    del a, b
+    return best
+
+
+def run_reference(args):
+    """The reference's own CPU solvers (oracle/_ref/ref_harness, LinQT's src/*.cpp built here)
+    on a bounded sample: one of the 8 random vectors per step, the full M = 512, nump = 1024."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle as orc
+    from linqt_b200 import formats
+    if not orc.ref_available():
+        print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref is not built (needs the reference checkout)"}))
+        return
+    N, H, V, bw, bc, st = build_inputs(0)
+    w = WORKLOAD
+    d = tempfile.mkdtemp(prefix="linqt_bench_ref_")
+    os.makedirs(os.path.join(d, "operators"))
+    formats.write_csr(os.path.join(d, "operators", "gr.HAM.CSR"), N, *H)
+    formats.write_csr(os.path.join(d, "operators", "gr.VX.CSR"), N, *V)
+    lo, hi = bc - bw / 2, bc + bw / 2
+    open(os.path.join(d, "BOUNDS"), "w").write("%.17g %.17g\n" % (lo, hi))
+    threads = os.cpu_count() or 1
+    nnz = nnz_full(N, H)
+    total_s, total_units = 0.0, 0.0
+    for it in range(args.warmup + args.steps):
+        col = it % w["R"]
+        sp = os.path.join(d, "st%d.txt" % col)
+        if not os.path.exists(sp):
+            formats.write_vector_states(sp, st[col:col + 1])
+        a = orc.run_ref_harness(["nonEq", "gr", "VX", "VX", w["M"], os.path.basename(sp)], d, threads=threads)
+        b = orc.run_ref_harness(["kuboFFT", "gr", "VX", "VX", w["M"], w["nump"], 1, os.path.basename(sp)], d,
+                                threads=threads)
+        if it >= args.warmup:
+            total_s += a["seconds"] + b["seconds"]
+            total_units += 2 * w["M"] * 1 * nnz
+    value = total_units / total_s
+    cfg = dict(WORKLOAD)
+    cfg.update(parallelism="cpu", l2="n/a (CPU)")
+    sample = "1 of the 8 random vectors per step (M=512, nump=1024): CorrelationExpansionMoments + Kubo_solver_FFT"
+    print(json.dumps({"impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus,
+                      "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * total_s / args.steps,
+                      "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+                      "data": "synthetic (seeded)", "config": cfg,
+                      "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": "reference",
+                                       "sample": sample},
+                      "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}))
+
+
+def cpu_baseline_sample():
+    """Reference CPU solvers on one random vector of the same workload (rank 0, N=1 only)."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle as orc
+    from linqt_b200 import formats
+    if not orc.ref_available():
+        return None
+    N, H, V, bw, bc, st = build_inputs(0)
+    w = WORKLOAD
+    d = tempfile.mkdtemp(prefix="linqt_cpu_")
+    os.makedirs(os.path.join(d, "operators"))
+    formats.write_csr(os.path.join(d, "operators", "gr.HAM.CSR"), N, *H)
+    formats.write_csr(os.path.join(d, "operators", "gr.VX.CSR"), N, *V)
+    open(os.path.join(d, "BOUNDS"), "w").write("%.17g %.17g\n" % (bc - bw / 2, bc + bw / 2))
+    formats.write_vector_states(os.path.join(d, "st.txt"), st[:1])
+    threads = os.cpu_count() or 1
+    a = orc.run_ref_harness(["nonEq", "gr", "VX", "VX", w["M"], "st.txt"], d, threads=threads)
+    b = orc.run_ref_harness(["kuboFFT", "gr", "VX", "VX", w["M"], w["nump"], 1, "st.txt"], d, threads=threads)
+    secs = a["seconds"] + b["seconds"]
+    return {"value": 2 * w["M"] * nnz_full(N, H) / secs, "unit": UNIT, "cores": threads, "kind": "reference",
+            "sample": "1 of 8 random vectors, M=512, nump=1024 (CorrelationExpansionMoments %.2fs + "
+                      "Kubo_solver_FFT %.2fs)" % (a["seconds"], b["seconds"])}
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="linqt", choices=["linqt", "reference"])
+    ap.add_argument("--precision", default="fp64", choices=["fp64", "mixed"])
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    # size overrides, for profiling captures on a smaller case of the same kernels
+    ap.add_argument("--lx", type=int, default=None)
+    ap.add_argument("--ly", type=int, default=None)
+    ap.add_argument("--moments", type=int, default=None)
+    ap.add_argument("--vectors", type=int, default=None)
+    args = ap.parse_args()
+    for k, v in (("Lx", args.lx), ("Ly", args.ly), ("M", args.moments), ("R", args.vectors)):
+        if v:
+            WORKLOAD[k] = v
+            WORKLOAD["workload"] = "kubo_bastin_graphene_%dx%d_M%d_R%d" % (WORKLOAD["Lx"], WORKLOAD["Ly"],
+                                                                         WORKLOAD["M"], WORKLOAD["R"])
+    args.warmup = max(args.warmup, 3)
+
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+
+    if args.impl == "reference":
+        if rank == 0:
+            run_reference(args)
+        return
+
+    import torch
+    import linqt_b200 as lq
+
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300), device_id=torch.device("cuda", local))
+
+    w = WORKLOAD
+    N, H, V, bw, bc, st = build_inputs(rank)
+    nnz = nnz_full(N, H)
+    M, R, nump = w["M"], w["R"], w["nump"]
+    stream = torch.cuda.current_stream()
+    sess = lq.Session(local)
+    sess.set_stream(stream)
+    Hg = lq.Operator.from_csr(N, *H, session=sess)
+    Hg.rescale_to_chebyshev(bw, bc)
+    Vg = lq.Operator.from_csr(N, *V, session=sess)
+    assert Hg.nnz == nnz
+    prec = lq.PREC_FP64 if args.precision == "fp64" else lq.PREC_MIXED
+    opts = lq.make_opts(precision=prec)
+
+    st_dev = torch.from_numpy(st.view(np.float64).copy()).cuda()
+    mu_dev = torch.zeros(2 * M * M, dtype=torch.float64, device="cuda")
+    out_dev = torch.zeros(3 * nump, dtype=torch.float64, device="cuda")
+
+    def solve_dev():
+        lq.kubo_bastin_dev(Hg, Vg, Vg, st_dev, R, M, nump, bw, bc, mu_dev, out_dev, opts=opts, session=sess)
+
+    for _ in range(args.warmup):
+        solve_dev()
+    torch.cuda.synchronize()
+    sess.enable_timing(True)
+    sess.phase_times(reset=True)
+
+    def barrier():
+        if dist is not None:
+            dist.barrier()
+
+    with ClockSampler(local) as clocks:
+        barrier()
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(args.steps):
+            solve_dev()
+        e1.record(stream)
+        torch.cuda.synchronize()
+        barrier()
+    dev_ms = e0.elapsed_time(e1) / args.steps
+    phase_ms, phase_launches = sess.phase_times(reset=True)
+    sess.enable_timing(False)
+    clk = clocks.summary()
+
+    # ---- end to end through the host-pointer C ABI call (pinned host buffers)
+    st_pin = torch.from_numpy(st.view(np.float64).copy()).pin_memory()
+    mu_pin = torch.zeros(2 * M * M, dtype=torch.float64).pin_memory()
+    E_pin = torch.zeros(nump, dtype=torch.float64).pin_memory()
+    s_pin = torch.zeros(nump, dtype=torch.float64).pin_memory()
+
+    def solve_host():
+        lq.kubo_bastin_host_ptr(Hg, Vg, Vg, st_pin.data_ptr(), R, M, nump, bw, bc, mu_pin.data_ptr(), E_pin.data_ptr(),
+                                s_pin.data_ptr(), opts=opts, session=sess)
+
+    for _ in range(2):
+        solve_host()
+    barrier()
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        solve_host()
+    torch.cuda.synchronize()
+    barrier()
+    e2e_ms = 1e3 * (time.perf_counter() - t0) / args.steps
+
+    def max_over_ranks(x):
+        if dist is None:
+            return x
+        t = torch.tensor([x], dtype=torch.float64, device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
+
+    dev_ms = max_over_ranks(dev_ms)
+    e2e_ms = max_over_ranks(e2e_ms)
+    units = 2 * M * R * nnz  # recursion steps x nnz per solve and rank
+    value = world * units / (dev_ms * 1e-3)
+    e2e = world * units / (e2e_ms * 1e-3)
+
+    # ---- roofline of the dominant phase
+    hbm_peak, bf16_peak, peak_src = measured_peaks()
+    K = N * R
+    esz = 16 if prec == lq.PREC_FP64 else 8
+    rec_bytes_per_step = nnz * (16 + 4) + 4 * (N + 1) + 3 * 16 * N * R
+    phases = {
+        "recursion": {"ms": phase_ms[0] / args.steps, "launches": phase_launches[0] // args.steps,
+                      "bytes": 2 * M * rec_bytes_per_step},
+        "contraction": {"ms": phase_ms[1] / args.steps, "launches": phase_launches[1] // args.steps,
+                        "flops": 8.0 * M * M * K},
+        "fft": {"ms": phase_ms[2] / args.steps, "launches": phase_launches[2] // args.steps,
+                "flops": 8.0 * K * 5 * nump * np.log2(nump)},
+        "other": {"ms": phase_ms[3] / args.steps, "launches": phase_launches[3] // args.steps},
+    }
+    fp64_peak = fp64_peak_tflops(torch, "cuda")
+    dom = max(("recursion", "contraction", "fft"), key=lambda k: phases[k]["ms"])
+    if dom == "recursion":
+        ach = phases[dom]["bytes"] / (phases[dom]["ms"] * 1e-3) / 1e9
+        roof = {"kernel": "cheb_step (recursion)", "bound": "hbm", "achieved": ach, "peak": hbm_peak, "unit": "GB/s",
+                "frac": ach / hbm_peak, "peak_source": peak_src}
+    else:
+        ach = phases[dom]["flops"] / (phases[dom]["ms"] * 1e-3) / 1e12
+        roof = {"kernel": {"contraction": "zgemm_cn_f64 (mu_nm contraction)", "fft": "kubo_fft (per-site DFTs)"}[dom],
+                "bound": "tensor", "pipe": "fp64", "achieved": ach, "peak": fp64_peak, "unit": "TFLOP/s",
+                "frac": ach / fp64_peak, "peak_source": "FP64 DGEMM (torch.matmul 8192^3) measured in this run"}
+    roof["traffic"] = None
+    rec_ach = phases["recursion"]["bytes"] / (phases["recursion"]["ms"] * 1e-3) / 1e9
+    for k in phases:
+        phases[k]["ms"] = round(phases[k]["ms"], 4)
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        try:
+            cpu = cpu_baseline_sample()
+        except Exception as ex:  # report, do not fail the GPU measurement
+            cpu = {"error": str(ex)[:200]}
+
+    if rank == 0:
+        cfg = dict(WORKLOAD)
+        cfg.update(parallelism="replicas%d" % world if world > 1 else "single",
+                   l2="inputs larger than L2: 4.3 GB of Chebyshev blocks written and read per solve",
+                   nnz_full=nnz, N=N)
+        line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+                "warmup": args.warmup, "ms_per_step": dev_ms, "higher_is_better": True, "scaling": "weak",
+                "vs_baseline": None, "dtype": "f64" if prec == lq.PREC_FP64 else "f32+tf32x3",
+                "data": "synthetic (seeded lattice, random-phase states)", "config": cfg,
+                "e2e": {"value": e2e, "unit": UNIT, "ms_per_step": e2e_ms,
+                        "h2d_bytes_per_step": int(st.nbytes), "d2h_bytes_per_step": int(16 * M * M + 16 * nump)},
+                "gpu_launches": int(sum(phase_launches) // args.steps * args.steps),
+                "roofline": roof,
+                "roofline_recursion": {"bound": "hbm", "achieved": rec_ach, "peak": hbm_peak, "unit": "GB/s",
+                                       "frac": rec_ach / hbm_peak, "peak_source": peak_src},
+                "phases": phases, "fp64_peak_tflops": fp64_peak, "clocks": clk, "cpu_baseline": cpu}
+        print(json.dumps(line))
+    if dist is not None:
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

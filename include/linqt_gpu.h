@@ -136,6 +136,19 @@ int linqt_kubo_fft_dev(linqt_session *s, const linqt_op *H, const linqt_op *opl,
                        const double *states_dev, int R, int M, int nump, int formula, double band_width,
                        double band_center, const linqt_opts *opts, double *out_dev /* 3*nump: E, sigma, integrand */);
 
+/* One Kubo-Bastin solve: the L/R Chebyshev blocks (L_m = T_m(H) OPL r, R_m = OPR T_m(H) r)
+ * are computed once and feed both the 2D moment table of linqt_moments2d (mu, may be NULL)
+ * and the FFT Bastin reconstruction of linqt_kubo_fft with formula LINQT_KUBO_BASTIN
+ * (E/sigma/integrand, may be NULL).  The reference computes the same two results with two
+ * separate solvers, each running its own recursion: chebyshev::CorrelationExpansionMoments
+ * (src/chebyshev_solver.cpp:86-172) and Kubo_solver_FFT::compute (src/Kubo_solver_FFT.cpp:12-72). */
+int linqt_kubo_bastin(linqt_session *s, const linqt_op *H, const linqt_op *opl, const linqt_op *opr,
+                      const double *states, int R, int M, int nump, double band_width, double band_center,
+                      const linqt_opts *opts, double *mu, double *E, double *sigma, double *integrand);
+int linqt_kubo_bastin_dev(linqt_session *s, const linqt_op *H, const linqt_op *opl, const linqt_op *opr,
+                          const double *states_dev, int R, int M, int nump, double band_width, double band_center,
+                          const linqt_opts *opts, double *mu_dev, double *out_dev /* 3*nump or NULL */);
+
 /* ---- reconstructions (FP64 on the device) ------------------------------- */
 /* Moments1D::ApplyJacksonKernel (src/chebyshev_moments1D.cpp:68-87) followed by the DOS of
  * spectralFunctionFromChebmom_FFTgrid (src/spectralFunctionFromChebmom_FFTgrid.cpp:35-75).

@@ -171,8 +171,9 @@ class Operator:
         X = x.reshape(-1, 1) if single else x
         n, ncols = X.shape
         # the C ABI takes ncols column-major vectors: transpose to (ncols, n) contiguous
-        xt = np.ascontiguousarray(X.T)
-        yt = np.zeros_like(xt) if y is None else np.ascontiguousarray(_c128(y).reshape(n, ncols).T)
+        # (copies: with one column the transpose is already contiguous and would alias the caller's arrays)
+        xt = np.array(X.T, order="C", copy=True)
+        yt = np.zeros_like(xt) if y is None else np.array(_c128(y).reshape(n, ncols).T, order="C", copy=True)
         av = np.array([complex(a).real, complex(a).imag])
         bv = np.array([complex(b).real, complex(b).imag])
         check(load().linqt_op_multiply(_sh(session or self.session), self.h, _dp(av), _dp(xt.view(np.float64)),
@@ -241,6 +242,41 @@ def kubo_fft_dev(H, opl, opr, states_dev, R, M, nump, formula, band_width, band_
     check(load().linqt_kubo_fft_dev(_sh(session), H.h, _oph(opl), _oph(opr), ctypes.c_void_p(_ptr(states_dev)), R, M,
                                     nump, formula, band_width, band_center, ctypes.byref(o),
                                     ctypes.c_void_p(_ptr(out_dev))))
+
+
+def kubo_bastin(H, opl, opr, states, M, nump, band_width, band_center, want_mu=True, want_fft=True, opts=None,
+                session=None):
+    """One Kubo-Bastin solve: (mu[M, M] or None, (E, sigma, integrand) or None)."""
+    st = np.atleast_2d(_c128(states))
+    R = st.shape[0]
+    mu = np.zeros((M, M), np.complex128) if want_mu else None
+    E, s, integ = (np.zeros(nump), np.zeros(nump), np.zeros(nump)) if want_fft else (None, None, None)
+    o = opts or make_opts()
+    nul = ctypes.POINTER(ctypes.c_double)()
+    check(load().linqt_kubo_bastin(_sh(session), H.h, _oph(opl), _oph(opr), _dp(st.view(np.float64)), R, M, nump,
+                                   band_width, band_center, ctypes.byref(o),
+                                   _dp(mu.view(np.float64)) if want_mu else nul,
+                                   _dp(E) if want_fft else nul, _dp(s) if want_fft else nul,
+                                   _dp(integ) if want_fft else nul))
+    return mu, ((E, s, integ) if want_fft else None)
+
+
+def kubo_bastin_host_ptr(H, opl, opr, states_ptr, R, M, nump, band_width, band_center, mu_ptr, E_ptr, sigma_ptr,
+                         opts=None, session=None):
+    """Same as kubo_bastin with raw host pointers (e.g. pinned torch tensors)."""
+    o = opts or make_opts()
+    P = ctypes.POINTER(ctypes.c_double)
+    check(load().linqt_kubo_bastin(_sh(session), H.h, _oph(opl), _oph(opr), ctypes.cast(states_ptr, P), R, M, nump,
+                                   band_width, band_center, ctypes.byref(o), ctypes.cast(mu_ptr, P),
+                                   ctypes.cast(E_ptr, P), ctypes.cast(sigma_ptr, P), P()))
+
+
+def kubo_bastin_dev(H, opl, opr, states_dev, R, M, nump, band_width, band_center, mu_dev, out_dev, opts=None,
+                    session=None):
+    o = opts or make_opts()
+    check(load().linqt_kubo_bastin_dev(_sh(session), H.h, _oph(opl), _oph(opr), ctypes.c_void_p(_ptr(states_dev)), R,
+                                       M, nump, band_width, band_center, ctypes.byref(o),
+                                       ctypes.c_void_p(_ptr(mu_dev)), ctypes.c_void_p(_ptr(out_dev))))
 
 
 def dos_from_moments(mu, N, band_width, band_center, broad_meV, session=None):

@@ -544,6 +544,60 @@ void moments2d_for_server(Session *s, const DeviceOp &H, const DeviceOp *opl, co
 }
 
 // ---------------------------------------------------------------------------
+// One Kubo-Bastin solve: the L/R blocks are computed once per vector chunk and feed
+// both the moment contraction (CorrelationExpansionMoments) and the per-site FFT
+// reconstruction (Kubo_solver_FFT with formula KUBO_BASTIN).  mu or out may be NULL.
+// ---------------------------------------------------------------------------
+static void kubo_bastin_dev(Session *s, const DeviceOp &H, const DeviceOp *opl, const DeviceOp *opr,
+                            const double2 *states, int R, int M, int nump, double bw, double bc,
+                            const linqt_opts &o, double2 *mu, double *out) {
+  LQ_REQUIRE(R > 0 && M > 0, "kubo_bastin: R and M must be positive");
+  LQ_REQUIRE(!out || nump >= M, "kubo_bastin: nump must be >= M");
+  LQ_REQUIRE(bw > 0, "kubo_bastin: band_width must be positive");
+  if (o.precision != LINQT_PREC_FP64) fail(LINQT_ERR_UNSUPPORTED, "kubo_bastin: FP64 only in this build");
+  const int N = H.n;
+  const size_t extra = sizeof(double2) * ((size_t)M * M * 64 + 2 * (size_t)std::max(nump, 1) * 1024);
+  const Chunking ch = pick_chunks(s, N, R, M, sizeof(double2), o, extra);
+  const size_t blk = sizeof(double2) * (size_t)N * ch.Rc;
+  char *Ls = (char *)s->get("lr_L", blk * M);
+  char *Rs = (char *)s->get("lr_R", blk * M);
+  char *tmp = (char *)s->get("lr_tmp", blk * 4);
+  double2 *raw = nullptr, *acc = nullptr, *acc_c = nullptr;
+  if (mu) {
+    raw = (double2 *)s->get("mu_raw", sizeof(double2) * (size_t)M * M);
+    LQ_CUDA(cudaMemsetAsync(raw, 0, sizeof(double2) * (size_t)M * M, s->stream));
+  }
+  if (out) {
+    acc = (double2 *)s->get("kubo_acc", sizeof(double2) * 2 * (size_t)nump);
+    acc_c = (double2 *)s->get("kubo_acc_c", sizeof(double2) * 2 * (size_t)nump);
+    LQ_CUDA(cudaMemsetAsync(acc, 0, sizeof(double2) * 2 * (size_t)nump, s->stream));
+  }
+  for (int c = 0; c < ch.nchunks; ++c) {
+    void *phi = tmp + 3 * blk;
+    {
+      PhaseScope ph(s, PH_RECURSION);
+      chunk_block(s, states, N, R, c * ch.Rc, ch.Rc, phi, false);
+      ph.launches(1 + lr_vectors(s, H, opl, opr, phi, M, ch.Rc, false, Ls, Rs, tmp, o.format));
+    }
+    if (mu) {
+      PhaseScope ph(s, PH_CONTRACT);
+      mu_contract(s, Ls, Rs, M, (long)N * ch.Rc, false, o.precision, raw);
+      ph.launches(2);
+    }
+    if (out) {
+      PhaseScope ph(s, PH_FFT);
+      kubo_fft_sites(s, Ls, Rs, (long)N * ch.Rc, M, nump, LINQT_KUBO_BASTIN, false, acc_c);
+      add_into(s, acc, acc_c, 2 * nump);
+      ph.launches(4);
+    }
+  }
+  PhaseScope ph(s, PH_OTHER);
+  if (mu) mu_finalize(s, raw, M, R, mu);
+  if (out) kubo_postprocess(s, acc, R, nump, LINQT_KUBO_BASTIN, N, bw, bc, out);
+  ph.launches((mu ? 1 : 0) + (out ? 1 : 0));
+}
+
+// ---------------------------------------------------------------------------
 // host staging helpers
 // ---------------------------------------------------------------------------
 struct DevBuf {
@@ -875,6 +929,47 @@ int linqt_kubo_fft(linqt_session *s, const linqt_op *H, const linqt_op *opl, con
     std::memcpy(E, h.data(), sizeof(double) * nump);
     std::memcpy(sigma, h.data() + nump, sizeof(double) * nump);
     if (integrand) std::memcpy(integrand, h.data() + 2 * (size_t)nump, sizeof(double) * nump);
+  });
+}
+
+int linqt_kubo_bastin_dev(linqt_session *s, const linqt_op *H, const linqt_op *opl, const linqt_op *opr,
+                          const double *states_dev, int R, int M, int nump, double band_width, double band_center,
+                          const linqt_opts *opts, double *mu_dev, double *out_dev) {
+  return guarded([&] {
+    check_op(H, "H");
+    LQ_REQUIRE(states_dev && (mu_dev || out_dev), "NULL pointer");
+    kubo_bastin_dev(resolve(s), H->op, dop(opl), dop(opr), (const double2 *)states_dev, R, M, nump, band_width,
+                    band_center, defaults(opts), (double2 *)mu_dev, out_dev);
+  });
+}
+
+int linqt_kubo_bastin(linqt_session *s, const linqt_op *H, const linqt_op *opl, const linqt_op *opr,
+                      const double *states, int R, int M, int nump, double band_width, double band_center,
+                      const linqt_opts *opts, double *mu, double *E, double *sigma, double *integrand) {
+  return guarded([&] {
+    check_op(H, "H");
+    LQ_REQUIRE(states && R > 0 && M > 0, "bad argument");
+    LQ_REQUIRE(mu || (E && sigma), "nothing to compute");
+    Session *r = resolve(s);
+    const size_t sb = sizeof(double2) * (size_t)R * H->op.n;
+    const size_t mb = sizeof(double2) * (size_t)M * M;
+    const bool want_fft = E && sigma;
+    double2 *d_st = (double2 *)r->get("io_states", sb);
+    double2 *d_mu = mu ? (double2 *)r->get("io_mu", mb) : nullptr;
+    double *d_out = want_fft ? (double *)r->get("io_kubo", sizeof(double) * 3 * (size_t)nump) : nullptr;
+    LQ_CUDA(cudaMemcpyAsync(d_st, states, sb, cudaMemcpyHostToDevice, r->stream));
+    kubo_bastin_dev(r, H->op, dop(opl), dop(opr), d_st, R, M, nump, band_width, band_center, defaults(opts), d_mu,
+                    d_out);
+    if (mu) LQ_CUDA(cudaMemcpyAsync(mu, d_mu, mb, cudaMemcpyDeviceToHost, r->stream));
+    std::vector<double> h(want_fft ? 3 * (size_t)nump : 0);
+    if (want_fft)
+      LQ_CUDA(cudaMemcpyAsync(h.data(), d_out, sizeof(double) * h.size(), cudaMemcpyDeviceToHost, r->stream));
+    LQ_CUDA(cudaStreamSynchronize(r->stream));
+    if (want_fft) {
+      std::memcpy(E, h.data(), sizeof(double) * nump);
+      std::memcpy(sigma, h.data() + nump, sizeof(double) * nump);
+      if (integrand) std::memcpy(integrand, h.data() + 2 * (size_t)nump, sizeof(double) * nump);
+    }
   });
 }
 

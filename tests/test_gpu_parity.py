@@ -177,6 +177,17 @@ def test_kubo_fft(oracle_lib, honey, formula, nump):
         assert rel(integ, io) < TOL
 
 
+def test_kubo_bastin_combined_equals_separate(honey):
+    st = lattices.random_phase_states(honey["N"], 3, seed=31)
+    M, nump = 48, 256
+    mu, (E, s, integ) = lq.kubo_bastin(honey["Hg"], honey["Vg"], honey["Vg"], st, M, nump, honey["bw"], honey["bc"])
+    mu2 = lq.moments2d(honey["Hg"], honey["Vg"], honey["Vg"], st, M)
+    E2, s2, i2 = lq.kubo_fft(honey["Hg"], honey["Vg"], honey["Vg"], st, M, nump, lq.KUBO_BASTIN, honey["bw"],
+                             honey["bc"])
+    assert np.array_equal(mu, mu2)  # same kernels, same order: bitwise
+    assert np.array_equal(s, s2) and np.array_equal(E, E2) and np.array_equal(integ, i2)
+
+
 def test_dos_from_moments(oracle_lib, square):
     st = lattices.random_phase_states(square["N"], 2, seed=12)
     M = 256
