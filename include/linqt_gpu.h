@@ -149,6 +149,37 @@ int linqt_kubo_bastin_dev(linqt_session *s, const linqt_op *H, const linqt_op *o
                           const double *states_dev, int R, int M, int nump, double band_width, double band_center,
                           const linqt_opts *opts, double *mu_dev, double *out_dev /* 3*nump or NULL */);
 
+/* ---- 1D moments without device allocation ------------------------------- */
+/* No counterpart in the reference: LinQT allocates host vectors per call and has no
+ * notion of device memory.
+ *
+ * For callers that must not call cudaMalloc or cudaFree while they run.  The regular
+ * entry points draw on a per-session workspace cache, and a cache miss or resize calls
+ * cudaMalloc/cudaFree; cudaFree synchronises the whole device.  That does not suit a
+ * serving loop with a latency bound, a thread sharing the GPU with a framework whose
+ * caching allocator owns the device memory, or code that may not call the CUDA
+ * allocation API at all.
+ *
+ * Computes the same result as linqt_moments1d_dev(NULL, H, NULL, ...) with default
+ * options: FP64, identity operator, mu_dev[2*M] from the R states at states_dev (R x N
+ * complex doubles).  Everything is enqueued on cuda_stream (NULL = the legacy default
+ * stream) and the call returns without synchronising.  Scratch lives in one
+ * statically sized __device__ array of LINQT_NOALLOC_SCRATCH_BYTES that every GPU
+ * loading the library holds until exit.
+ *
+ * Limits:
+ *   - 3 Chebyshev blocks of N x Rc complex doubles (Rc = min(256, next power of two
+ *     >= R)) plus reduction buffers must fit in that array; a larger solve is
+ *     rejected with LINQT_ERR_INVALID and a message giving the size it needs.
+ *   - The first call on a device resolves the array's device address
+ *     (cudaGetSymbolAddress); make that first call before any stream capture.
+ *   - All calls share the one array, which keeps the last call's contents.  Calls
+ *     that overlap on the GPU (two streams, or two host threads) race on it and must
+ *     be serialised by the caller. */
+#define LINQT_NOALLOC_SCRATCH_BYTES (32u * 1024u * 1024u)
+int linqt_moments1d_noalloc(const linqt_op *H, const double *states_dev, int R, int M, double *mu_dev,
+                            void *cuda_stream);
+
 /* ---- reconstructions (FP64 on the device) ------------------------------- */
 /* Moments1D::ApplyJacksonKernel (src/chebyshev_moments1D.cpp:68-87) followed by the DOS of
  * spectralFunctionFromChebmom_FFTgrid (src/spectralFunctionFromChebmom_FFTgrid.cpp:35-75).

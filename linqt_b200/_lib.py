@@ -75,6 +75,7 @@ SIGNATURES = {
                                   c_double, ctypes.POINTER(Opts), P_double, P_double, P_double, P_double]),
     "linqt_kubo_bastin_dev": (c_int, [c_void_p, c_void_p, c_void_p, c_void_p, c_void_p, c_int, c_int, c_int,
                                       c_double, c_double, ctypes.POINTER(Opts), c_void_p, c_void_p]),
+    "linqt_moments1d_noalloc": (c_int, [c_void_p, c_void_p, c_int, c_int, c_void_p, c_void_p]),
     "linqt_dos_from_moments": (c_int, [c_void_p, P_double, c_int, c_int, c_double, c_double, c_double, P_double,
                                        P_double, P_int]),
     "linqt_bastin_from_moments": (c_int, [c_void_p, P_double, c_int, c_int, c_int, c_double, c_double, c_double,

@@ -208,6 +208,13 @@ def moments1d_dev(H, op, states_dev, R, M, mu_dev, opts=None, session=None):
                                      ctypes.byref(o), ctypes.c_void_p(_ptr(mu_dev))))
 
 
+def moments1d_noalloc(H, states_dev, R, M, mu_dev, stream=0):
+    """1D moments (identity operator, FP64) with no device allocation: scratch lives in a
+    fixed static device array (see linqt_moments1d_noalloc in include/linqt_gpu.h)."""
+    check(load().linqt_moments1d_noalloc(H.h, ctypes.c_void_p(_ptr(states_dev)), R, M, ctypes.c_void_p(_ptr(mu_dev)),
+                                         ctypes.c_void_p(stream)))
+
+
 def moments2d(H, opl, opr, states, M, opts=None, session=None):
     """mu[M, M] of chebyshev::CorrelationExpansionMoments (row index follows OPL)."""
     st = np.atleast_2d(_c128(states))

@@ -231,6 +231,15 @@ int jackson_cut(int M, double band_width, double broad);
 double jackson_factor(int m, int Mom);
 void jackson2d_dev(Session *s, const double2 *mu, int M0, int M1, int M0t, int M1t, double2 *out);
 
+// explicit-stream / caller-scratch launchers (spmm.cu, mu_gemm.cu) for the no-alloc entry point
+int cheb_step_grid(int sm_count, int n, int R);
+void cheb_step_scratch(cudaStream_t st, int sm_count, const DeviceOp &H, const StepArgs &a, int R,
+                       double2 *partials, unsigned *counter);
+void states_to_block_stream(cudaStream_t st, int sm_count, const double2 *states, void *block, int N, int R,
+                            int Rpad);
+void moments1d_from_dots_stream(cudaStream_t st, const double2 *dots, int steps, int M, int R, int mode,
+                                double2 *mu);
+
 // small utilities (util.cu)
 void sum_chunks(Session *s, double2 *d, int len, int nchunks);       // d[0:len] += sum_{c>0} d[c*len : ...]
 void add_into(Session *s, double2 *dst, const double2 *src, int len); // dst += src

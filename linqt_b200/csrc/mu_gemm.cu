@@ -191,6 +191,12 @@ void mu_finalize(Session *s, const double2 *mu_raw, int M, int R, double2 *mu) {
   LQ_LAUNCHED();
 }
 
+void moments1d_from_dots_stream(cudaStream_t st, const double2 *dots, int steps, int M, int R, int mode,
+                                double2 *mu) {
+  k_moments1d<<<(M + 255) / 256, 256, 0, st>>>(dots, steps, M, (double)R, mode, mu);
+  LQ_LAUNCHED();
+}
+
 void moments1d_from_dots(Session *s, const double2 *dots, int steps, int M, int R, int mode, double2 *mu) {
   k_moments1d<<<(M + 255) / 256, 256, 0, s->stream>>>(dots, steps, M, (double)R, mode, mu);
   LQ_LAUNCHED();

@@ -303,6 +303,48 @@ void spmm(Session *s, const DeviceOp &A, double2 alpha, const void *x, double2 b
     dispatch_width<double, SpmmF>(R, s, A, alpha, x, beta, y);
 }
 
+// ---------------------------------------------------------------------------
+// Launchers with an explicit stream and caller-supplied scratch (used by the
+// entry point that allocates nothing).  They launch the same kernels with the same
+// grid as cheb_step / states_to_block, so results are bitwise identical.
+// ---------------------------------------------------------------------------
+namespace {
+template <class T, int TPR, int VPT>
+struct StepScratchF {
+  static void run(cudaStream_t st, int sm_count, const DeviceOp &H, const StepArgs &a, double2 *partials,
+                  unsigned *counter) {
+    using C = typename cplx_t<T>::type;
+    const long need = ((long)H.n * TPR + kThreads - 1) / kThreads;
+    const int grid = (int)std::max(1L, std::min(need, (long)sm_count * 8));
+    const int first = a.yprev == nullptr;
+    k_step_csr<T, TPR, VPT, false><<<grid, kThreads, 0, st>>>(
+        H.n, H.d_rowptr, H.d_col, (const C *)H.d_val64, nullptr, nullptr, nullptr, (const C *)a.x,
+        (const C *)a.yprev, (C *)a.y, nullptr, (const C *)a.phi, first, a.dot_mode, partials, counter, a.dots);
+    LQ_LAUNCHED();
+  }
+};
+}  // namespace
+
+int cheb_step_grid(int sm_count, int n, int R) {
+  const int tpr = R >= 32 ? 32 : R;
+  const long need = ((long)n * tpr + kThreads - 1) / kThreads;
+  return (int)std::max(1L, std::min(need, (long)sm_count * 8));
+}
+
+void cheb_step_scratch(cudaStream_t st, int sm_count, const DeviceOp &H, const StepArgs &a, int R,
+                       double2 *partials, unsigned *counter) {
+  if (a.V) fail(LINQT_ERR_UNSUPPORTED, "cheb_step_scratch: no fused second operator");
+  dispatch_width<double, StepScratchF>(R, st, sm_count, H, a, partials, counter);
+}
+
+void states_to_block_stream(cudaStream_t st, int sm_count, const double2 *states, void *block, int N, int R,
+                            int Rpad) {
+  const long total = (long)N * Rpad;
+  const int grid = (int)std::max(1L, std::min((total + 255) / 256, (long)sm_count * 16));
+  k_states_to_block<double><<<grid, 256, 0, st>>>(states, (double2 *)block, N, R, Rpad);
+  LQ_LAUNCHED();
+}
+
 void states_to_block(Session *s, const double2 *states, void *block, int N, int R, int Rpad, bool fp32) {
   const long total = (long)N * Rpad;
   const int grid = (int)std::max(1L, std::min((total + 255) / 256, (long)s->sm_count * 16));
