@@ -68,9 +68,10 @@ typedef struct linqt_opts {
   int precision;    /* LINQT_PREC_* */
   int format;       /* LINQT_FORMAT_*: sparse format of H in the recursion */
   int block_width;  /* vector columns per recursion block (0 = all R, or the autotuned chunk) */
-  int doubling;     /* 1D only: 1 = use T_{2n} = 2T_n^2 - T_0 (identity operator only); 0 = direct <r|T_n r> */
-  int use_graphs;   /* 1 = replay the recursion as a captured CUDA graph */
-  int reserved[11];
+  int doubling;     /* 1D: 0 = doubling identities when the operator is the identity, 1 = force them, 2 = direct <r|T_n r> */
+  int use_graphs;   /* reserved (0) */
+  int step_launches; /* 1 = one kernel launch per recursion step instead of one persistent cooperative launch */
+  int reserved[10];
 } linqt_opts;
 
 /* ---- library / sessions ------------------------------------------------ */
@@ -81,6 +82,8 @@ int linqt_session_destroy(linqt_session *s);
 /* Run the session's work on an externally owned stream (e.g. torch's current stream). */
 int linqt_session_set_stream(linqt_session *s, void *cuda_stream);
 int linqt_session_get_stream(linqt_session *s, void **cuda_stream);
+/* Wait for the session's work; reports LINQT_ERR_TIMEOUT if a persistent recursion
+ * kernel's bounded grid-barrier wait gave up since the last check. */
 int linqt_session_synchronize(linqt_session *s);
 /* Release cached device workspaces. */
 int linqt_session_trim(linqt_session *s);

@@ -44,9 +44,12 @@ def _ptr(x):
     return x.data_ptr()
 
 
-def make_opts(precision=PREC_FP64, fmt=0, block_width=0, doubling=0, use_graphs=0):
+def make_opts(precision=PREC_FP64, fmt=0, block_width=0, doubling=0, step_launches=0):
+    """Solver options (linqt_opts).  doubling: 0 auto, 1 force, 2 off.  step_launches: 1 = one launch per
+    recursion step instead of the persistent cooperative kernel."""
     o = Opts()
-    o.precision, o.format, o.block_width, o.doubling, o.use_graphs = precision, fmt, block_width, doubling, use_graphs
+    o.precision, o.format, o.block_width, o.doubling, o.step_launches = (precision, fmt, block_width, doubling,
+                                                                         step_launches)
     return o
 
 

@@ -76,7 +76,8 @@ void *Session::get(const std::string &name, size_t bytes) {
                               cudaGetErrorString(e));
   }
   // counters used by the last-block reductions must start at zero
-  if (name.find("counter") != std::string::npos) LQ_CUDA(cudaMemsetAsync(p, 0, bytes, stream));
+  if (name.find("counter") != std::string::npos || name.find("barrier") != std::string::npos)
+    LQ_CUDA(cudaMemsetAsync(p, 0, bytes, stream));
   ws[name] = {p, bytes};
   return p;
 }
@@ -312,6 +313,21 @@ static void moments1d_dev(Session *s, const DeviceOp &H, const DeviceOp *op, con
     void *phi = b2;
     chunk_block(s, states, N, R, c * Rc, Rc, phi, fp32);
     launches++;
+    if (!o.step_launches) {
+      void *x0 = phi;
+      if (!doubling) {
+        if (op) {
+          spmm(s, *op, make_double2(1, 0), phi, make_double2(0, 0), b0, Rc, fp32);  // T_0 = OP phi
+          launches++;
+        } else {
+          LQ_CUDA(cudaMemcpyAsync(b0, phi, blk, cudaMemcpyDeviceToDevice, s->stream));
+        }
+        x0 = b0;
+      }
+      recur_1d(s, H, phi, x0, b1, steps, M, doubling ? 2 : 1, Rc, fp32, cd);
+      launches += 2;
+      continue;
+    }
     void *x;
     if (doubling) {
       x = phi;  // T_0 = phi
@@ -365,10 +381,20 @@ static void moments1d_dev(Session *s, const DeviceOp &H, const DeviceOp *op, con
 // Lstore/Rstore: M blocks of N x Rc (site-major) each.
 // ---------------------------------------------------------------------------
 static long lr_vectors(Session *s, const DeviceOp &H, const DeviceOp *opl, const DeviceOp *opr, void *phi, int M,
-                       int Rc, bool fp32, char *Lstore, char *Rstore, char *tmp3, int format) {
+                       int Rc, bool fp32, char *Lstore, char *Rstore, char *tmp3, int format, bool step_launches) {
   const size_t esz = fp32 ? sizeof(float2) : sizeof(double2);
   const size_t blk = esz * (size_t)H.n * Rc;
   long launches = 0;
+  if (!step_launches) {
+    // one cooperative launch advances both recursions (recur.cu)
+    if (opl)
+      spmm(s, *opl, make_double2(1, 0), phi, make_double2(0, 0), Lstore, Rc, fp32);
+    else
+      LQ_CUDA(cudaMemcpyAsync(Lstore, phi, blk, cudaMemcpyDeviceToDevice, s->stream));
+    if (!opr) LQ_CUDA(cudaMemcpyAsync(Rstore, phi, blk, cudaMemcpyDeviceToDevice, s->stream));
+    recur_lr(s, H, opr, Lstore, Rstore, phi, tmp3, M, Rc, fp32);
+    return opl ? 2 : 1;
+  }
   // ---- L side: the recursion runs in place inside the store
   if (opl) {
     spmm(s, *opl, make_double2(1, 0), phi, make_double2(0, 0), Lstore, Rc, fp32);
@@ -476,7 +502,7 @@ static void moments2d_dev(Session *s, const DeviceOp &H, const DeviceOp *opl, co
     {
       PhaseScope ph(s, PH_RECURSION);
       chunk_block(s, states, N, R, c * ch.Rc, ch.Rc, phi, false);
-      ph.launches(1 + lr_vectors(s, H, opl, opr, phi, M, ch.Rc, false, Ls, Rs, tmp, o.format));
+      ph.launches(1 + lr_vectors(s, H, opl, opr, phi, M, ch.Rc, false, Ls, Rs, tmp, o.format, o.step_launches != 0));
     }
     {
       PhaseScope ph(s, PH_CONTRACT);
@@ -515,7 +541,7 @@ static void kubo_fft_dev(Session *s, const DeviceOp &H, const DeviceOp *opl, con
     {
       PhaseScope ph(s, PH_RECURSION);
       chunk_block(s, states, N, R, c * ch.Rc, ch.Rc, phi, false);
-      ph.launches(1 + lr_vectors(s, H, opl, opr, phi, M, ch.Rc, false, Ls, Rs, tmp, o.format));
+      ph.launches(1 + lr_vectors(s, H, opl, opr, phi, M, ch.Rc, false, Ls, Rs, tmp, o.format, o.step_launches != 0));
     }
     {
       PhaseScope ph(s, PH_FFT);
@@ -577,7 +603,7 @@ static void kubo_bastin_dev(Session *s, const DeviceOp &H, const DeviceOp *opl, 
     {
       PhaseScope ph(s, PH_RECURSION);
       chunk_block(s, states, N, R, c * ch.Rc, ch.Rc, phi, false);
-      ph.launches(1 + lr_vectors(s, H, opl, opr, phi, M, ch.Rc, false, Ls, Rs, tmp, o.format));
+      ph.launches(1 + lr_vectors(s, H, opl, opr, phi, M, ch.Rc, false, Ls, Rs, tmp, o.format, o.step_launches != 0));
     }
     if (mu) {
       PhaseScope ph(s, PH_CONTRACT);
@@ -676,7 +702,11 @@ int linqt_session_get_stream(linqt_session *s, void **stream) {
 }
 
 int linqt_session_synchronize(linqt_session *s) {
-  return guarded([&] { LQ_CUDA(cudaStreamSynchronize(resolve(s)->stream)); });
+  return guarded([&] {
+    Session *r = resolve(s);
+    LQ_CUDA(cudaStreamSynchronize(r->stream));
+    check_device_errors(r);
+  });
 }
 
 int linqt_session_trim(linqt_session *s) {
@@ -869,6 +899,7 @@ int linqt_moments1d(linqt_session *s, const linqt_op *H, const linqt_op *op, con
     moments1d_dev(r, H->op, dop(op), d_st, R, M, defaults(opts), d_mu);
     LQ_CUDA(cudaMemcpyAsync(mu, d_mu, sizeof(double2) * (size_t)M, cudaMemcpyDeviceToHost, r->stream));
     LQ_CUDA(cudaStreamSynchronize(r->stream));
+    check_device_errors(r);
   });
 }
 
@@ -896,6 +927,7 @@ int linqt_moments2d(linqt_session *s, const linqt_op *H, const linqt_op *opl, co
     moments2d_dev(r, H->op, dop(opl), dop(opr), d_st, R, M, defaults(opts), d_mu);
     LQ_CUDA(cudaMemcpyAsync(mu, d_mu, mb, cudaMemcpyDeviceToHost, r->stream));
     LQ_CUDA(cudaStreamSynchronize(r->stream));
+    check_device_errors(r);
   });
 }
 
@@ -926,6 +958,7 @@ int linqt_kubo_fft(linqt_session *s, const linqt_op *H, const linqt_op *opl, con
     std::vector<double> h(3 * (size_t)nump);
     LQ_CUDA(cudaMemcpyAsync(h.data(), d_out, sizeof(double) * h.size(), cudaMemcpyDeviceToHost, r->stream));
     LQ_CUDA(cudaStreamSynchronize(r->stream));
+    check_device_errors(r);
     std::memcpy(E, h.data(), sizeof(double) * nump);
     std::memcpy(sigma, h.data() + nump, sizeof(double) * nump);
     if (integrand) std::memcpy(integrand, h.data() + 2 * (size_t)nump, sizeof(double) * nump);
@@ -965,6 +998,7 @@ int linqt_kubo_bastin(linqt_session *s, const linqt_op *H, const linqt_op *opl, 
     if (want_fft)
       LQ_CUDA(cudaMemcpyAsync(h.data(), d_out, sizeof(double) * h.size(), cudaMemcpyDeviceToHost, r->stream));
     LQ_CUDA(cudaStreamSynchronize(r->stream));
+    check_device_errors(r);
     if (want_fft) {
       std::memcpy(E, h.data(), sizeof(double) * nump);
       std::memcpy(sigma, h.data() + nump, sizeof(double) * nump);

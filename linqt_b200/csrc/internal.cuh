@@ -159,6 +159,7 @@ struct Session {
   long phase_launches[4] = {0, 0, 0, 0};
   int sm_count = 148;
   size_t hbm_budget = 0;  // 0 = no limit beyond the device
+  bool barrier_used = false;  // a persistent kernel ran since the last error check
 
   void *get(const std::string &name, size_t bytes);  // cached device buffer, >= bytes
   void trim();
@@ -239,6 +240,14 @@ void states_to_block_stream(cudaStream_t st, int sm_count, const double2 *states
                             int Rpad);
 void moments1d_from_dots_stream(cudaStream_t st, const double2 *dots, int steps, int M, int R, int mode,
                                 double2 *mu);
+
+// persistent recursions (recur.cu): one cooperative launch per recursion
+void recur_lr(Session *s, const DeviceOp &H, const DeviceOp *V, void *Lstore, void *Rstore, const void *phi,
+              void *tbuf, int M, int R, bool fp32);
+void recur_1d(Session *s, const DeviceOp &H, const void *phi, void *x0, void *b1, int steps, int M, int mode, int R,
+              bool fp32, double2 *dots);
+// after a stream synchronisation: fail with LINQT_ERR_TIMEOUT if a persistent kernel's barrier gave up
+void check_device_errors(Session *s);
 
 // small utilities (util.cu)
 void sum_chunks(Session *s, double2 *d, int len, int nchunks);       // d[0:len] += sum_{c>0} d[c*len : ...]

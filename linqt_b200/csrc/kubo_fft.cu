@@ -161,6 +161,30 @@ __global__ void k_prefactors(int M, int nump, double2 *__restrict__ pf) {
 
 constexpr int kFftThreads = 512;
 
+__device__ __forceinline__ void cp_async16(void *smem, const void *gmem) {
+  const unsigned sa = (unsigned)__cvta_generic_to_shared(smem);
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(sa), "l"(gmem));
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::); }
+__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_group 0;\n" ::); }
+
+// Issue the asynchronous copies of site l's bra_m = L[m][l] and ket_m = Rv[m][l], m < M,
+// into stage[0..M) and stage[M..2M).
+__device__ __forceinline__ void stage_site(double2 *stage, const double2 *__restrict__ L,
+                                           const double2 *__restrict__ Rv, long K, int M, long l) {
+  for (int m = threadIdx.x; m < M; m += blockDim.x) {
+    cp_async16(stage + m, L + (size_t)m * K + l);
+    cp_async16(stage + M + m, Rv + (size_t)m * K + l);
+  }
+  cp_async_commit();
+}
+
+// Shared-memory layout (double2 units):
+//   buf   NSEQ * 16 * (P + 1)   the transforms, 16 rows of P (+1 pad) per sequence
+//   tw1   16 * P                w_n^{m1 k2} at [k2 * P + m1]   (pass 1)
+//   tw2   16 * R3               w_P^{a c}   at [c * R3 + a]    (pass 2)
+//   pfs   M                     prefactors
+//   stage 2 * 2M                double-buffered bra/ket of the current and next site
 template <int R3, int NSEQ>
 __global__ void __launch_bounds__(kFftThreads)
     k_kubo_fft(const double2 *__restrict__ L, const double2 *__restrict__ Rv, long K, long chunk, int M,
@@ -171,33 +195,51 @@ __global__ void __launch_bounds__(kFftThreads)
   constexpr int SEQ = 16 * ROW; // per-sequence footprint
   constexpr int KPT = (n + kFftThreads - 1) / kFftThreads;
   extern __shared__ double2 sm[];
-  double2 *buf = sm;                    // NSEQ * SEQ
-  double2 *tw = sm + NSEQ * SEQ;        // n twiddles exp(2 pi i t / n)
-  double2 *pfs = tw + n;                // M prefactors
-  for (int t = threadIdx.x; t < n; t += blockDim.x) {
+  double2 *buf = sm;
+  double2 *tw1 = buf + NSEQ * SEQ;
+  double2 *tw2 = tw1 + 16 * P;
+  double2 *pfs = tw2 + 16 * R3;
+  double2 *stage = pfs + M;  // 2 buffers of 2M
+  const long lbeg = (long)blockIdx.x * chunk;
+  const long lend = min(K, lbeg + chunk);
+  if (lbeg < lend) stage_site(stage, L, Rv, K, M, lbeg);
+  for (int t = threadIdx.x; t < 16 * P; t += blockDim.x) {
+    const int k2 = t / P, m1 = t % P;
     double sn, cs;
-    sincospi(2.0 * t / n, &sn, &cs);
-    tw[t] = make_double2(cs, sn);
+    sincospi(2.0 * (double)(m1 * k2) / n, &sn, &cs);
+    tw1[t] = make_double2(cs, sn);
+  }
+  for (int t = threadIdx.x; t < 16 * R3; t += blockDim.x) {
+    const int c = t / R3, a = t % R3;
+    double sn, cs;
+    sincospi(2.0 * (double)(a * c) / P, &sn, &cs);
+    tw2[t] = make_double2(cs, sn);
   }
   for (int m = threadIdx.x; m < M; m += blockDim.x) pfs[m] = pf_g[m];
   double2 accp[KPT], accw[KPT];
 #pragma unroll
   for (int q = 0; q < KPT; ++q) accp[q] = accw[q] = make_double2(0, 0);
-  __syncthreads();
 
-  const long lbeg = (long)blockIdx.x * chunk;
-  const long lend = min(K, lbeg + chunk);
+  int cur = 0;
   for (long l = lbeg; l < lend; ++l) {
+    cp_async_wait_all();
+    __syncthreads();  // stage[cur] complete and visible; the previous site is fully consumed
+    const double2 *bra = stage + cur * 2 * M, *ket = bra + M;
+    if (l + 1 < lend) stage_site(stage + (cur ^ 1) * 2 * M, L, Rv, K, M, l + 1);
     // ---- pass 1: x_s[m1 + P m2], m2 < 16 -> 16-point DFT over m2, twiddle w_n^{m1 k2}
     for (int item = threadIdx.x; item < NSEQ * P; item += blockDim.x) {
       const int s = item / P, m1 = item % P;
+      const double *src = (const double *)((s & 2) ? ket : bra) + (s & 1);  // Re or Im part
+      const bool deriv = s >= 4;
       double2 v[16];
 #pragma unroll
       for (int m2 = 0; m2 < 16; ++m2) {
         const int m = m1 + P * m2;
         if (m < M) {
-          const double2 bra = __ldg(L + (size_t)m * K + l), ket = __ldg(Rv + (size_t)m * K + l);
-          v[m2] = seq_input(s, bra, ket, pfs[m], m);
+          double f = src[2 * m];
+          if (deriv) f *= (double)m;
+          const double2 pf = pfs[m];
+          v[m2] = make_double2(pf.x * f, pf.y * f);
         } else {
           v[m2] = make_double2(0, 0);
         }
@@ -209,7 +251,7 @@ __global__ void __launch_bounds__(kFftThreads)
 #pragma unroll
         for (int q2 = 0; q2 < 4; ++q2) {
           const int k2 = q1 + 4 * q2;
-          row[k2 * ROW + m1] = cmul(v[4 * q1 + q2], tw[(m1 * k2) % n]);
+          row[k2 * ROW + m1] = k2 ? cmul(v[4 * q1 + q2], tw1[k2 * P + m1]) : v[4 * q1 + q2];
         }
     }
     __syncthreads();
@@ -236,7 +278,7 @@ __global__ void __launch_bounds__(kFftThreads)
 #pragma unroll
           for (int q2 = 0; q2 < 4; ++q2) {
             const int c = q1 + 4 * q2;
-            row[c * R3 + a] = R3 == 1 ? v[4 * q1 + q2] : cmul(v[4 * q1 + q2], tw[(a * c * 16) % n]);
+            row[c * R3 + a] = R3 == 1 ? v[4 * q1 + q2] : cmul(v[4 * q1 + q2], tw2[c * R3 + a]);
           }
       }
       __syncthreads();
@@ -260,14 +302,11 @@ __global__ void __launch_bounds__(kFftThreads)
         __syncthreads();
         if (active) {
           double2 *row = buf + s * SEQ + k2 * ROW;
-          // store X[k1 = c + 16 d] at row k2, column k1 (column index < P)
 #pragma unroll
           for (int d = 0; d < R3; ++d) row[c + 16 * d] = v[d];
         }
         __syncthreads();
       }
-    } else {
-      // R3 == 1: pass 2 wrote X[k2 + 16 c] at row k2, column c already
     }
     // ---- products: X_s[k] lives at buf[s*SEQ + (k % 16)*ROW + k / 16]
 #pragma unroll
@@ -281,8 +320,9 @@ __global__ void __launch_bounds__(kFftThreads)
           greenwood_product(X, SEQ, accp[q]);
       }
     }
-    __syncthreads();
+    cur ^= 1;
   }
+  cp_async_wait_all();
   double2 *out = part + (size_t)blockIdx.x * 2 * n;
 #pragma unroll
   for (int q = 0; q < KPT; ++q) {
@@ -361,62 +401,59 @@ __global__ void k_sum_parts(const double2 *__restrict__ part, int nb, int len, d
   }
 }
 
-// rearrange_crescent_order (src/Kubo_solver_FFT_postProcess.cpp:98-116)
-__device__ void rearrange(double *x, double *tmp, int n) {
-  for (int k = 0; k < n; ++k) tmp[k] = x[k];
-  for (int k = 0; k < n / 2; ++k) {
-    x[2 * k] = tmp[k];
-    x[2 * k + 1] = tmp[n - k - 1];
-  }
-  for (int k = 0; k < n / 2; ++k) {
-    const double t = x[k];
-    x[k] = x[n - k - 1];
-    x[n - k - 1] = t;
-  }
+// Index map of rearrange_crescent_order (src/Kubo_solver_FFT_postProcess.cpp:98-116): the
+// reference interleaves x[k] and x[n-k-1] (k < n/2) and then reverses the array, so output j
+// holds y[n-1-j] with y[2k] = x[k], y[2k+1] = x[n-k-1] and, for odd n, y[n-1] = x[n-1].
+__device__ __forceinline__ int rearranged_source(int j, int n) {
+  const int i = n - 1 - j;
+  const int h = n / 2;
+  if ((i & 1) == 0 && i / 2 < h) return i / 2;
+  if ((i & 1) == 1 && (i - 1) / 2 < h) return n - (i - 1) / 2 - 1;
+  return i;
 }
 
-// Post-processing (single thread, FP64): final_data = acc / R (the running mean of
-// Kubo_solver_FFT::update_data over R states), then Bastin_postProcess
-// (src/Kubo_solver_FFT_postProcess.cpp:120-273) or Greenwood_postProcess (:279-397).
-// out = [E (nump), sigma (nump), integrand (nump)]; scratch = 3*nump doubles.
+// Post-processing: final_data = acc / R (the running mean of Kubo_solver_FFT::update_data
+// over R states), then Bastin_postProcess (src/Kubo_solver_FFT_postProcess.cpp:120-273) or
+// Greenwood_postProcess (:279-397).  out = [E (nump), sigma (nump), integrand (nump)].
+// The integrand is evaluated in parallel; the left-rectangle cumulative integral
+// (integration_linqt, :36-47) runs in index order on one thread.
 __global__ void k_kubo_post(const double2 *__restrict__ acc, double R, int nump, int formula, double N, double a,
                             double b, double *__restrict__ out, double *__restrict__ scratch) {
-  if (threadIdx.x || blockIdx.x) return;
   double *E = out, *sig = out + nump, *integ = out + 2 * nump;
-  double *Ek = scratch, *tmp = scratch + nump;
+  double *Er = scratch;  // rearranged reduced energies
   const double omega = N / (a * a);
-  for (int k = 0; k < nump; ++k) {
-    Ek[k] = cos(M_PI * (2 * k + 0.5) / nump);
-    E[k] = Ek[k];
-  }
-  rearrange(E, tmp, nump);
-  if (formula == LINQT_KUBO_BASTIN) {
-    for (int k = 0; k < nump; ++k) {
+  for (int j = threadIdx.x; j < nump; j += blockDim.x) {
+    const int k = rearranged_source(j, nump);
+    const double Ek = cos(M_PI * (2 * k + 0.5) / nump);
+    Er[j] = Ek;
+    if (formula == LINQT_KUBO_BASTIN) {
       const double pr = acc[k].x / R, wi = acc[k + nump].y / R;
-      double v = Ek[k] * pr - (sqrt(1.0 - Ek[k] * Ek[k]) * wi);
-      v *= 1.0 / pow((1.0 - Ek[k] * Ek[k]), 2.0);
+      double v = Ek * pr - (sqrt(1.0 - Ek * Ek) * wi);
+      v *= 1.0 / pow((1.0 - Ek * Ek), 2.0);
       v *= omega / (M_PI);
-      integ[k] = v;
+      integ[j] = v;
+    } else {
+      sig[j] = 2.0 * omega * (acc[k].x / R) / (1.0 - Ek * Ek) / (2 * M_PI);
+      integ[j] = 0.0;
     }
-    rearrange(integ, tmp, nump);
+  }
+  __syncthreads();
+  if (formula == LINQT_KUBO_BASTIN && threadIdx.x == 0) {
     double s = 0;
     for (int i = 0; i < nump - 1; ++i) {
-      s += integ[i] * (E[i + 1] - E[i]);
+      s += integ[i] * (Er[i + 1] - Er[i]);
       sig[i] = s;
     }
     sig[nump - 1] = 0.0;
-  } else {
-    for (int k = 0; k < nump; ++k) sig[k] = 2.0 * omega * (acc[k].x / R) / (1.0 - Ek[k] * Ek[k]) / (2 * M_PI);
-    rearrange(sig, tmp, nump);
-    for (int k = 0; k < nump; ++k) integ[k] = 0.0;
   }
-  for (int k = 0; k < nump; ++k) E[k] = a * E[k] - b;
+  __syncthreads();
+  for (int j = threadIdx.x; j < nump; j += blockDim.x) E[j] = a * Er[j] - b;
 }
 
 template <int R3, int NSEQ>
 void launch_fft(Session *s, const double2 *L, const double2 *Rv, long K, int M, const double2 *pf, double2 *acc) {
   constexpr int n = 256 * R3;
-  const size_t smem = sizeof(double2) * ((size_t)NSEQ * 16 * (16 * R3 + 1) + n + M);
+  const size_t smem = sizeof(double2) * ((size_t)NSEQ * 16 * (16 * R3 + 1) + 16 * 16 * R3 + 16 * R3 + 5 * (size_t)M);
   if (smem > 227 * 1024) fail(LINQT_ERR_UNSUPPORTED, "kubo_fft: nump too large for the shared-memory FFT");
   LQ_CUDA(cudaFuncSetAttribute(k_kubo_fft<R3, NSEQ>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
   const int nb = (int)std::max(1L, std::min(K, (long)s->sm_count));
@@ -475,8 +512,8 @@ void kubo_fft_sites(Session *s, const void *Lv, const void *Rvv, long nsites, in
 void kubo_postprocess(Session *s, const double2 *acc, int R, int nump, int formula, int N, double band_width,
                       double band_center, double *out) {
   double *scratch = (double *)s->get("kubo_post", sizeof(double) * 3 * (size_t)nump);
-  k_kubo_post<<<1, 32, 0, s->stream>>>(acc, (double)R, nump, formula, (double)N, band_width / 2.0, band_center, out,
-                                       scratch);
+  k_kubo_post<<<1, 1024, 0, s->stream>>>(acc, (double)R, nump, formula, (double)N, band_width / 2.0, band_center,
+                                         out, scratch);
   LQ_LAUNCHED();
 }
 

@@ -6,10 +6,10 @@
 // Both operands are "K-major": moment m's block T_m is N*R contiguous complex
 // numbers, so K = N*R and the contraction also sums over the R random vectors.
 //
-// FP64 path: CUDA-core DFMA with 64x64 complex output tiles per CTA, 4x4 complex
-// outputs per thread, cp.async double-buffered 16-deep K slices in shared memory,
-// split-K over the long K axis with a fixed-order FP64 reduction (deterministic).
-// (B200 has no FP64 tcgen05 kind; its FP64 tensor rate equals the DFMA rate.)
+// FP64 path: FP64 tensor-core MMA (mma.sync m8n8k4 f64; there is no FP64 tcgen05 kind)
+// on 64x64 complex output tiles per CTA (8 warps of 32x16), cp.async double-buffered
+// 16-deep K slices in padded shared memory (conflict-free fragment loads), split-K over
+// the long K axis with a fixed-order FP64 reduction (deterministic).
 #include "internal.cuh"
 
 namespace linqt {
@@ -45,20 +45,33 @@ __device__ __forceinline__ void load_tile(double2 (*sm)[LDS], const double2 *__r
   }
 }
 
-__global__ void __launch_bounds__(256) k_zgemm_cn_f64(const double2 *__restrict__ L, const double2 *__restrict__ Rv,
-                                                      int MA, int MB, long K, long kchunk, double2 *__restrict__ part) {
+// D += A * B on an 8x8x4 FP64 tensor-core tile (mma.sync m8n8k4 f64).  Fragments:
+// a = A[lane/4][lane%4], b = B[k = lane%4][n = lane/4], d = {D[lane/4][2(lane%4)], D[lane/4][2(lane%4)+1]}.
+__device__ __forceinline__ void dmma(double &d0, double &d1, double a, double b) {
+  asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0,%1}, {%2}, {%3}, {%0,%1};\n"
+               : "+d"(d0), "+d"(d1)
+               : "d"(a), "d"(b));
+}
+
+// 64x64 complex output tile per CTA, 8 warps as 2 (rows) x 4 (cols), 32x16 complex per warp
+// = 4 x 2 tiles of 8x8; conj(A) B = (Ar Br + Ai Bi) + i (Ar Bi - Ai Br): four real DMMAs per tile.
+__global__ void __launch_bounds__(256, 2) k_zgemm_cn_f64(const double2 *__restrict__ L, const double2 *__restrict__ Rv,
+                                                         int MA, int MB, long K, long kchunk,
+                                                         double2 *__restrict__ part) {
   extern __shared__ double2 smem[];
   double2(*As)[BM][LDS] = reinterpret_cast<double2(*)[BM][LDS]>(smem);
   double2(*Bs)[BN][LDS] = reinterpret_cast<double2(*)[BN][LDS]>(smem + 2 * BM * LDS);
-  const int tx = threadIdx.x & 15, ty = threadIdx.x >> 4;
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int wm = warp >> 2, wn = warp & 3;
+  const int fr = lane >> 2, fk = lane & 3;
   const int m0 = blockIdx.y * BM, m1 = blockIdx.x * BN;
   const long kbeg = (long)blockIdx.z * kchunk;
   const long kend = min(K, kbeg + kchunk);
-  double2 acc[4][4];
+  double cre[4][2][2], cim[4][2][2];
 #pragma unroll
   for (int i = 0; i < 4; ++i)
 #pragma unroll
-    for (int j = 0; j < 4; ++j) acc[i][j] = make_double2(0, 0);
+    for (int j = 0; j < 2; ++j) cre[i][j][0] = cre[i][j][1] = cim[i][j][0] = cim[i][j][1] = 0.0;
   if (kbeg < kend) {
     const int nk = (int)((kend - kbeg + BK - 1) / BK);
     load_tile(As[0], L, MA, K, m0, kbeg, kend);
@@ -74,16 +87,30 @@ __global__ void __launch_bounds__(256) k_zgemm_cn_f64(const double2 *__restrict_
       cp_async_wait<1>();
       __syncthreads();
 #pragma unroll
-      for (int kk = 0; kk < BK; ++kk) {
-        double2 a[4], b[4];
+      for (int ks = 0; ks < BK / 4; ++ks) {
+        double ar[4], ai[4], br[2], bi[2];
 #pragma unroll
-        for (int i = 0; i < 4; ++i) a[i] = As[cur][ty + 16 * i][kk];
+        for (int i = 0; i < 4; ++i) {
+          const double2 a = As[cur][wm * 32 + i * 8 + fr][ks * 4 + fk];
+          ar[i] = a.x;
+          ai[i] = -a.y;  // conj(A)
+        }
 #pragma unroll
-        for (int j = 0; j < 4; ++j) b[j] = Bs[cur][tx + 16 * j][kk];
+        for (int j = 0; j < 2; ++j) {
+          const double2 b = Bs[cur][wn * 16 + j * 8 + fr][ks * 4 + fk];
+          br[j] = b.x;
+          bi[j] = b.y;
+        }
 #pragma unroll
         for (int i = 0; i < 4; ++i)
 #pragma unroll
-          for (int j = 0; j < 4; ++j) acc[i][j] = cfma_conj(a[i], b[j], acc[i][j]);
+          for (int j = 0; j < 2; ++j) {
+            // (ar + i ai)(br + i bi) with ai = -Im(A): re = ar br - ai bi, im = ar bi + ai br
+            dmma(cre[i][j][0], cre[i][j][1], ar[i], br[j]);
+            dmma(cre[i][j][0], cre[i][j][1], -ai[i], bi[j]);
+            dmma(cim[i][j][0], cim[i][j][1], ar[i], bi[j]);
+            dmma(cim[i][j][0], cim[i][j][1], ai[i], br[j]);
+          }
       }
       __syncthreads();
     }
@@ -92,13 +119,15 @@ __global__ void __launch_bounds__(256) k_zgemm_cn_f64(const double2 *__restrict_
   double2 *out = part + (size_t)blockIdx.z * MA * MB;
 #pragma unroll
   for (int i = 0; i < 4; ++i) {
-    const int r = m0 + ty + 16 * i;
+    const int r = m0 + wm * 32 + i * 8 + fr;
     if (r >= MA) continue;
 #pragma unroll
-    for (int j = 0; j < 4; ++j) {
-      const int c = m1 + tx + 16 * j;
-      if (c < MB) out[(size_t)r * MB + c] = acc[i][j];
-    }
+    for (int j = 0; j < 2; ++j)
+#pragma unroll
+      for (int h = 0; h < 2; ++h) {
+        const int c = m1 + wn * 16 + j * 8 + 2 * fk + h;
+        if (c < MB) out[(size_t)r * MB + c] = make_double2(cre[i][j][h], cim[i][j][h]);
+      }
   }
 }
 

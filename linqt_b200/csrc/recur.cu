@@ -1,0 +1,392 @@
+// Persistent recursion kernels: a whole Chebyshev recursion in one cooperative launch.
+//
+// One launch per recursion step (spmm.cu) costs a launch gap and a cold start per step.
+// At LinQT's sizes a step is 1-10 us of memory traffic, so the gaps are a large part of
+// it.  Here every CTA owns a fixed contiguous range of rows and loops over the steps.
+// Between steps the CTAs meet at a grid barrier with a bounded spin: after
+// kSpinLimit polls a CTA sets the error flag and the kernel returns, so a bad launch
+// cannot hang the GPU.  The host reports LINQT_ERR_TIMEOUT.
+//
+// Step semantics are those of spmm.cu (Moments::Iterate, src/chebyshev_moments.cpp:157-162;
+// Vectors::IterateAll / Multiply, src/chebyshev_vectors.cpp:4-51).  k_recur_lr advances the
+// L recursion (in place inside its store) and the R recursion (rotating blocks, V*T_m into
+// its store) together.  They share the row's H loads.  k_recur_1d runs the 1D moment
+// recursion with the dot products of every step written as per-CTA partials, reduced
+// afterwards in a fixed order.
+//
+// Vectors written in one step are read by other CTAs in the next, so vector loads use
+// ld.global.cg (L2, bypassing the non-coherent L1); the operators use the read-only path.
+#include "internal.cuh"
+
+namespace linqt {
+
+namespace {
+
+constexpr int kThreads = 256;
+constexpr long kSpinLimit = 1L << 24;  // polls of ~0.1 us: well above any step, far below a hang
+
+struct Barrier {
+  unsigned count;
+  unsigned gen;
+  int err;
+  int pad;
+};
+
+template <class C>
+__device__ __forceinline__ C ldv(const C *p) {
+  return __ldcg(p);
+}
+
+__device__ __forceinline__ double2 zero2(double2) { return make_double2(0, 0); }
+__device__ __forceinline__ float2 zero2(float2) { return make_float2(0, 0); }
+
+// Grid barrier (all CTAs co-resident: cooperative launch).  Returns false if the wait gave up.
+__device__ bool grid_barrier(Barrier *bar, unsigned nblocks) {
+  __shared__ int ok;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    ok = 1;
+    volatile unsigned *vgen = &bar->gen;
+    const unsigned g = *vgen;
+    __threadfence();
+    const unsigned arrived = atomicAdd(&bar->count, 1u);
+    if (arrived == nblocks - 1) {
+      bar->count = 0;
+      __threadfence();
+      atomicAdd(&bar->gen, 1u);
+    } else {
+      long spins = 0;
+      while (*vgen == g) {
+        if (*(volatile int *)&bar->err) {
+          ok = 0;
+          break;
+        }
+        if (++spins > kSpinLimit) {
+          atomicExch(&bar->err, 1);
+          ok = 0;
+          break;
+        }
+        __nanosleep(64);
+      }
+    }
+    __threadfence();
+  }
+  __syncthreads();
+  return ok != 0;
+}
+
+__device__ __forceinline__ double2 shfl_down2(double2 v, int o) {
+  v.x = __shfl_down_sync(0xffffffffu, v.x, o);
+  v.y = __shfl_down_sync(0xffffffffu, v.y, o);
+  return v;
+}
+
+// block sums of (d0, d1), valid in thread 0
+__device__ void block_sum2(double2 &d0, double2 &d1) {
+  __shared__ double2 sh[2][kThreads / 32];
+  for (int o = 16; o > 0; o >>= 1) {
+    d0 = cadd(d0, shfl_down2(d0, o));
+    d1 = cadd(d1, shfl_down2(d1, o));
+  }
+  const int w = threadIdx.x >> 5, l = threadIdx.x & 31;
+  if (l == 0) {
+    sh[0][w] = d0;
+    sh[1][w] = d1;
+  }
+  __syncthreads();
+  if (w == 0) {
+    d0 = l < kThreads / 32 ? sh[0][l] : make_double2(0, 0);
+    d1 = l < kThreads / 32 ? sh[1][l] : make_double2(0, 0);
+    for (int o = 16; o > 0; o >>= 1) {
+      d0 = cadd(d0, shfl_down2(d0, o));
+      d1 = cadd(d1, shfl_down2(d1, o));
+    }
+  }
+  __syncthreads();
+}
+
+// ---------------------------------------------------------------------------
+// L and R recursions of CorrelationExpansionMoments / Kubo_solver_FFT.
+//   L: Lst[0] given (OPL phi); Lst[m+1] = 2 H Lst[m] - Lst[m-1] (Lst[1] = H Lst[0]), m+1 < M.
+//   R (HAS_V): T_0 = phi, T_{m+1} = tb[m % 3]; Rst[m] = V T_m for m < M.
+//   R (!HAS_V): Rst[0] given (phi); in place like L.
+// ---------------------------------------------------------------------------
+template <class T, int TPR, int VPT, bool HAS_V>
+__global__ void __launch_bounds__(kThreads)
+    k_recur_lr(int n, const int *__restrict__ rp, const int *__restrict__ ci,
+               const typename cplx_t<T>::type *__restrict__ hv, const int *__restrict__ vrp,
+               const int *__restrict__ vci, const typename cplx_t<T>::type *__restrict__ vv,
+               typename cplx_t<T>::type *Lst, typename cplx_t<T>::type *Rst, const typename cplx_t<T>::type *phi,
+               typename cplx_t<T>::type *tb, int M, size_t blk, Barrier *bar) {
+  using C = typename cplx_t<T>::type;
+  constexpr int R = TPR * VPT;
+  const int lane = threadIdx.x % TPR;
+  constexpr int gpb = kThreads / TPR;
+  const int per = (n + gridDim.x - 1) / gridDim.x;
+  const int r0 = blockIdx.x * per, r1 = min(n, r0 + per);
+  for (int m = 0; m < M; ++m) {
+    const bool doL = m + 1 < M;
+    const C *xL = Lst + (size_t)m * blk;
+    const C *pL = m ? Lst + (size_t)(m - 1) * blk : nullptr;
+    C *yL = Lst + (size_t)(m + 1) * blk;
+    const C *xR, *pR;
+    C *yR;
+    if (HAS_V) {
+      xR = m == 0 ? phi : tb + (size_t)((m - 1) % 3) * blk;
+      pR = m == 0 ? nullptr : (m == 1 ? phi : tb + (size_t)((m - 2) % 3) * blk);
+      yR = doL ? tb + (size_t)(m % 3) * blk : nullptr;
+    } else {
+      xR = Rst + (size_t)m * blk;
+      pR = m ? Rst + (size_t)(m - 1) * blk : nullptr;
+      yR = doL ? Rst + (size_t)(m + 1) * blk : nullptr;
+    }
+    for (int row = r0 + threadIdx.x / TPR; row < r1; row += gpb) {
+      C aL[VPT], aR[VPT];
+#pragma unroll
+      for (int u = 0; u < VPT; ++u) aL[u] = aR[u] = zero2(C());
+      const int b = rp[row], e = rp[row + 1];
+#pragma unroll 4
+      for (int k = b; k < e; ++k) {
+        const int j = __ldg(ci + k);
+        const C h = __ldg(hv + k);
+        const size_t off = (size_t)j * R + lane;
+#pragma unroll
+        for (int u = 0; u < VPT; ++u) {
+          if (doL) aL[u] = cfma(h, ldv(xL + off + u * TPR), aL[u]);
+          aR[u] = cfma(h, ldv(xR + off + u * TPR), aR[u]);
+        }
+      }
+      const size_t base = (size_t)row * R + lane;
+      if (HAS_V) {
+        C aV[VPT];
+#pragma unroll
+        for (int u = 0; u < VPT; ++u) aV[u] = zero2(C());
+        const int vb = vrp[row], ve = vrp[row + 1];
+#pragma unroll 4
+        for (int k = vb; k < ve; ++k) {
+          const int j = __ldg(vci + k);
+          const C h = __ldg(vv + k);
+          const size_t off = (size_t)j * R + lane;
+#pragma unroll
+          for (int u = 0; u < VPT; ++u) aV[u] = cfma(h, ldv(xR + off + u * TPR), aV[u]);
+        }
+        C *vo = Rst + (size_t)m * blk;
+#pragma unroll
+        for (int u = 0; u < VPT; ++u) vo[base + u * TPR] = aV[u];
+      }
+#pragma unroll
+      for (int u = 0; u < VPT; ++u) {
+        const size_t idx = base + u * TPR;
+        if (doL) {
+          C y = aL[u];
+          if (pL) {
+            const C p = ldv(pL + idx);
+            y.x = 2 * y.x - p.x;
+            y.y = 2 * y.y - p.y;
+          }
+          yL[idx] = y;
+        }
+        if (yR) {
+          C y = aR[u];
+          if (pR) {
+            const C p = ldv(pR + idx);
+            y.x = 2 * y.x - p.x;
+            y.y = 2 * y.y - p.y;
+          }
+          yR[idx] = y;
+        }
+      }
+    }
+    if (m + 1 < M && !grid_barrier(bar, gridDim.x)) return;
+  }
+}
+
+// ---------------------------------------------------------------------------
+// 1D moments (chebyshev::SpectralMoments, src/chebyshev_solver.cpp:176-199).
+//   mode 1 (direct):   x_0 = T_0 in b0; partial[s] = <phi|T_s>.
+//   mode 2 (doubling): x_0 = phi;      partial[s] = (<T_s|T_s>, <T_{s+1}|T_s>).
+// The recursion runs in place: T_{s+1} overwrites T_{s-1}; T_1 goes to b1.
+// partials: [steps][grid][2] per-CTA sums.
+// ---------------------------------------------------------------------------
+template <class T, int TPR, int VPT>
+__global__ void __launch_bounds__(kThreads)
+    k_recur_1d(int n, const int *__restrict__ rp, const int *__restrict__ ci,
+               const typename cplx_t<T>::type *__restrict__ hv, const typename cplx_t<T>::type *phi,
+               typename cplx_t<T>::type *x0, typename cplx_t<T>::type *b1, int steps, int M, int mode,
+               double2 *__restrict__ partials, Barrier *bar) {
+  using C = typename cplx_t<T>::type;
+  constexpr int R = TPR * VPT;
+  const int lane = threadIdx.x % TPR;
+  constexpr int gpb = kThreads / TPR;
+  const int per = (n + gridDim.x - 1) / gridDim.x;
+  const int r0 = blockIdx.x * per, r1 = min(n, r0 + per);
+  C *prev = nullptr, *cur = x0;
+  for (int s = 0; s < steps; ++s) {
+    const bool need_y = mode == 2 ? (2 * s + 1 < M) : (s + 1 < M);
+    C *y = need_y ? (prev ? prev : b1) : nullptr;
+    double2 d0 = make_double2(0, 0), d1 = make_double2(0, 0);
+    for (int row = r0 + threadIdx.x / TPR; row < r1; row += gpb) {
+      C acc[VPT];
+#pragma unroll
+      for (int u = 0; u < VPT; ++u) acc[u] = zero2(C());
+      const int b = rp[row], e = rp[row + 1];
+#pragma unroll 4
+      for (int k = b; k < e; ++k) {
+        const int j = __ldg(ci + k);
+        const C h = __ldg(hv + k);
+        const C *xr = cur + (size_t)j * R + lane;
+#pragma unroll
+        for (int u = 0; u < VPT; ++u) acc[u] = cfma(h, ldv(xr + u * TPR), acc[u]);
+      }
+      const size_t base = (size_t)row * R + lane;
+#pragma unroll
+      for (int u = 0; u < VPT; ++u) {
+        const size_t idx = base + u * TPR;
+        C yn = acc[u];
+        if (prev) {
+          const C p = ldv(prev + idx);
+          yn.x = 2 * yn.x - p.x;
+          yn.y = 2 * yn.y - p.y;
+        }
+        if (y) y[idx] = yn;
+        const double2 xi = to_d2(ldv(cur + idx));
+        if (mode == 1) {
+          d0 = cfma_conj(to_d2(ldv(phi + idx)), xi, d0);
+        } else {
+          d0 = cfma_conj(xi, xi, d0);
+          d1 = cfma_conj(to_d2(yn), xi, d1);
+        }
+      }
+    }
+    block_sum2(d0, d1);
+    if (threadIdx.x == 0) {
+      partials[((size_t)s * gridDim.x + blockIdx.x) * 2] = d0;
+      partials[((size_t)s * gridDim.x + blockIdx.x) * 2 + 1] = d1;
+    }
+    if (!need_y) break;
+    if (!grid_barrier(bar, gridDim.x)) return;
+    prev = cur;
+    cur = y;
+  }
+}
+
+// dots[2s + i] = sum_b partials[s][b][i]  (fixed order)
+__global__ void k_reduce_step_partials(const double2 *__restrict__ partials, int steps, int nb,
+                                       double2 *__restrict__ dots) {
+  for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < 2 * steps; t += gridDim.x * blockDim.x) {
+    const int s = t >> 1, i = t & 1;
+    double2 acc = make_double2(0, 0);
+    for (int b = 0; b < nb; ++b) acc = cadd(acc, partials[((size_t)s * nb + b) * 2 + i]);
+    dots[t] = acc;
+  }
+}
+
+int coop_grid(const void *func, int sm_count, int n_rows, int tpr) {
+  int per_sm = 0;
+  LQ_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, func, kThreads, 0));
+  if (per_sm <= 0) fail(LINQT_ERR_UNSUPPORTED, "persistent recursion: kernel does not fit on an SM");
+  const long need = ((long)n_rows * tpr + kThreads - 1) / kThreads;
+  return (int)std::max(1L, std::min((long)per_sm * sm_count, need));
+}
+
+template <class T, int TPR, int VPT>
+struct LRF {
+  static void run(Session *s, const DeviceOp &H, const DeviceOp *V, void *Lst, void *Rst, const void *phi, void *tb,
+                  int M, size_t blk, Barrier *bar) {
+    using C = typename cplx_t<T>::type;
+    const bool fp32 = sizeof(T) == 4;
+    const C *hv = fp32 ? (const C *)H.d_val32 : (const C *)H.d_val64;
+    const int *vrp = V ? V->d_rowptr : nullptr, *vci = V ? V->d_col : nullptr;
+    const C *vv = V ? (fp32 ? (const C *)V->d_val32 : (const C *)V->d_val64) : nullptr;
+    int n = H.n;
+    C *L = (C *)Lst, *Rs = (C *)Rst, *tbuf = (C *)tb;
+    const C *ph = (const C *)phi;
+    void *args[] = {&n, (void *)&H.d_rowptr, (void *)&H.d_col, (void *)&hv, (void *)&vrp, (void *)&vci, (void *)&vv,
+                    &L, &Rs, (void *)&ph, &tbuf, &M, &blk, &bar};
+    const void *f = V ? (const void *)k_recur_lr<T, TPR, VPT, true> : (const void *)k_recur_lr<T, TPR, VPT, false>;
+    const int grid = coop_grid(f, s->sm_count, n, TPR);
+    LQ_CUDA(cudaLaunchCooperativeKernel(f, dim3(grid), dim3(kThreads), args, 0, s->stream));
+  }
+};
+
+template <class T, int TPR, int VPT>
+struct OneDF {
+  static void run(Session *s, const DeviceOp &H, const void *phi, void *x0, void *b1, int steps, int M, int mode,
+                  double2 *dots, Barrier *bar) {
+    using C = typename cplx_t<T>::type;
+    const bool fp32 = sizeof(T) == 4;
+    const C *hv = fp32 ? (const C *)H.d_val32 : (const C *)H.d_val64;
+    const void *f = (const void *)k_recur_1d<T, TPR, VPT>;
+    const int grid = coop_grid(f, s->sm_count, H.n, TPR);
+    double2 *partials = (double2 *)s->get("rec1d_part", sizeof(double2) * 2 * (size_t)steps * grid);
+    int n = H.n;
+    const C *ph = (const C *)phi;
+    C *xx = (C *)x0, *bb = (C *)b1;
+    void *args[] = {&n, (void *)&H.d_rowptr, (void *)&H.d_col, (void *)&hv, (void *)&ph, &xx, &bb, &steps, &M, &mode,
+                    &partials, &bar};
+    LQ_CUDA(cudaLaunchCooperativeKernel(f, dim3(grid), dim3(kThreads), args, 0, s->stream));
+    k_reduce_step_partials<<<(2 * steps + 255) / 256, 256, 0, s->stream>>>(partials, steps, grid, dots);
+    LQ_LAUNCHED();
+  }
+};
+
+template <class T, template <class, int, int> class F, class... Args>
+void dispatch(int R, Args &&...args) {
+  switch (R) {
+    case 1: return F<T, 1, 1>::run(args...);
+    case 2: return F<T, 2, 1>::run(args...);
+    case 4: return F<T, 4, 1>::run(args...);
+    case 8: return F<T, 8, 1>::run(args...);
+    case 16: return F<T, 16, 1>::run(args...);
+    case 32: return F<T, 32, 1>::run(args...);
+    case 64: return F<T, 32, 2>::run(args...);
+    case 128: return F<T, 32, 4>::run(args...);
+    case 256: return F<T, 32, 8>::run(args...);
+    default: fail(LINQT_ERR_UNSUPPORTED, "block width must be a power of two <= 256");
+  }
+}
+
+// The barrier's count/generation restart at zero for every launch; its error flag is
+// sticky until check_device_errors reads it.
+Barrier *barrier_for(Session *s) {
+  Barrier *bar = (Barrier *)s->get("rec_barrier", sizeof(Barrier));
+  LQ_CUDA(cudaMemsetAsync(bar, 0, 2 * sizeof(unsigned), s->stream));
+  s->barrier_used = true;
+  return bar;
+}
+
+}  // namespace
+
+void recur_lr(Session *s, const DeviceOp &H, const DeviceOp *V, void *Lstore, void *Rstore, const void *phi,
+              void *tbuf, int M, int R, bool fp32) {
+  const size_t blk = (size_t)H.n * R;
+  Barrier *bar = barrier_for(s);
+  if (fp32)
+    dispatch<float, LRF>(R, s, H, V, Lstore, Rstore, phi, tbuf, M, blk, bar);
+  else
+    dispatch<double, LRF>(R, s, H, V, Lstore, Rstore, phi, tbuf, M, blk, bar);
+  LQ_LAUNCHED();
+}
+
+void recur_1d(Session *s, const DeviceOp &H, const void *phi, void *x0, void *b1, int steps, int M, int mode, int R,
+              bool fp32, double2 *dots) {
+  Barrier *bar = barrier_for(s);
+  if (fp32)
+    dispatch<float, OneDF>(R, s, H, phi, x0, b1, steps, M, mode, dots, bar);
+  else
+    dispatch<double, OneDF>(R, s, H, phi, x0, b1, steps, M, mode, dots, bar);
+}
+
+void check_device_errors(Session *s) {
+  if (!s->barrier_used) return;
+  Barrier *bar = (Barrier *)s->get("rec_barrier", sizeof(Barrier));
+  int err = 0;
+  LQ_CUDA(cudaMemcpy(&err, &bar->err, sizeof(int), cudaMemcpyDeviceToHost));
+  s->barrier_used = false;
+  if (err) {
+    LQ_CUDA(cudaMemset(&bar->err, 0, sizeof(int)));
+    fail(LINQT_ERR_TIMEOUT, "persistent recursion: a grid barrier wait expired; results of the solve are invalid");
+  }
+}
+
+}  // namespace linqt

@@ -93,21 +93,23 @@ def test_spectral_bounds(honey):
     assert -1.0 < lo < 0 < hi < 1.0
 
 
-@pytest.mark.parametrize("R", [1, 3])
+@pytest.mark.parametrize("R", [1, 3, 40])
 @pytest.mark.parametrize("doubling", [0, 2])
-def test_moments1d_identity(oracle_lib, square, R, doubling):
+@pytest.mark.parametrize("step_launches", [0, 1])
+def test_moments1d_identity(oracle_lib, square, R, doubling, step_launches):
     st = lattices.random_phase_states(square["N"], R, seed=12)
     M = 200
-    got = lq.moments1d(square["Hg"], None, st, M, opts=lq.make_opts(doubling=doubling))
+    got = lq.moments1d(square["Hg"], None, st, M, opts=lq.make_opts(doubling=doubling, step_launches=step_launches))
     want = oracle_lib.moments1d(square["Ho"], None, st, M)
     assert rel(got, want) < TOL
     assert abs(got[0] - 1.0) < 1e-12  # normalised states: mu_0 = 1
 
 
-def test_moments1d_with_operator(oracle_lib, honey):
+@pytest.mark.parametrize("step_launches", [0, 1])
+def test_moments1d_with_operator(oracle_lib, honey, step_launches):
     st = lattices.random_phase_states(honey["N"], 2, seed=7)
     M = 96
-    got = lq.moments1d(honey["Hg"], honey["Vg"], st, M)
+    got = lq.moments1d(honey["Hg"], honey["Vg"], st, M, opts=lq.make_opts(step_launches=step_launches))
     want = oracle_lib.moments1d(honey["Ho"], honey["Vo"], st, M)
     assert rel(got, want) < TOL
 
@@ -120,19 +122,21 @@ def test_moments1d_default_state_odd_M(oracle_lib, square):
     assert rel(got, want) < TOL
 
 
-@pytest.mark.parametrize("R,M", [(1, 40), (3, 64), (5, 33)])
-def test_moments2d_velocity(oracle_lib, honey, R, M):
+@pytest.mark.parametrize("R,M", [(1, 40), (3, 64), (5, 33), (64, 16)])
+@pytest.mark.parametrize("step_launches", [0, 1])
+def test_moments2d_velocity(oracle_lib, honey, R, M, step_launches):
     st = lattices.random_phase_states(honey["N"], R, seed=22)
-    got = lq.moments2d(honey["Hg"], honey["Vg"], honey["Vg"], st, M)
+    got = lq.moments2d(honey["Hg"], honey["Vg"], honey["Vg"], st, M, opts=lq.make_opts(step_launches=step_launches))
     want = oracle_lib.moments2d(honey["Ho"], honey["Vo"], honey["Vo"], st, M)
     assert rel(got, want) < TOL
     assert np.abs(got - got.conj().T).max() < 1e-14 * np.abs(got).max()
 
 
-def test_moments2d_identity_operators(oracle_lib, honey):
+@pytest.mark.parametrize("step_launches", [0, 1])
+def test_moments2d_identity_operators(oracle_lib, honey, step_launches):
     st = lattices.random_phase_states(honey["N"], 2, seed=3)
     M = 48
-    got = lq.moments2d(honey["Hg"], None, None, st, M)
+    got = lq.moments2d(honey["Hg"], None, None, st, M, opts=lq.make_opts(step_launches=step_launches))
     want = oracle_lib.moments2d(honey["Ho"], None, None, st, M)
     assert rel(got, want) < TOL
 
