@@ -198,7 +198,8 @@ def main():
     ap.add_argument("--steps", type=int, default=10)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="linqt", choices=["linqt", "reference"])
-    ap.add_argument("--precision", default="fp64", choices=["fp64", "mixed"])
+    ap.add_argument("--precision", default="fp64", choices=["fp64", "mixed", "fp32"])
+    ap.add_argument("--no-compare", action="store_true", help="skip the mixed-vs-FP64 accuracy run")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     # size overrides, for profiling captures on a smaller case of the same kernels
     ap.add_argument("--lx", type=int, default=None)
@@ -243,7 +244,7 @@ def main():
     Hg.rescale_to_chebyshev(bw, bc)
     Vg = lq.Operator.from_csr(N, *V, session=sess)
     assert Hg.nnz == nnz
-    prec = lq.PREC_FP64 if args.precision == "fp64" else lq.PREC_MIXED
+    prec = {"fp64": lq.PREC_FP64, "mixed": lq.PREC_MIXED, "fp32": lq.PREC_FP32}[args.precision]
     opts = lq.make_opts(precision=prec)
 
     st_dev = torch.from_numpy(st.view(np.float64).copy()).cuda()
@@ -342,6 +343,55 @@ def main():
     for k in phases:
         phases[k]["ms"] = round(phases[k]["ms"], 4)
 
+    # ---- the other precision on the same inputs: throughput and accuracy against FP64
+    other = None
+    if not args.no_compare:
+        other_prec = lq.PREC_MIXED if prec == lq.PREC_FP64 else lq.PREC_FP64
+        oopts = lq.make_opts(precision=other_prec)
+        mu_o = torch.zeros_like(mu_dev)
+        out_o = torch.zeros_like(out_dev)
+
+        def solve_other():
+            lq.kubo_bastin_dev(Hg, Vg, Vg, st_dev, R, M, nump, bw, bc, mu_o, out_o, opts=oopts, session=sess)
+
+        for _ in range(args.warmup):
+            solve_other()
+        torch.cuda.synchronize()
+        sess.enable_timing(True)
+        sess.phase_times(reset=True)
+        barrier()
+        torch.cuda.synchronize()
+        f0, f1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        f0.record(stream)
+        for _ in range(args.steps):
+            solve_other()
+        f1.record(stream)
+        torch.cuda.synchronize()
+        barrier()
+        o_ms = max_over_ranks(f0.elapsed_time(f1) / args.steps)
+        o_phase, o_launch = sess.phase_times(reset=True)
+        sess.enable_timing(False)
+        solve_dev()
+        torch.cuda.synchronize()
+        mu64 = (mu_dev if prec == lq.PREC_FP64 else mu_o).cpu().numpy().view(np.complex128)
+        mulo = (mu_o if prec == lq.PREC_FP64 else mu_dev).cpu().numpy().view(np.complex128)
+        s64 = (out_dev if prec == lq.PREC_FP64 else out_o).cpu().numpy()[nump:2 * nump]
+        slo = (out_o if prec == lq.PREC_FP64 else out_dev).cpu().numpy()[nump:2 * nump]
+        lo_i, hi_i = int(0.05 * nump), int(0.95 * nump)  # interior 90 % of the energy window
+        err_sigma = float(np.abs(slo - s64)[lo_i:hi_i].max() / np.abs(s64[lo_i:hi_i]).max())
+        err_mu = float(np.abs(mulo - mu64).max() / np.abs(mu64).max())
+        name = "mixed" if other_prec == lq.PREC_MIXED else "fp64"
+        other = {"precision": name, "value": world * units / (o_ms * 1e-3), "ms_per_step": o_ms,
+                 "phases_ms": {k: round(v / args.steps, 4) for k, v in zip(("recursion", "contraction", "fft", "other"),
+                                                                           o_phase)},
+                 "err_mu_vs_fp64": err_mu, "err_sigma_vs_fp64_interior90": err_sigma,
+                 "dtype": "f32 recursion + 3xTF32 tcgen05 contraction (FP32 TMEM accumulation over 2048-float "
+                          "chunks, FP64 across chunks) + FP64 FFT" if name == "mixed" else "f64"}
+        # tensor-pipe view of the tcgen05 contraction: 3 split products x real GEMM (2M x M x 4K flops)
+        if name == "mixed" and o_phase[1] > 0:
+            tc_flops = 3 * 2.0 * (2 * M) * M * (2 * K)
+            other["contraction_tf32_tflops"] = tc_flops / (o_phase[1] / args.steps * 1e-3) / 1e12
+
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         try:
@@ -364,7 +414,8 @@ def main():
                 "roofline": roof,
                 "roofline_recursion": {"bound": "hbm", "achieved": rec_ach, "peak": hbm_peak, "unit": "GB/s",
                                        "frac": rec_ach / hbm_peak, "peak_source": peak_src},
-                "phases": phases, "fp64_peak_tflops": fp64_peak, "clocks": clk, "cpu_baseline": cpu}
+                "phases": phases, "fp64_peak_tflops": fp64_peak, "clocks": clk, "cpu_baseline": cpu,
+                "other_precision": other}
         print(json.dumps(line))
     if dist is not None:
         dist.destroy_process_group()

@@ -479,6 +479,17 @@ static Chunking pick_chunks(Session *s, int N, int R, int M, size_t esz, const l
   return {Rc, (R + Rc - 1) / Rc};
 }
 
+// FP32 recursions need FP32 copies of the operators; returns whether the blocks are FP32.
+static bool prepare_precision(const linqt_opts &o, const DeviceOp &H, const DeviceOp *a, const DeviceOp *b) {
+  LQ_REQUIRE(o.precision == LINQT_PREC_FP64 || o.precision == LINQT_PREC_MIXED || o.precision == LINQT_PREC_FP32,
+             "unknown precision");
+  if (o.precision == LINQT_PREC_FP64) return false;
+  const_cast<DeviceOp &>(H).ensure_fp32();
+  if (a) const_cast<DeviceOp &>(*a).ensure_fp32();
+  if (b) const_cast<DeviceOp &>(*b).ensure_fp32();
+  return true;
+}
+
 // ---------------------------------------------------------------------------
 // 2D moments: chebyshev::CorrelationExpansionMoments (src/chebyshev_solver.cpp:86-172)
 // ---------------------------------------------------------------------------
@@ -486,11 +497,10 @@ static void moments2d_dev(Session *s, const DeviceOp &H, const DeviceOp *opl, co
                           const double2 *states, int R, int M, const linqt_opts &o, double2 *mu) {
   LQ_REQUIRE(R > 0 && M > 0, "moments2d: R and M must be positive");
   LQ_REQUIRE((!opl || opl->n == H.n) && (!opr || opr->n == H.n), "moments2d: operator dimension mismatch");
-  if (o.precision != LINQT_PREC_FP64)
-    fail(LINQT_ERR_UNSUPPORTED, "moments2d: mixed precision is provided by the tensor-core build");
+  const bool fp32 = prepare_precision(o, H, opl, opr);
   const int N = H.n;
-  const size_t esz = sizeof(double2);
-  const Chunking ch = pick_chunks(s, N, R, M, esz, o, sizeof(double2) * (size_t)M * M * 64);
+  const size_t esz = fp32 ? sizeof(float2) : sizeof(double2);
+  const Chunking ch = pick_chunks(s, N, R, M, esz, o, sizeof(double2) * (size_t)M * M * 66);
   const size_t blk = esz * (size_t)N * ch.Rc;
   char *Ls = (char *)s->get("lr_L", blk * M);
   char *Rs = (char *)s->get("lr_R", blk * M);
@@ -501,12 +511,12 @@ static void moments2d_dev(Session *s, const DeviceOp &H, const DeviceOp *opl, co
     void *phi = tmp + 3 * blk;
     {
       PhaseScope ph(s, PH_RECURSION);
-      chunk_block(s, states, N, R, c * ch.Rc, ch.Rc, phi, false);
-      ph.launches(1 + lr_vectors(s, H, opl, opr, phi, M, ch.Rc, false, Ls, Rs, tmp, o.format, o.step_launches != 0));
+      chunk_block(s, states, N, R, c * ch.Rc, ch.Rc, phi, fp32);
+      ph.launches(1 + lr_vectors(s, H, opl, opr, phi, M, ch.Rc, fp32, Ls, Rs, tmp, o.format, o.step_launches != 0));
     }
     {
       PhaseScope ph(s, PH_CONTRACT);
-      mu_contract(s, Ls, Rs, M, (long)N * ch.Rc, false, o.precision, raw);
+      mu_contract(s, Ls, Rs, M, (long)N * ch.Rc, fp32, o.precision, raw);
       ph.launches(2);
     }
   }
@@ -526,10 +536,11 @@ static void kubo_fft_dev(Session *s, const DeviceOp &H, const DeviceOp *opl, con
   LQ_REQUIRE(nump >= M, "kubo_fft: nump must be >= M (pre_factors are indexed m < M, src/Bastin_FFTs.cpp:18-21)");
   LQ_REQUIRE(formula == LINQT_KUBO_BASTIN || formula == LINQT_KUBO_GREENWOOD, "kubo_fft: unknown formula");
   LQ_REQUIRE(bw > 0, "kubo_fft: band_width must be positive");
-  if (o.precision != LINQT_PREC_FP64) fail(LINQT_ERR_UNSUPPORTED, "kubo_fft: FP64 only");
+  const bool fp32 = prepare_precision(o, H, opl, opr);
   const int N = H.n;
-  const Chunking ch = pick_chunks(s, N, R, M, sizeof(double2), o, sizeof(double2) * 2 * (size_t)nump * 1024);
-  const size_t blk = sizeof(double2) * (size_t)N * ch.Rc;
+  const size_t esz = fp32 ? sizeof(float2) : sizeof(double2);
+  const Chunking ch = pick_chunks(s, N, R, M, esz, o, sizeof(double2) * 2 * (size_t)nump * 1024);
+  const size_t blk = esz * (size_t)N * ch.Rc;
   char *Ls = (char *)s->get("lr_L", blk * M);
   char *Rs = (char *)s->get("lr_R", blk * M);
   char *tmp = (char *)s->get("lr_tmp", blk * 4);
@@ -540,12 +551,12 @@ static void kubo_fft_dev(Session *s, const DeviceOp &H, const DeviceOp *opl, con
     void *phi = tmp + 3 * blk;
     {
       PhaseScope ph(s, PH_RECURSION);
-      chunk_block(s, states, N, R, c * ch.Rc, ch.Rc, phi, false);
-      ph.launches(1 + lr_vectors(s, H, opl, opr, phi, M, ch.Rc, false, Ls, Rs, tmp, o.format, o.step_launches != 0));
+      chunk_block(s, states, N, R, c * ch.Rc, ch.Rc, phi, fp32);
+      ph.launches(1 + lr_vectors(s, H, opl, opr, phi, M, ch.Rc, fp32, Ls, Rs, tmp, o.format, o.step_launches != 0));
     }
     {
       PhaseScope ph(s, PH_FFT);
-      kubo_fft_sites(s, Ls, Rs, (long)N * ch.Rc, M, nump, formula, false, acc_c);
+      kubo_fft_sites(s, Ls, Rs, (long)N * ch.Rc, M, nump, formula, fp32, acc_c);
       add_into(s, acc, acc_c, 2 * nump);
       ph.launches(4);
     }
@@ -580,11 +591,12 @@ static void kubo_bastin_dev(Session *s, const DeviceOp &H, const DeviceOp *opl, 
   LQ_REQUIRE(R > 0 && M > 0, "kubo_bastin: R and M must be positive");
   LQ_REQUIRE(!out || nump >= M, "kubo_bastin: nump must be >= M");
   LQ_REQUIRE(bw > 0, "kubo_bastin: band_width must be positive");
-  if (o.precision != LINQT_PREC_FP64) fail(LINQT_ERR_UNSUPPORTED, "kubo_bastin: FP64 only in this build");
+  const bool fp32 = prepare_precision(o, H, opl, opr);
   const int N = H.n;
-  const size_t extra = sizeof(double2) * ((size_t)M * M * 64 + 2 * (size_t)std::max(nump, 1) * 1024);
-  const Chunking ch = pick_chunks(s, N, R, M, sizeof(double2), o, extra);
-  const size_t blk = sizeof(double2) * (size_t)N * ch.Rc;
+  const size_t esz = fp32 ? sizeof(float2) : sizeof(double2);
+  const size_t extra = sizeof(double2) * ((size_t)M * M * 66 + 2 * (size_t)std::max(nump, 1) * 1024);
+  const Chunking ch = pick_chunks(s, N, R, M, esz, o, extra);
+  const size_t blk = esz * (size_t)N * ch.Rc;
   char *Ls = (char *)s->get("lr_L", blk * M);
   char *Rs = (char *)s->get("lr_R", blk * M);
   char *tmp = (char *)s->get("lr_tmp", blk * 4);
@@ -602,17 +614,17 @@ static void kubo_bastin_dev(Session *s, const DeviceOp &H, const DeviceOp *opl, 
     void *phi = tmp + 3 * blk;
     {
       PhaseScope ph(s, PH_RECURSION);
-      chunk_block(s, states, N, R, c * ch.Rc, ch.Rc, phi, false);
-      ph.launches(1 + lr_vectors(s, H, opl, opr, phi, M, ch.Rc, false, Ls, Rs, tmp, o.format, o.step_launches != 0));
+      chunk_block(s, states, N, R, c * ch.Rc, ch.Rc, phi, fp32);
+      ph.launches(1 + lr_vectors(s, H, opl, opr, phi, M, ch.Rc, fp32, Ls, Rs, tmp, o.format, o.step_launches != 0));
     }
     if (mu) {
       PhaseScope ph(s, PH_CONTRACT);
-      mu_contract(s, Ls, Rs, M, (long)N * ch.Rc, false, o.precision, raw);
+      mu_contract(s, Ls, Rs, M, (long)N * ch.Rc, fp32, o.precision, raw);
       ph.launches(2);
     }
     if (out) {
       PhaseScope ph(s, PH_FFT);
-      kubo_fft_sites(s, Ls, Rs, (long)N * ch.Rc, M, nump, LINQT_KUBO_BASTIN, false, acc_c);
+      kubo_fft_sites(s, Ls, Rs, (long)N * ch.Rc, M, nump, LINQT_KUBO_BASTIN, fp32, acc_c);
       add_into(s, acc, acc_c, 2 * nump);
       ph.launches(4);
     }

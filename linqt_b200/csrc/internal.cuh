@@ -211,6 +211,11 @@ void zgemm_cn(Session *s, const double2 *A, int MA, const double2 *B, int MB, lo
 void mu_contract(Session *s, const void *L, const void *Rv, int M, long K, bool fp32_inputs, int precision,
                  double2 *mu_raw);
 void mu_finalize(Session *s, const double2 *mu_raw, int M, int R, double2 *mu);
+void reduce_parts_into(Session *s, const double2 *part, int S, long MM, double2 *dst);
+// tcgen05 split-TF32 contraction of FP32 Chebyshev blocks (mu_tc.cu)
+bool mu_tc_supported(long K);
+void mu_contract_tc(Session *s, const void *L, const void *Rv, int M, long K, double2 *mu_raw);
+int mu_tc_check_error(Session *s);
 
 // FFT path: accumulate p/w over all sites into acc[2*nump] (complex)
 void kubo_fft_sites(Session *s, const void *L, const void *Rv, long nsites, int M, int nump, int formula,

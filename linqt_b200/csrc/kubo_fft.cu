@@ -165,16 +165,23 @@ __device__ __forceinline__ void cp_async16(void *smem, const void *gmem) {
   const unsigned sa = (unsigned)__cvta_generic_to_shared(smem);
   asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(sa), "l"(gmem));
 }
+__device__ __forceinline__ void cp_async8(void *smem, const void *gmem) {
+  const unsigned sa = (unsigned)__cvta_generic_to_shared(smem);
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(sa), "l"(gmem));
+}
 __device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::); }
 __device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_group 0;\n" ::); }
+__device__ __forceinline__ void cp_async_el(double2 *smem, const double2 *g) { cp_async16(smem, g); }
+__device__ __forceinline__ void cp_async_el(float2 *smem, const float2 *g) { cp_async8(smem, g); }
 
 // Issue the asynchronous copies of site l's bra_m = L[m][l] and ket_m = Rv[m][l], m < M,
 // into stage[0..M) and stage[M..2M).
-__device__ __forceinline__ void stage_site(double2 *stage, const double2 *__restrict__ L,
-                                           const double2 *__restrict__ Rv, long K, int M, long l) {
+template <class Tin>
+__device__ __forceinline__ void stage_site(Tin *stage, const Tin *__restrict__ L, const Tin *__restrict__ Rv, long K,
+                                           int M, long l) {
   for (int m = threadIdx.x; m < M; m += blockDim.x) {
-    cp_async16(stage + m, L + (size_t)m * K + l);
-    cp_async16(stage + M + m, Rv + (size_t)m * K + l);
+    cp_async_el(stage + m, L + (size_t)m * K + l);
+    cp_async_el(stage + M + m, Rv + (size_t)m * K + l);
   }
   cp_async_commit();
 }
@@ -185,9 +192,9 @@ __device__ __forceinline__ void stage_site(double2 *stage, const double2 *__rest
 //   tw2   16 * R3               w_P^{a c}   at [c * R3 + a]    (pass 2)
 //   pfs   M                     prefactors
 //   stage 2 * 2M                double-buffered bra/ket of the current and next site
-template <int R3, int NSEQ>
+template <int R3, int NSEQ, class Tin>
 __global__ void __launch_bounds__(kFftThreads)
-    k_kubo_fft(const double2 *__restrict__ L, const double2 *__restrict__ Rv, long K, long chunk, int M,
+    k_kubo_fft(const Tin *__restrict__ L, const Tin *__restrict__ Rv, long K, long chunk, int M,
                const double2 *__restrict__ pf_g, double2 *__restrict__ part) {
   constexpr int P = 16 * R3;    // n / 16
   constexpr int n = 16 * P;     // nump
@@ -199,7 +206,7 @@ __global__ void __launch_bounds__(kFftThreads)
   double2 *tw1 = buf + NSEQ * SEQ;
   double2 *tw2 = tw1 + 16 * P;
   double2 *pfs = tw2 + 16 * R3;
-  double2 *stage = pfs + M;  // 2 buffers of 2M
+  Tin *stage = reinterpret_cast<Tin *>(pfs + M);  // 2 buffers of 2M
   const long lbeg = (long)blockIdx.x * chunk;
   const long lend = min(K, lbeg + chunk);
   if (lbeg < lend) stage_site(stage, L, Rv, K, M, lbeg);
@@ -224,19 +231,20 @@ __global__ void __launch_bounds__(kFftThreads)
   for (long l = lbeg; l < lend; ++l) {
     cp_async_wait_all();
     __syncthreads();  // stage[cur] complete and visible; the previous site is fully consumed
-    const double2 *bra = stage + cur * 2 * M, *ket = bra + M;
+    const Tin *bra = stage + cur * 2 * M, *ket = bra + M;
     if (l + 1 < lend) stage_site(stage + (cur ^ 1) * 2 * M, L, Rv, K, M, l + 1);
     // ---- pass 1: x_s[m1 + P m2], m2 < 16 -> 16-point DFT over m2, twiddle w_n^{m1 k2}
     for (int item = threadIdx.x; item < NSEQ * P; item += blockDim.x) {
       const int s = item / P, m1 = item % P;
-      const double *src = (const double *)((s & 2) ? ket : bra) + (s & 1);  // Re or Im part
+      using Tr = decltype(Tin::x);
+      const Tr *src = (const Tr *)((s & 2) ? ket : bra) + (s & 1);  // Re or Im part
       const bool deriv = s >= 4;
       double2 v[16];
 #pragma unroll
       for (int m2 = 0; m2 < 16; ++m2) {
         const int m = m1 + P * m2;
         if (m < M) {
-          double f = src[2 * m];
+          double f = (double)src[2 * m];
           if (deriv) f *= (double)m;
           const double2 pf = pfs[m];
           v[m2] = make_double2(pf.x * f, pf.y * f);
@@ -335,9 +343,9 @@ __global__ void __launch_bounds__(kFftThreads)
 }
 
 // Direct DFT for any nump: one CTA per site at a time, thread per frequency.
-template <int NSEQ>
+template <int NSEQ, class Tin>
 __global__ void __launch_bounds__(256)
-    k_kubo_dft(const double2 *__restrict__ L, const double2 *__restrict__ Rv, long K, long chunk, int M, int nump,
+    k_kubo_dft(const Tin *__restrict__ L, const Tin *__restrict__ Rv, long K, long chunk, int M, int nump,
                const double2 *__restrict__ pf_g, const double2 *__restrict__ twg, double2 *__restrict__ part) {
   extern __shared__ double2 sm[];
   double2 *bk = sm;  // bra[M], ket[M]
@@ -352,8 +360,8 @@ __global__ void __launch_bounds__(256)
   for (long l = lbeg; l < lend; ++l) {
     __syncthreads();
     for (int m = threadIdx.x; m < M; m += blockDim.x) {
-      bk[m] = L[(size_t)m * K + l];
-      bk[M + m] = Rv[(size_t)m * K + l];
+      bk[m] = to_d2(L[(size_t)m * K + l]);
+      bk[M + m] = to_d2(Rv[(size_t)m * K + l]);
     }
     __syncthreads();
     for (int q = 0; q < kpt; ++q) {
@@ -450,48 +458,42 @@ __global__ void k_kubo_post(const double2 *__restrict__ acc, double R, int nump,
   for (int j = threadIdx.x; j < nump; j += blockDim.x) E[j] = a * Er[j] - b;
 }
 
-template <int R3, int NSEQ>
-void launch_fft(Session *s, const double2 *L, const double2 *Rv, long K, int M, const double2 *pf, double2 *acc) {
+template <int R3, int NSEQ, class Tin>
+void launch_fft(Session *s, const Tin *L, const Tin *Rv, long K, int M, const double2 *pf, double2 *acc) {
   constexpr int n = 256 * R3;
-  const size_t smem = sizeof(double2) * ((size_t)NSEQ * 16 * (16 * R3 + 1) + 16 * 16 * R3 + 16 * R3 + 5 * (size_t)M);
+  const size_t smem = sizeof(double2) * ((size_t)NSEQ * 16 * (16 * R3 + 1) + 16 * 16 * R3 + 16 * R3 + (size_t)M) +
+                      sizeof(Tin) * 4 * (size_t)M;
   if (smem > 227 * 1024) fail(LINQT_ERR_UNSUPPORTED, "kubo_fft: nump too large for the shared-memory FFT");
-  LQ_CUDA(cudaFuncSetAttribute(k_kubo_fft<R3, NSEQ>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  LQ_CUDA(cudaFuncSetAttribute(k_kubo_fft<R3, NSEQ, Tin>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
   const int nb = (int)std::max(1L, std::min(K, (long)s->sm_count));
   const long chunk = (K + nb - 1) / nb;
   double2 *part = (double2 *)s->get("kubo_part", sizeof(double2) * 2 * (size_t)n * nb);
-  k_kubo_fft<R3, NSEQ><<<nb, kFftThreads, smem, s->stream>>>(L, Rv, K, chunk, M, pf, part);
+  k_kubo_fft<R3, NSEQ, Tin><<<nb, kFftThreads, smem, s->stream>>>(L, Rv, K, chunk, M, pf, part);
   LQ_LAUNCHED();
   k_sum_parts<<<(2 * n + 255) / 256, 256, 0, s->stream>>>(part, nb, 2 * n, acc);
   LQ_LAUNCHED();
 }
 
-template <int NSEQ>
-void launch_dft(Session *s, const double2 *L, const double2 *Rv, long K, int M, int nump, const double2 *pf,
-                double2 *acc) {
+template <int NSEQ, class Tin>
+void launch_dft(Session *s, const Tin *L, const Tin *Rv, long K, int M, int nump, const double2 *pf, double2 *acc) {
   double2 *tw = (double2 *)s->get("kubo_tw", sizeof(double2) * nump);
   k_twiddles<<<(nump + 255) / 256, 256, 0, s->stream>>>(nump, tw);
   LQ_LAUNCHED();
   const size_t smem = sizeof(double2) * 2 * (size_t)M;
   if (smem > 227 * 1024) fail(LINQT_ERR_UNSUPPORTED, "kubo_fft: M too large for the direct DFT");
-  LQ_CUDA(cudaFuncSetAttribute(k_kubo_dft<NSEQ>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  LQ_CUDA(cudaFuncSetAttribute(k_kubo_dft<NSEQ, Tin>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
   const int nb = (int)std::max(1L, std::min(K, (long)s->sm_count * 4));
   const long chunk = (K + nb - 1) / nb;
   double2 *part = (double2 *)s->get("kubo_part", sizeof(double2) * 2 * (size_t)nump * nb);
-  k_kubo_dft<NSEQ><<<nb, 256, smem, s->stream>>>(L, Rv, K, chunk, M, nump, pf, tw, part);
+  k_kubo_dft<NSEQ, Tin><<<nb, 256, smem, s->stream>>>(L, Rv, K, chunk, M, nump, pf, tw, part);
   LQ_LAUNCHED();
   k_sum_parts<<<(2 * nump + 255) / 256, 256, 0, s->stream>>>(part, nb, 2 * nump, acc);
   LQ_LAUNCHED();
 }
 
-}  // namespace
-
-void kubo_fft_sites(Session *s, const void *Lv, const void *Rvv, long nsites, int M, int nump, int formula,
-                    bool fp32_inputs, double2 *acc) {
-  if (fp32_inputs) fail(LINQT_ERR_UNSUPPORTED, "kubo_fft: FP32 Chebyshev vectors are not supported");
-  const double2 *L = (const double2 *)Lv, *Rv = (const double2 *)Rvv;
-  double2 *pf = (double2 *)s->get("kubo_pf", sizeof(double2) * M);
-  k_prefactors<<<(M + 255) / 256, 256, 0, s->stream>>>(M, nump, pf);
-  LQ_LAUNCHED();
+template <class Tin>
+void kubo_fft_sites_t(Session *s, const Tin *L, const Tin *Rv, long nsites, int M, int nump, int formula,
+                      const double2 *pf, double2 *acc) {
   const bool bastin = formula == LINQT_KUBO_BASTIN;
   const bool pow2 = nump >= 256 && nump <= 2048 && (nump & (nump - 1)) == 0;
   const bool fits = pow2 && (bastin ? nump <= 1024 : true);
@@ -507,6 +509,19 @@ void kubo_fft_sites(Session *s, const void *Lv, const void *Rvv, long nsites, in
     launch_dft<8>(s, L, Rv, nsites, M, nump, pf, acc);
   else
     launch_dft<4>(s, L, Rv, nsites, M, nump, pf, acc);
+}
+
+}  // namespace
+
+void kubo_fft_sites(Session *s, const void *Lv, const void *Rvv, long nsites, int M, int nump, int formula,
+                    bool fp32_inputs, double2 *acc) {
+  double2 *pf = (double2 *)s->get("kubo_pf", sizeof(double2) * M);
+  k_prefactors<<<(M + 255) / 256, 256, 0, s->stream>>>(M, nump, pf);
+  LQ_LAUNCHED();
+  if (fp32_inputs)
+    kubo_fft_sites_t(s, (const float2 *)Lv, (const float2 *)Rvv, nsites, M, nump, formula, pf, acc);
+  else
+    kubo_fft_sites_t(s, (const double2 *)Lv, (const double2 *)Rvv, nsites, M, nump, formula, pf, acc);
 }
 
 void kubo_postprocess(Session *s, const double2 *acc, int R, int nump, int formula, int N, double band_width,

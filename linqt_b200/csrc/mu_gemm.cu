@@ -29,10 +29,18 @@ __device__ __forceinline__ void cp_async_wait() {
   asm volatile("cp.async.wait_group %0;\n" ::"n"(N));
 }
 
-// Load a BM x BK tile of rows [row0, row0+BM) and k in [k0, k0+BK) of a K-major matrix.
-__device__ __forceinline__ void load_tile(double2 (*sm)[LDS], const double2 *__restrict__ g, int M, long K, int row0,
-                                          long k0, long kend) {
-  // 256 threads x 4 double2: thread t covers row t>>2, k slots (t&3)*4 .. +3
+__device__ __forceinline__ void cp_async8(void *smem, const void *gmem, bool valid) {
+  const unsigned s = (unsigned)__cvta_generic_to_shared(smem);
+  const int n = valid ? 8 : 0;
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 8, %2;\n" ::"r"(s), "l"(gmem), "r"(n));
+}
+
+// Load a BM x BK tile of rows [row0, row0+BM) and k in [k0, k0+BK) of a K-major matrix of
+// complex values (double2, or float2 for FP32 Chebyshev blocks).
+template <class Tc>
+__device__ __forceinline__ void load_tile(Tc (*sm)[LDS], const Tc *__restrict__ g, int M, long K, int row0, long k0,
+                                          long kend) {
+  // 256 threads x 4 elements: thread t covers row t>>2, k slots (t&3)*4 .. +3
   const int t = threadIdx.x;
   const int r = t >> 2, kq = (t & 3) * 4;
   const int row = row0 + r;
@@ -40,8 +48,11 @@ __device__ __forceinline__ void load_tile(double2 (*sm)[LDS], const double2 *__r
   for (int q = 0; q < 4; ++q) {
     const long k = k0 + kq + q;
     const bool ok = row < M && k < kend;
-    const double2 *src = ok ? g + (size_t)row * K + k : g;
-    cp_async16(&sm[r][kq + q], src, ok);
+    const Tc *src = ok ? g + (size_t)row * K + k : g;
+    if constexpr (sizeof(Tc) == 16)
+      cp_async16(&sm[r][kq + q], src, ok);
+    else
+      cp_async8(&sm[r][kq + q], src, ok);
   }
 }
 
@@ -55,12 +66,13 @@ __device__ __forceinline__ void dmma(double &d0, double &d1, double a, double b)
 
 // 64x64 complex output tile per CTA, 8 warps as 2 (rows) x 4 (cols), 32x16 complex per warp
 // = 4 x 2 tiles of 8x8; conj(A) B = (Ar Br + Ai Bi) + i (Ar Bi - Ai Br): four real DMMAs per tile.
-__global__ void __launch_bounds__(256, 2) k_zgemm_cn_f64(const double2 *__restrict__ L, const double2 *__restrict__ Rv,
-                                                         int MA, int MB, long K, long kchunk,
-                                                         double2 *__restrict__ part) {
-  extern __shared__ double2 smem[];
-  double2(*As)[BM][LDS] = reinterpret_cast<double2(*)[BM][LDS]>(smem);
-  double2(*Bs)[BN][LDS] = reinterpret_cast<double2(*)[BN][LDS]>(smem + 2 * BM * LDS);
+template <class Tc>
+__global__ void __launch_bounds__(256, 2) k_zgemm_cn_f64(const Tc *__restrict__ L, const Tc *__restrict__ Rv, int MA,
+                                                         int MB, long K, long kchunk, double2 *__restrict__ part) {
+  extern __shared__ double2 smem_d[];
+  Tc *smem = reinterpret_cast<Tc *>(smem_d);
+  Tc(*As)[BM][LDS] = reinterpret_cast<Tc(*)[BM][LDS]>(smem);
+  Tc(*Bs)[BN][LDS] = reinterpret_cast<Tc(*)[BN][LDS]>(smem + 2 * BM * LDS);
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int wm = warp >> 2, wn = warp & 3;
   const int fr = lane >> 2, fk = lane & 3;
@@ -91,13 +103,13 @@ __global__ void __launch_bounds__(256, 2) k_zgemm_cn_f64(const double2 *__restri
         double ar[4], ai[4], br[2], bi[2];
 #pragma unroll
         for (int i = 0; i < 4; ++i) {
-          const double2 a = As[cur][wm * 32 + i * 8 + fr][ks * 4 + fk];
+          const double2 a = to_d2(As[cur][wm * 32 + i * 8 + fr][ks * 4 + fk]);
           ar[i] = a.x;
           ai[i] = -a.y;  // conj(A)
         }
 #pragma unroll
         for (int j = 0; j < 2; ++j) {
-          const double2 b = Bs[cur][wn * 16 + j * 8 + fr][ks * 4 + fk];
+          const double2 b = to_d2(Bs[cur][wn * 16 + j * 8 + fr][ks * 4 + fk]);
           br[j] = b.x;
           bi[j] = b.y;
         }
@@ -181,10 +193,8 @@ __global__ void k_moments1d(const double2 *__restrict__ dots, int steps, int M, 
   }
 }
 
-}  // namespace
-
-// C(i, j) (+)= sum_k conj(A[i][k]) * B[j][k] for i < MA, j < MB  (FP64, deterministic split-K)
-void zgemm_cn(Session *s, const double2 *A, int MA, const double2 *B, int MB, long K, double2 *C, bool accumulate) {
+template <class Tc>
+void zgemm_cn_t(Session *s, const Tc *A, int MA, const Tc *B, int MB, long K, double2 *C, bool accumulate) {
   const int tiles = ((MA + BM - 1) / BM) * ((MB + BN - 1) / BN);
   const long target = (long)s->sm_count * 2 * 2;
   long S = std::max(1L, (target + tiles - 1) / tiles);
@@ -194,10 +204,10 @@ void zgemm_cn(Session *s, const double2 *A, int MA, const double2 *B, int MB, lo
   kchunk = (kchunk + BK - 1) / BK * BK;
   S = (K + kchunk - 1) / kchunk;
   double2 *part = (double2 *)s->get("zgemm_parts", sizeof(double2) * (size_t)S * MA * MB);
-  const size_t smem = sizeof(double2) * 2 * (BM + BN) * LDS;
-  LQ_CUDA(cudaFuncSetAttribute(k_zgemm_cn_f64, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  const size_t smem = sizeof(Tc) * 2 * (BM + BN) * LDS;
+  LQ_CUDA(cudaFuncSetAttribute(k_zgemm_cn_f64<Tc>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
   dim3 grid((MB + BN - 1) / BN, (MA + BM - 1) / BM, (unsigned)S);
-  k_zgemm_cn_f64<<<grid, 256, smem, s->stream>>>(A, B, MA, MB, K, kchunk, part);
+  k_zgemm_cn_f64<Tc><<<grid, 256, smem, s->stream>>>(A, B, MA, MB, K, kchunk, part);
   LQ_LAUNCHED();
   const long MM = (long)MA * MB;
   if (!accumulate) LQ_CUDA(cudaMemsetAsync(C, 0, sizeof(double2) * MM, s->stream));
@@ -206,11 +216,29 @@ void zgemm_cn(Session *s, const double2 *A, int MA, const double2 *B, int MB, lo
   LQ_LAUNCHED();
 }
 
+}  // namespace
+
+// C(i, j) (+)= sum_k conj(A[i][k]) * B[j][k] for i < MA, j < MB  (FP64 MMA, deterministic split-K)
+void zgemm_cn(Session *s, const double2 *A, int MA, const double2 *B, int MB, long K, double2 *C, bool accumulate) {
+  zgemm_cn_t<double2>(s, A, MA, B, MB, K, C, accumulate);
+}
+
+// dst += sum_z part[z]  (fixed order over z)
+void reduce_parts_into(Session *s, const double2 *part, int S, long MM, double2 *dst) {
+  const int g2 = (int)std::max(1L, std::min((MM + 255) / 256, (long)s->sm_count * 8));
+  k_reduce_parts<<<g2, 256, 0, s->stream>>>(part, S, MM, dst);
+  LQ_LAUNCHED();
+}
+
 void mu_contract(Session *s, const void *L, const void *Rv, int M, long K, bool fp32_inputs, int precision,
                  double2 *mu_raw) {
-  if (fp32_inputs) fail(LINQT_ERR_INTERNAL, "mu_contract: FP32 operands take the tensor-core path");
-  (void)precision;
-  zgemm_cn(s, (const double2 *)L, M, (const double2 *)Rv, M, K, mu_raw, true);
+  if (!fp32_inputs) {
+    zgemm_cn_t<double2>(s, (const double2 *)L, M, (const double2 *)Rv, M, K, mu_raw, true);
+  } else if (precision == LINQT_PREC_MIXED && mu_tc_supported(K)) {
+    mu_contract_tc(s, L, Rv, M, K, mu_raw);  // tcgen05 3xTF32 (mu_tc.cu)
+  } else {
+    zgemm_cn_t<float2>(s, (const float2 *)L, M, (const float2 *)Rv, M, K, mu_raw, true);  // FP64 MMA on FP32 data
+  }
 }
 
 void mu_finalize(Session *s, const double2 *mu_raw, int M, int R, double2 *mu) {

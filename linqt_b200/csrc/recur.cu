@@ -379,14 +379,17 @@ void recur_1d(Session *s, const DeviceOp &H, const void *phi, void *x0, void *b1
 
 void check_device_errors(Session *s) {
   if (!s->barrier_used) return;
-  Barrier *bar = (Barrier *)s->get("rec_barrier", sizeof(Barrier));
-  int err = 0;
-  LQ_CUDA(cudaMemcpy(&err, &bar->err, sizeof(int), cudaMemcpyDeviceToHost));
   s->barrier_used = false;
-  if (err) {
-    LQ_CUDA(cudaMemset(&bar->err, 0, sizeof(int)));
-    fail(LINQT_ERR_TIMEOUT, "persistent recursion: a grid barrier wait expired; results of the solve are invalid");
+  int err = 0;
+  auto it = s->ws.find("rec_barrier");
+  if (it != s->ws.end()) {
+    Barrier *bar = (Barrier *)it->second.first;
+    LQ_CUDA(cudaMemcpy(&err, &bar->err, sizeof(int), cudaMemcpyDeviceToHost));
+    if (err) LQ_CUDA(cudaMemset(&bar->err, 0, sizeof(int)));
   }
+  if (err) fail(LINQT_ERR_TIMEOUT, "persistent recursion: a grid barrier wait expired; results of the solve are invalid");
+  if (mu_tc_check_error(s))
+    fail(LINQT_ERR_TIMEOUT, "tensor-core contraction: a pipeline wait expired; results of the solve are invalid");
 }
 
 }  // namespace linqt

@@ -242,3 +242,44 @@ def test_errors_are_reported(honey):
     assert e.value.code == -1 and "nump" in str(e.value)
     with pytest.raises(lq.LinqtError):
         lq.Operator.from_csr(3, [0, 1, 2, 3], [0, 1, 5], [1.0, 1.0, 1.0])
+
+
+# ---------------------------------------------------------------------------
+# precision modes: FP32 recursion + FP64 contraction (PREC_FP32) and FP32 recursion +
+# tcgen05 3xTF32 contraction (PREC_MIXED).  Bounds are the measured accuracy of the
+# modes (stated in DESIGN.md), checked against the FP64 path.
+# ---------------------------------------------------------------------------
+@pytest.mark.parametrize("R,M", [(2, 32), (3, 100), (8, 130)])
+def test_mixed_precision_moments2d(honey, R, M):
+    st = lattices.random_phase_states(honey["N"], R, seed=22)
+    m64 = lq.moments2d(honey["Hg"], honey["Vg"], honey["Vg"], st, M)
+    m32 = lq.moments2d(honey["Hg"], honey["Vg"], honey["Vg"], st, M, opts=lq.make_opts(precision=lq.PREC_FP32))
+    mmx = lq.moments2d(honey["Hg"], honey["Vg"], honey["Vg"], st, M, opts=lq.make_opts(precision=lq.PREC_MIXED))
+    assert rel(m32, m64) < 1e-5      # FP32 recursion
+    assert rel(mmx, m32) < 1e-4      # tensor-core contraction of the same FP32 blocks
+    assert rel(mmx, m64) < 1e-4
+    assert np.abs(mmx - mmx.conj().T).max() < 1e-12 * np.abs(mmx).max()
+
+
+def test_mixed_precision_large_k_multi_pass():
+    """K = 2 * 16384 * 32 floats: several K passes of the tensor-core kernel."""
+    N, H, V = lattices.honeycomb(128, 64, t=-2.7, W=1.0, seed=21)
+    bw, bc = bounds_of(N, H)
+    Hg, Vg = gpu_op(N, H, bw, bc), gpu_op(N, V)
+    st = lattices.random_phase_states(N, 32, seed=22)
+    M = 16
+    m32 = lq.moments2d(Hg, Vg, Vg, st, M, opts=lq.make_opts(precision=lq.PREC_FP32))
+    mmx = lq.moments2d(Hg, Vg, Vg, st, M, opts=lq.make_opts(precision=lq.PREC_MIXED))
+    assert rel(mmx, m32) < 2e-4
+
+
+@pytest.mark.parametrize("precision", [lq.PREC_FP32, lq.PREC_MIXED])
+def test_mixed_precision_kubo_bastin(honey, precision):
+    st = lattices.random_phase_states(honey["N"], 4, seed=9)
+    M, nump = 64, 256
+    mu64, (E64, s64, _) = lq.kubo_bastin(honey["Hg"], honey["Vg"], honey["Vg"], st, M, nump, honey["bw"], honey["bc"])
+    mu, (E, s, _) = lq.kubo_bastin(honey["Hg"], honey["Vg"], honey["Vg"], st, M, nump, honey["bw"], honey["bc"],
+                                   opts=lq.make_opts(precision=precision))
+    assert np.array_equal(E, E64)
+    assert rel(s, s64) < 1e-4
+    assert rel(mu, mu64) < 1e-4
