@@ -105,6 +105,29 @@ __device__ void block_sum2(double2 &d0, double2 &d1) {
   __syncthreads();
 }
 
+
+// Copy this CTA's rows [r0, r1) of a CSR operator into shared memory at `dst` and return
+// pointers that index like the global arrays (rowptr by global row, col/val by global
+// entry).  `dst` is 16-byte aligned; returns the bytes used.
+template <class C>
+__device__ size_t cache_rows(const int *__restrict__ rp, const int *__restrict__ ci, const C *__restrict__ v, int r0,
+                             int r1, unsigned char *dst, const int *&rp_o, const int *&ci_o, const C *&v_o) {
+  const int k0 = rp[r0], k1 = rp[r1];
+  const int nnz = k1 - k0, nr = r1 - r0;
+  C *sv = reinterpret_cast<C *>(dst);
+  int *sc = reinterpret_cast<int *>(sv + nnz);
+  int *sr = sc + nnz;
+  for (int k = threadIdx.x; k < nnz; k += blockDim.x) {
+    sv[k] = v[k0 + k];
+    sc[k] = ci[k0 + k];
+  }
+  for (int i = threadIdx.x; i <= nr; i += blockDim.x) sr[i] = rp[r0 + i];
+  rp_o = sr - r0;
+  ci_o = sc - k0;
+  v_o = sv - k0;
+  return ((size_t)nnz * (sizeof(C) + 4) + (size_t)(nr + 1) * 4 + 15) & ~(size_t)15;
+}
+
 // ---------------------------------------------------------------------------
 // L and R recursions of CorrelationExpansionMoments / Kubo_solver_FFT.
 //   L: Lst[0] given (OPL phi); Lst[m+1] = 2 H Lst[m] - Lst[m-1] (Lst[1] = H Lst[0]), m+1 < M.
@@ -113,17 +136,23 @@ __device__ void block_sum2(double2 &d0, double2 &d1) {
 // ---------------------------------------------------------------------------
 template <class T, int TPR, int VPT, bool HAS_V>
 __global__ void __launch_bounds__(kThreads)
-    k_recur_lr(int n, const int *__restrict__ rp, const int *__restrict__ ci,
-               const typename cplx_t<T>::type *__restrict__ hv, const int *__restrict__ vrp,
-               const int *__restrict__ vci, const typename cplx_t<T>::type *__restrict__ vv,
-               typename cplx_t<T>::type *Lst, typename cplx_t<T>::type *Rst, const typename cplx_t<T>::type *phi,
-               typename cplx_t<T>::type *tb, int M, size_t blk, Barrier *bar) {
+    k_recur_lr(int n, const int *rp, const int *ci, const typename cplx_t<T>::type *hv, const int *vrp,
+               const int *vci, const typename cplx_t<T>::type *vv, typename cplx_t<T>::type *Lst,
+               typename cplx_t<T>::type *Rst, const typename cplx_t<T>::type *phi, typename cplx_t<T>::type *tb, int M,
+               size_t blk, Barrier *bar, int cache) {
   using C = typename cplx_t<T>::type;
   constexpr int R = TPR * VPT;
   const int lane = threadIdx.x % TPR;
   constexpr int gpb = kThreads / TPR;
   const int per = (n + gridDim.x - 1) / gridDim.x;
-  const int r0 = blockIdx.x * per, r1 = min(n, r0 + per);
+  const int r0 = min(n, blockIdx.x * per), r1 = min(n, r0 + per);
+  if (cache) {
+    // the operators do not change during the recursion: keep this CTA's rows on chip
+    extern __shared__ __align__(16) unsigned char smc[];
+    size_t off = cache_rows<C>(rp, ci, hv, r0, r1, smc, rp, ci, hv);
+    if (HAS_V) cache_rows<C>(vrp, vci, vv, r0, r1, smc + off, vrp, vci, vv);
+    __syncthreads();
+  }
   for (int m = 0; m < M; ++m) {
     const bool doL = m + 1 < M;
     const C *xL = Lst + (size_t)m * blk;
@@ -147,8 +176,8 @@ __global__ void __launch_bounds__(kThreads)
       const int b = rp[row], e = rp[row + 1];
 #pragma unroll 4
       for (int k = b; k < e; ++k) {
-        const int j = __ldg(ci + k);
-        const C h = __ldg(hv + k);
+        const int j = ci[k];
+        const C h = hv[k];
         const size_t off = (size_t)j * R + lane;
 #pragma unroll
         for (int u = 0; u < VPT; ++u) {
@@ -164,8 +193,8 @@ __global__ void __launch_bounds__(kThreads)
         const int vb = vrp[row], ve = vrp[row + 1];
 #pragma unroll 4
         for (int k = vb; k < ve; ++k) {
-          const int j = __ldg(vci + k);
-          const C h = __ldg(vv + k);
+          const int j = vci[k];
+          const C h = vv[k];
           const size_t off = (size_t)j * R + lane;
 #pragma unroll
           for (int u = 0; u < VPT; ++u) aV[u] = cfma(h, ldv(xR + off + u * TPR), aV[u]);
@@ -210,16 +239,20 @@ __global__ void __launch_bounds__(kThreads)
 // ---------------------------------------------------------------------------
 template <class T, int TPR, int VPT>
 __global__ void __launch_bounds__(kThreads)
-    k_recur_1d(int n, const int *__restrict__ rp, const int *__restrict__ ci,
-               const typename cplx_t<T>::type *__restrict__ hv, const typename cplx_t<T>::type *phi,
-               typename cplx_t<T>::type *x0, typename cplx_t<T>::type *b1, int steps, int M, int mode,
-               double2 *__restrict__ partials, Barrier *bar) {
+    k_recur_1d(int n, const int *rp, const int *ci, const typename cplx_t<T>::type *hv,
+               const typename cplx_t<T>::type *phi, typename cplx_t<T>::type *x0, typename cplx_t<T>::type *b1,
+               int steps, int M, int mode, double2 *__restrict__ partials, Barrier *bar, int cache) {
   using C = typename cplx_t<T>::type;
   constexpr int R = TPR * VPT;
   const int lane = threadIdx.x % TPR;
   constexpr int gpb = kThreads / TPR;
   const int per = (n + gridDim.x - 1) / gridDim.x;
-  const int r0 = blockIdx.x * per, r1 = min(n, r0 + per);
+  const int r0 = min(n, blockIdx.x * per), r1 = min(n, r0 + per);
+  if (cache) {
+    extern __shared__ __align__(16) unsigned char smc1[];
+    cache_rows<C>(rp, ci, hv, r0, r1, smc1, rp, ci, hv);
+    __syncthreads();
+  }
   C *prev = nullptr, *cur = x0;
   for (int s = 0; s < steps; ++s) {
     const bool need_y = mode == 2 ? (2 * s + 1 < M) : (s + 1 < M);
@@ -232,8 +265,8 @@ __global__ void __launch_bounds__(kThreads)
       const int b = rp[row], e = rp[row + 1];
 #pragma unroll 4
       for (int k = b; k < e; ++k) {
-        const int j = __ldg(ci + k);
-        const C h = __ldg(hv + k);
+        const int j = ci[k];
+        const C h = hv[k];
         const C *xr = cur + (size_t)j * R + lane;
 #pragma unroll
         for (int u = 0; u < VPT; ++u) acc[u] = cfma(h, ldv(xr + u * TPR), acc[u]);
@@ -281,12 +314,48 @@ __global__ void k_reduce_step_partials(const double2 *__restrict__ partials, int
   }
 }
 
-int coop_grid(const void *func, int sm_count, int n_rows, int tpr) {
+// Largest contiguous row slice (entries of one or two operators) a CTA owns for a given grid.
+size_t max_slice_bytes(const DeviceOp &H, const DeviceOp *V, int grid, size_t esz) {
+  const int n = H.n;
+  const int per = (n + grid - 1) / grid;
+  size_t worst = 0;
+  for (int b = 0; b < grid; ++b) {
+    const int r0 = std::min(n, b * per), r1 = std::min(n, r0 + per);
+    size_t bytes = ((size_t)(H.rowptr[r1] - H.rowptr[r0]) * (esz + 4) + (size_t)(r1 - r0 + 1) * 4 + 15) & ~(size_t)15;
+    if (V) bytes += ((size_t)(V->rowptr[r1] - V->rowptr[r0]) * (esz + 4) + (size_t)(r1 - r0 + 1) * 4 + 15) & ~(size_t)15;
+    worst = std::max(worst, bytes);
+  }
+  return worst;
+}
+
+// Cooperative grid: as many co-resident CTAs as fit (at most one CTA's worth of rows per
+// group of TPR threads).  The operator slices are cached in shared memory when they fit.
+int coop_setup(const void *func, int sm_count, const DeviceOp &H, const DeviceOp *V, int tpr, size_t esz,
+               size_t *smem) {
+  const int n = H.n;
+  const long need = ((long)n * tpr + kThreads - 1) / kThreads;
   int per_sm = 0;
   LQ_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, func, kThreads, 0));
   if (per_sm <= 0) fail(LINQT_ERR_UNSUPPORTED, "persistent recursion: kernel does not fit on an SM");
-  const long need = ((long)n_rows * tpr + kThreads - 1) / kThreads;
-  return (int)std::max(1L, std::min((long)per_sm * sm_count, need));
+  int grid = (int)std::max(1L, std::min((long)per_sm * sm_count, need));
+  const size_t limit = 96 * 1024;
+  size_t bytes = max_slice_bytes(H, V, grid, esz);
+  if (bytes <= limit) {
+    LQ_CUDA(cudaFuncSetAttribute(func, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes));
+    int per_sm2 = 0;
+    LQ_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm2, func, kThreads, bytes));
+    const int grid2 = (int)std::max(1L, std::min((long)per_sm2 * sm_count, need));
+    if (grid2 < grid) {  // fewer CTAs fit with the cache: recompute the slices
+      grid = grid2;
+      bytes = max_slice_bytes(H, V, grid, esz);
+    }
+    if (per_sm2 > 0 && bytes <= limit) {
+      *smem = bytes;
+      return grid;
+    }
+  }
+  *smem = 0;
+  return grid;
 }
 
 template <class T, int TPR, int VPT>
@@ -301,11 +370,13 @@ struct LRF {
     int n = H.n;
     C *L = (C *)Lst, *Rs = (C *)Rst, *tbuf = (C *)tb;
     const C *ph = (const C *)phi;
-    void *args[] = {&n, (void *)&H.d_rowptr, (void *)&H.d_col, (void *)&hv, (void *)&vrp, (void *)&vci, (void *)&vv,
-                    &L, &Rs, (void *)&ph, &tbuf, &M, &blk, &bar};
     const void *f = V ? (const void *)k_recur_lr<T, TPR, VPT, true> : (const void *)k_recur_lr<T, TPR, VPT, false>;
-    const int grid = coop_grid(f, s->sm_count, n, TPR);
-    LQ_CUDA(cudaLaunchCooperativeKernel(f, dim3(grid), dim3(kThreads), args, 0, s->stream));
+    size_t smem = 0;
+    const int grid = coop_setup(f, s->sm_count, H, V, TPR, sizeof(C), &smem);
+    int cache = smem > 0;
+    void *args[] = {&n,    (void *)&H.d_rowptr, (void *)&H.d_col, (void *)&hv, (void *)&vrp, (void *)&vci,
+                    (void *)&vv, &L, &Rs, (void *)&ph, &tbuf, &M, &blk, &bar, &cache};
+    LQ_CUDA(cudaLaunchCooperativeKernel(f, dim3(grid), dim3(kThreads), args, smem, s->stream));
   }
 };
 
@@ -317,14 +388,16 @@ struct OneDF {
     const bool fp32 = sizeof(T) == 4;
     const C *hv = fp32 ? (const C *)H.d_val32 : (const C *)H.d_val64;
     const void *f = (const void *)k_recur_1d<T, TPR, VPT>;
-    const int grid = coop_grid(f, s->sm_count, H.n, TPR);
+    size_t smem = 0;
+    const int grid = coop_setup(f, s->sm_count, H, nullptr, TPR, sizeof(C), &smem);
+    int cache = smem > 0;
     double2 *partials = (double2 *)s->get("rec1d_part", sizeof(double2) * 2 * (size_t)steps * grid);
     int n = H.n;
     const C *ph = (const C *)phi;
     C *xx = (C *)x0, *bb = (C *)b1;
     void *args[] = {&n, (void *)&H.d_rowptr, (void *)&H.d_col, (void *)&hv, (void *)&ph, &xx, &bb, &steps, &M, &mode,
-                    &partials, &bar};
-    LQ_CUDA(cudaLaunchCooperativeKernel(f, dim3(grid), dim3(kThreads), args, 0, s->stream));
+                    &partials, &bar, &cache};
+    LQ_CUDA(cudaLaunchCooperativeKernel(f, dim3(grid), dim3(kThreads), args, smem, s->stream));
     k_reduce_step_partials<<<(2 * steps + 255) / 256, 256, 0, s->stream>>>(partials, steps, grid, dots);
     LQ_LAUNCHED();
   }

@@ -1,8 +1,8 @@
 // Serving: continuous batching of DOS and Kubo-Bastin solves on one GPU.
 //
 // LinQT has no server (its drivers run one solve per process); this is the request
-// loop of the B200 build.  Requests are queued at submit (states copied to pinned
-// host memory), admitted in arrival order when an execution slot is free and their
+// loop of the B200 build.  Requests are queued at submit (states copied to host
+// memory the server owns), admitted in arrival order when an execution slot is free and their
 // estimated device footprint fits in the HBM budget, and run on the slot's own CUDA
 // stream, so solves admitted at different times overlap on the device.  Each slot
 // owns a session whose workspace budget is fixed, which makes the chunking -- and
@@ -43,13 +43,20 @@ struct Job {
   clk::time_point t_submit;
 };
 
-size_t estimate_footprint(const linqt_request &r, int n) {
+// Device bytes a request may hold: every workspace of the solver it runs (state copy,
+// Chebyshev blocks, per-step partials, contraction partials), with the same block width
+// the solver picks when the budget allows it.
+size_t estimate_footprint(const linqt_request &r, int n, int sm_count) {
   int Rc = 1;
   while (Rc < r.R && Rc < 256) Rc <<= 1;
-  const size_t esz = sizeof(double2);
-  const size_t io = esz * (size_t)r.R * n;
-  if (r.kind == LINQT_REQ_DOS) return io + esz * (size_t)n * Rc * 4 + esz * (size_t)r.M * 4 + (1 << 20);
-  return io + esz * (size_t)n * Rc * (2 * (size_t)r.M + 4) + esz * (size_t)r.M * r.M * 64 + (1 << 20);
+  const size_t esz = r.precision == LINQT_PREC_FP64 ? sizeof(double2) : sizeof(float2);
+  const size_t io = sizeof(double2) * ((size_t)r.R * n + (size_t)r.M * (r.kind == LINQT_REQ_DOS ? 1 : r.M));
+  if (r.kind == LINQT_REQ_DOS) {
+    const size_t steps = (size_t)r.M / 2 + 1;
+    return io + esz * (size_t)n * Rc * 3 + sizeof(double2) * (2 * steps * ((size_t)sm_count * 32 + 1) + 2 * steps) +
+           (1 << 20);
+  }
+  return io + esz * (size_t)n * Rc * (2 * (size_t)r.M + 4) + sizeof(double2) * (size_t)r.M * r.M * 66 + (1 << 20);
 }
 
 }  // namespace
@@ -57,7 +64,7 @@ size_t estimate_footprint(const linqt_request &r, int n) {
 struct linqt_server {
   int device = 0;
   size_t budget = 0, in_use = 0;
-  int max_active = 1;
+  int max_active = 1, sm_count = 148;
   std::mutex mu;
   std::condition_variable cv, done_cv;
   std::deque<std::shared_ptr<Job>> queue;
@@ -95,16 +102,14 @@ struct linqt_server {
       std::string err;
       try {
         Session &s = sess->s;
-        s.hbm_budget = job->footprint;
         const DeviceOp &H = job->req.H->op;
         const DeviceOp *op = job->req.op ? &job->req.op->op : nullptr;
         const int n = H.n, R = job->req.R, M = job->req.M;
         const size_t sb = sizeof(double2) * (size_t)R * n;
         const size_t mb = sizeof(double2) * (size_t)M * (job->req.kind == LINQT_REQ_DOS ? 1 : M);
-        s.hbm_budget = 0;  // io buffers are part of the estimate; solver buffers bounded below
+        s.hbm_budget = job->footprint;  // fixed per request: chunking independent of the other requests
         double2 *d_st = (double2 *)s.get("io_states", sb);
         double2 *d_mu = (double2 *)s.get("io_mu", mb);
-        s.hbm_budget = job->footprint + sb + mb;
         LQ_CUDA(cudaMemcpyAsync(d_st, job->states.data(), sb, cudaMemcpyHostToDevice, s.stream));
         if (job->req.kind == LINQT_REQ_DOS)
           moments1d_for_server(&s, H, op, d_st, R, M, job->req.precision, d_mu);
@@ -112,6 +117,7 @@ struct linqt_server {
           moments2d_for_server(&s, H, op, op, d_st, R, M, job->req.precision, d_mu);
         LQ_CUDA(cudaMemcpyAsync(job->req.mu_out, d_mu, mb, cudaMemcpyDeviceToHost, s.stream));
         LQ_CUDA(cudaStreamSynchronize(s.stream));
+        check_device_errors(&s);
         s.trim();
       } catch (const Error &e) {
         rc = e.code;
@@ -152,6 +158,7 @@ int linqt_server_create(int device, size_t hbm_budget_bytes, int max_active, lin
     s->device = device;
     s->budget = hbm_budget_bytes ? hbm_budget_bytes : (size_t)(fr * 0.8);
     s->max_active = max_active;
+    LQ_CUDA(cudaDeviceGetAttribute(&s->sm_count, cudaDevAttrMultiProcessorCount, device));
     for (int i = 0; i < max_active; ++i) s->workers.emplace_back([p = s.get()] { p->worker(); });
     *out = s.release();
     return LINQT_OK;
@@ -170,7 +177,7 @@ int linqt_server_submit(linqt_server *srv, const linqt_request *req, long *ticke
     job->req = *req;
     const int n = req->H->op.n;
     job->states.assign((const double2 *)req->states, (const double2 *)req->states + (size_t)req->R * n);
-    job->footprint = estimate_footprint(*req, n);
+    job->footprint = estimate_footprint(*req, n, srv->sm_count);
     if (job->footprint > srv->budget)
       fail(LINQT_ERR_NOMEM, "server: request footprint " + std::to_string(job->footprint >> 20) +
                                 " MiB exceeds the HBM budget");

@@ -1,0 +1,225 @@
+"""Serving: continuous batching of DOS and Kubo-Bastin moment solves.
+
+`Server` wraps linqt_server_* (csrc/server.cu): requests are queued with their states
+copied at submit, admitted in arrival order as execution slots and HBM budget free up,
+and run on per-slot CUDA streams, so requests arriving while others run overlap on the
+device.  Each slot's workspace budget is fixed, so a request's chunking (and with the
+fixed-order reductions its result) does not depend on what else is running.
+
+`request_stream` draws the seeded request mix of the serving benchmark; `run_stream`
+replays it with Poisson arrival times and reports p50/p99 latency and throughput.
+"""
+import ctypes
+import time
+
+import numpy as np
+
+from . import lattices
+from ._lib import Request, check, load
+from .core import PREC_FP64, PREC_MIXED, Operator, moments1d, moments2d, make_opts
+
+REQ_DOS, REQ_KUBO_BASTIN = 0, 1
+
+
+class Server:
+    def __init__(self, device=0, hbm_budget_bytes=0, max_active=4):
+        h = ctypes.c_void_p()
+        check(load().linqt_server_create(device, hbm_budget_bytes, max_active, ctypes.byref(h)))
+        self.h = h
+        self._keep = {}
+
+    def submit(self, kind, H, op, states, M, precision=PREC_FP64):
+        st = np.ascontiguousarray(np.atleast_2d(states), dtype=np.complex128)
+        R = st.shape[0]
+        out = np.zeros(M if kind == REQ_DOS else M * M, np.complex128)
+        req = Request()
+        req.kind, req.H, req.op = kind, H.h, (op.h if op is not None else None)
+        req.states = st.view(np.float64).ctypes.data_as(ctypes.POINTER(ctypes.c_double))
+        req.R, req.M, req.precision = R, M, precision
+        req.mu_out = out.view(np.float64).ctypes.data_as(ctypes.POINTER(ctypes.c_double))
+        t = ctypes.c_long()
+        check(load().linqt_server_submit(self.h, ctypes.byref(req), ctypes.byref(t)))
+        self._keep[t.value] = (out, H, op, M, kind)
+        return t.value
+
+    def poll(self, ticket):
+        st, lat = ctypes.c_int(), ctypes.c_double()
+        check(load().linqt_server_poll(self.h, ticket, ctypes.byref(st), ctypes.byref(lat)))
+        return st.value, lat.value
+
+    def result(self, ticket):
+        out, _, _, M, kind = self._keep[ticket]
+        return out if kind == REQ_DOS else out.reshape(M, M)
+
+    def wait_all(self):
+        check(load().linqt_server_wait_all(self.h))
+
+    def close(self):
+        if getattr(self, "h", None):
+            check(load().linqt_server_destroy(self.h))
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def _family(name, N_target, seed):
+    """A lattice of the family with about N_target sites: (N, H, V or None, bounds)."""
+    if name == "square":
+        L = max(4, int(round(N_target ** 0.5)))
+        N, H = lattices.square_lattice(L, 1.0, 1.0, seed)
+        V = None
+    elif name == "honeycomb":
+        L = max(4, int(round((N_target / 2) ** 0.5)))
+        N, H, V = lattices.honeycomb(L, L, -2.7, 1.0, seed)
+    else:
+        L = max(4, int(round((N_target / 4) ** 0.5)))
+        N, H, V = lattices.kane_mele(L, L, seed=seed)
+    lo, hi = lattices.gershgorin_bounds(N, *H)
+    return N, H, V, (1.05 * lo, 1.05 * hi)
+
+
+def request_stream(n_requests=200, seed=52, arrival_seed=51, n_min=1e4, n_max=2e5, m_min=128, m_max=512, r_max=16,
+                   rate_hz=None):
+    """Seeded request mix: 70 % DOS / 30 % Kubo-Bastin, square / honeycomb / Kane-Mele lattices,
+    N log-uniform in [n_min, n_max], M uniform in [m_min, m_max] (rounded to 16), R in [1, r_max],
+    precision FP64 or mixed; Poisson arrival gaps (exponential) from arrival_seed."""
+    u = lattices.uniform(seed, 6 * n_requests).reshape(n_requests, 6)
+    reqs = []
+    for i in range(n_requests):
+        kind = REQ_DOS if u[i, 0] < 0.7 else REQ_KUBO_BASTIN
+        fam = ["square", "honeycomb", "kane_mele"][min(2, int(u[i, 1] * 3))]
+        if kind == REQ_KUBO_BASTIN and fam == "square":
+            fam = "honeycomb"  # Kubo needs a velocity operator
+        N = float(np.exp(np.log(n_min) + u[i, 2] * (np.log(n_max) - np.log(n_min))))
+        M = int(round((m_min + u[i, 3] * (m_max - m_min)) / 16) * 16)
+        if kind == REQ_KUBO_BASTIN:
+            M = max(m_min, M // 2)
+        R = 1 + int(u[i, 4] * r_max)
+        prec = PREC_FP64 if u[i, 5] < 0.5 else PREC_MIXED
+        reqs.append(dict(kind=kind, family=fam, N=N, M=M, R=R, precision=prec))
+    a = lattices.uniform(arrival_seed, n_requests)
+    gaps = -np.log(1.0 - a)  # unit-rate exponential gaps, scaled by the caller
+    return reqs, gaps
+
+
+def _prepare(reqs, session=None):
+    """Operators (device resident) and states per request; lattices shared by family and size."""
+    cache = {}
+    prepared = []
+    for i, r in enumerate(reqs):
+        key = (r["family"], int(r["N"]))
+        if key not in cache:
+            N, H, V, (lo, hi) = _family(r["family"], r["N"], seed=31 + len(cache))
+            Hg = Operator.from_csr(N, *H, session=session)
+            Hg.rescale_to_chebyshev(hi - lo, (hi + lo) / 2)
+            Vg = Operator.from_csr(N, *V, session=session) if V is not None else None
+            cache[key] = (N, Hg, Vg)
+        N, Hg, Vg = cache[key]
+        st = lattices.random_phase_states(N, r["R"], seed=1000 + i)
+        prepared.append((Hg, Vg, st))
+    return prepared
+
+
+def run_serial(reqs, prepared, fp64_only=True):
+    """The same stream one request at a time on the plain FP64 path (host API)."""
+    t0 = time.perf_counter()
+    lat = []
+    for r, (Hg, Vg, st) in zip(reqs, prepared):
+        t = time.perf_counter()
+        o = make_opts(precision=PREC_FP64 if fp64_only else r["precision"])
+        if r["kind"] == REQ_DOS:
+            moments1d(Hg, None, st, r["M"], opts=o)
+        else:
+            moments2d(Hg, Vg, Vg, st, r["M"], opts=o)
+        lat.append(1e3 * (time.perf_counter() - t))
+    return time.perf_counter() - t0, np.array(lat)
+
+
+def run_stream(reqs, prepared, gaps, mean_gap_s, max_active=4, hbm_budget_bytes=0, device=0):
+    """Replay the stream with arrival times cumsum(gaps) * mean_gap_s; returns (latencies ms, makespan s)."""
+    srv = Server(device, hbm_budget_bytes, max_active)
+    arrivals = np.cumsum(gaps) * mean_gap_s
+    tickets = []
+    t0 = time.perf_counter()
+    for i, (r, (Hg, Vg, st)) in enumerate(zip(reqs, prepared)):
+        now = time.perf_counter() - t0
+        if arrivals[i] > now:
+            time.sleep(arrivals[i] - now)
+        op = Vg if r["kind"] == REQ_KUBO_BASTIN else None
+        tickets.append(srv.submit(r["kind"], Hg, op, st, r["M"], r["precision"]))
+    srv.wait_all()
+    makespan = time.perf_counter() - t0
+    lat = []
+    for t in tickets:
+        status, ms = srv.poll(t)
+        if status != 2:
+            raise RuntimeError("request %d ended with status %d" % (t, status))
+        lat.append(ms)
+    srv.close()
+    return np.array(lat), makespan
+
+
+def fifo_latencies(arrivals, service):
+    """Latencies (same unit as the inputs) of a single FIFO server with the given service times."""
+    t, lat = 0.0, []
+    for a, s in zip(arrivals, service):
+        t = max(t, a) + s
+        lat.append(t - a)
+    return np.array(lat)
+
+
+def main(argv=None):
+    """Serving benchmark: one JSON line with p50/p99 latency and throughput of the seeded stream
+    through the server, next to the same stream served one request at a time on the FP64 path."""
+    import argparse
+    import json
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--requests", type=int, default=200)
+    ap.add_argument("--load", type=float, default=1.0,
+                    help="offered load: arrival rate / serial FP64 service rate")
+    ap.add_argument("--max-active", type=int, default=4)
+    ap.add_argument("--n-max", type=float, default=2e5)
+    ap.add_argument("--m-max", type=int, default=512)
+    ap.add_argument("--r-max", type=int, default=16)
+    a = ap.parse_args(argv)
+    reqs, gaps = request_stream(a.requests, n_max=a.n_max, m_max=a.m_max, r_max=a.r_max)
+    prepared = _prepare(reqs)
+    # warm-up: every operator once in both precisions (FP32 value copies, library load)
+    seen = set()
+    warm_r, warm_p = [], []
+    for r, p in zip(reqs, prepared):
+        key = (id(p[0]), r["kind"])
+        if key not in seen:
+            seen.add(key)
+            for prec in (PREC_FP64, PREC_MIXED):
+                warm_r.append(dict(r, M=32, precision=prec))
+                warm_p.append(p)
+    run_serial(warm_r, warm_p, fp64_only=False)
+    t_ser, svc = run_serial(reqs, prepared, fp64_only=True)
+    t_mix, svc_mix = run_serial(reqs, prepared, fp64_only=False)
+    mean_gap = t_ser / len(reqs) / a.load
+    arrivals = np.cumsum(gaps) * mean_gap
+    lat_ser = 1e3 * fifo_latencies(arrivals, svc / 1e3)
+    lat, makespan = run_stream(reqs, prepared, gaps, mean_gap, max_active=a.max_active)
+    lat_sat, makespan_sat = run_stream(reqs, prepared, np.zeros_like(gaps), 0.0, max_active=a.max_active)
+    q = lambda x, p: float(np.percentile(x, p))
+    out = {
+        "metric": "serving_stream", "requests": len(reqs), "offered_load": a.load,
+        "mean_interarrival_ms": 1e3 * mean_gap, "max_active": a.max_active,
+        "stream": {"n_range": [1e4, a.n_max], "m_range": [128, a.m_max], "r_max": a.r_max,
+                   "dos_fraction": sum(r["kind"] == REQ_DOS for r in reqs) / len(reqs)},
+        "server": {"p50_ms": q(lat, 50), "p99_ms": q(lat, 99), "requests_per_s": len(reqs) / makespan},
+        "serial_fp64": {"p50_ms": q(lat_ser, 50), "p99_ms": q(lat_ser, 99), "requests_per_s": len(reqs) / t_ser},
+        "serial_request_precision_requests_per_s": len(reqs) / t_mix,
+        "server_saturated": {"p50_ms": q(lat_sat, 50), "p99_ms": q(lat_sat, 99),
+                             "requests_per_s": len(reqs) / makespan_sat},
+    }
+    print(json.dumps(out))
+
+
+if __name__ == "__main__":
+    main()
