@@ -35,7 +35,7 @@
 extern "C" {
 #endif
 
-#define LINQT_ABI_VERSION 1
+#define LINQT_ABI_VERSION 2
 
 enum {
   LINQT_OK = 0,
@@ -110,6 +110,14 @@ int linqt_op_multiply(linqt_session *s, const linqt_op *op, const double a[2], c
 /* Gershgorin bounds of the Hermitian operator in FP64 on the device (replaces
  * utility::SpectralBounds, src/chebyshev_solver.cpp:8-23, which reads ./BOUNDS). */
 int linqt_spectral_bounds(linqt_session *s, const linqt_op *op, double *lo, double *hi);
+
+/* ---- states -------------------------------------------------------------- */
+/* R random-phase states r_i = exp(i phi_i)/sqrt(N), phi = 2 pi u, written R x N
+ * (state-major, interleaved complex) to device memory.  u comes from Philox4x32-10 with
+ * key = seed and counter = (index lo, index hi, 0, 0), index = r*N + i; u = (x >> 11) 2^-53
+ * with x = (w0 << 32) | w1.  Replaces the phase filler qstates::FillWithRandomPhase
+ * (include/quantum_states.hpp:231-252), which LinQT declares but never calls. */
+int linqt_random_phase_states_dev(linqt_session *s, int N, int R, unsigned long long seed, double *states_dev);
 
 /* ---- moment solvers ------------------------------------------------------ */
 /* chebyshev::SpectralMoments (src/chebyshev_solver.cpp:176-199): mu[2*M] =
@@ -206,16 +214,19 @@ typedef struct linqt_request {
   int kind;              /* LINQT_REQ_* */
   const linqt_op *H;     /* rescaled Hamiltonian (device resident) */
   const linqt_op *op;    /* DOS: optional operator; Kubo: velocity used on both sides */
-  const double *states;  /* host, R x N (copied at submit) */
+  const double *states;  /* host, R x N (copied at submit); NULL: random phases from seed, made on the device */
   int R, M;
   int precision;         /* LINQT_PREC_* */
   double *mu_out;        /* host result buffer: 2*M (DOS) or 2*M*M (Kubo) */
+  unsigned long long seed; /* states == NULL: as linqt_random_phase_states_dev(N = H's dimension, R, seed) */
 } linqt_request;
 int linqt_server_create(int device, size_t hbm_budget_bytes, int max_active, linqt_server **out);
 int linqt_server_submit(linqt_server *srv, const linqt_request *req, long *ticket);
 /* status: 0 pending, 1 running, 2 done, <0 error code; latency in ms once done */
 int linqt_server_poll(linqt_server *srv, long ticket, int *status, double *latency_ms);
 int linqt_server_wait_all(linqt_server *srv);
+/* forget a finished request (its ticket becomes unknown); LINQT_ERR_INVALID while it is queued or running */
+int linqt_server_release(linqt_server *srv, long ticket);
 int linqt_server_destroy(linqt_server *srv);
 
 #ifdef __cplusplus

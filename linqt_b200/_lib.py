@@ -38,12 +38,13 @@ class Opts(ctypes.Structure):
 
 class Request(ctypes.Structure):
     _fields_ = [("kind", c_int), ("H", c_void_p), ("op", c_void_p), ("states", P_double), ("R", c_int),
-                ("M", c_int), ("precision", c_int), ("mu_out", P_double)]
+                ("M", c_int), ("precision", c_int), ("mu_out", P_double), ("seed", ctypes.c_ulonglong)]
 
 
 # name -> (restype, argtypes)
 SIGNATURES = {
     "linqt_abi_version": (c_int, []),
+    "linqt_random_phase_states_dev": (c_int, [c_void_p, c_int, c_int, ctypes.c_ulonglong, c_void_p]),
     "linqt_last_error": (ctypes.c_char_p, []),
     "linqt_session_create": (c_int, [c_int, ctypes.POINTER(c_void_p)]),
     "linqt_session_destroy": (c_int, [c_void_p]),
@@ -86,10 +87,14 @@ SIGNATURES = {
     "linqt_server_submit": (c_int, [c_void_p, ctypes.POINTER(Request), P_long]),
     "linqt_server_poll": (c_int, [c_void_p, c_long, P_int, P_double]),
     "linqt_server_wait_all": (c_int, [c_void_p]),
+    "linqt_server_release": (c_int, [c_void_p, c_long]),
     "linqt_server_destroy": (c_int, [c_void_p]),
 }
 
 _lib = None
+
+
+ABI_VERSION = 2  # LINQT_ABI_VERSION of include/linqt_gpu.h
 
 
 def load():
@@ -104,6 +109,9 @@ def load():
             f = getattr(L, name)
             f.restype = res
             f.argtypes = args
+        if L.linqt_abi_version() != ABI_VERSION:
+            raise RuntimeError("liblinqt_gpu.so has ABI version %d, the bindings expect %d: rebuild it"
+                               % (L.linqt_abi_version(), ABI_VERSION))
         _lib = L
     return _lib
 

@@ -205,6 +205,12 @@ def moments1d(H, op, states, M, opts=None, session=None):
     return mu
 
 
+def random_phase_states_dev(N, R, seed, out_dev, session=None):
+    """R random-phase states (R x N complex128, device) from the seeded Philox generator;
+    equal to lattices.random_phase_states(N, R, seed) up to the last bit of sin/cos."""
+    check(load().linqt_random_phase_states_dev(_sh(session), N, R, seed, ctypes.c_void_p(_ptr(out_dev))))
+
+
 def moments1d_dev(H, op, states_dev, R, M, mu_dev, opts=None, session=None):
     o = opts or make_opts()
     check(load().linqt_moments1d_dev(_sh(session), H.h, _oph(op), ctypes.c_void_p(_ptr(states_dev)), R, M,

@@ -53,27 +53,27 @@ static void init_session(Session &s, int device) {
   s.sm_count = sms;
 }
 
+// Workspaces come from the device's stream-ordered memory pool: growing or trimming a
+// buffer is a cudaFreeAsync on the session stream, which (unlike cudaFree) does not
+// synchronise the device, so sessions on other streams keep running.
 void *Session::get(const std::string &name, size_t bytes) {
   if (bytes == 0) bytes = 16;
   auto it = ws.find(name);
   if (it != ws.end() && it->second.second >= bytes) return it->second.first;
   if (it != ws.end()) {
-    LQ_CUDA(cudaStreamSynchronize(stream));
-    LQ_CUDA(cudaFree(it->second.first));
+    LQ_CUDA(cudaFreeAsync(it->second.first, stream));
     ws.erase(it);
   }
-  if (hbm_budget) {
-    size_t used = 0;
-    for (auto &kv : ws) used += kv.second.second;
-    if (used + bytes > hbm_budget)
-      fail(LINQT_ERR_NOMEM, "workspace '" + name + "' exceeds the session HBM budget");
-  }
   void *p = nullptr;
-  cudaError_t e = cudaMalloc(&p, bytes);
+  cudaError_t e = cudaMallocAsync(&p, bytes, stream);
   if (e != cudaSuccess) {
     cudaGetLastError();
-    fail(LINQT_ERR_NOMEM, "cudaMalloc(" + std::to_string(bytes) + ") for '" + name + "' failed: " +
+    fail(LINQT_ERR_NOMEM, "cudaMallocAsync(" + std::to_string(bytes) + ") for '" + name + "' failed: " +
                               cudaGetErrorString(e));
+  }
+  if ((uintptr_t)p & 255) {  // the TMA descriptors and vector loads rely on this
+    cudaFreeAsync(p, stream);
+    fail(LINQT_ERR_INTERNAL, "workspace '" + name + "' is not 256-byte aligned");
   }
   // counters used by the last-block reductions must start at zero
   if (name.find("counter") != std::string::npos || name.find("barrier") != std::string::npos)
@@ -83,9 +83,9 @@ void *Session::get(const std::string &name, size_t bytes) {
 }
 
 void Session::trim() {
-  if (stream) cudaStreamSynchronize(stream);
-  for (auto &kv : ws) cudaFree(kv.second.first);
+  for (auto &kv : ws) cudaFreeAsync(kv.second.first, stream);
   ws.clear();
+  if (stream) cudaStreamSynchronize(stream);
 }
 
 Session::~Session() {
@@ -567,16 +567,18 @@ static void kubo_fft_dev(Session *s, const DeviceOp &H, const DeviceOp *opl, con
 }
 
 void moments1d_for_server(Session *s, const DeviceOp &H, const DeviceOp *op, const double2 *states, int R, int M,
-                          int precision, double2 *mu) {
+                          int precision, int block_width, double2 *mu) {
   linqt_opts o = defaults(nullptr);
   o.precision = precision;
+  o.block_width = block_width;
   moments1d_dev(s, H, op, states, R, M, o, mu);
 }
 
 void moments2d_for_server(Session *s, const DeviceOp &H, const DeviceOp *opl, const DeviceOp *opr,
-                          const double2 *states, int R, int M, int precision, double2 *mu) {
+                          const double2 *states, int R, int M, int precision, int block_width, double2 *mu) {
   linqt_opts o = defaults(nullptr);
   o.precision = precision;
+  o.block_width = block_width;
   moments2d_dev(s, H, opl, opr, states, R, M, o, mu);
 }
 
@@ -886,6 +888,13 @@ int linqt_spectral_bounds(linqt_session *s, const linqt_op *op, double *lo, doub
     check_op(op, "op");
     LQ_REQUIRE(lo && hi, "NULL output");
     gershgorin(resolve(s), op->op, lo, hi);
+  });
+}
+
+int linqt_random_phase_states_dev(linqt_session *s, int N, int R, unsigned long long seed, double *states_dev) {
+  return guarded([&] {
+    LQ_REQUIRE(states_dev, "NULL pointer");
+    random_phase_states(resolve(s), N, R, seed, (double2 *)states_dev);
   });
 }
 

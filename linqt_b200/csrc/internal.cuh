@@ -158,7 +158,7 @@ struct Session {
   double phase_ms[4] = {0, 0, 0, 0};
   long phase_launches[4] = {0, 0, 0, 0};
   int sm_count = 148;
-  size_t hbm_budget = 0;  // 0 = no limit beyond the device
+  size_t hbm_budget = 0;  // chunking budget; 0 = what the device has free
   bool barrier_used = false;  // a persistent kernel ran since the last error check
 
   void *get(const std::string &name, size_t bytes);  // cached device buffer, >= bytes
@@ -212,6 +212,8 @@ void mu_contract(Session *s, const void *L, const void *Rv, int M, long K, bool 
                  double2 *mu_raw);
 void mu_finalize(Session *s, const double2 *mu_raw, int M, int R, double2 *mu);
 void reduce_parts_into(Session *s, const double2 *part, int S, long MM, double2 *dst);
+// R random-phase states (R x N, state-major) from Philox4x32-10 with the given seed (states.cu)
+void random_phase_states(Session *s, int N, int R, unsigned long long seed, double2 *out);
 // tcgen05 split-TF32 contraction of FP32 Chebyshev blocks (mu_tc.cu)
 bool mu_tc_supported(long K);
 void mu_contract_tc(Session *s, const void *L, const void *Rv, int M, long K, double2 *mu_raw);

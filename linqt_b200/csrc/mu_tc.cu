@@ -360,8 +360,9 @@ int mu_tc_check_error(Session *s) {
   auto it = s->ws.find("mu_tc_err_barrier");
   if (it == s->ws.end()) return 0;
   int h = 0;
-  LQ_CUDA(cudaMemcpy(&h, it->second.first, sizeof(int), cudaMemcpyDeviceToHost));
-  if (h) LQ_CUDA(cudaMemset(it->second.first, 0, sizeof(int)));
+  LQ_CUDA(cudaMemcpyAsync(&h, it->second.first, sizeof(int), cudaMemcpyDeviceToHost, s->stream));
+  LQ_CUDA(cudaStreamSynchronize(s->stream));
+  if (h) LQ_CUDA(cudaMemsetAsync(it->second.first, 0, sizeof(int), s->stream));
   return h;
 }
 

@@ -16,6 +16,9 @@
 //
 // Vectors written in one step are read by other CTAs in the next, so vector loads use
 // ld.global.cg (L2, bypassing the non-coherent L1); the operators use the read-only path.
+#include <memory>
+#include <unordered_map>
+
 #include "internal.cuh"
 
 namespace linqt {
@@ -337,25 +340,65 @@ int coop_setup(const void *func, int sm_count, const DeviceOp &H, const DeviceOp
   int per_sm = 0;
   LQ_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, func, kThreads, 0));
   if (per_sm <= 0) fail(LINQT_ERR_UNSUPPORTED, "persistent recursion: kernel does not fit on an SM");
-  int grid = (int)std::max(1L, std::min((long)per_sm * sm_count, need));
+  const int grid0 = (int)std::max(1L, std::min((long)per_sm * sm_count, need));
   const size_t limit = 96 * 1024;
-  size_t bytes = max_slice_bytes(H, V, grid, esz);
-  if (bytes <= limit) {
-    LQ_CUDA(cudaFuncSetAttribute(func, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes));
-    int per_sm2 = 0;
-    LQ_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm2, func, kThreads, bytes));
-    const int grid2 = (int)std::max(1L, std::min((long)per_sm2 * sm_count, need));
-    if (grid2 < grid) {  // fewer CTAs fit with the cache: recompute the slices
-      grid = grid2;
-      bytes = max_slice_bytes(H, V, grid, esz);
-    }
-    if (per_sm2 > 0 && bytes <= limit) {
+  // the attribute is per function and shared by all threads: always the same value
+  LQ_CUDA(cudaFuncSetAttribute(func, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)limit));
+  // Fewer CTAs fit with the cache, and fewer CTAs have larger slices: shrink the grid
+  // until the slices of `grid` CTAs fit `grid` co-resident CTAs.
+  int grid = grid0;
+  for (int it = 0; it < 16; ++it) {
+    const size_t bytes = max_slice_bytes(H, V, grid, esz);
+    if (bytes > limit) break;
+    int p = 0;
+    LQ_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&p, func, kThreads, bytes));
+    if (p <= 0) break;
+    const int g = (int)std::max(1L, std::min((long)p * sm_count, need));
+    if (g >= grid) {
       *smem = bytes;
       return grid;
     }
+    grid = g;
   }
   *smem = 0;
-  return grid;
+  return grid0;
+}
+
+// Cooperative kernels of all sessions on a device run one after another on one lane
+// stream.  A grid barrier needs every CTA of its grid resident; two persistent grids
+// that each fill the device, launched from two sessions' streams, could hold half the
+// SMs each and wait on each other until the spin limit.  The session stream hands over
+// to the lane with an event and waits for the kernel with another, so the order seen
+// by the caller's stream is unchanged.
+struct CoopLane {
+  std::mutex mu;
+  cudaStream_t stream = nullptr;
+};
+
+void coop_launch(Session *s, const void *f, int grid, void **args, size_t smem) {
+  static std::mutex table_mu;
+  static std::unordered_map<int, std::unique_ptr<CoopLane>> lanes;
+  CoopLane *lane;
+  {
+    std::lock_guard<std::mutex> g(table_mu);
+    auto &p = lanes[s->device];
+    if (!p) {
+      p.reset(new CoopLane);
+      LQ_CUDA(cudaStreamCreateWithFlags(&p->stream, cudaStreamNonBlocking));
+    }
+    lane = p.get();
+  }
+  std::lock_guard<std::mutex> g(lane->mu);
+  cudaEvent_t in, out;
+  LQ_CUDA(cudaEventCreateWithFlags(&in, cudaEventDisableTiming));
+  LQ_CUDA(cudaEventCreateWithFlags(&out, cudaEventDisableTiming));
+  LQ_CUDA(cudaEventRecord(in, s->stream));
+  LQ_CUDA(cudaStreamWaitEvent(lane->stream, in, 0));
+  LQ_CUDA(cudaLaunchCooperativeKernel(f, dim3(grid), dim3(kThreads), args, smem, lane->stream));
+  LQ_CUDA(cudaEventRecord(out, lane->stream));
+  LQ_CUDA(cudaStreamWaitEvent(s->stream, out, 0));
+  LQ_CUDA(cudaEventDestroy(in));
+  LQ_CUDA(cudaEventDestroy(out));
 }
 
 template <class T, int TPR, int VPT>
@@ -376,7 +419,7 @@ struct LRF {
     int cache = smem > 0;
     void *args[] = {&n,    (void *)&H.d_rowptr, (void *)&H.d_col, (void *)&hv, (void *)&vrp, (void *)&vci,
                     (void *)&vv, &L, &Rs, (void *)&ph, &tbuf, &M, &blk, &bar, &cache};
-    LQ_CUDA(cudaLaunchCooperativeKernel(f, dim3(grid), dim3(kThreads), args, smem, s->stream));
+    coop_launch(s, f, grid, args, smem);
   }
 };
 
@@ -397,7 +440,7 @@ struct OneDF {
     C *xx = (C *)x0, *bb = (C *)b1;
     void *args[] = {&n, (void *)&H.d_rowptr, (void *)&H.d_col, (void *)&hv, (void *)&ph, &xx, &bb, &steps, &M, &mode,
                     &partials, &bar, &cache};
-    LQ_CUDA(cudaLaunchCooperativeKernel(f, dim3(grid), dim3(kThreads), args, smem, s->stream));
+    coop_launch(s, f, grid, args, smem);
     k_reduce_step_partials<<<(2 * steps + 255) / 256, 256, 0, s->stream>>>(partials, steps, grid, dots);
     LQ_LAUNCHED();
   }
@@ -457,8 +500,9 @@ void check_device_errors(Session *s) {
   auto it = s->ws.find("rec_barrier");
   if (it != s->ws.end()) {
     Barrier *bar = (Barrier *)it->second.first;
-    LQ_CUDA(cudaMemcpy(&err, &bar->err, sizeof(int), cudaMemcpyDeviceToHost));
-    if (err) LQ_CUDA(cudaMemset(&bar->err, 0, sizeof(int)));
+    LQ_CUDA(cudaMemcpyAsync(&err, &bar->err, sizeof(int), cudaMemcpyDeviceToHost, s->stream));
+    LQ_CUDA(cudaStreamSynchronize(s->stream));
+    if (err) LQ_CUDA(cudaMemsetAsync(&bar->err, 0, sizeof(int), s->stream));
   }
   if (err) fail(LINQT_ERR_TIMEOUT, "persistent recursion: a grid barrier wait expired; results of the solve are invalid");
   if (mu_tc_check_error(s))

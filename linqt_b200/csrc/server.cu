@@ -1,17 +1,21 @@
 // Serving: continuous batching of DOS and Kubo-Bastin solves on one GPU.
 //
 // LinQT has no server (its drivers run one solve per process); this is the request
-// loop of the B200 build.  Requests are queued at submit (states copied to host
-// memory the server owns), admitted in arrival order when an execution slot is free and their
-// estimated device footprint fits in the HBM budget, and run on the slot's own CUDA
-// stream, so solves admitted at different times overlap on the device.  Each slot
-// owns a session whose workspace budget is fixed, which makes the chunking -- and
-// with the fixed-order reductions the result -- independent of what else runs.
+// loop of the B200 build.  Requests are queued at submit (states copied into pinned
+// host blocks the server recycles), admitted in arrival order when an execution slot
+// is free and their estimated device footprint fits in the HBM budget, and run on the
+// slot's own CUDA stream, so solves admitted at different times overlap on the device.
+// Workspaces come from the device's stream-ordered pool, which the server keeps
+// populated up to its budget: a request's buffers are returned with cudaFreeAsync and
+// reused by the next, with no device-wide synchronisation between requests.  Each
+// request's chunking budget is its own footprint, which makes the chunking -- and with
+// the fixed-order reductions the result -- independent of what else runs.
 #include <atomic>
 #include <chrono>
 #include <condition_variable>
 #include <cstring>
 #include <deque>
+#include <map>
 #include <memory>
 #include <thread>
 #include <unordered_map>
@@ -21,9 +25,9 @@
 namespace linqt {
 // solver entry points of api.cu
 void moments1d_for_server(Session *s, const DeviceOp &H, const DeviceOp *op, const double2 *states, int R, int M,
-                          int precision, double2 *mu);
+                          int precision, int block_width, double2 *mu);
 void moments2d_for_server(Session *s, const DeviceOp &H, const DeviceOp *opl, const DeviceOp *opr,
-                          const double2 *states, int R, int M, int precision, double2 *mu);
+                          const double2 *states, int R, int M, int precision, int block_width, double2 *mu);
 }  // namespace linqt
 
 using namespace linqt;
@@ -35,8 +39,10 @@ typedef std::chrono::steady_clock clk;
 struct Job {
   long ticket = 0;
   linqt_request req{};
-  std::vector<double2> states;  // host copy
+  void *states = nullptr;  // pinned host copy (server pool); NULL: generated on the device
+  size_t states_cap = 0;
   size_t footprint = 0;
+  int block_width = 1;
   int status = 0;  // 0 pending, 1 running, 2 done, <0 error
   double latency_ms = 0;
   std::string error;
@@ -44,19 +50,26 @@ struct Job {
 };
 
 // Device bytes a request may hold: every workspace of the solver it runs (state copy,
-// Chebyshev blocks, per-step partials, contraction partials), with the same block width
-// the solver picks when the budget allows it.
-size_t estimate_footprint(const linqt_request &r, int n, int sm_count) {
-  int Rc = 1;
-  while (Rc < r.R && Rc < 256) Rc <<= 1;
+// Chebyshev blocks, per-step partials, contraction partials) at vector-block width Rc.
+size_t estimate_footprint(const linqt_request &r, int n, int sm_count, int Rc) {
   const size_t esz = r.precision == LINQT_PREC_FP64 ? sizeof(double2) : sizeof(float2);
   const size_t io = sizeof(double2) * ((size_t)r.R * n + (size_t)r.M * (r.kind == LINQT_REQ_DOS ? 1 : r.M));
   if (r.kind == LINQT_REQ_DOS) {
-    const size_t steps = (size_t)r.M / 2 + 1;
-    return io + esz * (size_t)n * Rc * 3 + sizeof(double2) * (2 * steps * ((size_t)sm_count * 32 + 1) + 2 * steps) +
-           (1 << 20);
+    const size_t steps = (size_t)r.M / 2 + 1, chunks = (r.R + Rc - 1) / Rc;
+    return io + esz * (size_t)n * Rc * 3 +
+           sizeof(double2) * (2 * steps * ((size_t)sm_count * 32 + 1) + 2 * steps * chunks) + (1 << 20);
   }
   return io + esz * (size_t)n * Rc * (2 * (size_t)r.M + 4) + sizeof(double2) * (size_t)r.M * r.M * 66 + (1 << 20);
+}
+
+// Vector-block width of a request: the widest power of two up to R whose footprint fits in
+// `cap` (the server's budget shared by its slots), so that one large request cannot hold
+// the device alone; width 1 when none does.
+int pick_width(const linqt_request &r, int n, int sm_count, size_t cap) {
+  int Rc = 1;
+  while (Rc < r.R && Rc < 256) Rc <<= 1;
+  while (Rc > 1 && estimate_footprint(r, n, sm_count, Rc) > cap) Rc >>= 1;
+  return Rc;
 }
 
 }  // namespace
@@ -73,6 +86,37 @@ struct linqt_server {
   int running = 0;
   bool stop = false;
   std::vector<std::thread> workers;
+  // pinned host blocks by power-of-two capacity, recycled across requests
+  std::multimap<size_t, void *> pinned_free;
+  std::vector<void *> pinned_all;
+  cudaMemPool_t pool = nullptr;
+  uint64_t old_threshold = 0;
+
+  void *pinned_get(size_t bytes, size_t *cap) {
+    size_t c = 4096;
+    while (c < bytes) c <<= 1;
+    {
+      std::lock_guard<std::mutex> g(mu);
+      auto it = pinned_free.lower_bound(c);
+      if (it != pinned_free.end() && it->first <= 4 * c) {
+        void *p = it->second;
+        *cap = it->first;
+        pinned_free.erase(it);
+        return p;
+      }
+    }
+    void *p = nullptr;
+    LQ_CUDA(cudaMallocHost(&p, c));
+    {
+      std::lock_guard<std::mutex> g(mu);
+      pinned_all.push_back(p);
+    }
+    *cap = c;
+    return p;
+  }
+  void pinned_put_locked(void *p, size_t cap) {
+    if (p) pinned_free.emplace(cap, p);
+  }
 
   void worker() {
     std::unique_ptr<linqt_session> sess(new linqt_session);
@@ -100,6 +144,8 @@ struct linqt_server {
       }
       int rc = 0;
       std::string err;
+      void *res_host = nullptr;
+      size_t res_cap = 0;
       try {
         Session &s = sess->s;
         const DeviceOp &H = job->req.H->op;
@@ -110,15 +156,20 @@ struct linqt_server {
         s.hbm_budget = job->footprint;  // fixed per request: chunking independent of the other requests
         double2 *d_st = (double2 *)s.get("io_states", sb);
         double2 *d_mu = (double2 *)s.get("io_mu", mb);
-        LQ_CUDA(cudaMemcpyAsync(d_st, job->states.data(), sb, cudaMemcpyHostToDevice, s.stream));
-        if (job->req.kind == LINQT_REQ_DOS)
-          moments1d_for_server(&s, H, op, d_st, R, M, job->req.precision, d_mu);
+        res_host = pinned_get(mb, &res_cap);
+        if (job->states)
+          LQ_CUDA(cudaMemcpyAsync(d_st, job->states, sb, cudaMemcpyHostToDevice, s.stream));
         else
-          moments2d_for_server(&s, H, op, op, d_st, R, M, job->req.precision, d_mu);
-        LQ_CUDA(cudaMemcpyAsync(job->req.mu_out, d_mu, mb, cudaMemcpyDeviceToHost, s.stream));
+          random_phase_states(&s, n, R, job->req.seed, d_st);
+        if (job->req.kind == LINQT_REQ_DOS)
+          moments1d_for_server(&s, H, op, d_st, R, M, job->req.precision, job->block_width, d_mu);
+        else
+          moments2d_for_server(&s, H, op, op, d_st, R, M, job->req.precision, job->block_width, d_mu);
+        LQ_CUDA(cudaMemcpyAsync(res_host, d_mu, mb, cudaMemcpyDeviceToHost, s.stream));
         LQ_CUDA(cudaStreamSynchronize(s.stream));
         check_device_errors(&s);
-        s.trim();
+        s.trim();  // stream-ordered frees back to the pool for the next request
+        std::memcpy(job->req.mu_out, res_host, mb);
       } catch (const Error &e) {
         rc = e.code;
         err = e.what();
@@ -134,8 +185,9 @@ struct linqt_server {
         job->status = rc ? rc : 2;
         job->error = err;
         job->latency_ms = std::chrono::duration<double, std::milli>(clk::now() - job->t_submit).count();
-        job->states.clear();
-        job->states.shrink_to_fit();
+        pinned_put_locked(job->states, job->states_cap);
+        pinned_put_locked(res_host, res_cap);
+        job->states = nullptr;
       }
       cv.notify_all();
       done_cv.notify_all();
@@ -159,6 +211,11 @@ int linqt_server_create(int device, size_t hbm_budget_bytes, int max_active, lin
     s->budget = hbm_budget_bytes ? hbm_budget_bytes : (size_t)(fr * 0.8);
     s->max_active = max_active;
     LQ_CUDA(cudaDeviceGetAttribute(&s->sm_count, cudaDevAttrMultiProcessorCount, device));
+    // keep up to the budget cached in the device pool between requests (restored at destroy)
+    LQ_CUDA(cudaDeviceGetDefaultMemPool(&s->pool, device));
+    LQ_CUDA(cudaMemPoolGetAttribute(s->pool, cudaMemPoolAttrReleaseThreshold, &s->old_threshold));
+    uint64_t thr = s->budget;
+    LQ_CUDA(cudaMemPoolSetAttribute(s->pool, cudaMemPoolAttrReleaseThreshold, &thr));
     for (int i = 0; i < max_active; ++i) s->workers.emplace_back([p = s.get()] { p->worker(); });
     *out = s.release();
     return LINQT_OK;
@@ -170,17 +227,22 @@ int linqt_server_create(int device, size_t hbm_budget_bytes, int max_active, lin
 
 int linqt_server_submit(linqt_server *srv, const linqt_request *req, long *ticket) {
   try {
-    if (!srv || !req || !ticket || !req->H || !req->states || !req->mu_out) fail(LINQT_ERR_INVALID, "server: NULL");
+    if (!srv || !req || !ticket || !req->H || !req->mu_out) fail(LINQT_ERR_INVALID, "server: NULL");
     if (req->R <= 0 || req->M <= 0) fail(LINQT_ERR_INVALID, "server: R and M must be positive");
     if (req->kind != LINQT_REQ_DOS && req->kind != LINQT_REQ_KUBO_BASTIN) fail(LINQT_ERR_INVALID, "server: kind");
     auto job = std::make_shared<Job>();
     job->req = *req;
     const int n = req->H->op.n;
-    job->states.assign((const double2 *)req->states, (const double2 *)req->states + (size_t)req->R * n);
-    job->footprint = estimate_footprint(*req, n, srv->sm_count);
+    job->block_width = pick_width(*req, n, srv->sm_count, srv->budget / srv->max_active);
+    job->footprint = estimate_footprint(*req, n, srv->sm_count, job->block_width);
     if (job->footprint > srv->budget)
       fail(LINQT_ERR_NOMEM, "server: request footprint " + std::to_string(job->footprint >> 20) +
                                 " MiB exceeds the HBM budget");
+    if (req->states) {
+      const size_t sb = sizeof(double2) * (size_t)req->R * n;
+      job->states = srv->pinned_get(sb, &job->states_cap);
+      std::memcpy(job->states, req->states, sb);
+    }
     job->t_submit = clk::now();
     {
       std::lock_guard<std::mutex> g(srv->mu);
@@ -224,6 +286,21 @@ int linqt_server_wait_all(linqt_server *srv) {
   return LINQT_OK;
 }
 
+int linqt_server_release(linqt_server *srv, long ticket) {
+  if (!srv) {
+    set_last_error("server: NULL");
+    return LINQT_ERR_INVALID;
+  }
+  std::lock_guard<std::mutex> g(srv->mu);
+  auto it = srv->jobs.find(ticket);
+  if (it == srv->jobs.end() || it->second->status == 0 || it->second->status == 1) {
+    set_last_error("server: release of an unknown or unfinished ticket");
+    return LINQT_ERR_INVALID;
+  }
+  srv->jobs.erase(it);
+  return LINQT_OK;
+}
+
 int linqt_server_destroy(linqt_server *srv) {
   if (!srv) return LINQT_OK;
   {
@@ -232,6 +309,11 @@ int linqt_server_destroy(linqt_server *srv) {
   }
   srv->cv.notify_all();
   for (auto &t : srv->workers) t.join();
+  for (void *p : srv->pinned_all) cudaFreeHost(p);
+  if (srv->pool) {
+    cudaMemPoolSetAttribute(srv->pool, cudaMemPoolAttrReleaseThreshold, &srv->old_threshold);
+    cudaMemPoolTrimTo(srv->pool, 0);
+  }
   delete srv;
   return LINQT_OK;
 }

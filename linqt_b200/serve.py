@@ -16,7 +16,8 @@ import numpy as np
 
 from . import lattices
 from ._lib import Request, check, load
-from .core import PREC_FP64, PREC_MIXED, Operator, moments1d, moments2d, make_opts
+from .core import (PREC_FP64, PREC_MIXED, Operator, Session, make_opts, moments1d_dev, moments2d_dev,
+                   random_phase_states_dev)
 
 REQ_DOS, REQ_KUBO_BASTIN = 0, 1
 
@@ -28,13 +29,21 @@ class Server:
         self.h = h
         self._keep = {}
 
-    def submit(self, kind, H, op, states, M, precision=PREC_FP64):
-        st = np.ascontiguousarray(np.atleast_2d(states), dtype=np.complex128)
-        R = st.shape[0]
-        out = np.zeros(M if kind == REQ_DOS else M * M, np.complex128)
+    def submit(self, kind, H, op, states, M, precision=PREC_FP64, R=None, seed=None):
+        """Queue one request.  `states` (R x N, host) are copied at submit; with states=None
+        the server makes R random-phase states on the device from `seed`."""
         req = Request()
+        if states is not None:
+            st = np.ascontiguousarray(np.atleast_2d(states), dtype=np.complex128)
+            R = st.shape[0]
+            req.states = st.view(np.float64).ctypes.data_as(ctypes.POINTER(ctypes.c_double))
+        else:
+            if R is None or seed is None:
+                raise ValueError("states=None needs R and seed")
+            req.states = None
+            req.seed = seed
+        out = np.zeros(M if kind == REQ_DOS else M * M, np.complex128)
         req.kind, req.H, req.op = kind, H.h, (op.h if op is not None else None)
-        req.states = st.view(np.float64).ctypes.data_as(ctypes.POINTER(ctypes.c_double))
         req.R, req.M, req.precision = R, M, precision
         req.mu_out = out.view(np.float64).ctypes.data_as(ctypes.POINTER(ctypes.c_double))
         t = ctypes.c_long()
@@ -50,6 +59,11 @@ class Server:
     def result(self, ticket):
         out, _, _, M, kind = self._keep[ticket]
         return out if kind == REQ_DOS else out.reshape(M, M)
+
+    def release(self, ticket):
+        """Forget a finished request: the server's record and the Python-side buffers."""
+        check(load().linqt_server_release(self.h, ticket))
+        self._keep.pop(ticket, None)
 
     def wait_all(self):
         check(load().linqt_server_wait_all(self.h))
@@ -107,7 +121,8 @@ def request_stream(n_requests=200, seed=52, arrival_seed=51, n_min=1e4, n_max=2e
 
 
 def _prepare(reqs, session=None):
-    """Operators (device resident) and states per request; lattices shared by family and size."""
+    """Device-resident operators per request (lattices shared by family and size) and the
+    seed of each request's random-phase states."""
     cache = {}
     prepared = []
     for i, r in enumerate(reqs):
@@ -119,38 +134,51 @@ def _prepare(reqs, session=None):
             Vg = Operator.from_csr(N, *V, session=session) if V is not None else None
             cache[key] = (N, Hg, Vg)
         N, Hg, Vg = cache[key]
-        st = lattices.random_phase_states(N, r["R"], seed=1000 + i)
-        prepared.append((Hg, Vg, st))
+        prepared.append((Hg, Vg, 1000 + i))
     return prepared
 
 
-def run_serial(reqs, prepared, fp64_only=True):
-    """The same stream one request at a time on the plain FP64 path (host API)."""
+def run_serial(reqs, prepared, fp64_only=True, session=None):
+    """The same stream one request at a time on the plain FP64 path: states made on the device
+    from the request's seed, the solver's device entry point, the moments read back to the host.
+    Pass a `session` bound to torch's current stream to keep its workspaces across calls."""
+    import torch
+    sess = session or Session(stream=torch.cuda.current_stream().cuda_stream)  # ordered with torch's copies
     t0 = time.perf_counter()
     lat = []
-    for r, (Hg, Vg, st) in zip(reqs, prepared):
+    for r, (Hg, Vg, seed) in zip(reqs, prepared):
         t = time.perf_counter()
         o = make_opts(precision=PREC_FP64 if fp64_only else r["precision"])
+        N, R, M = Hg.n, r["R"], r["M"]
+        st = torch.empty(2 * R * N, dtype=torch.float64, device="cuda")
+        random_phase_states_dev(N, R, seed, st, session=sess)
         if r["kind"] == REQ_DOS:
-            moments1d(Hg, None, st, r["M"], opts=o)
+            mu = torch.empty(2 * M, dtype=torch.float64, device="cuda")
+            moments1d_dev(Hg, None, st, R, M, mu, opts=o, session=sess)
         else:
-            moments2d(Hg, Vg, Vg, st, r["M"], opts=o)
+            mu = torch.empty(2 * M * M, dtype=torch.float64, device="cuda")
+            moments2d_dev(Hg, Vg, Vg, st, R, M, mu, opts=o, session=sess)
+        mu.cpu()
         lat.append(1e3 * (time.perf_counter() - t))
-    return time.perf_counter() - t0, np.array(lat)
+    t_total = time.perf_counter() - t0
+    if session is None:
+        sess.close()
+    return t_total, np.array(lat)
 
 
-def run_stream(reqs, prepared, gaps, mean_gap_s, max_active=4, hbm_budget_bytes=0, device=0):
-    """Replay the stream with arrival times cumsum(gaps) * mean_gap_s; returns (latencies ms, makespan s)."""
-    srv = Server(device, hbm_budget_bytes, max_active)
+def run_stream(reqs, prepared, gaps, mean_gap_s, max_active=4, hbm_budget_bytes=0, device=0, server=None):
+    """Replay the stream with arrival times cumsum(gaps) * mean_gap_s; returns (latencies ms, makespan s).
+    A given `server` is reused (and stays open); otherwise one is created for the run."""
+    srv = server if server is not None else Server(device, hbm_budget_bytes, max_active)
     arrivals = np.cumsum(gaps) * mean_gap_s
     tickets = []
     t0 = time.perf_counter()
-    for i, (r, (Hg, Vg, st)) in enumerate(zip(reqs, prepared)):
+    for i, (r, (Hg, Vg, seed)) in enumerate(zip(reqs, prepared)):
         now = time.perf_counter() - t0
         if arrivals[i] > now:
             time.sleep(arrivals[i] - now)
         op = Vg if r["kind"] == REQ_KUBO_BASTIN else None
-        tickets.append(srv.submit(r["kind"], Hg, op, st, r["M"], r["precision"]))
+        tickets.append(srv.submit(r["kind"], Hg, op, None, r["M"], r["precision"], R=r["R"], seed=seed))
     srv.wait_all()
     makespan = time.perf_counter() - t0
     lat = []
@@ -159,7 +187,9 @@ def run_stream(reqs, prepared, gaps, mean_gap_s, max_active=4, hbm_budget_bytes=
         if status != 2:
             raise RuntimeError("request %d ended with status %d" % (t, status))
         lat.append(ms)
-    srv.close()
+        srv.release(t)
+    if server is None:
+        srv.close()
     return np.array(lat), makespan
 
 
@@ -179,7 +209,7 @@ def main(argv=None):
     import json
     ap = argparse.ArgumentParser()
     ap.add_argument("--requests", type=int, default=200)
-    ap.add_argument("--load", type=float, default=1.0,
+    ap.add_argument("--load", type=float, default=1.5,
                     help="offered load: arrival rate / serial FP64 service rate")
     ap.add_argument("--max-active", type=int, default=4)
     ap.add_argument("--n-max", type=float, default=2e5)
@@ -198,14 +228,24 @@ def main(argv=None):
             for prec in (PREC_FP64, PREC_MIXED):
                 warm_r.append(dict(r, M=32, precision=prec))
                 warm_p.append(p)
-    run_serial(warm_r, warm_p, fp64_only=False)
-    t_ser, svc = run_serial(reqs, prepared, fp64_only=True)
-    t_mix, svc_mix = run_serial(reqs, prepared, fp64_only=False)
+    import torch
+    sess = Session(stream=torch.cuda.current_stream().cuda_stream)
+    run_serial(warm_r, warm_p, fp64_only=False, session=sess)
+    # untimed passes of the whole stream: workspaces, pinned blocks and the device pool
+    # reach their steady-state sizes before anything is timed
+    run_serial(reqs, prepared, fp64_only=True, session=sess)
+    run_serial(reqs, prepared, fp64_only=False, session=sess)
+    srv = Server(0, 0, a.max_active)
+    run_stream(reqs, prepared, np.zeros_like(gaps), 0.0, server=srv)
+    t_ser, svc = run_serial(reqs, prepared, fp64_only=True, session=sess)
+    t_mix, svc_mix = run_serial(reqs, prepared, fp64_only=False, session=sess)
+    sess.close()
     mean_gap = t_ser / len(reqs) / a.load
     arrivals = np.cumsum(gaps) * mean_gap
     lat_ser = 1e3 * fifo_latencies(arrivals, svc / 1e3)
-    lat, makespan = run_stream(reqs, prepared, gaps, mean_gap, max_active=a.max_active)
-    lat_sat, makespan_sat = run_stream(reqs, prepared, np.zeros_like(gaps), 0.0, max_active=a.max_active)
+    lat, makespan = run_stream(reqs, prepared, gaps, mean_gap, server=srv)
+    lat_sat, makespan_sat = run_stream(reqs, prepared, np.zeros_like(gaps), 0.0, server=srv)
+    srv.close()
     q = lambda x, p: float(np.percentile(x, p))
     out = {
         "metric": "serving_stream", "requests": len(reqs), "offered_load": a.load,

@@ -67,3 +67,32 @@ def test_admission_rejects_requests_over_budget():
         srv.submit(serve.REQ_KUBO_BASTIN, Hg, Vg, st, 2048)  # 2 x 2048 blocks of N x 4 complex doubles
     assert e.value.code == -3
     srv.close()
+
+
+def test_device_states_match_host_generator():
+    torch = pytest.importorskip("torch")
+    N, R, seed = 3001, 5, 2024
+    d = torch.empty(2 * R * N, dtype=torch.float64, device="cuda")
+    lq.random_phase_states_dev(N, R, seed, d)
+    got = d.cpu().numpy().view(np.complex128).reshape(R, N)
+    ref = lattices.random_phase_states(N, R, seed)
+    # same Philox words; sin/cos may differ from the host's libm in the last bit
+    assert np.abs(got - ref).max() * np.sqrt(N) <= 4e-16
+
+
+def test_seeded_requests_match_host_states():
+    N, Hg, Vg = _ops("kane_mele", 2500, seed=3)
+    srv = serve.Server(0, 0, 3)
+    t1 = srv.submit(serve.REQ_DOS, Hg, None, None, 120, R=3, seed=77)
+    t2 = srv.submit(serve.REQ_KUBO_BASTIN, Hg, Vg, None, 40, R=2, seed=78)
+    srv.wait_all()
+    st1 = lattices.random_phase_states(N, 3, 77)
+    st2 = lattices.random_phase_states(N, 2, 78)
+    ref1 = lq.moments1d(Hg, None, st1, 120)
+    ref2 = lq.moments2d(Hg, Vg, Vg, st2, 40)
+    assert np.abs(srv.result(t1) - ref1).max() <= 1e-12 * np.abs(ref1).max()
+    assert np.abs(srv.result(t2) - ref2).max() <= 1e-12 * np.abs(ref2).max()
+    srv.release(t1)
+    with pytest.raises(lq.LinqtError):
+        srv.poll(t1)
+    srv.close()
