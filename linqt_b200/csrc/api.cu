@@ -529,43 +529,6 @@ static void moments2d_dev(Session *s, const DeviceOp &H, const DeviceOp *opl, co
 // Kubo_solver_FFT::compute (src/Kubo_solver_FFT.cpp:12-136)
 // ---------------------------------------------------------------------------
 
-static void kubo_fft_dev(Session *s, const DeviceOp &H, const DeviceOp *opl, const DeviceOp *opr,
-                         const double2 *states, int R, int M, int nump, int formula, double bw, double bc,
-                         const linqt_opts &o, double *out) {
-  LQ_REQUIRE(R > 0 && M > 0, "kubo_fft: R and M must be positive");
-  LQ_REQUIRE(nump >= M, "kubo_fft: nump must be >= M (pre_factors are indexed m < M, src/Bastin_FFTs.cpp:18-21)");
-  LQ_REQUIRE(formula == LINQT_KUBO_BASTIN || formula == LINQT_KUBO_GREENWOOD, "kubo_fft: unknown formula");
-  LQ_REQUIRE(bw > 0, "kubo_fft: band_width must be positive");
-  const bool fp32 = prepare_precision(o, H, opl, opr);
-  const int N = H.n;
-  const size_t esz = fp32 ? sizeof(float2) : sizeof(double2);
-  const Chunking ch = pick_chunks(s, N, R, M, esz, o, sizeof(double2) * 2 * (size_t)nump * 1024);
-  const size_t blk = esz * (size_t)N * ch.Rc;
-  char *Ls = (char *)s->get("lr_L", blk * M);
-  char *Rs = (char *)s->get("lr_R", blk * M);
-  char *tmp = (char *)s->get("lr_tmp", blk * 4);
-  double2 *acc = (double2 *)s->get("kubo_acc", sizeof(double2) * 2 * (size_t)nump);
-  double2 *acc_c = (double2 *)s->get("kubo_acc_c", sizeof(double2) * 2 * (size_t)nump);
-  LQ_CUDA(cudaMemsetAsync(acc, 0, sizeof(double2) * 2 * (size_t)nump, s->stream));
-  for (int c = 0; c < ch.nchunks; ++c) {
-    void *phi = tmp + 3 * blk;
-    {
-      PhaseScope ph(s, PH_RECURSION);
-      chunk_block(s, states, N, R, c * ch.Rc, ch.Rc, phi, fp32);
-      ph.launches(1 + lr_vectors(s, H, opl, opr, phi, M, ch.Rc, fp32, Ls, Rs, tmp, o.format, o.step_launches != 0));
-    }
-    {
-      PhaseScope ph(s, PH_FFT);
-      kubo_fft_sites(s, Ls, Rs, (long)N * ch.Rc, M, nump, formula, fp32, acc_c);
-      add_into(s, acc, acc_c, 2 * nump);
-      ph.launches(4);
-    }
-  }
-  PhaseScope ph(s, PH_OTHER);
-  kubo_postprocess(s, acc, R, nump, formula, N, bw, bc, out);
-  ph.launches(1);
-}
-
 void moments1d_for_server(Session *s, const DeviceOp &H, const DeviceOp *op, const double2 *states, int R, int M,
                           int precision, int block_width, double2 *mu) {
   linqt_opts o = defaults(nullptr);
@@ -583,20 +546,23 @@ void moments2d_for_server(Session *s, const DeviceOp &H, const DeviceOp *opl, co
 }
 
 // ---------------------------------------------------------------------------
-// One Kubo-Bastin solve: the L/R blocks are computed once per vector chunk and feed
-// both the moment contraction (CorrelationExpansionMoments) and the per-site FFT
-// reconstruction (Kubo_solver_FFT with formula KUBO_BASTIN).  mu or out may be NULL.
+// One Kubo solve: the L/R blocks are computed once per vector chunk and feed the moment
+// contraction (CorrelationExpansionMoments) and the per-site transforms of
+// Kubo_solver_FFT (formula KUBO_BASTIN or KUBO_GREENWOOD).  mu or out may be NULL.
 // ---------------------------------------------------------------------------
-static void kubo_bastin_dev(Session *s, const DeviceOp &H, const DeviceOp *opl, const DeviceOp *opr,
-                            const double2 *states, int R, int M, int nump, double bw, double bc,
-                            const linqt_opts &o, double2 *mu, double *out) {
-  LQ_REQUIRE(R > 0 && M > 0, "kubo_bastin: R and M must be positive");
-  LQ_REQUIRE(!out || nump >= M, "kubo_bastin: nump must be >= M");
-  LQ_REQUIRE(bw > 0, "kubo_bastin: band_width must be positive");
+static void kubo_solve(Session *s, const DeviceOp &H, const DeviceOp *opl, const DeviceOp *opr,
+                       const double2 *states, int R, int M, int nump, int formula, double bw, double bc,
+                       const linqt_opts &o, double2 *mu, double *out) {
+  LQ_REQUIRE(R > 0 && M > 0, "kubo: R and M must be positive");
+  LQ_REQUIRE(!out || nump >= M, "kubo: nump must be >= M (pre_factors are indexed m < M, src/Bastin_FFTs.cpp:18-21)");
+  LQ_REQUIRE(formula == LINQT_KUBO_BASTIN || formula == LINQT_KUBO_GREENWOOD, "kubo: unknown formula");
+  LQ_REQUIRE(bw > 0, "kubo: band_width must be positive");
   const bool fp32 = prepare_precision(o, H, opl, opr);
   const int N = H.n;
   const size_t esz = fp32 ? sizeof(float2) : sizeof(double2);
-  const size_t extra = sizeof(double2) * ((size_t)M * M * 66 + 2 * (size_t)std::max(nump, 1) * 1024);
+  size_t extra = 0;
+  if (mu) extra += sizeof(double2) * (size_t)M * M * 66;
+  if (out) extra += sizeof(double2) * 2 * (size_t)std::max(nump, 1) * 1024;
   const Chunking ch = pick_chunks(s, N, R, M, esz, o, extra);
   const size_t blk = esz * (size_t)N * ch.Rc;
   char *Ls = (char *)s->get("lr_L", blk * M);
@@ -609,8 +575,8 @@ static void kubo_bastin_dev(Session *s, const DeviceOp &H, const DeviceOp *opl, 
   }
   if (out) {
     acc = (double2 *)s->get("kubo_acc", sizeof(double2) * 2 * (size_t)nump);
-    acc_c = (double2 *)s->get("kubo_acc_c", sizeof(double2) * 2 * (size_t)nump);
     LQ_CUDA(cudaMemsetAsync(acc, 0, sizeof(double2) * 2 * (size_t)nump, s->stream));
+    acc_c = (double2 *)s->get("kubo_acc_c", sizeof(double2) * 2 * (size_t)nump);
   }
   for (int c = 0; c < ch.nchunks; ++c) {
     void *phi = tmp + 3 * blk;
@@ -626,15 +592,27 @@ static void kubo_bastin_dev(Session *s, const DeviceOp &H, const DeviceOp *opl, 
     }
     if (out) {
       PhaseScope ph(s, PH_FFT);
-      kubo_fft_sites(s, Ls, Rs, (long)N * ch.Rc, M, nump, LINQT_KUBO_BASTIN, fp32, acc_c);
+      kubo_fft_sites(s, Ls, Rs, (long)N * ch.Rc, M, nump, formula, fp32, acc_c);
       add_into(s, acc, acc_c, 2 * nump);
       ph.launches(4);
     }
   }
   PhaseScope ph(s, PH_OTHER);
   if (mu) mu_finalize(s, raw, M, R, mu);
-  if (out) kubo_postprocess(s, acc, R, nump, LINQT_KUBO_BASTIN, N, bw, bc, out);
+  if (out) kubo_postprocess(s, acc, R, nump, formula, N, bw, bc, out);
   ph.launches((mu ? 1 : 0) + (out ? 1 : 0));
+}
+
+static void kubo_fft_dev(Session *s, const DeviceOp &H, const DeviceOp *opl, const DeviceOp *opr,
+                         const double2 *states, int R, int M, int nump, int formula, double bw, double bc,
+                         const linqt_opts &o, double *out) {
+  kubo_solve(s, H, opl, opr, states, R, M, nump, formula, bw, bc, o, nullptr, out);
+}
+
+static void kubo_bastin_dev(Session *s, const DeviceOp &H, const DeviceOp *opl, const DeviceOp *opr,
+                            const double2 *states, int R, int M, int nump, double bw, double bc,
+                            const linqt_opts &o, double2 *mu, double *out) {
+  kubo_solve(s, H, opl, opr, states, R, M, nump, LINQT_KUBO_BASTIN, bw, bc, o, mu, out);
 }
 
 // ---------------------------------------------------------------------------

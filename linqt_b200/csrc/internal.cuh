@@ -220,6 +220,8 @@ void mu_contract_tc(Session *s, const void *L, const void *Rv, int M, long K, do
 int mu_tc_check_error(Session *s);
 
 // FFT path: accumulate p/w over all sites into acc[2*nump] (complex)
+// prefactors pf_m of Kubo_solver_FFT (kubo_fft.cu)
+void kubo_prefactors(Session *s, int M, int nump, double2 *pf);
 void kubo_fft_sites(Session *s, const void *L, const void *Rv, long nsites, int M, int nump, int formula,
                     bool fp32_inputs, double2 *acc);
 void kubo_postprocess(Session *s, const double2 *acc, int R, int nump, int formula, int N, double band_width,

@@ -186,34 +186,67 @@ __device__ __forceinline__ void stage_site(Tin *stage, const Tin *__restrict__ L
   cp_async_commit();
 }
 
+// 16-point DFT of a sequence whose upper half is zero (v[8..15] = 0 on entry), same
+// output order as dft16.  The first radix-4 stage reduces to two-point sums.
+__device__ __forceinline__ void dft16_half(double2 (&v)[16]) {
+#pragma unroll
+  for (int r2 = 0; r2 < 4; ++r2) {
+    const double2 a0 = v[r2], a1 = v[4 + r2];
+    v[r2] = cadd(a0, a1);
+    v[8 + r2] = csub(a0, a1);
+    v[4 + r2] = cadd(a0, mul_i(a1));
+    v[12 + r2] = csub(a0, mul_i(a1));
+  }
+#pragma unroll
+  for (int q1 = 1; q1 < 4; ++q1)
+#pragma unroll
+    for (int r2 = 1; r2 < 4; ++r2) v[4 * q1 + r2] = cmul(v[4 * q1 + r2], w16(q1 * r2));
+#pragma unroll
+  for (int q1 = 0; q1 < 4; ++q1) dft4(v[4 * q1], v[4 * q1 + 1], v[4 * q1 + 2], v[4 * q1 + 3]);
+}
+
+// Bastin / Greenwood products from the transforms of one frequency held in registers
+__device__ __forceinline__ void bastin_products_reg(int k, int n, const double2 (&x)[8], double2 &p, double2 &w) {
+  bastin_products(k, n, x, 1, p, w);
+}
+__device__ __forceinline__ void greenwood_product_reg(const double2 (&x)[4], double2 &p) { greenwood_product(x, 1, p); }
+
 // Shared-memory layout (double2 units):
 //   buf   NSEQ * 16 * (P + 1)   the transforms, 16 rows of P (+1 pad) per sequence
-//   tw1   16 * P                w_n^{m1 k2} at [k2 * P + m1]   (pass 1)
+//   tw1   P                     w_n^{m1}                       (pass 1; powers formed in registers)
 //   tw2   16 * R3               w_P^{a c}   at [c * R3 + a]    (pass 2)
 //   pfs   M                     prefactors
 //   stage 2 * 2M                double-buffered bra/ket of the current and next site
-template <int R3, int NSEQ, class Tin>
+//
+// Per site: pass 1 (16-point DFTs over m2 from the staged site, twiddles w_n^{m1 k2},
+// written to row k2), barrier, pass 2 (16-point DFTs over b within each row, in place:
+// an item reads and writes the same 16 slots), barrier, then the last R3-point DFTs and
+// the products straight from registers: thread pair (k2, c) computes the R3-point DFT of
+// every sequence and keeps the outputs d = h, h + 2, ... (h = the thread's half), so no
+// transform is written back.  Bank mapping: consecutive threads take consecutive m1 (pass
+// 1) or consecutive rows k2 (pass 2, final) and the row pitch P + 1 is odd, so every
+// 8-thread phase of a 16-byte access touches 8 distinct bank groups.
+template <int R3, int NSEQ, bool HALF, class Tin>
 __global__ void __launch_bounds__(kFftThreads)
     k_kubo_fft(const Tin *__restrict__ L, const Tin *__restrict__ Rv, long K, long chunk, int M,
                const double2 *__restrict__ pf_g, double2 *__restrict__ part) {
-  constexpr int P = 16 * R3;    // n / 16
-  constexpr int n = 16 * P;     // nump
-  constexpr int ROW = P + 1;    // padded row of the 16 x P arrangement
-  constexpr int SEQ = 16 * ROW; // per-sequence footprint
-  constexpr int KPT = (n + kFftThreads - 1) / kFftThreads;
+  constexpr int P = 16 * R3;     // n / 16
+  constexpr int n = 16 * P;      // nump
+  constexpr int ROW = P + 1;     // padded row of the 16 x P arrangement
+  constexpr int SEQ = 16 * ROW;  // per-sequence footprint
+  constexpr int ND = R3 >= 2 ? R3 / 2 : 1;  // final outputs per thread
   extern __shared__ double2 sm[];
   double2 *buf = sm;
   double2 *tw1 = buf + NSEQ * SEQ;
-  double2 *tw2 = tw1 + 16 * P;
+  double2 *tw2 = tw1 + P;
   double2 *pfs = tw2 + 16 * R3;
   Tin *stage = reinterpret_cast<Tin *>(pfs + M);  // 2 buffers of 2M
   const long lbeg = (long)blockIdx.x * chunk;
   const long lend = min(K, lbeg + chunk);
   if (lbeg < lend) stage_site(stage, L, Rv, K, M, lbeg);
-  for (int t = threadIdx.x; t < 16 * P; t += blockDim.x) {
-    const int k2 = t / P, m1 = t % P;
+  for (int t = threadIdx.x; t < P; t += blockDim.x) {
     double sn, cs;
-    sincospi(2.0 * (double)(m1 * k2) / n, &sn, &cs);
+    sincospi(2.0 * (double)t / n, &sn, &cs);
     tw1[t] = make_double2(cs, sn);
   }
   for (int t = threadIdx.x; t < 16 * R3; t += blockDim.x) {
@@ -223,9 +256,13 @@ __global__ void __launch_bounds__(kFftThreads)
     tw2[t] = make_double2(cs, sn);
   }
   for (int m = threadIdx.x; m < M; m += blockDim.x) pfs[m] = pf_g[m];
-  double2 accp[KPT], accw[KPT];
+  // final-stage role of this thread: half h of the pair (k2f, cf)
+  const int h = threadIdx.x & 1, pair = threadIdx.x >> 1;
+  const int k2f = pair % 16, cf = pair / 16;  // pair < 256 for kFftThreads = 512
+  const bool fin = (R3 >= 2 || h == 0);
+  double2 accp[ND], accw[ND];
 #pragma unroll
-  for (int q = 0; q < KPT; ++q) accp[q] = accw[q] = make_double2(0, 0);
+  for (int j = 0; j < ND; ++j) accp[j] = accw[j] = make_double2(0, 0);
 
   int cur = 0;
   for (long l = lbeg; l < lend; ++l) {
@@ -243,7 +280,7 @@ __global__ void __launch_bounds__(kFftThreads)
 #pragma unroll
       for (int m2 = 0; m2 < 16; ++m2) {
         const int m = m1 + P * m2;
-        if (m < M) {
+        if ((!HALF || m2 < 8) && m < M) {
           double f = (double)src[2 * m];
           if (deriv) f *= (double)m;
           const double2 pf = pfs[m];
@@ -252,92 +289,86 @@ __global__ void __launch_bounds__(kFftThreads)
           v[m2] = make_double2(0, 0);
         }
       }
-      dft16(v);
+      if constexpr (HALF)
+        dft16_half(v);
+      else
+        dft16(v);
+      // w^{q1 + 4 q2} = w^{q1} w^{4 q2}, w = w_n^{m1}
+      const double2 w1 = tw1[m1];
+      const double2 w2 = cmul(w1, w1), w3 = cmul(w2, w1), w4 = cmul(w2, w2);
+      const double2 w8 = cmul(w4, w4), w12 = cmul(w8, w4);
       double2 *row = buf + s * SEQ;
 #pragma unroll
       for (int q1 = 0; q1 < 4; ++q1)
 #pragma unroll
         for (int q2 = 0; q2 < 4; ++q2) {
           const int k2 = q1 + 4 * q2;
-          row[k2 * ROW + m1] = k2 ? cmul(v[4 * q1 + q2], tw1[k2 * P + m1]) : v[4 * q1 + q2];
+          double2 x = v[4 * q1 + q2];
+          if (q1 == 1) x = cmul(x, w1);
+          if (q1 == 2) x = cmul(x, w2);
+          if (q1 == 3) x = cmul(x, w3);
+          if (q2 == 1) x = cmul(x, w4);
+          if (q2 == 2) x = cmul(x, w8);
+          if (q2 == 3) x = cmul(x, w12);
+          row[k2 * ROW + m1] = x;
         }
     }
     __syncthreads();
-    // ---- pass 2: for row k2, m1 = a + R3 b: 16-point DFT over b, twiddle w_P^{a c}
-    {
+    // ---- pass 2: for row k2, m1 = a + R3 b: 16-point DFT over b, twiddle w_P^{a c}, in place
+    for (int item = threadIdx.x; item < NSEQ * 16 * R3; item += blockDim.x) {
+      const int k2 = item % 16, a = (item / 16) % R3, s = item / (16 * R3);
+      double2 *row = buf + s * SEQ + k2 * ROW;
       double2 v[16];
-      int s = 0, k2 = 0, a = 0;
-      const int items = NSEQ * 16 * R3;
-      const bool active = threadIdx.x < items;  // items <= kFftThreads for all instantiations
-      if (active) {
-        s = threadIdx.x / (16 * R3);
-        k2 = (threadIdx.x / R3) % 16;
-        a = threadIdx.x % R3;
-        const double2 *row = buf + s * SEQ + k2 * ROW;
 #pragma unroll
-        for (int b = 0; b < 16; ++b) v[b] = row[a + R3 * b];
-      }
-      __syncthreads();
-      if (active) {
-        dft16(v);
-        double2 *row = buf + s * SEQ + k2 * ROW;
+      for (int b = 0; b < 16; ++b) v[b] = row[a + R3 * b];
+      dft16(v);
 #pragma unroll
-        for (int q1 = 0; q1 < 4; ++q1)
+      for (int q1 = 0; q1 < 4; ++q1)
 #pragma unroll
-          for (int q2 = 0; q2 < 4; ++q2) {
-            const int c = q1 + 4 * q2;
-            row[c * R3 + a] = R3 == 1 ? v[4 * q1 + q2] : cmul(v[4 * q1 + q2], tw2[c * R3 + a]);
-          }
-      }
-      __syncthreads();
+        for (int q2 = 0; q2 < 4; ++q2) {
+          const int c = q1 + 4 * q2;
+          row[c * R3 + a] = (R3 == 1 || c == 0) ? v[4 * q1 + q2] : cmul(v[4 * q1 + q2], tw2[c * R3 + a]);
+        }
     }
-    // ---- pass 3: for row k2 and c < 16: R3-point DFT over a -> X[k2 + 16 c + 256 d]
-    if constexpr (R3 > 1) {
-      for (int base = 0; base < NSEQ * 256; base += blockDim.x) {
-        const int item = base + threadIdx.x;
+    __syncthreads();
+    // ---- final: R3-point DFT over a of row k2f, column cf -> X[k2f + 16 cf + 256 d], and
+    // the products for this thread's outputs d = h + 2 j
+    if (fin) {
+      double2 X[ND][NSEQ];
+#pragma unroll
+      for (int s = 0; s < NSEQ; ++s) {
+        const double2 *row = buf + s * SEQ + k2f * ROW + cf * R3;
         double2 v[R3];
-        int s = 0, k2 = 0, c = 0;
-        const bool active = item < NSEQ * 256;
-        if (active) {
-          s = item / 256;
-          k2 = (item / 16) % 16;
-          c = item % 16;
-          const double2 *row = buf + s * SEQ + k2 * ROW;
 #pragma unroll
-          for (int a = 0; a < R3; ++a) v[a] = row[c * R3 + a];
-          dft_small<R3>(v);
-        }
-        __syncthreads();
-        if (active) {
-          double2 *row = buf + s * SEQ + k2 * ROW;
+        for (int a = 0; a < R3; ++a) v[a] = row[a];
+        dft_small<R3>(v);
 #pragma unroll
-          for (int d = 0; d < R3; ++d) row[c + 16 * d] = v[d];
+        for (int j = 0; j < ND; ++j) {
+          if constexpr (R3 >= 2)
+            X[j][s] = h ? v[2 * j + 1] : v[2 * j];  // constant indices: v stays in registers
+          else
+            X[j][s] = v[0];
         }
-        __syncthreads();
       }
-    }
-    // ---- products: X_s[k] lives at buf[s*SEQ + (k % 16)*ROW + k / 16]
 #pragma unroll
-    for (int q = 0; q < KPT; ++q) {
-      const int k = threadIdx.x + q * kFftThreads;
-      if (k < n) {
-        const double2 *X = buf + (k % 16) * ROW + k / 16;
+      for (int j = 0; j < ND; ++j) {
+        const int k = k2f + 16 * cf + 256 * (R3 >= 2 ? h + 2 * j : 0);
         if constexpr (NSEQ == 8)
-          bastin_products(k, n, X, SEQ, accp[q], accw[q]);
+          bastin_products_reg(k, n, X[j], accp[j], accw[j]);
         else
-          greenwood_product(X, SEQ, accp[q]);
+          greenwood_product_reg(X[j], accp[j]);
       }
     }
     cur ^= 1;
   }
   cp_async_wait_all();
   double2 *out = part + (size_t)blockIdx.x * 2 * n;
+  if (fin) {
 #pragma unroll
-  for (int q = 0; q < KPT; ++q) {
-    const int k = threadIdx.x + q * kFftThreads;
-    if (k < n) {
-      out[k] = accp[q];
-      out[k + n] = accw[q];
+    for (int j = 0; j < ND; ++j) {
+      const int k = k2f + 16 * cf + 256 * (R3 >= 2 ? h + 2 * j : 0);
+      out[k] = accp[j];
+      out[k + n] = accw[j];
     }
   }
 }
@@ -461,14 +492,23 @@ __global__ void k_kubo_post(const double2 *__restrict__ acc, double R, int nump,
 template <int R3, int NSEQ, class Tin>
 void launch_fft(Session *s, const Tin *L, const Tin *Rv, long K, int M, const double2 *pf, double2 *acc) {
   constexpr int n = 256 * R3;
-  const size_t smem = sizeof(double2) * ((size_t)NSEQ * 16 * (16 * R3 + 1) + 16 * 16 * R3 + 16 * R3 + (size_t)M) +
+  const size_t smem = sizeof(double2) * ((size_t)NSEQ * 16 * (16 * R3 + 1) + 16 * R3 + 16 * R3 + (size_t)M) +
                       sizeof(Tin) * 4 * (size_t)M;
   if (smem > 227 * 1024) fail(LINQT_ERR_UNSUPPORTED, "kubo_fft: nump too large for the shared-memory FFT");
-  LQ_CUDA(cudaFuncSetAttribute(k_kubo_fft<R3, NSEQ, Tin>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
   const int nb = (int)std::max(1L, std::min(K, (long)s->sm_count));
   const long chunk = (K + nb - 1) / nb;
   double2 *part = (double2 *)s->get("kubo_part", sizeof(double2) * 2 * (size_t)n * nb);
-  k_kubo_fft<R3, NSEQ, Tin><<<nb, kFftThreads, smem, s->stream>>>(L, Rv, K, chunk, M, pf, part);
+  // every output k < n is written by exactly one thread of each CTA (pairs cover 16 x 16,
+  // halves cover the R3 outputs), so the partials need no clearing
+  if (2 * M <= n) {
+    LQ_CUDA(cudaFuncSetAttribute(k_kubo_fft<R3, NSEQ, true, Tin>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 (int)smem));
+    k_kubo_fft<R3, NSEQ, true, Tin><<<nb, kFftThreads, smem, s->stream>>>(L, Rv, K, chunk, M, pf, part);
+  } else {
+    LQ_CUDA(cudaFuncSetAttribute(k_kubo_fft<R3, NSEQ, false, Tin>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 (int)smem));
+    k_kubo_fft<R3, NSEQ, false, Tin><<<nb, kFftThreads, smem, s->stream>>>(L, Rv, K, chunk, M, pf, part);
+  }
   LQ_LAUNCHED();
   k_sum_parts<<<(2 * n + 255) / 256, 256, 0, s->stream>>>(part, nb, 2 * n, acc);
   LQ_LAUNCHED();
@@ -513,11 +553,15 @@ void kubo_fft_sites_t(Session *s, const Tin *L, const Tin *Rv, long nsites, int 
 
 }  // namespace
 
+void kubo_prefactors(Session *s, int M, int nump, double2 *pf) {
+  k_prefactors<<<(M + 255) / 256, 256, 0, s->stream>>>(M, nump, pf);
+  LQ_LAUNCHED();
+}
+
 void kubo_fft_sites(Session *s, const void *Lv, const void *Rvv, long nsites, int M, int nump, int formula,
                     bool fp32_inputs, double2 *acc) {
   double2 *pf = (double2 *)s->get("kubo_pf", sizeof(double2) * M);
-  k_prefactors<<<(M + 255) / 256, 256, 0, s->stream>>>(M, nump, pf);
-  LQ_LAUNCHED();
+  kubo_prefactors(s, M, nump, pf);
   if (fp32_inputs)
     kubo_fft_sites_t(s, (const float2 *)Lv, (const float2 *)Rvv, nsites, M, nump, formula, pf, acc);
   else
