@@ -16,7 +16,10 @@ namespace linqt {
 
 namespace {
 
-constexpr int BM = 64, BN = 64, BK = 16, LDS = BK + 1;  // LDS: padded smem row (double2)
+// LDS: smem row pitch in elements.  Fragment loads read rows fr = lane/4 (two per 8-lane
+// phase) at k = lane%4; a pitch of 4 mod 8 puts those 8 accesses on distinct 16-byte bank
+// groups, and the tile stores walk k fastest, which is conflict-free for any pitch.
+constexpr int BM = 64, BN = 64, BK = 16, LDS = BK + 4;
 
 __device__ __forceinline__ void cp_async16(void *smem, const void *gmem, bool valid) {
   const unsigned s = (unsigned)__cvta_generic_to_shared(smem);
@@ -40,19 +43,19 @@ __device__ __forceinline__ void cp_async8(void *smem, const void *gmem, bool val
 template <class Tc>
 __device__ __forceinline__ void load_tile(Tc (*sm)[LDS], const Tc *__restrict__ g, int M, long K, int row0, long k0,
                                           long kend) {
-  // 256 threads x 4 elements: thread t covers row t>>2, k slots (t&3)*4 .. +3
-  const int t = threadIdx.x;
-  const int r = t >> 2, kq = (t & 3) * 4;
-  const int row = row0 + r;
+  // 256 threads x 4 elements: element e = t + 256 q is row e / BK, k slot e % BK
 #pragma unroll
   for (int q = 0; q < 4; ++q) {
-    const long k = k0 + kq + q;
+    const int e = threadIdx.x + 256 * q;
+    const int r = e / BK, kk = e % BK;
+    const int row = row0 + r;
+    const long k = k0 + kk;
     const bool ok = row < M && k < kend;
     const Tc *src = ok ? g + (size_t)row * K + k : g;
     if constexpr (sizeof(Tc) == 16)
-      cp_async16(&sm[r][kq + q], src, ok);
+      cp_async16(&sm[r][kk], src, ok);
     else
-      cp_async8(&sm[r][kq + q], src, ok);
+      cp_async8(&sm[r][kk], src, ok);
   }
 }
 
@@ -65,7 +68,10 @@ __device__ __forceinline__ void dmma(double &d0, double &d1, double a, double b)
 }
 
 // 64x64 complex output tile per CTA, 8 warps as 2 (rows) x 4 (cols), 32x16 complex per warp
-// = 4 x 2 tiles of 8x8; conj(A) B = (Ar Br + Ai Bi) + i (Ar Bi - Ai Br): four real DMMAs per tile.
+// = 4 x 2 tiles of 8x8.  With a = conj(A) = ar + i ai (ai = -Im A) and b = br + i bi, three
+// real DMMAs per tile (Gauss): t1 = ar br, t2 = ai bi, t3 = (ar + ai)(br + bi), and
+// conj(A) B = (t1 - t2) + i (t3 - t1 - t2) in the epilogue -- 3/4 of the tensor-core work of
+// the four-product form, at the cost of one rounding-level cancellation in the imaginary part.
 template <class Tc>
 __global__ void __launch_bounds__(256, 2) k_zgemm_cn_f64(const Tc *__restrict__ L, const Tc *__restrict__ Rv, int MA,
                                                          int MB, long K, long kchunk, double2 *__restrict__ part) {
@@ -79,11 +85,13 @@ __global__ void __launch_bounds__(256, 2) k_zgemm_cn_f64(const Tc *__restrict__ 
   const int m0 = blockIdx.y * BM, m1 = blockIdx.x * BN;
   const long kbeg = (long)blockIdx.z * kchunk;
   const long kend = min(K, kbeg + kchunk);
-  double cre[4][2][2], cim[4][2][2];
+  double t1[4][2][2], t2[4][2][2], t3[4][2][2];
 #pragma unroll
   for (int i = 0; i < 4; ++i)
 #pragma unroll
-    for (int j = 0; j < 2; ++j) cre[i][j][0] = cre[i][j][1] = cim[i][j][0] = cim[i][j][1] = 0.0;
+    for (int j = 0; j < 2; ++j)
+#pragma unroll
+      for (int h = 0; h < 2; ++h) t1[i][j][h] = t2[i][j][h] = t3[i][j][h] = 0.0;
   if (kbeg < kend) {
     const int nk = (int)((kend - kbeg + BK - 1) / BK);
     load_tile(As[0], L, MA, K, m0, kbeg, kend);
@@ -117,12 +125,17 @@ __global__ void __launch_bounds__(256, 2) k_zgemm_cn_f64(const Tc *__restrict__ 
         for (int i = 0; i < 4; ++i)
 #pragma unroll
           for (int j = 0; j < 2; ++j) {
-            // (ar + i ai)(br + i bi) with ai = -Im(A): re = ar br - ai bi, im = ar bi + ai br
-            dmma(cre[i][j][0], cre[i][j][1], ar[i], br[j]);
-            dmma(cre[i][j][0], cre[i][j][1], -ai[i], bi[j]);
-            dmma(cim[i][j][0], cim[i][j][1], ar[i], bi[j]);
-            dmma(cim[i][j][0], cim[i][j][1], ai[i], br[j]);
+            dmma(t1[i][j][0], t1[i][j][1], ar[i], br[j]);
+            dmma(t2[i][j][0], t2[i][j][1], ai[i], bi[j]);
           }
+#pragma unroll
+        for (int i = 0; i < 4; ++i) ar[i] += ai[i];
+#pragma unroll
+        for (int j = 0; j < 2; ++j) br[j] += bi[j];
+#pragma unroll
+        for (int i = 0; i < 4; ++i)
+#pragma unroll
+          for (int j = 0; j < 2; ++j) dmma(t3[i][j][0], t3[i][j][1], ar[i], br[j]);
       }
       __syncthreads();
     }
@@ -138,7 +151,8 @@ __global__ void __launch_bounds__(256, 2) k_zgemm_cn_f64(const Tc *__restrict__ 
 #pragma unroll
       for (int h = 0; h < 2; ++h) {
         const int c = m1 + wn * 16 + j * 8 + 2 * fk + h;
-        if (c < MB) out[(size_t)r * MB + c] = make_double2(cre[i][j][h], cim[i][j][h]);
+        if (c < MB)
+          out[(size_t)r * MB + c] = make_double2(t1[i][j][h] - t2[i][j][h], t3[i][j][h] - t1[i][j][h] - t2[i][j][h]);
       }
   }
 }
