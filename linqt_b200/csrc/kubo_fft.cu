@@ -213,7 +213,7 @@ __device__ __forceinline__ void greenwood_product_reg(const double2 (&x)[4], dou
 
 // Shared-memory layout (double2 units):
 //   buf   NSEQ * 16 * (P + 1)   the transforms, 16 rows of P (+1 pad) per sequence
-//   tw1   P                     w_n^{m1}                       (pass 1; powers formed in registers)
+//   tw1   16 * P                w_n^{m1 k2} at [k2 * P + m1]   (pass 1)
 //   tw2   16 * R3               w_P^{a c}   at [c * R3 + a]    (pass 2)
 //   pfs   M                     prefactors
 //   stage 2 * 2M                double-buffered bra/ket of the current and next site
@@ -238,15 +238,16 @@ __global__ void __launch_bounds__(kFftThreads)
   extern __shared__ double2 sm[];
   double2 *buf = sm;
   double2 *tw1 = buf + NSEQ * SEQ;
-  double2 *tw2 = tw1 + P;
+  double2 *tw2 = tw1 + 16 * P;
   double2 *pfs = tw2 + 16 * R3;
   Tin *stage = reinterpret_cast<Tin *>(pfs + M);  // 2 buffers of 2M
   const long lbeg = (long)blockIdx.x * chunk;
   const long lend = min(K, lbeg + chunk);
   if (lbeg < lend) stage_site(stage, L, Rv, K, M, lbeg);
-  for (int t = threadIdx.x; t < P; t += blockDim.x) {
+  for (int t = threadIdx.x; t < 16 * P; t += blockDim.x) {
+    const int k2 = t / P, m1 = t % P;
     double sn, cs;
-    sincospi(2.0 * (double)t / n, &sn, &cs);
+    sincospi(2.0 * (double)(m1 * k2) / n, &sn, &cs);
     tw1[t] = make_double2(cs, sn);
   }
   for (int t = threadIdx.x; t < 16 * R3; t += blockDim.x) {
@@ -293,24 +294,13 @@ __global__ void __launch_bounds__(kFftThreads)
         dft16_half(v);
       else
         dft16(v);
-      // w^{q1 + 4 q2} = w^{q1} w^{4 q2}, w = w_n^{m1}
-      const double2 w1 = tw1[m1];
-      const double2 w2 = cmul(w1, w1), w3 = cmul(w2, w1), w4 = cmul(w2, w2);
-      const double2 w8 = cmul(w4, w4), w12 = cmul(w8, w4);
       double2 *row = buf + s * SEQ;
 #pragma unroll
       for (int q1 = 0; q1 < 4; ++q1)
 #pragma unroll
         for (int q2 = 0; q2 < 4; ++q2) {
           const int k2 = q1 + 4 * q2;
-          double2 x = v[4 * q1 + q2];
-          if (q1 == 1) x = cmul(x, w1);
-          if (q1 == 2) x = cmul(x, w2);
-          if (q1 == 3) x = cmul(x, w3);
-          if (q2 == 1) x = cmul(x, w4);
-          if (q2 == 2) x = cmul(x, w8);
-          if (q2 == 3) x = cmul(x, w12);
-          row[k2 * ROW + m1] = x;
+          row[k2 * ROW + m1] = k2 ? cmul(v[4 * q1 + q2], tw1[k2 * P + m1]) : v[4 * q1 + q2];
         }
     }
     __syncthreads();
@@ -341,13 +331,19 @@ __global__ void __launch_bounds__(kFftThreads)
         double2 v[R3];
 #pragma unroll
         for (int a = 0; a < R3; ++a) v[a] = row[a];
-        dft_small<R3>(v);
+        if constexpr (R3 == 1) {
+          X[0][s] = v[0];
+        } else if constexpr (R3 == 2) {  // X_h = v0 + (-1)^h v1
+          X[0][s] = h ? csub(v[0], v[1]) : cadd(v[0], v[1]);
+        } else if constexpr (R3 == 4) {  // half h: {X0, X2} from v0 + v2, v1 + v3; {X1, X3} from the differences
+          const double2 e = h ? csub(v[0], v[2]) : cadd(v[0], v[2]);
+          const double2 o = h ? mul_i(csub(v[1], v[3])) : cadd(v[1], v[3]);
+          X[0][s] = cadd(e, o);
+          X[1][s] = csub(e, o);
+        } else {
+          dft_small<R3>(v);
 #pragma unroll
-        for (int j = 0; j < ND; ++j) {
-          if constexpr (R3 >= 2)
-            X[j][s] = h ? v[2 * j + 1] : v[2 * j];  // constant indices: v stays in registers
-          else
-            X[j][s] = v[0];
+          for (int j = 0; j < ND; ++j) X[j][s] = h ? v[2 * j + 1] : v[2 * j];  // constant indices
         }
       }
 #pragma unroll
@@ -492,7 +488,7 @@ __global__ void k_kubo_post(const double2 *__restrict__ acc, double R, int nump,
 template <int R3, int NSEQ, class Tin>
 void launch_fft(Session *s, const Tin *L, const Tin *Rv, long K, int M, const double2 *pf, double2 *acc) {
   constexpr int n = 256 * R3;
-  const size_t smem = sizeof(double2) * ((size_t)NSEQ * 16 * (16 * R3 + 1) + 16 * R3 + 16 * R3 + (size_t)M) +
+  const size_t smem = sizeof(double2) * ((size_t)NSEQ * 16 * (16 * R3 + 1) + 16 * 16 * R3 + 16 * R3 + (size_t)M) +
                       sizeof(Tin) * 4 * (size_t)M;
   if (smem > 227 * 1024) fail(LINQT_ERR_UNSUPPORTED, "kubo_fft: nump too large for the shared-memory FFT");
   const int nb = (int)std::max(1L, std::min(K, (long)s->sm_count));
