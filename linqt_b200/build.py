@@ -1,9 +1,11 @@
-"""Build liblinqt_gpu.so in-tree with nvcc for sm_100a.
+"""Build liblinqt_gpu.so in-tree with nvcc for sm_100a, and liblinqt_facade.so.
 
     python -m linqt_b200.build          # or linqt_b200.build.build()
 
-The library is compiled from linqt_b200/csrc/*.cu with the CUDA runtime linked
-statically, so the .so carries no dependency on a particular libcudart.
+The GPU library is compiled from linqt_b200/csrc/*.cu with the CUDA runtime linked
+statically, so the .so carries no dependency on a particular libcudart.  The facade
+library (linqt_b200/facade: LinQT's C++ classes on the C ABI) is plain C++ linked
+against it.
 """
 import glob
 import os
@@ -14,6 +16,8 @@ import sys
 HERE = os.path.dirname(os.path.abspath(__file__))
 CSRC = os.path.join(HERE, "csrc")
 LIB = os.path.join(HERE, "liblinqt_gpu.so")
+FACADE = os.path.join(HERE, "facade")
+FACADE_LIB = os.path.join(HERE, "liblinqt_facade.so")
 ROOT = os.path.dirname(HERE)
 
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
@@ -40,15 +44,32 @@ def needs_build():
     return any(os.path.getmtime(p) > t for p in deps)
 
 
-def build(force=False, verbose=False, extra=()):
-    if not force and not needs_build():
-        return LIB
-    cmd = [nvcc()] + ARCH + FLAGS + list(extra) + ["-I", os.path.join(ROOT, "include"), "-o", LIB] + sources()
+def build_facade(force=False, verbose=False):
+    srcs = glob.glob(os.path.join(FACADE, "*.cpp"))
+    deps = srcs + glob.glob(os.path.join(FACADE, "include", "*.hpp")) + [LIB, os.path.join(ROOT, "include", "linqt_gpu.h")]
+    if not force and os.path.exists(FACADE_LIB) and all(os.path.getmtime(p) <= os.path.getmtime(FACADE_LIB)
+                                                        for p in deps):
+        return FACADE_LIB
+    cmd = ["g++", "-std=c++17", "-O2", "-fPIC", "-shared", "-I", os.path.join(FACADE, "include"), "-I",
+           os.path.join(ROOT, "include"), "-o", FACADE_LIB] + srcs + ["-L", HERE, "-llinqt_gpu",
+                                                                      "-Wl,-rpath,$ORIGIN"]
     if verbose:
         print(" ".join(cmd))
     p = subprocess.run(cmd, capture_output=True, text=True)
     if p.returncode != 0:
-        raise RuntimeError("nvcc failed:\n" + p.stdout + p.stderr)
+        raise RuntimeError("g++ (facade) failed:\n" + p.stdout + p.stderr)
+    return FACADE_LIB
+
+
+def build(force=False, verbose=False, extra=()):
+    if force or needs_build():
+        cmd = [nvcc()] + ARCH + FLAGS + list(extra) + ["-I", os.path.join(ROOT, "include"), "-o", LIB] + sources()
+        if verbose:
+            print(" ".join(cmd))
+        p = subprocess.run(cmd, capture_output=True, text=True)
+        if p.returncode != 0:
+            raise RuntimeError("nvcc failed:\n" + p.stdout + p.stderr)
+    build_facade(force=force, verbose=verbose)
     return LIB
 
 

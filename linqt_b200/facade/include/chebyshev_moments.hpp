@@ -1,0 +1,158 @@
+// LinQT's Chebyshev-moment containers (include/chebyshev_moments.hpp of LinQT) for the
+// B200 library: Moments (expansion parameters and the non-owning Hamiltonian pointer),
+// Moments1D / Moments2D (moment tables with LinQT's .chebmom1D / .chebmom2D files) and
+// Vectors_sliced (the parameter carrier Kubo_solver_FFT takes).  The recursion vectors the
+// reference keeps in these objects live on the GPU inside the solvers instead.
+#ifndef CHEBYSHEV_MOMENTS
+#define CHEBYSHEV_MOMENTS
+
+#include <array>
+#include <cassert>
+#include <complex>
+#include <fstream>
+#include <limits>
+#include <string>
+#include <vector>
+
+#include "sparse_matrix.hpp"
+
+namespace chebyshev {
+const double CUTOFF = 1.00;
+
+class Moments {
+ public:
+  typedef std::complex<double> value_t;
+  typedef std::vector<value_t> vector_t;
+
+  Moments() {}
+
+  void getMomentsParams(Moments &mom) {
+    SetHamiltonian(mom.Hamiltonian());
+    SystemLabel(mom.SystemLabel());
+    BandWidth(mom.BandWidth());
+    BandCenter(mom.BandCenter());
+  }
+
+  size_t SystemSize() const { return system_size; }
+  string SystemLabel() const { return system_label; }
+  double BandWidth() const { return band_width; }
+  double HalfWidth() const { return BandWidth() / 2.0; }
+  double BandCenter() const { return band_center; }
+  double ScaleFactor() const { return chebyshev::CUTOFF / HalfWidth(); }
+  double ShiftFactor() const { return -BandCenter() / HalfWidth() / chebyshev::CUTOFF; }
+  vector_t &MomentVector() { return mu; }
+  value_t &MomentVector(const int i) { return mu[i]; }
+  SparseMatrixType &Hamiltonian() const { return *_pNHAM; }
+
+  void SetHamiltonian(SparseMatrixType &NHAM) {
+    if (SystemSize() == 0) SystemSize(NHAM.rank());
+    assert(NHAM.rank() == (int)SystemSize());
+    _pNHAM = &NHAM;
+  }
+  // H <- ScaleFactor H + ShiftFactor I, on the device copy of the operator
+  int Rescale2ChebyshevDomain() {
+    Hamiltonian().Rescale(ScaleFactor(), ShiftFactor());
+    return 0;
+  }
+  void SetAndRescaleHamiltonian(SparseMatrixType &NHAM) {
+    SetHamiltonian(NHAM);
+    Rescale2ChebyshevDomain();
+  }
+  void SystemSize(const int dim) { system_size = dim; }
+  void SystemLabel(string label) { system_label = label; }
+  void BandWidth(const double x) { band_width = x; }
+  void BandCenter(const double x) { band_center = x; }
+  void MomentVector(const vector_t _mu) { mu = _mu; }
+  double Rescale2ChebyshevDomain(const double energ) { return (energ - BandCenter()) / HalfWidth(); }
+
+  // the moment cut-off and Jackson factor of src/chebyshev_moments.cpp:24-40
+  int JacksonKernelMomCutOff(const double broad);
+  double JacksonKernel(const double m, const double Mom);
+
+ private:
+  SparseMatrixType *_pNHAM = nullptr;
+  std::string system_label;
+  size_t system_size = 0;
+  double band_width = 0, band_center = 0;
+  vector_t mu;
+};
+
+class Moments1D : public Moments {
+ public:
+  Moments1D() : _numMoms(0) {}
+  Moments1D(const size_t m0) : _numMoms(m0) { MomentVector(Moments::vector_t(_numMoms, 0.0)); }
+  Moments1D(std::string momfilename);
+
+  size_t MomentNumber() const { return _numMoms; }
+  size_t HighestMomentNumber() const { return _numMoms; }
+  Moments::value_t &operator()(const size_t m0) { return MomentVector(m0); }
+  void MomentNumber(const size_t numMoms);
+  void saveIn(std::string filename);
+  void ApplyJacksonKernel(const double broad);
+  void Print();
+
+ private:
+  size_t _numMoms;
+};
+
+class Moments2D : public Moments {
+ public:
+  Moments2D() : numMoms({0, 0}) {}
+  Moments2D(const size_t m0, const size_t m1) : numMoms({int(m0), int(m1)}) {
+    MomentVector(Moments::vector_t((size_t)numMoms[1] * numMoms[0], 0.0));
+  }
+  Moments2D(std::string momfilename);
+  Moments2D(Moments2D mom, const size_t m0, const size_t m1) {
+    getMomentsParams(mom);
+    numMoms = {int(m0), int(m1)};
+    MomentVector(Moments::vector_t((size_t)numMoms[1] * numMoms[0], 0.0));
+  }
+
+  array<int, 2> MomentNumber() const { return numMoms; }
+  int HighestMomentNumber(const int i) const { return numMoms[i]; }
+  int HighestMomentNumber() const { return numMoms[1] > numMoms[0] ? numMoms[1] : numMoms[0]; }
+  void MomentNumber(const int mom0, const int mom1);
+  Moments::value_t &operator()(const int m0, const int m1) { return MomentVector(m0 * numMoms[1] + m1); }
+  void ApplyJacksonKernel(const double b0, const double b1);
+  void saveIn(std::string filename);
+  void AddSubMatrix(Moments2D &sub, const int mL, const int mR) {
+    for (int m0 = 0; m0 < sub.HighestMomentNumber(0); m0++)
+      for (int m1 = 0; m1 < sub.HighestMomentNumber(1); m1++) (*this)(mL + m0, mR + m1) += sub(m0, m1);
+  }
+  void InsertSubMatrix(Moments2D &sub, const int mL, const int mR) {
+    for (int m0 = 0; m0 < sub.HighestMomentNumber(0); m0++)
+      for (int m1 = 0; m1 < sub.HighestMomentNumber(1); m1++) (*this)(mL + m0, mR + m1) = sub(m0, m1);
+  }
+  void Print();
+
+ private:
+  array<int, 2> numMoms;
+};
+
+// Parameters of Kubo_solver_FFT's recursion (number of moments, sections).  The vectors
+// themselves are device buffers of the solver.
+class Vectors_sliced : public Moments {
+ public:
+  Vectors_sliced() : numVecs_(0), num_sections_(1) {}
+  Vectors_sliced(const int numVecs, const size_t num_sections) : numVecs_(numVecs), num_sections_(num_sections) {}
+  Vectors_sliced(Moments &mom, const int numVecs, const size_t num_sections)
+      : numVecs_(numVecs), num_sections_(num_sections) {
+    getMomentsParams(mom);
+  }
+
+  int NumberOfVectors() const { return numVecs_; }
+  int NumberOfSections() const { return (int)num_sections_; }
+  void SetNumberOfVectors(const int x) { numVecs_ = x; }
+  int SetNumSections(const int x) {
+    num_sections_ = x;
+    return 0;
+  }
+
+ private:
+  int numVecs_;
+  size_t num_sections_;
+};
+
+}  // namespace chebyshev
+
+#endif

@@ -192,6 +192,40 @@ def test_kubo_bastin_combined_equals_separate(honey):
     assert np.array_equal(s, s2) and np.array_equal(E, E2) and np.array_equal(integ, i2)
 
 
+@pytest.fixture(scope="module")
+def diag_op(oracle_lib, honey):
+    """A second operator (diagonal, random) so that OPL != OPR."""
+    N = honey["N"]
+    D = lattices.upper_csr(N, np.arange(N), np.arange(N), lattices.disorder(N, 2.0, 5) + 0j)
+    return dict(Dg=gpu_op(N, D), Do=oracle_op(oracle_lib, D))
+
+
+def test_moments2d_distinct_operators(oracle_lib, honey, diag_op):
+    st = lattices.random_phase_states(honey["N"], 3, seed=44)
+    M = 48
+    got = lq.moments2d(honey["Hg"], honey["Vg"], diag_op["Dg"], st, M)
+    want = oracle_lib.moments2d(honey["Ho"], honey["Vo"], diag_op["Do"], st, M)
+    assert rel(got, want) < TOL
+    swapped = lq.moments2d(honey["Hg"], diag_op["Dg"], honey["Vg"], st, M)
+    assert rel(swapped, want) > 1e-3
+
+
+@pytest.mark.parametrize("formula", [lq.KUBO_BASTIN, lq.KUBO_GREENWOOD])
+def test_kubo_fft_distinct_operators(oracle_lib, honey, diag_op, formula):
+    st = lattices.random_phase_states(honey["N"], 2, seed=45)
+    M, nump = 48, 256
+    E, s, integ = lq.kubo_fft(honey["Hg"], honey["Vg"], diag_op["Dg"], st, M, nump, formula, honey["bw"],
+                              honey["bc"])
+    Eo, so, io, _ = oracle_lib.kubo_fft(honey["Ho"], honey["Vo"], diag_op["Do"], st, M, nump, formula, honey["N"],
+                                        honey["bw"], honey["bc"])
+    assert rel(s, so) < TOL
+    mu, (E2, s2, i2) = lq.kubo_bastin(honey["Hg"], honey["Vg"], diag_op["Dg"], st, M, nump, honey["bw"],
+                                      honey["bc"])
+    if formula == lq.KUBO_BASTIN:
+        assert np.array_equal(s, s2)
+        assert rel(mu, oracle_lib.moments2d(honey["Ho"], honey["Vo"], diag_op["Do"], st, M)) < TOL
+
+
 def test_dos_from_moments(oracle_lib, square):
     st = lattices.random_phase_states(square["N"], 2, seed=12)
     M = 256

@@ -102,3 +102,43 @@ def test_reference_driver_on_golden_chain(tmp_path):
     n, bw, bc, mu = formats.read_chebmom2d(str(tmp_path / "NonEqOpVX-VXlinear_chainKPM_M100x100_statedefault.chebmom2D"))
     ref = golden["mu100"][..., 0] + 1j * golden["mu100"][..., 1]
     assert rel(mu, ref) < 1e-13
+
+
+def _graphene_with_diagonal(tmp_path, oracle_lib, R, seed):
+    """Graphene with V_x and a second, diagonal operator DG, so that OPL != OPR."""
+    N, H, V = lattices.honeycomb(6, 5, t=-2.7, W=1.0, seed=21)
+    D = lattices.upper_csr(N, np.arange(N), np.arange(N), lattices.disorder(N, 2.0, 5) + 0j)
+    st = lattices.random_phase_states(N, R, seed=seed)
+    lo, hi = lattices.gershgorin_bounds(N, *H)
+    d = setup_dir(oracle_lib, tmp_path, "gr", {"HAM": (N, H), "VX": (N, V), "DG": (N, D)},
+                  (1.05 * lo, 1.05 * hi), st)
+    ops = {k: oracle_lib.Op(*formats.read_csr(os.path.join(d, "operators", "gr.%s.CSR" % k))[1:])
+           for k in ("VX", "DG")}
+    return N, d, ops, (1.05 * (hi - lo), 1.05 * (hi + lo) / 2)
+
+
+def test_correlation_moments_operator_order_vs_ref(oracle_lib, tmp_path):
+    """CorrelationExpansionMoments(OPL, OPR, ...) (src/chebyshev_solver.cpp:86): the first operator
+    is OPL, the one the first moment index follows."""
+    N, d, ops, _ = _graphene_with_diagonal(tmp_path, oracle_lib, 3, 22)
+    out = oracle_lib.run_ref_harness(["nonEq", "gr", "VX", "DG", 40, "states.txt"], d)
+    n, bw, bc, mu_ref = formats.read_chebmom2d(os.path.join(d, out["out"]))
+    Ho = oracle_lib.Op(*formats.read_csr(os.path.join(d, "operators", "gr.HAM.CSR"))[1:]).rescale(2 / bw,
+                                                                                                   -bc / (bw / 2))
+    st = formats.read_state_file(os.path.join(d, "states.txt"))
+    assert rel(oracle_lib.moments2d(Ho, ops["VX"], ops["DG"], st, 40), mu_ref) < 1e-12
+    assert rel(oracle_lib.moments2d(Ho, ops["DG"], ops["VX"], st, 40), mu_ref) > 1e-3  # the order matters
+
+
+@pytest.mark.parametrize("formula", [0, 1])
+def test_kubo_fft_operator_order_vs_ref(oracle_lib, tmp_path, formula):
+    """Kubo_solver_FFT::compute(OPL, OPR, gen) (src/Kubo_solver_FFT.cpp:12) with OPL != OPR."""
+    N, d, ops, (bw, bc) = _graphene_with_diagonal(tmp_path, oracle_lib, 2, 23)
+    M, nump = 32, 64
+    out = oracle_lib.run_ref_harness(["kuboFFT", "gr", "VX", "DG", M, nump, formula, "states.txt"], d)
+    ref = np.loadtxt(os.path.join(d, out["out"]))
+    Ho = oracle_lib.Op(*formats.read_csr(os.path.join(d, "operators", "gr.HAM.CSR"))[1:]).rescale(2 / bw,
+                                                                                                   -bc / (bw / 2))
+    st = formats.read_state_file(os.path.join(d, "states.txt"))
+    E, s, integ, _ = oracle_lib.kubo_fft(Ho, ops["VX"], ops["DG"], st, M, nump, formula, N, bw, bc)
+    assert np.abs(s - ref[:, 1]).max() < 2e-6 * np.abs(s).max()
