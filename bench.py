@@ -338,7 +338,13 @@ def main():
         roof = {"kernel": {"contraction": "zgemm_cn_f64 (mu_nm contraction)", "fft": "kubo_fft (per-site DFTs)"}[dom],
                 "bound": "tensor", "pipe": "fp64", "achieved": ach, "peak": fp64_peak, "unit": "TFLOP/s",
                 "frac": ach / fp64_peak, "peak_source": "FP64 DGEMM (torch.matmul 8192^3) measured in this run"}
-    roof["traffic"] = None
+    # DRAM bytes per launch of the dominant kernel: ncu capture of the 64x64-cell case
+    # (M = 256, K = 65,536; dram__bytes_read.sum + dram__bytes_write.sum), scaled by M*K,
+    # which the operand reads of both kernels are proportional to
+    traffic_per_mk = {"contraction": (566779904 + 27903744) / (256 * 65536),
+                      "fft": (545405952 + 114432) / (256 * 65536)}
+    roof["traffic"] = (traffic_per_mk[dom] * M * K) if dom in traffic_per_mk else None
+    roof["traffic_unit"] = "bytes per launch (scaled from the 64x64-cell ncu capture)"
     rec_ach = phases["recursion"]["bytes"] / (phases["recursion"]["ms"] * 1e-3) / 1e9
     for k in phases:
         phases[k]["ms"] = round(phases[k]["ms"], 4)
