@@ -156,6 +156,11 @@ __global__ void __launch_bounds__(kThreads)
     if (HAS_V) cache_rows<C>(vrp, vci, vv, r0, r1, smc + off, vrp, vci, vv);
     __syncthreads();
   }
+  // Rows: with the operators cached, this CTA's contiguous range; otherwise tiles of gpb
+  // rows dealt round-robin, so that all CTAs sweep the rows together and a row's
+  // neighbours (read by nearby tiles at about the same time) are still in L2.
+  const int rfirst = cache ? r0 : blockIdx.x * gpb, rend = cache ? r1 : n;
+  const int rstep = cache ? gpb : gridDim.x * gpb;
   for (int m = 0; m < M; ++m) {
     const bool doL = m + 1 < M;
     const C *xL = Lst + (size_t)m * blk;
@@ -172,7 +177,7 @@ __global__ void __launch_bounds__(kThreads)
       pR = m ? Rst + (size_t)(m - 1) * blk : nullptr;
       yR = doL ? Rst + (size_t)(m + 1) * blk : nullptr;
     }
-    for (int row = r0 + threadIdx.x / TPR; row < r1; row += gpb) {
+    for (int row = rfirst + threadIdx.x / TPR; row < rend; row += rstep) {
       C aL[VPT], aR[VPT];
 #pragma unroll
       for (int u = 0; u < VPT; ++u) aL[u] = aR[u] = zero2(C());
@@ -256,12 +261,14 @@ __global__ void __launch_bounds__(kThreads)
     cache_rows<C>(rp, ci, hv, r0, r1, smc1, rp, ci, hv);
     __syncthreads();
   }
+  const int rfirst = cache ? r0 : blockIdx.x * gpb, rend = cache ? r1 : n;  // as in k_recur_lr
+  const int rstep = cache ? gpb : gridDim.x * gpb;
   C *prev = nullptr, *cur = x0;
   for (int s = 0; s < steps; ++s) {
     const bool need_y = mode == 2 ? (2 * s + 1 < M) : (s + 1 < M);
     C *y = need_y ? (prev ? prev : b1) : nullptr;
     double2 d0 = make_double2(0, 0), d1 = make_double2(0, 0);
-    for (int row = r0 + threadIdx.x / TPR; row < r1; row += gpb) {
+    for (int row = rfirst + threadIdx.x / TPR; row < rend; row += rstep) {
       C acc[VPT];
 #pragma unroll
       for (int u = 0; u < VPT; ++u) acc[u] = zero2(C());

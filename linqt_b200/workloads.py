@@ -1,0 +1,129 @@
+"""Timing of the other workload families (one JSON line each), next to bench.py's
+Kubo-Bastin graphene workload:
+
+    python -m linqt_b200.workloads dos      # square L=256, 1 vector, M=1024, DOS (full size)
+    python -m linqt_b200.workloads cubic    # cubic Anderson L=100 (N=1e6), 64 vectors, M=1024 (1 of 4 seeds)
+    python -m linqt_b200.workloads spin     # Kane-Mele with spin, 64x64 cells, R=8, M=512, nump=1024
+
+Each line gives the device time per solve (CUDA events on the session stream, warm-up
+first), Chebyshev steps*nnz/s, the recursion's algorithmic bytes per second, and for the
+mixed-precision solve its error against FP64.  `spin` is the spin-transport case scaled
+from 512x512 cells, M = 1024, R = 32 (2.8e17 flop of contraction) to a size that runs in
+seconds; `cubic` is one disorder seed of the four.
+"""
+import argparse
+import json
+
+import numpy as np
+
+from . import lattices
+from .core import PREC_FP64, PREC_MIXED, Operator, Session, make_opts, kubo_bastin_dev, moments1d_dev
+
+
+def _timed(fn, reps, torch):
+    for _ in range(2):
+        fn()
+    torch.cuda.synchronize()
+    a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    a.record()
+    for _ in range(reps):
+        fn()
+    b.record()
+    torch.cuda.synchronize()
+    return a.elapsed_time(b) / reps
+
+
+def _ops(N, H, extra=()):
+    lo, hi = lattices.gershgorin_bounds(N, *H)
+    bw, bc = 1.05 * (hi - lo), (hi + lo) / 2
+    sess = Session()
+    import torch
+    sess.set_stream(torch.cuda.current_stream())
+    Hg = Operator.from_csr(N, *H, session=sess)
+    Hg.rescale_to_chebyshev(bw, bc)
+    return sess, bw, bc, Hg, [Operator.from_csr(N, *X, session=sess) for X in extra]
+
+
+def run_1d(name, N, H, R, M, reps, phase_seed):
+    import torch
+    sess, bw, bc, Hg, _ = _ops(N, H)
+    st = lattices.random_phase_states(N, R, seed=phase_seed)
+    st_dev = torch.from_numpy(st.view(np.float64).copy()).cuda()
+    out = {}
+    for prec in (PREC_FP64, PREC_MIXED):
+        mu = torch.zeros(2 * M, dtype=torch.float64, device="cuda")
+        o = make_opts(precision=prec)
+        ms = _timed(lambda: moments1d_dev(Hg, None, st_dev, R, M, mu, opts=o, session=sess), reps, torch)
+        out[prec] = (ms, mu.cpu().numpy().view(np.complex128))
+    nnz = Hg.nnz
+    ms64, mu64 = out[PREC_FP64]
+    msmx, mumx = out[PREC_MIXED]
+    steps = M * R  # algorithmic recursion steps (columns x moments); the doubling identities do half
+    Rc = 1 << (R - 1).bit_length()
+    bytes_step = nnz * (16 + 4) + 4 * (N + 1) + 3 * 16 * N * Rc
+    executed_steps = (M + 1) // 2
+    return {
+        "workload": name, "N": N, "nnz_full": nnz, "R": R, "M": M,
+        "fp64": {"ms_per_solve": ms64, "steps_nnz_per_s": steps * nnz / (ms64 * 1e-3),
+                 "recursion_GBps": executed_steps * bytes_step / (ms64 * 1e-3) / 1e9},
+        "mixed": {"ms_per_solve": msmx, "steps_nnz_per_s": steps * nnz / (msmx * 1e-3),
+                  "err_mu_vs_fp64": float(np.abs(mumx - mu64).max() / np.abs(mu64).max())},
+    }
+
+
+def run_spin(Lc, R, M, nump, reps):
+    import torch
+    N, H, J = lattices.kane_mele(Lc, Lc, seed=31)
+    sess, bw, bc, Hg, (Jg,) = _ops(N, H, [J])
+    st = lattices.random_phase_states(N, R, seed=32)
+    st_dev = torch.from_numpy(st.view(np.float64).copy()).cuda()
+    res = {}
+    for prec in (PREC_FP64, PREC_MIXED):
+        mu = torch.zeros(2 * M * M, dtype=torch.float64, device="cuda")
+        out = torch.zeros(3 * nump, dtype=torch.float64, device="cuda")
+        o = make_opts(precision=prec)
+        sess.enable_timing(True)
+        sess.phase_times(reset=True)
+        ms = _timed(lambda: kubo_bastin_dev(Hg, Jg, Jg, st_dev, R, M, nump, bw, bc, mu, out, opts=o, session=sess),
+                    reps, torch)
+        ph, _ = sess.phase_times(reset=True)
+        sess.enable_timing(False)
+        n = reps + 2
+        res[prec] = (ms, [round(x / n, 3) for x in ph], mu.cpu().numpy().view(np.complex128),
+                     out.cpu().numpy()[nump:2 * nump])
+    nnz = Hg.nnz
+    lo, hi = int(0.05 * nump), int(0.95 * nump)
+    s64, smx = res[PREC_FP64][3], res[PREC_MIXED][3]
+    return {
+        "workload": "spin_kane_mele_%dx%d" % (Lc, Lc), "N": N, "nnz_full": nnz, "R": R, "M": M, "nump": nump,
+        "operator": "{s_z, V_x}/2",
+        "fp64": {"ms_per_solve": res[PREC_FP64][0], "phases_ms": res[PREC_FP64][1],
+                 "steps_nnz_per_s": 2 * M * R * nnz / (res[PREC_FP64][0] * 1e-3),
+                 "contraction_TFLOPs": 8.0 * M * M * N * R / (res[PREC_FP64][1][1] * 1e-3) / 1e12},
+        "mixed": {"ms_per_solve": res[PREC_MIXED][0], "phases_ms": res[PREC_MIXED][1],
+                  "steps_nnz_per_s": 2 * M * R * nnz / (res[PREC_MIXED][0] * 1e-3),
+                  "err_mu_vs_fp64": float(np.abs(res[PREC_MIXED][2] - res[PREC_FP64][2]).max()
+                                          / np.abs(res[PREC_FP64][2]).max()),
+                  "err_sigma_vs_fp64_interior90": float(np.abs(smx[lo:hi] - s64[lo:hi]).max()
+                                                        / np.abs(s64[lo:hi]).max())},
+    }
+
+
+def main(argv=None):
+    ap = argparse.ArgumentParser()
+    ap.add_argument("workload", choices=["dos", "cubic", "spin"])
+    ap.add_argument("--reps", type=int, default=5)
+    a = ap.parse_args(argv)
+    if a.workload == "dos":
+        N, H = lattices.square_lattice(256, 1.0, 1.0, 11)
+        r = run_1d("dos_square_256", N, H, 1, 1024, a.reps, 12)
+    elif a.workload == "cubic":
+        N, H = lattices.cubic_lattice(100, 1.0, 2.0, 41)
+        r = run_1d("dos_cubic_100_seed41", N, H, 64, 1024, a.reps, 45)
+    else:
+        r = run_spin(64, 8, 512, 1024, a.reps)
+    print(json.dumps(r))
+
+
+if __name__ == "__main__":
+    main()

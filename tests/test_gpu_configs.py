@@ -1,0 +1,103 @@
+"""Parity on the other workload families at sizes the oracle finishes in seconds:
+
+- plain DOS on the square lattice (1 vector, M = 1024, DOS on the Chebyshev grid);
+- spin transport on the Kane-Mele honeycomb with spin (4 orbitals per cell, NNN spin-orbit
+  and Rashba terms) with the spin-velocity operator {s_z, V_x}/2, FP64 and mixed;
+- large-DOS batching on the 3D cubic Anderson lattice (7-point stencil): many vectors in one
+  block, several disorder seeds, FP64 and mixed.
+"""
+import numpy as np
+import pytest
+
+import linqt_b200 as lq
+from linqt_b200 import lattices
+
+pytestmark = pytest.mark.gpu
+TOL = 1e-10
+
+
+def rel(a, b):
+    a, b = np.asarray(a), np.asarray(b)
+    return float(np.abs(a - b).max() / max(np.abs(b).max(), 1e-300))
+
+
+def ops(orc, N, H, extra=(), pad=1.05):
+    lo, hi = lattices.gershgorin_bounds(N, *H)
+    bw, bc = pad * (hi - lo), (hi + lo) / 2
+    Hg = lq.Operator.from_csr(N, *H)
+    Hg.rescale_to_chebyshev(bw, bc)
+    Ho = orc.Op(*H).rescale(2 / bw, -bc / (bw / 2))
+    return bw, bc, Hg, Ho, [(lq.Operator.from_csr(N, *X), orc.Op(*X)) for X in extra]
+
+
+def test_square_dos_one_vector_m1024(oracle_lib):
+    N, H = lattices.square_lattice(64, t=1.0, W=1.0, seed=11)
+    bw, bc = 2 * 1.05 * 4.5, 0.0
+    Hg = lq.Operator.from_csr(N, *H)
+    Hg.rescale_to_chebyshev(bw, bc)
+    Ho = oracle_lib.Op(*H).rescale(2 / bw, -bc / (bw / 2))
+    st = lattices.random_phase_states(N, 1, seed=12)
+    mu = lq.moments1d(Hg, None, st, 1024)
+    ref = oracle_lib.moments1d(Ho, None, st, 1024)
+    assert rel(mu, ref) < TOL
+    assert abs(mu[0] - 1.0) < 1e-12  # mu_0 = <r|r> for one normalised state
+    E, d = lq.dos_from_moments(mu, N, bw, bc, broad_meV=5.0)
+    Eo, do = oracle_lib.dos_fftgrid(oracle_lib.jackson1d(ref, bw, 5.0), N, bw, bc)
+    assert rel(E, Eo) < 1e-14 and rel(d, do) < 1e-10
+
+
+@pytest.fixture(scope="module")
+def kane_mele(oracle_lib):
+    N, H, J = lattices.kane_mele(6, 5, seed=31)
+    bw, bc, Hg, Ho, ((Jg, Jo),) = ops(oracle_lib, N, H, [J])
+    return dict(N=N, bw=bw, bc=bc, Hg=Hg, Ho=Ho, Jg=Jg, Jo=Jo)
+
+
+def test_kane_mele_spin_correlation(oracle_lib, kane_mele):
+    k = kane_mele
+    st = lattices.random_phase_states(k["N"], 3, seed=32)
+    M = 96
+    mu = lq.moments2d(k["Hg"], k["Jg"], k["Jg"], st, M)
+    ref = oracle_lib.moments2d(k["Ho"], k["Jo"], k["Jo"], st, M)
+    assert rel(mu, ref) < TOL
+    assert np.abs(mu - mu.conj().T).max() < 1e-13 * np.abs(mu).max()
+
+
+@pytest.mark.parametrize("precision,tol", [(lq.PREC_FP64, 1e-10), (lq.PREC_MIXED, 2e-4)])
+def test_kane_mele_spin_kubo_bastin(oracle_lib, kane_mele, precision, tol):
+    k = kane_mele
+    st = lattices.random_phase_states(k["N"], 2, seed=33)
+    M, nump = 64, 256
+    mu, (E, s, integ) = lq.kubo_bastin(k["Hg"], k["Jg"], k["Jg"], st, M, nump, k["bw"], k["bc"],
+                                       opts=lq.make_opts(precision=precision))
+    Eo, so, io, _ = oracle_lib.kubo_fft(k["Ho"], k["Jo"], k["Jo"], st, M, nump, lq.KUBO_BASTIN, k["N"], k["bw"],
+                                        k["bc"])
+    assert rel(E, Eo) < 1e-14
+    lo, hi = int(0.05 * nump), int(0.95 * nump)
+    assert rel(s[lo:hi], so[lo:hi]) < tol
+    assert rel(mu, oracle_lib.moments2d(k["Ho"], k["Jo"], k["Jo"], st, M)) < tol
+
+
+@pytest.mark.parametrize("seed", [41, 42, 43, 44])
+def test_cubic_dos_many_vectors(oracle_lib, seed):
+    N, H = lattices.cubic_lattice(10, t=1.0, W=2.0, seed=seed)
+    bw, bc, Hg, Ho, _ = ops(oracle_lib, N, H)
+    st = lattices.random_phase_states(N, 40, seed=45)  # ragged: padded to a 64-wide block
+    M = 512
+    mu = lq.moments1d(Hg, None, st, M)
+    ref = oracle_lib.moments1d(Ho, None, st, M)
+    assert rel(mu, ref) < TOL
+    mx = lq.moments1d(Hg, None, st, M, opts=lq.make_opts(precision=lq.PREC_MIXED))
+    assert rel(mx, ref) < 1e-4
+
+
+def test_large_operator_rows_not_cached(oracle_lib):
+    """N = 1e6 cubic lattice: the per-CTA operator slices exceed the shared-memory cache, so
+    the persistent recursions deal rows to CTAs in round-robin tiles."""
+    N, H = lattices.cubic_lattice(100, t=1.0, W=2.0, seed=42)
+    bw, bc, Hg, Ho, _ = ops(oracle_lib, N, H)
+    st = lattices.random_phase_states(N, 1, seed=46)
+    mu = lq.moments1d(Hg, None, st, 48)
+    assert rel(mu, oracle_lib.moments1d(Ho, None, st, 48)) < TOL
+    mu2 = lq.moments2d(Hg, None, None, st, 12)
+    assert rel(mu2, oracle_lib.moments2d(Ho, None, None, st, 12)) < TOL
