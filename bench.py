@@ -48,6 +48,21 @@ def build_inputs(rank=0):
     return N, H, V, bw, bc, st
 
 
+def max_over_ranks(x, dist, device):
+    """The slowest rank's time (replicas run the same work; the job ends with the last)."""
+    if dist is None:
+        return x
+    import torch
+    t = torch.tensor([x], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def whole_job_rates(units_per_rank, world, dev_ms, e2e_ms):
+    """Whole-job throughput: all ranks' units over the max-over-ranks times."""
+    return world * units_per_rank / (dev_ms * 1e-3), world * units_per_rank / (e2e_ms * 1e-3)
+
+
 def nnz_full(N, H):
     rp, col, _ = H
     rows = np.repeat(np.arange(N), np.diff(rp))
@@ -300,18 +315,10 @@ def main():
     barrier()
     e2e_ms = 1e3 * (time.perf_counter() - t0) / args.steps
 
-    def max_over_ranks(x):
-        if dist is None:
-            return x
-        t = torch.tensor([x], dtype=torch.float64, device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        return float(t.item())
-
-    dev_ms = max_over_ranks(dev_ms)
-    e2e_ms = max_over_ranks(e2e_ms)
+    dev_ms = max_over_ranks(dev_ms, dist, "cuda")
+    e2e_ms = max_over_ranks(e2e_ms, dist, "cuda")
     units = 2 * M * R * nnz  # recursion steps x nnz per solve and rank
-    value = world * units / (dev_ms * 1e-3)
-    e2e = world * units / (e2e_ms * 1e-3)
+    value, e2e = whole_job_rates(units, world, dev_ms, e2e_ms)
 
     # ---- roofline of the dominant phase
     hbm_peak, bf16_peak, peak_src = measured_peaks()
@@ -374,7 +381,7 @@ def main():
         f1.record(stream)
         torch.cuda.synchronize()
         barrier()
-        o_ms = max_over_ranks(f0.elapsed_time(f1) / args.steps)
+        o_ms = max_over_ranks(f0.elapsed_time(f1) / args.steps, dist, "cuda")
         o_phase, o_launch = sess.phase_times(reset=True)
         sess.enable_timing(False)
         solve_dev()
