@@ -203,6 +203,33 @@ int linqt_dos_from_moments(linqt_session *s, const double *mu, int M, int N, dou
 int linqt_bastin_from_moments(linqt_session *s, const double *mu, int M0, int M1, int N, double band_width,
                               double band_center, double broad_meV, double xbound, int num_div, double *E,
                               double *sigma, int *num_out);
+/* LinQT's energy-sum post-processors on a 2D table: Moments2D::ApplyJacksonKernel(broad,
+ * broad) and then, for variant
+ *   LINQT_SUM_BASTIN      kuboBastinFromChebmom{,_FFTgrid}   (running left-rectangle integral)
+ *   LINQT_SUM_GREENWOOD   kuboGreenwoodFromChebmom{,_FFTgrid} (the kernel itself)
+ *   LINQT_SUM_BASTIN_I    kuboBastinIFromChebmom             (mean of neighbouring points)
+ *   LINQT_SUM_BASTIN_II   kuboBastinIIFromChebmom            (running sum of (k_i + k_{i+1}) dE)
+ *   LINQT_SUM_BASTIN_SEA  kuboBastinSeaFromChebmom           (running trapezoid integral)
+ *   LINQT_SUM_BASTIN_SURF kuboBastinSurfFromChebmom          (mean of neighbouring points)
+ * on grid LINQT_GRID_UNIFORM (num_div points in [-xbound, xbound]; num_div <= 0: 30*M'),
+ * LINQT_GRID_CHEBYSHEV (x_i = cos(pi (2i + 1/2)/num_div), the _FFTgrid Greenwood order;
+ * num_div <= 0: M') or LINQT_GRID_CHEBYSHEV_ASCENDING (the same points in the ascending order
+ * of the _FFTgrid Bastin driver).  M' = max of the truncated moment counts.  Writes
+ * *num_out = num_div - 1 points: E = x a + c and the driver's second column.  The drivers
+ * other than kuboBastinFromChebmom use xbound = 1, where the first point divides by zero;
+ * the same non-finite values result here.  Files src/kubo*FromChebmom*.cpp:33-90. */
+enum {
+  LINQT_SUM_BASTIN = 0,
+  LINQT_SUM_GREENWOOD = 1,
+  LINQT_SUM_BASTIN_I = 2,
+  LINQT_SUM_BASTIN_II = 3,
+  LINQT_SUM_BASTIN_SEA = 4,
+  LINQT_SUM_BASTIN_SURF = 5
+};
+enum { LINQT_GRID_UNIFORM = 0, LINQT_GRID_CHEBYSHEV = 1, LINQT_GRID_CHEBYSHEV_ASCENDING = 2 };
+int linqt_kubo_from_moments(linqt_session *s, const double *mu, int M0, int M1, int N, double band_width,
+                            double band_center, double broad_meV, int variant, int grid, double xbound, int num_div,
+                            double *E, double *out, int *num_out);
 /* Jackson kernels alone (in place on host arrays; returns the truncated sizes). */
 int linqt_jackson1d(double *mu, int M, double band_width, double broad_meV, int *M_out);
 int linqt_jackson2d(double *mu, int M0, int M1, double band_width, double b0, double b1, int *M0_out, int *M1_out);

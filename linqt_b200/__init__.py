@@ -10,11 +10,12 @@ from .core import (KUBO_BASTIN, KUBO_GREENWOOD, PREC_FP32, PREC_FP64, PREC_MIXED
                    STORAGE_GENERAL, STORAGE_HERMITIAN_UPPER, Operator, Session, bastin_from_moments,
                    dos_from_moments, jackson1d, jackson2d, kubo_bastin, kubo_bastin_dev, kubo_bastin_host_ptr,
                    kubo_fft, kubo_fft_dev, make_opts, moments1d,
-                   moments1d_dev, moments1d_noalloc, moments2d, moments2d_dev, random_phase_states_dev)
+                   moments1d_dev, moments1d_noalloc, moments2d, moments2d_dev, random_phase_states_dev,
+                   kubo_from_moments, GRID_UNIFORM, GRID_CHEBYSHEV, GRID_CHEBYSHEV_ASCENDING)
 
 __all__ = [
     "LinqtError", "load", "Operator", "Session", "moments1d", "moments1d_dev", "moments1d_noalloc", "moments2d", "moments2d_dev",
     "kubo_fft", "kubo_fft_dev", "kubo_bastin", "kubo_bastin_dev", "kubo_bastin_host_ptr", "dos_from_moments", "bastin_from_moments", "jackson1d", "jackson2d",
     "make_opts", "PREC_FP64", "PREC_MIXED", "PREC_FP32", "KUBO_GREENWOOD", "KUBO_BASTIN",
-    "STORAGE_HERMITIAN_UPPER", "STORAGE_GENERAL", "random_phase_states_dev",
+    "STORAGE_HERMITIAN_UPPER", "STORAGE_GENERAL", "random_phase_states_dev", "kubo_from_moments",
 ]

@@ -81,6 +81,8 @@ SIGNATURES = {
                                        P_double, P_int]),
     "linqt_bastin_from_moments": (c_int, [c_void_p, P_double, c_int, c_int, c_int, c_double, c_double, c_double,
                                           c_double, c_int, P_double, P_double, P_int]),
+    "linqt_kubo_from_moments": (c_int, [c_void_p, P_double, c_int, c_int, c_int, c_double, c_double, c_double, c_int,
+                                        c_int, c_double, c_int, P_double, P_double, P_int]),
     "linqt_jackson1d": (c_int, [P_double, c_int, c_double, c_double, P_int]),
     "linqt_jackson2d": (c_int, [P_double, c_int, c_int, c_double, c_double, c_double, P_int, P_int]),
     "linqt_server_create": (c_int, [c_int, ctypes.c_size_t, c_int, ctypes.POINTER(c_void_p)]),

@@ -318,6 +318,25 @@ def bastin_from_moments(mu, N, band_width, band_center, broad_meV, xbound=0.99, 
     return E[: n.value], s[: n.value]
 
 
+SUM_VARIANTS = {"bastin": 0, "greenwood": 1, "bastin_I": 2, "bastin_II": 3, "bastin_sea": 4, "bastin_surf": 5}
+GRID_UNIFORM, GRID_CHEBYSHEV, GRID_CHEBYSHEV_ASCENDING = 0, 1, 2
+
+
+def kubo_from_moments(mu, N, band_width, band_center, broad_meV, variant="bastin", grid=GRID_UNIFORM, xbound=1.0,
+                      num_div=0, session=None):
+    """(E, column) of LinQT's energy-sum post-processor `variant` (kubo*FromChebmom*) on a 2D table,
+    Jackson kernel included; see linqt_kubo_from_moments in include/linqt_gpu.h."""
+    m = np.ascontiguousarray(mu, dtype=np.complex128)
+    M0, M1 = m.shape
+    cap = num_div if num_div > 0 else 30 * max(M0, M1)
+    E, out = np.zeros(cap), np.zeros(cap)
+    n = ctypes.c_int()
+    check(load().linqt_kubo_from_moments(_sh(session), _dp(m.view(np.float64)), M0, M1, N, band_width, band_center,
+                                         broad_meV, SUM_VARIANTS[variant], grid, xbound, num_div, _dp(E), _dp(out),
+                                         ctypes.byref(n)))
+    return E[: n.value], out[: n.value]
+
+
 def jackson1d(mu, band_width, broad_meV):
     m = _c128(mu).copy()
     n = ctypes.c_int()

@@ -1076,4 +1076,30 @@ int linqt_bastin_from_moments(linqt_session *s, const double *mu, int M0, int M1
   });
 }
 
+int linqt_kubo_from_moments(linqt_session *s, const double *mu, int M0, int M1, int N, double band_width,
+                            double band_center, double broad_meV, int variant, int grid, double xbound, int num_div,
+                            double *E, double *out, int *num_out) {
+  return guarded([&] {
+    LQ_REQUIRE(mu && E && out && M0 > 0 && M1 > 0 && band_width > 0 && broad_meV > 0, "bad argument");
+    LQ_REQUIRE(variant >= LINQT_SUM_BASTIN && variant <= LINQT_SUM_BASTIN_SURF, "unknown variant");
+    LQ_REQUIRE(grid >= LINQT_GRID_UNIFORM && grid <= LINQT_GRID_CHEBYSHEV_ASCENDING, "unknown grid");
+    LQ_REQUIRE(grid != LINQT_GRID_UNIFORM || (xbound > 0 && xbound <= 1), "xbound must lie in (0, 1]");
+    Session *r = resolve(s);
+    const int T0 = jackson_cut(M0, band_width, broad_meV), T1 = jackson_cut(M1, band_width, broad_meV);
+    const int Mt = std::max(T0, T1);
+    const int nd = num_div > 0 ? num_div : (grid == LINQT_GRID_UNIFORM ? 30 * Mt : Mt);
+    LQ_REQUIRE(nd >= 2, "num_div must be >= 2");
+    double2 *d_mu = (double2 *)r->get("bas_mu", sizeof(double2) * (size_t)M0 * M1);
+    double2 *d_muj = (double2 *)r->get("bas_muj", sizeof(double2) * (size_t)T0 * T1);
+    double *d_out = (double *)r->get("bas_out", sizeof(double) * 2 * (size_t)nd);
+    LQ_CUDA(cudaMemcpyAsync(d_mu, mu, sizeof(double2) * (size_t)M0 * M1, cudaMemcpyHostToDevice, r->stream));
+    jackson2d_dev(r, d_mu, M0, M1, T0, T1, d_muj);
+    energy_sums(r, d_muj, T0, T1, N, band_width, band_center, variant, grid, xbound, nd, d_out, d_out + nd);
+    LQ_CUDA(cudaMemcpyAsync(E, d_out, sizeof(double) * (nd - 1), cudaMemcpyDeviceToHost, r->stream));
+    LQ_CUDA(cudaMemcpyAsync(out, d_out + nd, sizeof(double) * (nd - 1), cudaMemcpyDeviceToHost, r->stream));
+    LQ_CUDA(cudaStreamSynchronize(r->stream));
+    if (num_out) *num_out = nd - 1;
+  });
+}
+
 }  // extern "C"

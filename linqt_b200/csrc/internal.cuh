@@ -147,6 +147,17 @@ struct DeviceOp {
 // ---------------------------------------------------------------------------
 // sessions: stream + workspace cache + phase timing
 // ---------------------------------------------------------------------------
+// Index map of rearrange_crescent_order (src/Kubo_solver_FFT_postProcess.cpp:98-116): the
+// reference interleaves x[k] and x[n-k-1] (k < n/2) and then reverses the array, so output j
+// holds y[n-1-j] with y[2k] = x[k], y[2k+1] = x[n-k-1] and, for odd n, y[n-1] = x[n-1].
+__host__ __device__ inline int rearranged_source(int j, int n) {
+  const int i = n - 1 - j;
+  const int h = n / 2;
+  if ((i & 1) == 0 && i / 2 < h) return i / 2;
+  if ((i & 1) == 1 && (i - 1) / 2 < h) return n - (i - 1) / 2 - 1;
+  return i;
+}
+
 enum Phase { PH_RECURSION = 0, PH_CONTRACT = 1, PH_FFT = 2, PH_OTHER = 3 };
 
 struct Session {
@@ -230,6 +241,10 @@ void kubo_postprocess(Session *s, const double2 *acc, int R, int nump, int formu
 // reconstructions
 void dos_grid(Session *s, const double2 *mu, int M, int N, double band_width, double band_center, double *E,
               double *dos);
+// LinQT's post-processor sums (variant 0 Bastin, 1 Greenwood, 2 Bastin I, 3 Bastin II, 4 sea,
+// 5 surface) on a Jackson-damped device table; grid 0 uniform, 1 Chebyshev nodes, 2 ascending
+void energy_sums(Session *s, const double2 *mu, int M0, int M1, int N, double band_width, double band_center,
+                 int variant, int grid, double xbound, int num_div, double *E, double *out);
 void bastin_grid(Session *s, const double2 *mu, int M0, int M1, int N, double band_width, double band_center,
                  double xbound, int num_div, double *E, double *sigma);
 

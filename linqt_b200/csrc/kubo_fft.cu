@@ -436,17 +436,6 @@ __global__ void k_sum_parts(const double2 *__restrict__ part, int nb, int len, d
   }
 }
 
-// Index map of rearrange_crescent_order (src/Kubo_solver_FFT_postProcess.cpp:98-116): the
-// reference interleaves x[k] and x[n-k-1] (k < n/2) and then reverses the array, so output j
-// holds y[n-1-j] with y[2k] = x[k], y[2k+1] = x[n-k-1] and, for odd n, y[n-1] = x[n-1].
-__device__ __forceinline__ int rearranged_source(int j, int n) {
-  const int i = n - 1 - j;
-  const int h = n / 2;
-  if ((i & 1) == 0 && i / 2 < h) return i / 2;
-  if ((i & 1) == 1 && (i - 1) / 2 < h) return n - (i - 1) / 2 - 1;
-  return i;
-}
-
 // Post-processing: final_data = acc / R (the running mean of Kubo_solver_FFT::update_data
 // over R states), then Bastin_postProcess (src/Kubo_solver_FFT_postProcess.cpp:120-273) or
 // Greenwood_postProcess (:279-397).  out = [E (nump), sigma (nump), integrand (nump)].

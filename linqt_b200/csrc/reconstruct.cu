@@ -48,50 +48,102 @@ __global__ void k_dos(const double2 *__restrict__ mu, int M, double N, double a,
   }
 }
 
-// Table conj(DgreenR_chebF(E_i, m)) for the Bastin sum (include/chebyshev_coefficients.hpp:25-32):
-// DG(x, m) = -i (x - i f0)^m (x + i m f0) / f0^3 with (x - i f0)^m = exp(-i m acos x).
-__global__ void k_dgreen_table(int num_div, int M1, double xbound, double2 *__restrict__ tab) {
+// ---------------------------------------------------------------------------
+// The energy sums of LinQT's post-processors (kuboBastinFromChebmom{,_FFTgrid},
+// kuboGreenwoodFromChebmom{,_FFTgrid}, kuboBastin{I,II,Sea,Surf}FromChebmom) on a
+// Jackson-damped table mu[M0][M1]:  kernel(x) = pref * sum_{m0,m1} f(x, m0, m1, mu).
+// Each is evaluated as Y(i, m0) = sum_m1 B(x_i, m1) mu(m0, m1) (an FP64 GEMM against a
+// coefficient table) and a per-energy sum over m0 with the left coefficient.  The
+// coefficient functions are those of include/chebyshev_coefficients.hpp:9-32:
+//   delta(x, m)  = cos(m acos x) / f0 / pi,            f0 = sqrt(1 - x^2)
+//   G(x, m)      = -i (x - i f0)^m / f0,                (x - i f0)^m = exp(-i m acos x)
+//   DG(x, m)     = -i (x - i f0)^m (x + i m f0) / f0^3
+// ---------------------------------------------------------------------------
+enum CoefKind { COEF_DELTA = 0, COEF_G = 1, COEF_DG = 2, COEF_REDG2 = 3 };
+
+// energy i of the grid: 0 uniform in [-xbound, xbound]; 1 cos(pi (2i + 1/2)/n); 2 grid 1 in
+// the ascending order of rearrange_crescent_order (src/kuboBastinFromChebmom_FFTgrid.cpp:18-36)
+__device__ __host__ inline double grid_energy(int grid, int i, int n, double xbound) {
+  if (grid == 0) return -xbound + i * (2 * xbound) / (n - 1);
+  if (grid == 2) i = rearranged_source(i, n);
+  return cos(M_PI * (2 * i + 0.5) / n);
+}
+
+__device__ inline double2 coef(int kind, double x, int m) {
+  const double f0 = sqrt(1.0 - x * x), th = acos(x);
+  double sn, cs;
+  sincos(m * th, &sn, &cs);
+  if (kind == COEF_DELTA) return make_double2(cs / f0 / M_PI, 0.0);
+  const double2 p = make_double2(cs, -sn);  // (x - i f0)^m
+  if (kind == COEF_G) return make_double2(p.y / f0, -p.x / f0);  // -i p / f0
+  const double2 q = cmul(p, make_double2(x, m * f0));             // * (x + i m f0)
+  const double inv = 1.0 / (f0 * f0 * f0);
+  const double2 dg = make_double2(q.y * inv, -q.x * inv);          // -i q / f0^3
+  if (kind == COEF_DG) return dg;
+  return make_double2(dg.x + dg.x, 0.0);                           // Re DG + conj(Re DG)
+}
+
+// tab(i, m) = conj(B(x_i, m)): zgemm_cn conjugates its first operand
+__global__ void k_coef_table(int kind, int grid, int num_div, int M1, double xbound, double2 *__restrict__ tab) {
   const long tot = (long)num_div * M1;
   for (long t = blockIdx.x * (long)blockDim.x + threadIdx.x; t < tot; t += (long)gridDim.x * blockDim.x) {
     const int i = (int)(t / M1), m = (int)(t % M1);
-    const double x = -xbound + i * (2 * xbound) / (num_div - 1);
-    const double f0 = sqrt(1.0 - x * x), th = acos(x);
-    double sn, cs;
-    sincos(m * th, &sn, &cs);
-    const double2 p = make_double2(cs, -sn);            // (x - i f0)^m
-    const double2 q = cmul(p, make_double2(x, m * f0));  // * (x + i m f0)
-    const double inv = 1.0 / (f0 * f0 * f0);
-    const double2 dg = make_double2(q.y * inv, -q.x * inv);  // -i * q / f0^3
-    tab[t] = cconj(dg);
+    tab[t] = cconj(coef(kind, grid_energy(grid, i, num_div, xbound), m));
   }
 }
 
-// kernel_i = -2N/a^2 sum_m0 delta(E_i, m0) Im(Y(i, m0)),  Y(i, m0) = sum_m1 DG(E_i,m1) mu(m0,m1)
-// (src/kuboBastinFromChebmom.cpp:63-72).  One warp per energy.
-__global__ void k_bastin_kernel(const double2 *__restrict__ Y, int num_div, int M0, double pref, double xbound,
-                                double *__restrict__ kern) {
+// kernel_i = pref * sum_m0 (left coefficient x Y), one warp per energy, fixed order
+__global__ void k_energy_sums(int variant, int grid, const double2 *__restrict__ Y1, const double2 *__restrict__ Y2,
+                              int num_div, int M0, double pref, double xbound, double *__restrict__ kern) {
   const int w = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, l = threadIdx.x & 31;
   if (w >= num_div) return;
-  const double x = -xbound + w * (2 * xbound) / (num_div - 1);
-  const double f0 = sqrt(1.0 - x * x), th = acos(x);
+  const double x = grid_energy(grid, w, num_div, xbound);
   double acc = 0.0;
-  for (int m0 = l; m0 < M0; m0 += 32) acc += cos(m0 * th) / f0 / M_PI * Y[(size_t)w * M0 + m0].y;
+  for (int m0 = l; m0 < M0; m0 += 32) {
+    const double2 y1 = Y1[(size_t)w * M0 + m0];
+    switch (variant) {
+      case 0:  // Bastin: delta(m0) Im(DG(m1) mu)
+      case 1:  // Greenwood: delta(m0) Im(G(m1) mu)
+      case 2:  // Bastin I: as Greenwood
+        acc += coef(COEF_DELTA, x, m0).x * y1.y;
+        break;
+      case 3: {  // Bastin II: -Re(G(m0) DG(m1) mu - DG(m0) G(m1) mu)
+        const double2 y2 = Y2[(size_t)w * M0 + m0];
+        const double2 t = csub(cmul(coef(COEF_G, x, m0), y1), cmul(coef(COEF_DG, x, m0), y2));
+        acc += -t.x;
+        break;
+      }
+      case 4: {  // sea: -Re((G - conj G)(m0) (2 Re DG)(m1) mu)
+        const double2 g = coef(COEF_G, x, m0);
+        acc += -cmul(csub(g, cconj(g)), y1).x;
+        break;
+      }
+      default:  // surface: delta(m0) delta(m1) Re mu
+        acc += coef(COEF_DELTA, x, m0).x * y1.x;
+        break;
+    }
+  }
   for (int o = 16; o > 0; o >>= 1) acc += __shfl_down_sync(0xffffffffu, acc, o);
   if (l == 0) kern[w] = acc * pref;
 }
 
-// left-rectangle cumulative integral (src/kuboBastinFromChebmom.cpp:74-81); single thread,
-// fixed order, FP64
-__global__ void k_bastin_integrate(const double *__restrict__ kern, int num_div, double xbound, double a, double bc,
-                                   double *__restrict__ E, double *__restrict__ sigma) {
+// the drivers' output columns (num_div - 1 points); single thread, fixed order, FP64
+__global__ void k_energy_output(int variant, int grid, const double *__restrict__ kern, int num_div, double xbound,
+                                double a, double bc, double *__restrict__ E, double *__restrict__ out) {
   if (threadIdx.x != 0 || blockIdx.x != 0) return;
   double acc = 0.0;
   for (int i = 0; i < num_div - 1; ++i) {
-    const double e0 = -xbound + i * (2 * xbound) / (num_div - 1);
-    const double e1 = -xbound + (i + 1) * (2 * xbound) / (num_div - 1);
-    acc += kern[i] * (e1 - e0);
+    const double e0 = grid_energy(grid, i, num_div, xbound), e1 = grid_energy(grid, i + 1, num_div, xbound);
+    const double de = e1 - e0;
     E[i] = e0 * a + bc;
-    sigma[i] = acc;
+    switch (variant) {
+      case 0: acc += kern[i] * de; out[i] = acc; break;
+      case 1: out[i] = kern[i]; break;
+      case 2: out[i] = 0.5 * (kern[i] + kern[i + 1]); break;
+      case 3: acc += (kern[i] + kern[i + 1]) * de; out[i] = acc; break;
+      case 4: acc += 0.5 * (kern[i] + kern[i + 1]) * de; out[i] = acc; break;
+      default: out[i] = (kern[i + 1] + kern[i]) / 2.0; break;
+    }
   }
 }
 
@@ -158,23 +210,37 @@ void dos_grid(Session *s, const double2 *mu, int M, int N, double band_width, do
   LQ_LAUNCHED();
 }
 
-void bastin_grid(Session *s, const double2 *mu, int M0, int M1, int N, double band_width, double band_center,
-                 double xbound, int num_div, double *E, double *sigma) {
-  double2 *tab = (double2 *)s->get("bastin_dg", sizeof(double2) * (size_t)num_div * M1);
-  double2 *Y = (double2 *)s->get("bastin_y", sizeof(double2) * (size_t)num_div * M0);
-  double *kern = (double *)s->get("bastin_kern", sizeof(double) * (size_t)num_div);
+void energy_sums(Session *s, const double2 *mu, int M0, int M1, int N, double band_width, double band_center,
+                 int variant, int grid, double xbound, int num_div, double *E, double *out) {
+  LQ_REQUIRE(variant >= 0 && variant <= 5 && grid >= 0 && grid <= 2 && num_div >= 2, "energy sums: bad argument");
+  static const int kind1[6] = {COEF_DG, COEF_G, COEF_G, COEF_DG, COEF_REDG2, COEF_DELTA};
+  double2 *tab = (double2 *)s->get("esum_tab", sizeof(double2) * (size_t)num_div * M1);
+  double2 *Y1 = (double2 *)s->get("esum_y1", sizeof(double2) * (size_t)num_div * M0);
+  double2 *Y2 = variant == 3 ? (double2 *)s->get("esum_y2", sizeof(double2) * (size_t)num_div * M0) : nullptr;
+  double *kern = (double *)s->get("esum_kern", sizeof(double) * (size_t)num_div);
   const long tot = (long)num_div * M1;
   const int g = (int)std::max(1L, std::min((tot + 255) / 256, (long)s->sm_count * 16));
-  k_dgreen_table<<<g, 256, 0, s->stream>>>(num_div, M1, xbound, tab);
+  // Y(i, m0) = sum_m1 conj(tab(i, m1)) mu(m0, m1) = sum_m1 B(x_i, m1) mu(m0, m1)
+  k_coef_table<<<g, 256, 0, s->stream>>>(kind1[variant], grid, num_div, M1, xbound, tab);
   LQ_LAUNCHED();
-  // Y(i, m0) = sum_m1 conj(tab(i, m1)) mu(m0, m1) = sum_m1 DG(E_i, m1) mu(m0, m1)
-  zgemm_cn(s, tab, num_div, mu, M0, M1, Y, false);
-  const double a = band_width / 2.0;
-  const double pref = -2.0 * N / a / a;
-  k_bastin_kernel<<<(num_div * 32 + 255) / 256, 256, 0, s->stream>>>(Y, num_div, M0, pref, xbound, kern);
+  zgemm_cn(s, tab, num_div, mu, M0, M1, Y1, false);
+  if (Y2) {
+    k_coef_table<<<g, 256, 0, s->stream>>>(COEF_G, grid, num_div, M1, xbound, tab);
+    LQ_LAUNCHED();
+    zgemm_cn(s, tab, num_div, mu, M0, M1, Y2, false);
+  }
+  const double a = band_width / 2.0, w = N / a / a;
+  const double pref[6] = {-2.0 * w, -w, -w, w / 2 / M_PI, w / 2 / M_PI, M_PI * w};
+  k_energy_sums<<<(num_div * 32 + 255) / 256, 256, 0, s->stream>>>(variant, grid, Y1, Y2, num_div, M0,
+                                                                    pref[variant], xbound, kern);
   LQ_LAUNCHED();
-  k_bastin_integrate<<<1, 32, 0, s->stream>>>(kern, num_div, xbound, a, band_center, E, sigma);
+  k_energy_output<<<1, 32, 0, s->stream>>>(variant, grid, kern, num_div, xbound, a, band_center, E, out);
   LQ_LAUNCHED();
+}
+
+void bastin_grid(Session *s, const double2 *mu, int M0, int M1, int N, double band_width, double band_center,
+                 double xbound, int num_div, double *E, double *sigma) {
+  energy_sums(s, mu, M0, M1, N, band_width, band_center, 0, 0, xbound, num_div, E, sigma);
 }
 
 void gershgorin(Session *s, const DeviceOp &A, double *lo, double *hi) {

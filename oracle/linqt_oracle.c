@@ -401,6 +401,92 @@ int lo_bastin_from_moments(const double *mu, int M0, int M1, int N, double band_
   return 0;
 }
 
+/* greenR_chebF (include/chebyshev_coefficients.hpp:16-23) */
+static cplx greenR_chebF(double x, double m) {
+  const double f0 = sqrt(1.0 - x * x);
+  const cplx fm = cpow(x - I * f0, m);
+  return -I * fm / f0;
+}
+
+/* rearrange_crescent_order of src/kuboBastinFromChebmom_FFTgrid.cpp:18-36 */
+static void lo_rearrange(double *v, int n) {
+  double *o = malloc(sizeof(double) * (size_t)n);
+  memcpy(o, v, sizeof(double) * (size_t)n);
+  for (int k = 0; k < n / 2; k++) {
+    v[2 * k] = o[k];
+    v[2 * k + 1] = o[n - k - 1];
+  }
+  for (int k = 0; k < n / 2; k++) {
+    const double t = v[k];
+    v[k] = v[n - k - 1];
+    v[n - k - 1] = t;
+  }
+  free(o);
+}
+
+/* The energy sums of LinQT's post-processors on a Jackson-damped table mu[M0][M1]:
+ *   variant 0 Bastin     (src/kuboBastinFromChebmom.cpp:63-81, _FFTgrid.cpp:88-106)
+ *   variant 1 Greenwood  (src/kuboGreenwoodFromChebmom.cpp:61-74, _FFTgrid.cpp:62-76)
+ *   variant 2 Bastin I   (src/kuboBastinIFromChebmom.cpp:63-84)
+ *   variant 3 Bastin II  (src/kuboBastinIIFromChebmom.cpp:62-88)
+ *   variant 4 Bastin sea (src/kuboBastinSeaFromChebmom.cpp:62-88)
+ *   variant 5 Bastin surface (src/kuboBastinSurfFromChebmom.cpp:62-82)
+ * grid 0: num_div points uniform in [-xbound, xbound]; grid 1: x_i = cos(pi (2i + 1/2)/num_div);
+ * grid 2: grid 1 in the rearranged (ascending) order of the Bastin FFT-grid driver.
+ * Writes num_div - 1 points: E = x a + c and the driver's output column. */
+int lo_kubo_from_moments(int variant, int grid, const double *mu, int M0, int M1, int N, double band_width,
+                         double band_center, double xbound, int num_div, double *E, double *out) {
+  if (num_div < 2 || variant < 0 || variant > 5 || grid < 0 || grid > 2) return -1;
+  const double a = band_width / 2.0, w = N / a / a;
+  double *kernel = calloc((size_t)num_div, sizeof(double));
+  double *en = malloc(sizeof(double) * (size_t)num_div);
+  for (int i = 0; i < num_div; i++)
+    en[i] = grid == 0 ? -xbound + i * (2 * xbound) / (num_div - 1) : cos(M_PI * (2 * i + 0.5) / num_div);
+  if (grid == 2) lo_rearrange(en, num_div);
+#pragma omp parallel for schedule(dynamic, 8)
+  for (int i = 0; i < num_div; i++) {
+    const double x = en[i];
+    double k = 0.0;
+    for (int m0 = 0; m0 < M0; m0++) {
+      const double d0 = delta_chebF(x, m0);
+      const cplx g0 = greenR_chebF(x, m0), dg0 = DgreenR_chebF(x, m0);
+      for (int m1 = 0; m1 < M1; m1++) {
+        const cplx muv = mu[2 * ((long)m0 * M1 + m1)] + I * mu[2 * ((long)m0 * M1 + m1) + 1];
+        switch (variant) {
+          case 0: k += d0 * cimag(DgreenR_chebF(x, m1) * muv); break;
+          case 1:
+          case 2: k += d0 * cimag(greenR_chebF(x, m1) * muv); break;
+          case 3: k += -creal((g0 * DgreenR_chebF(x, m1) - dg0 * greenR_chebF(x, m1)) * muv); break;
+          case 4: {
+            const double dgr = creal(DgreenR_chebF(x, m1));
+            k += -creal((g0 - conj(g0)) * (dgr + dgr) * muv);
+            break;
+          }
+          default: k += d0 * delta_chebF(x, m1) * creal(muv); break;
+        }
+      }
+    }
+    const double pref[6] = {-2.0 * w, -w, -w, w / 2 / M_PI, w / 2 / M_PI, M_PI * w};
+    kernel[i] = k * pref[variant];
+  }
+  double acc = 0.0;
+  for (int i = 0; i < num_div - 1; i++) {
+    const double de = en[i + 1] - en[i];
+    E[i] = en[i] * a + band_center;
+    switch (variant) {
+      case 0: acc += kernel[i] * de; out[i] = acc; break;
+      case 1: out[i] = kernel[i]; break;
+      case 2: out[i] = 0.5 * (kernel[i] + kernel[i + 1]); break;
+      case 3: acc += (kernel[i] + kernel[i + 1]) * de; out[i] = acc; break;
+      case 4: acc += 0.5 * (kernel[i] + kernel[i + 1]) * de; out[i] = acc; break;
+      default: out[i] = (kernel[i + 1] + kernel[i]) / 2.0; break;
+    }
+  }
+  free(kernel);
+  free(en);
+  return 0;
+}
+
 /* ---------------------------------------------------------------------------
  * Kubo_solver_FFT.  The reference uses FFTW backward DFTs (exponent +1,
  * unnormalised) of length nump on zero-padded inputs; here an iterative radix-2

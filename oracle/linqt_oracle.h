@@ -56,6 +56,8 @@ int lo_dos_fftgrid(const double *mu, int M, int N, double band_width, double ban
 
 /* Kubo-Bastin sigma(E) from a Jackson-damped 2D table (src/kuboBastinFromChebmom.cpp:35-81).
  * num_div energies in [-xbound, xbound]; writes num_div-1 points E[i], sigma[i]. */
+int lo_kubo_from_moments(int variant, int grid, const double *mu, int M0, int M1, int N, double band_width,
+                         double band_center, double xbound, int num_div, double *E, double *out);
 int lo_bastin_from_moments(const double *mu, int M0, int M1, int N, double band_width, double band_center,
                            double xbound, int num_div, double *E, double *sigma);
 

@@ -56,6 +56,8 @@ def lib():
         L.lo_dos_fftgrid.argtypes = [dp, ctypes.c_int, ctypes.c_int, ctypes.c_double, ctypes.c_double, dp, dp]
         L.lo_bastin_from_moments.argtypes = [dp, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_double,
                                              ctypes.c_double, ctypes.c_double, ctypes.c_int, dp, dp]
+        L.lo_kubo_from_moments.argtypes = [ctypes.c_int, ctypes.c_int, dp, ctypes.c_int, ctypes.c_int, ctypes.c_int,
+                                           ctypes.c_double, ctypes.c_double, ctypes.c_double, ctypes.c_int, dp, dp]
         L.lo_kubo_fft.argtypes = [vp, vp, vp, dp, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int,
                                   ctypes.c_int, ctypes.c_double, ctypes.c_double, dp, dp, dp, dp]
         _lib = L
@@ -175,6 +177,25 @@ def bastin_from_moments(mu, N, band_width, band_center, xbound=0.99, num_div=Non
     lib().lo_bastin_from_moments(_dp(m.view(np.float64)), M0, M1, N, band_width, band_center, xbound, num_div,
                                  _dp(E), _dp(s))
     return E, s
+
+
+# variants and grids of lo_kubo_from_moments
+FROM_MOM = {"bastin": 0, "greenwood": 1, "bastin_I": 2, "bastin_II": 3, "bastin_sea": 4, "bastin_surf": 5}
+GRID_UNIFORM, GRID_CHEBYSHEV, GRID_CHEBYSHEV_ASCENDING = 0, 1, 2
+
+
+def kubo_from_moments(mu, N, band_width, band_center, variant, grid=GRID_UNIFORM, xbound=1.0, num_div=None):
+    """(E, column) of LinQT's post-processor `variant` on a Jackson-damped table."""
+    m = np.ascontiguousarray(mu, dtype=np.complex128)
+    M0, M1 = m.shape
+    if num_div is None:
+        num_div = 30 * max(M0, M1) if grid == GRID_UNIFORM else max(M0, M1)
+    E, out = np.zeros(num_div - 1), np.zeros(num_div - 1)
+    rc = lib().lo_kubo_from_moments(FROM_MOM[variant], grid, _dp(m.view(np.float64)), M0, M1, N, band_width,
+                                    band_center, xbound, num_div, _dp(E), _dp(out))
+    if rc:
+        raise RuntimeError("lo_kubo_from_moments failed: %d" % rc)
+    return E, out
 
 
 def kubo_fft(H, opl, opr, states, M, nump, formula, N, band_width, band_center):

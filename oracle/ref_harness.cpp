@@ -9,10 +9,13 @@
 //   ref_harness spectral LABEL OP M STATEFILE
 //   ref_harness nonEq    LABEL OPR OPL M STATEFILE
 //   ref_harness kuboFFT  LABEL OPR OPL M NUMP FORMULA(0=Greenwood,1=Bastin) STATEFILE
+//   ref_harness frommom  II|Sea FILE.chebmom2D BROADENING XBOUND NUM_DIV(0 = 30 M)
 #include <omp.h>
 
 #include <chrono>
 #include <cstdio>
+#include <fstream>
+#include <vector>
 #include <cstdlib>
 #include <iostream>
 #include <string>
@@ -107,6 +110,48 @@ int main(int argc, char **argv) {
     solver.compute(OP[1], OP[2], gen);
     const double dt = std::chrono::duration<double>(clk::now() - t0).count();
     report("kuboFFT", dt, out);
+    return 0;
+  }
+  if (mode == "frommom" && argc == 7) {
+    // The energy sums of kuboBastinIIFromChebmom.cpp:62-88 / kuboBastinSeaFromChebmom.cpp:
+    // 62-88 on a uniform grid of the given half width (the drivers fix it at CUTOFF = 1,
+    // where the first point divides by zero), with the reference's own Moments2D reader,
+    // Jackson kernel and chebyshev_coefficients.hpp functions.
+    const std::string variant = argv[2];
+    chebyshev::Moments2D mu(argv[3]);
+    const double broad = std::atof(argv[4]), xbound = std::atof(argv[5]);
+    mu.ApplyJacksonKernel(broad, broad);
+    const int num_div = std::atoi(argv[6]) > 0 ? std::atoi(argv[6]) : 30 * mu.HighestMomentNumber();
+    std::vector<double> en(num_div), kernel(num_div, 0.0);
+    for (int i = 0; i < num_div; i++) en[i] = -xbound + i * (2 * xbound) / (num_div - 1);
+    const double w = mu.SystemSize() / mu.HalfWidth() / mu.HalfWidth() / 2 / M_PI;
+    for (int i = 0; i < num_div; i++) {
+      double out = 0.0;
+      const double x = en[i];
+      for (int m0 = 0; m0 < mu.HighestMomentNumber(0); m0++)
+        for (int m1 = 0; m1 < mu.HighestMomentNumber(1); m1++) {
+          if (variant == "II") {
+            out += -((greenR_chebF(x, m0) * DgreenR_chebF(x, m1) - DgreenR_chebF(x, m0) * greenR_chebF(x, m1)) *
+                     mu(m0, m1)).real();
+          } else {
+            const auto Gr = greenR_chebF(x, m0);
+            const auto Ga = std::conj(greenR_chebF(x, m0));
+            const auto DGr = DgreenR_chebF(x, m1).real();
+            const auto DGa = std::conj(DGr);
+            out += -((Gr - Ga) * (DGr + DGa) * mu(m0, m1)).real();
+          }
+        }
+      kernel[i] = out * w;
+    }
+    std::ofstream f("ref_frommom.dat");
+    f.precision(17);
+    double acc = 0;
+    for (int i = 0; i < num_div - 1; i++) {
+      const double de = en[i + 1] - en[i];
+      acc += (variant == "II" ? 1.0 : 0.5) * (kernel[i] + kernel[i + 1]) * de;
+      f << en[i] * mu.HalfWidth() + mu.BandCenter() << " " << acc << "\n";
+    }
+    report("frommom", 0.0, "ref_frommom.dat");
     return 0;
   }
   std::fprintf(stderr, "bad arguments\n");
