@@ -66,7 +66,9 @@ typedef struct linqt_session linqt_session;
 /* Solver options; zero-initialised = defaults (FP64, CSR, automatic tiling). */
 typedef struct linqt_opts {
   int precision;    /* LINQT_PREC_* */
-  int format;       /* LINQT_FORMAT_*: sparse format of H in the recursion */
+  int format;       /* sparse layout of H in the persistent recursions: LINQT_FORMAT_CSR (default),
+                       LINQT_FORMAT_SELL (SELL-C-sigma, C = 32, sigma = 8C) or LINQT_FORMAT_AUTO
+                       (autotuned among CSR and SELL with C = 8, 32; cached per operator) */
   int block_width;  /* vector columns per recursion block (0 = all R, or the autotuned chunk) */
   int doubling;     /* 1D: 0 = doubling identities when the operator is the identity, 1 = force them, 2 = direct <r|T_n r> */
   int use_graphs;   /* reserved (0) */

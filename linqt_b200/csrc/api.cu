@@ -5,6 +5,7 @@
 #include <algorithm>
 #include <cmath>
 #include <cstring>
+#include <functional>
 #include <memory>
 
 #include "internal.cuh"
@@ -205,19 +206,18 @@ void DeviceOp::free_device() {
   cudaFree(d_col);
   cudaFree(d_val64);
   cudaFree(d_val32);
-  cudaFree(d_sell_off);
-  cudaFree(d_sell_w);
-  cudaFree(d_sell_col);
-  cudaFree(d_sell_val64);
-  cudaFree(d_sell_val32);
   d_rowptr = d_col = nullptr;
   d_val64 = nullptr;
   d_val32 = nullptr;
-  d_sell_off = nullptr;
-  d_sell_w = d_sell_col = nullptr;
-  d_sell_val64 = nullptr;
-  d_sell_val32 = nullptr;
-  sell_C = 0;
+  for (auto &kv : sell) {
+    cudaFree(kv.second.d_perm);
+    cudaFree(kv.second.d_off);
+    cudaFree(kv.second.d_col);
+    cudaFree(kv.second.d_val64);
+    cudaFree(kv.second.d_val32);
+  }
+  sell.clear();
+  tuned.clear();
 }
 
 void DeviceOp::upload() {
@@ -242,6 +242,65 @@ void DeviceOp::upload() {
   version++;
 }
 
+// SELL-C-sigma: rows sorted by decreasing length inside windows of sigma = 8C rows
+// (stable), slices of C rows, each slice stored column-major with width = its longest
+// row; padding entries point at the row itself with value zero.
+const DeviceOp::Sell &DeviceOp::ensure_sell(int C, bool fp32) {
+  std::lock_guard<std::mutex> g(mu);
+  Sell &L = sell[C];
+  if (!L.d_perm) {
+    const int sigma = 8 * C;
+    std::vector<int> order(n);
+    for (int i = 0; i < n; ++i) order[i] = i;
+    auto len = [&](int r) { return rowptr[r + 1] - rowptr[r]; };
+    for (int w0 = 0; w0 < n; w0 += sigma)
+      std::stable_sort(order.begin() + w0, order.begin() + std::min(n, w0 + sigma),
+                       [&](int a, int b) { return len(a) > len(b); });
+    const int ns = (n + C - 1) / C;
+    std::vector<int> off(ns + 1, 0);
+    for (int sl = 0; sl < ns; ++sl) {
+      int w = 0;
+      for (int i = 0; i < C && sl * C + i < n; ++i) w = std::max(w, len(order[sl * C + i]));
+      LQ_REQUIRE((long)off[sl] + (long)w * C < (1L << 31), "SELL layout exceeds 2^31 entries");
+      off[sl + 1] = off[sl] + w * C;
+    }
+    L.len = std::max(1, off[ns]);
+    std::vector<int> sc(L.len, 0);
+    std::vector<double2> sv(L.len, make_double2(0, 0));
+    for (int sl = 0; sl < ns; ++sl)
+      for (int i = 0; i < C && sl * C + i < n; ++i) {
+        const int r = order[sl * C + i], w = (off[sl + 1] - off[sl]) / C;
+        for (int k = 0; k < w; ++k) {
+          const size_t q = (size_t)off[sl] + (size_t)k * C + i;
+          if (k < len(r)) {
+            sc[q] = col[rowptr[r] + k];
+            sv[q] = val[rowptr[r] + k];
+          } else {
+            sc[q] = r;
+          }
+        }
+      }
+    LQ_CUDA(cudaSetDevice(device));
+    LQ_CUDA(cudaMalloc(&L.d_perm, sizeof(int) * std::max(1, n)));
+    LQ_CUDA(cudaMalloc(&L.d_off, sizeof(int) * (ns + 1)));
+    LQ_CUDA(cudaMalloc(&L.d_col, sizeof(int) * L.len));
+    LQ_CUDA(cudaMalloc(&L.d_val64, sizeof(double2) * L.len));
+    LQ_CUDA(cudaMemcpy(L.d_perm, order.data(), sizeof(int) * n, cudaMemcpyHostToDevice));
+    LQ_CUDA(cudaMemcpy(L.d_off, off.data(), sizeof(int) * (ns + 1), cudaMemcpyHostToDevice));
+    LQ_CUDA(cudaMemcpy(L.d_col, sc.data(), sizeof(int) * L.len, cudaMemcpyHostToDevice));
+    LQ_CUDA(cudaMemcpy(L.d_val64, sv.data(), sizeof(double2) * L.len, cudaMemcpyHostToDevice));
+  }
+  if (fp32 && !L.d_val32) {
+    std::vector<double2> sv(L.len);
+    LQ_CUDA(cudaMemcpy(sv.data(), L.d_val64, sizeof(double2) * L.len, cudaMemcpyDeviceToHost));
+    std::vector<float2> v32(L.len);
+    for (size_t q = 0; q < L.len; ++q) v32[q] = make_float2((float)sv[q].x, (float)sv[q].y);
+    LQ_CUDA(cudaMalloc(&L.d_val32, sizeof(float2) * L.len));
+    LQ_CUDA(cudaMemcpy(L.d_val32, v32.data(), sizeof(float2) * L.len, cudaMemcpyHostToDevice));
+  }
+  return L;
+}
+
 void DeviceOp::ensure_fp32() {
   std::lock_guard<std::mutex> g(mu);
   if (d_val32) return;
@@ -250,8 +309,6 @@ void DeviceOp::ensure_fp32() {
   LQ_CUDA(cudaMalloc(&d_val32, sizeof(float2) * v.size()));
   LQ_CUDA(cudaMemcpy(d_val32, v.data(), sizeof(float2) * v.size(), cudaMemcpyHostToDevice));
 }
-
-void DeviceOp::ensure_sell(int) { fail(LINQT_ERR_UNSUPPORTED, "SELL-C layout not built in this library"); }
 
 // ---------------------------------------------------------------------------
 // block geometry
@@ -278,7 +335,57 @@ static linqt_opts defaults(const linqt_opts *o) {
   linqt_opts d;
   std::memset(&d, 0, sizeof(d));
   if (o) d = *o;
+  LQ_REQUIRE(d.format == LINQT_FORMAT_CSR || d.format == LINQT_FORMAT_SELL || d.format == LINQT_FORMAT_AUTO,
+             "opts.format: unknown sparse format");
   return d;
+}
+
+// ---------------------------------------------------------------------------
+// Sparse layout of a persistent recursion.  LINQT_FORMAT_CSR: the operator's CSR (whose
+// per-CTA row slices the kernels keep in shared memory when they fit); LINQT_FORMAT_SELL:
+// SELL-C-sigma with C = 32; LINQT_FORMAT_AUTO: the autotuner times a short run of the same
+// recursion (trial(C) with C = 0 for CSR, else the slice height) for CSR and SELL with
+// C in {8, 32}, keeps the fastest per operator pair, block width and precision, and returns
+// it.  Each candidate runs once untimed (building its layout) and once timed.
+// ---------------------------------------------------------------------------
+static int pick_layout(Session *s, const DeviceOp &H, const std::string &key, int format,
+                       const std::function<void(int)> &trial) {
+  if (format == LINQT_FORMAT_CSR) return 0;
+  if (format == LINQT_FORMAT_SELL) return 32;
+  DeviceOp &Hm = const_cast<DeviceOp &>(H);
+  {
+    std::lock_guard<std::mutex> g(Hm.mu);
+    auto it = Hm.tuned.find(key);
+    if (it != Hm.tuned.end()) return it->second;
+  }
+  cudaEvent_t a, b;
+  LQ_CUDA(cudaEventCreate(&a));
+  LQ_CUDA(cudaEventCreate(&b));
+  float best = 0;
+  int bestC = 0;
+  for (int C : {0, 8, 32}) {
+    trial(C);
+    LQ_CUDA(cudaEventRecord(a, s->stream));
+    trial(C);
+    LQ_CUDA(cudaEventRecord(b, s->stream));
+    LQ_CUDA(cudaEventSynchronize(b));
+    float ms = 0;
+    LQ_CUDA(cudaEventElapsedTime(&ms, a, b));
+    if (C == 0 || ms < best) {
+      best = ms;
+      bestC = C;
+    }
+  }
+  cudaEventDestroy(a);
+  cudaEventDestroy(b);
+  std::lock_guard<std::mutex> g(Hm.mu);
+  Hm.tuned[key] = bestC;
+  return bestC;
+}
+
+static std::string layout_key(const char *kind, const DeviceOp *V, int Rc, bool fp32) {
+  return std::string(kind) + ":" + std::to_string(Rc) + ":" + (fp32 ? "f32" : "f64") + ":" +
+         std::to_string((unsigned long long)(uintptr_t)V) + ":" + std::to_string(V ? V->version : 0);
 }
 
 // ---------------------------------------------------------------------------
@@ -304,9 +411,26 @@ static void moments1d_dev(Session *s, const DeviceOp &H, const DeviceOp *op, con
   const size_t blk = esz * (size_t)N * Rc;
   char *T = (char *)s->get("m1_T", 3 * blk);
   double2 *dots = (double2 *)s->get("m1_dots", sizeof(double2) * 2 * (size_t)steps * nchunks);
-  LQ_CUDA(cudaMemsetAsync(dots, 0, sizeof(double2) * 2 * (size_t)steps * nchunks, s->stream));
   PhaseScope ph(s, PH_RECURSION);
   long launches = 0;
+  int sellC = 0;
+  if (!o.step_launches)
+    sellC = pick_layout(s, H, layout_key("1d", op, Rc, fp32), o.format, [&](int C) {
+      // a short recursion on the first chunk (the real run below starts from scratch)
+      const int Mt = std::min(M, 32), st = doubling ? (Mt + 1) / 2 : Mt;
+      void *b0 = T, *b1 = T + blk, *b2 = T + 2 * blk;
+      chunk_block(s, states, N, R, 0, Rc, b2, fp32);
+      void *x0 = b2;
+      if (!doubling) {
+        if (op)
+          spmm(s, *op, make_double2(1, 0), b2, make_double2(0, 0), b0, Rc, fp32);
+        else
+          LQ_CUDA(cudaMemcpyAsync(b0, b2, blk, cudaMemcpyDeviceToDevice, s->stream));
+        x0 = b0;
+      }
+      recur_1d(s, H, b2, x0, b1, st, Mt, doubling ? 2 : 1, Rc, fp32, dots, C);
+    });
+  LQ_CUDA(cudaMemsetAsync(dots, 0, sizeof(double2) * 2 * (size_t)steps * nchunks, s->stream));
   for (int c = 0; c < nchunks; ++c) {
     void *b0 = T, *b1 = T + blk, *b2 = T + 2 * blk;
     double2 *cd = dots + (size_t)2 * steps * c;
@@ -324,7 +448,7 @@ static void moments1d_dev(Session *s, const DeviceOp &H, const DeviceOp *op, con
         }
         x0 = b0;
       }
-      recur_1d(s, H, phi, x0, b1, steps, M, doubling ? 2 : 1, Rc, fp32, cd);
+      recur_1d(s, H, phi, x0, b1, steps, M, doubling ? 2 : 1, Rc, fp32, cd, sellC);
       launches += 2;
       continue;
     }
@@ -387,12 +511,19 @@ static long lr_vectors(Session *s, const DeviceOp &H, const DeviceOp *opl, const
   long launches = 0;
   if (!step_launches) {
     // one cooperative launch advances both recursions (recur.cu)
-    if (opl)
-      spmm(s, *opl, make_double2(1, 0), phi, make_double2(0, 0), Lstore, Rc, fp32);
-    else
-      LQ_CUDA(cudaMemcpyAsync(Lstore, phi, blk, cudaMemcpyDeviceToDevice, s->stream));
-    if (!opr) LQ_CUDA(cudaMemcpyAsync(Rstore, phi, blk, cudaMemcpyDeviceToDevice, s->stream));
-    recur_lr(s, H, opr, Lstore, Rstore, phi, tmp3, M, Rc, fp32);
+    auto start = [&]() {
+      if (opl)
+        spmm(s, *opl, make_double2(1, 0), phi, make_double2(0, 0), Lstore, Rc, fp32);
+      else
+        LQ_CUDA(cudaMemcpyAsync(Lstore, phi, blk, cudaMemcpyDeviceToDevice, s->stream));
+      if (!opr) LQ_CUDA(cudaMemcpyAsync(Rstore, phi, blk, cudaMemcpyDeviceToDevice, s->stream));
+    };
+    const int sellC = pick_layout(s, H, layout_key("lr", opr, Rc, fp32), format, [&](int C) {
+      start();
+      recur_lr(s, H, opr, Lstore, Rstore, phi, tmp3, std::min(M, 16), Rc, fp32, C);
+    });
+    start();
+    recur_lr(s, H, opr, Lstore, Rstore, phi, tmp3, M, Rc, fp32, sellC);
     return opl ? 2 : 1;
   }
   // ---- L side: the recursion runs in place inside the store

@@ -127,19 +127,22 @@ struct DeviceOp {
   int *d_rowptr = nullptr, *d_col = nullptr;
   double2 *d_val64 = nullptr;
   float2 *d_val32 = nullptr;  // created on first mixed-precision use
-  // SELL-C layout (created on first use)
-  int sell_C = 0, sell_nslices = 0;
-  long sell_len = 0;
-  long *d_sell_off = nullptr;
-  int *d_sell_w = nullptr, *d_sell_col = nullptr;
-  double2 *d_sell_val64 = nullptr;
-  float2 *d_sell_val32 = nullptr;
   unsigned version = 0;  // bumped by rescale
+  // SELL-C-sigma copies of the expanded operator, by slice height C (built on first use)
+  struct Sell {
+    int *d_perm = nullptr, *d_off = nullptr, *d_col = nullptr;
+    double2 *d_val64 = nullptr;
+    float2 *d_val32 = nullptr;
+    size_t len = 0;
+  };
+  std::map<int, Sell> sell;
+  const Sell &ensure_sell(int C, bool fp32);
+  // format chosen by the autotuner, per (recursion kind, block width, precision, second operator)
+  std::map<std::string, int> tuned;
   std::mutex mu;
 
   CsrView csr64() const { return CsrView{n, nnz, d_rowptr, d_col, d_val64}; }
   void ensure_fp32();
-  void ensure_sell(int C);
   void free_device();
   void upload();
 };
@@ -266,10 +269,11 @@ void moments1d_from_dots_stream(cudaStream_t st, const double2 *dots, int steps,
                                 double2 *mu);
 
 // persistent recursions (recur.cu): one cooperative launch per recursion
+// sellC = 0: the operator's CSR; sellC > 0: its SELL-C-sigma layout with slice height sellC
 void recur_lr(Session *s, const DeviceOp &H, const DeviceOp *V, void *Lstore, void *Rstore, const void *phi,
-              void *tbuf, int M, int R, bool fp32);
+              void *tbuf, int M, int R, bool fp32, int sellC);
 void recur_1d(Session *s, const DeviceOp &H, const void *phi, void *x0, void *b1, int steps, int M, int mode, int R,
-              bool fp32, double2 *dots);
+              bool fp32, double2 *dots, int sellC);
 // after a stream synchronisation: fail with LINQT_ERR_TIMEOUT if a persistent kernel's barrier gave up
 void check_device_errors(Session *s);
 

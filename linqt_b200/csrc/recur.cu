@@ -109,6 +109,27 @@ __device__ void block_sum2(double2 &d0, double2 &d1) {
 }
 
 
+// The non-zeros of the row handled at position `pos`.  CSR: row = pos, entries
+// rp[row] .. rp[row+1] - 1.  SELL-C-sigma (sperm != NULL): rows sorted by length inside
+// windows of sigma rows, grouped in slices of C; slice s stores its entries column-major
+// (entry k of its i-th row at soff[s] + k*C + i, short rows padded with zeros), so the
+// rows of a warp read consecutive addresses at every k.  row = sperm[pos].
+__device__ __forceinline__ void sell_or_csr(int pos, const int *__restrict__ sperm, const int *__restrict__ soff,
+                                            int sC, const int *__restrict__ rp, int &row, int &b, int &e, int &st) {
+  if (sperm) {
+    const int sl = pos / sC, i = pos - sl * sC;
+    row = sperm[pos];
+    b = soff[sl] + i;
+    e = soff[sl + 1];
+    st = sC;
+  } else {
+    row = pos;
+    b = rp[pos];
+    e = rp[pos + 1];
+    st = 1;
+  }
+}
+
 // Copy this CTA's rows [r0, r1) of a CSR operator into shared memory at `dst` and return
 // pointers that index like the global arrays (rowptr by global row, col/val by global
 // entry).  `dst` is 16-byte aligned; returns the bytes used.
@@ -142,7 +163,8 @@ __global__ void __launch_bounds__(kThreads)
     k_recur_lr(int n, const int *rp, const int *ci, const typename cplx_t<T>::type *hv, const int *vrp,
                const int *vci, const typename cplx_t<T>::type *vv, typename cplx_t<T>::type *Lst,
                typename cplx_t<T>::type *Rst, const typename cplx_t<T>::type *phi, typename cplx_t<T>::type *tb, int M,
-               size_t blk, Barrier *bar, int cache) {
+               size_t blk, Barrier *bar, int cache, const int *__restrict__ sperm, const int *__restrict__ soff,
+               int sC) {
   using C = typename cplx_t<T>::type;
   constexpr int R = TPR * VPT;
   const int lane = threadIdx.x % TPR;
@@ -177,13 +199,14 @@ __global__ void __launch_bounds__(kThreads)
       pR = m ? Rst + (size_t)(m - 1) * blk : nullptr;
       yR = doL ? Rst + (size_t)(m + 1) * blk : nullptr;
     }
-    for (int row = rfirst + threadIdx.x / TPR; row < rend; row += rstep) {
+    for (int pos = rfirst + threadIdx.x / TPR; pos < rend; pos += rstep) {
+      int row, b, e, st;
+      sell_or_csr(pos, sperm, soff, sC, rp, row, b, e, st);
       C aL[VPT], aR[VPT];
 #pragma unroll
       for (int u = 0; u < VPT; ++u) aL[u] = aR[u] = zero2(C());
-      const int b = rp[row], e = rp[row + 1];
 #pragma unroll 4
-      for (int k = b; k < e; ++k) {
+      for (int k = b; k < e; k += st) {
         const int j = ci[k];
         const C h = hv[k];
         const size_t off = (size_t)j * R + lane;
@@ -249,7 +272,8 @@ template <class T, int TPR, int VPT>
 __global__ void __launch_bounds__(kThreads)
     k_recur_1d(int n, const int *rp, const int *ci, const typename cplx_t<T>::type *hv,
                const typename cplx_t<T>::type *phi, typename cplx_t<T>::type *x0, typename cplx_t<T>::type *b1,
-               int steps, int M, int mode, double2 *__restrict__ partials, Barrier *bar, int cache) {
+               int steps, int M, int mode, double2 *__restrict__ partials, Barrier *bar, int cache,
+               const int *__restrict__ sperm, const int *__restrict__ soff, int sC) {
   using C = typename cplx_t<T>::type;
   constexpr int R = TPR * VPT;
   const int lane = threadIdx.x % TPR;
@@ -268,13 +292,14 @@ __global__ void __launch_bounds__(kThreads)
     const bool need_y = mode == 2 ? (2 * s + 1 < M) : (s + 1 < M);
     C *y = need_y ? (prev ? prev : b1) : nullptr;
     double2 d0 = make_double2(0, 0), d1 = make_double2(0, 0);
-    for (int row = rfirst + threadIdx.x / TPR; row < rend; row += rstep) {
+    for (int pos = rfirst + threadIdx.x / TPR; pos < rend; pos += rstep) {
+      int row, b, e, st;
+      sell_or_csr(pos, sperm, soff, sC, rp, row, b, e, st);
       C acc[VPT];
 #pragma unroll
       for (int u = 0; u < VPT; ++u) acc[u] = zero2(C());
-      const int b = rp[row], e = rp[row + 1];
 #pragma unroll 4
-      for (int k = b; k < e; ++k) {
+      for (int k = b; k < e; k += st) {
         const int j = ci[k];
         const C h = hv[k];
         const C *xr = cur + (size_t)j * R + lane;
@@ -341,7 +366,7 @@ size_t max_slice_bytes(const DeviceOp &H, const DeviceOp *V, int grid, size_t es
 // Cooperative grid: as many co-resident CTAs as fit (at most one CTA's worth of rows per
 // group of TPR threads).  The operator slices are cached in shared memory when they fit.
 int coop_setup(const void *func, int sm_count, const DeviceOp &H, const DeviceOp *V, int tpr, size_t esz,
-               size_t *smem) {
+               size_t *smem, bool allow_cache = true) {
   const int n = H.n;
   const long need = ((long)n * tpr + kThreads - 1) / kThreads;
   int per_sm = 0;
@@ -354,7 +379,7 @@ int coop_setup(const void *func, int sm_count, const DeviceOp &H, const DeviceOp
   // Fewer CTAs fit with the cache, and fewer CTAs have larger slices: shrink the grid
   // until the slices of `grid` CTAs fit `grid` co-resident CTAs.
   int grid = grid0;
-  for (int it = 0; it < 16; ++it) {
+  for (int it = 0; allow_cache && it < 16; ++it) {
     const size_t bytes = max_slice_bytes(H, V, grid, esz);
     if (bytes > limit) break;
     int p = 0;
@@ -411,10 +436,18 @@ void coop_launch(Session *s, const void *f, int grid, void **args, size_t smem) 
 template <class T, int TPR, int VPT>
 struct LRF {
   static void run(Session *s, const DeviceOp &H, const DeviceOp *V, void *Lst, void *Rst, const void *phi, void *tb,
-                  int M, size_t blk, Barrier *bar) {
+                  int M, size_t blk, Barrier *bar, int sellC) {
     using C = typename cplx_t<T>::type;
     const bool fp32 = sizeof(T) == 4;
     const C *hv = fp32 ? (const C *)H.d_val32 : (const C *)H.d_val64;
+    const int *hci = H.d_col, *sperm = nullptr, *soff = nullptr;
+    if (sellC) {
+      const DeviceOp::Sell &L = const_cast<DeviceOp &>(H).ensure_sell(sellC, fp32);
+      hv = fp32 ? (const C *)L.d_val32 : (const C *)L.d_val64;
+      hci = L.d_col;
+      sperm = L.d_perm;
+      soff = L.d_off;
+    }
     const int *vrp = V ? V->d_rowptr : nullptr, *vci = V ? V->d_col : nullptr;
     const C *vv = V ? (fp32 ? (const C *)V->d_val32 : (const C *)V->d_val64) : nullptr;
     int n = H.n;
@@ -422,10 +455,12 @@ struct LRF {
     const C *ph = (const C *)phi;
     const void *f = V ? (const void *)k_recur_lr<T, TPR, VPT, true> : (const void *)k_recur_lr<T, TPR, VPT, false>;
     size_t smem = 0;
-    const int grid = coop_setup(f, s->sm_count, H, V, TPR, sizeof(C), &smem);
+    const int grid = coop_setup(f, s->sm_count, H, V, TPR, sizeof(C), &smem, sellC == 0);
     int cache = smem > 0;
-    void *args[] = {&n,    (void *)&H.d_rowptr, (void *)&H.d_col, (void *)&hv, (void *)&vrp, (void *)&vci,
-                    (void *)&vv, &L, &Rs, (void *)&ph, &tbuf, &M, &blk, &bar, &cache};
+    int sc = sellC;
+    void *args[] = {&n,    (void *)&H.d_rowptr, (void *)&hci, (void *)&hv, (void *)&vrp, (void *)&vci,
+                    (void *)&vv, &L, &Rs, (void *)&ph, &tbuf, &M, &blk, &bar, &cache,
+                    (void *)&sperm, (void *)&soff, &sc};
     coop_launch(s, f, grid, args, smem);
   }
 };
@@ -433,20 +468,30 @@ struct LRF {
 template <class T, int TPR, int VPT>
 struct OneDF {
   static void run(Session *s, const DeviceOp &H, const void *phi, void *x0, void *b1, int steps, int M, int mode,
-                  double2 *dots, Barrier *bar) {
+                  double2 *dots, Barrier *bar, int sellC) {
     using C = typename cplx_t<T>::type;
     const bool fp32 = sizeof(T) == 4;
     const C *hv = fp32 ? (const C *)H.d_val32 : (const C *)H.d_val64;
+    const int *hci = H.d_col, *sperm = nullptr, *soff = nullptr;
+    if (sellC) {
+      const DeviceOp::Sell &L = const_cast<DeviceOp &>(H).ensure_sell(sellC, fp32);
+      hv = fp32 ? (const C *)L.d_val32 : (const C *)L.d_val64;
+      hci = L.d_col;
+      sperm = L.d_perm;
+      soff = L.d_off;
+    }
     const void *f = (const void *)k_recur_1d<T, TPR, VPT>;
     size_t smem = 0;
-    const int grid = coop_setup(f, s->sm_count, H, nullptr, TPR, sizeof(C), &smem);
+    const int grid = coop_setup(f, s->sm_count, H, nullptr, TPR, sizeof(C), &smem, sellC == 0);
     int cache = smem > 0;
+    int sc = sellC;
     double2 *partials = (double2 *)s->get("rec1d_part", sizeof(double2) * 2 * (size_t)steps * grid);
     int n = H.n;
     const C *ph = (const C *)phi;
     C *xx = (C *)x0, *bb = (C *)b1;
-    void *args[] = {&n, (void *)&H.d_rowptr, (void *)&H.d_col, (void *)&hv, (void *)&ph, &xx, &bb, &steps, &M, &mode,
-                    &partials, &bar, &cache};
+    void *args[] = {&n,        (void *)&H.d_rowptr, (void *)&hci, (void *)&hv,    (void *)&ph, &xx, &bb, &steps,
+                    &M,        &mode,               &partials,    &bar,           &cache,      (void *)&sperm,
+                    (void *)&soff, &sc};
     coop_launch(s, f, grid, args, smem);
     k_reduce_step_partials<<<(2 * steps + 255) / 256, 256, 0, s->stream>>>(partials, steps, grid, dots);
     LQ_LAUNCHED();
@@ -481,23 +526,23 @@ Barrier *barrier_for(Session *s) {
 }  // namespace
 
 void recur_lr(Session *s, const DeviceOp &H, const DeviceOp *V, void *Lstore, void *Rstore, const void *phi,
-              void *tbuf, int M, int R, bool fp32) {
+              void *tbuf, int M, int R, bool fp32, int sellC) {
   const size_t blk = (size_t)H.n * R;
   Barrier *bar = barrier_for(s);
   if (fp32)
-    dispatch<float, LRF>(R, s, H, V, Lstore, Rstore, phi, tbuf, M, blk, bar);
+    dispatch<float, LRF>(R, s, H, V, Lstore, Rstore, phi, tbuf, M, blk, bar, sellC);
   else
-    dispatch<double, LRF>(R, s, H, V, Lstore, Rstore, phi, tbuf, M, blk, bar);
+    dispatch<double, LRF>(R, s, H, V, Lstore, Rstore, phi, tbuf, M, blk, bar, sellC);
   LQ_LAUNCHED();
 }
 
 void recur_1d(Session *s, const DeviceOp &H, const void *phi, void *x0, void *b1, int steps, int M, int mode, int R,
-              bool fp32, double2 *dots) {
+              bool fp32, double2 *dots, int sellC) {
   Barrier *bar = barrier_for(s);
   if (fp32)
-    dispatch<float, OneDF>(R, s, H, phi, x0, b1, steps, M, mode, dots, bar);
+    dispatch<float, OneDF>(R, s, H, phi, x0, b1, steps, M, mode, dots, bar, sellC);
   else
-    dispatch<double, OneDF>(R, s, H, phi, x0, b1, steps, M, mode, dots, bar);
+    dispatch<double, OneDF>(R, s, H, phi, x0, b1, steps, M, mode, dots, bar, sellC);
 }
 
 void check_device_errors(Session *s) {

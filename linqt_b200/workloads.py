@@ -4,6 +4,8 @@ Kubo-Bastin graphene workload:
     python -m linqt_b200.workloads dos      # square L=256, 1 vector, M=1024, DOS (full size)
     python -m linqt_b200.workloads cubic    # cubic Anderson L=100 (N=1e6), 64 vectors, M=1024 (1 of 4 seeds)
     python -m linqt_b200.workloads spin     # Kane-Mele with spin, 64x64 cells, R=8, M=512, nump=1024
+    python -m linqt_b200.workloads spin --moments 1024 --vectors 32 --reps 1   # the full moment and vector counts
+    python -m linqt_b200.workloads layouts  # DOS recursion per sparse layout (CSR, SELL-C-sigma, autotuned)
 
 Each line gives the device time per solve (CUDA events on the session stream, warm-up
 first), Chebyshev steps*nnz/s, the recursion's algorithmic bytes per second, and for the
@@ -109,10 +111,28 @@ def run_spin(Lc, R, M, nump, reps):
     }
 
 
+def run_layouts(N, H, R, M, reps, name):
+    """DOS recursion time per layout: CSR, SELL-C-sigma (C = 8, 32) and the autotuner's choice."""
+    import torch
+    sess, bw, bc, Hg, _ = _ops(N, H)
+    st = lattices.random_phase_states(N, R, seed=45)
+    st_dev = torch.from_numpy(st.view(np.float64).copy()).cuda()
+    mu = torch.zeros(2 * M, dtype=torch.float64, device="cuda")
+    out = {"workload": name, "N": N, "R": R, "M": M}
+    for label, fmt in (("csr", 0), ("sell32", 1), ("auto", 2)):
+        o = make_opts(fmt=fmt)
+        out[label + "_ms"] = _timed(lambda: moments1d_dev(Hg, None, st_dev, R, M, mu, opts=o, session=sess), reps,
+                                    torch)
+    return out
+
+
 def main(argv=None):
     ap = argparse.ArgumentParser()
-    ap.add_argument("workload", choices=["dos", "cubic", "spin"])
+    ap.add_argument("workload", choices=["dos", "cubic", "spin", "layouts"])
     ap.add_argument("--reps", type=int, default=5)
+    ap.add_argument("--cells", type=int, default=64, help="spin: Kane-Mele cells per side")
+    ap.add_argument("--moments", type=int, default=512, help="spin: M")
+    ap.add_argument("--vectors", type=int, default=8, help="spin: R")
     a = ap.parse_args(argv)
     if a.workload == "dos":
         N, H = lattices.square_lattice(256, 1.0, 1.0, 11)
@@ -120,8 +140,16 @@ def main(argv=None):
     elif a.workload == "cubic":
         N, H = lattices.cubic_lattice(100, 1.0, 2.0, 41)
         r = run_1d("dos_cubic_100_seed41", N, H, 64, 1024, a.reps, 45)
+    elif a.workload == "layouts":
+        N, H = lattices.cubic_lattice(100, 1.0, 2.0, 41)
+        rs = [run_layouts(N, H, R, 256, a.reps, "dos_cubic_100") for R in (1, 4, 64)]
+        N, H, _ = lattices.kane_mele(256, 256, seed=31)
+        rs += [run_layouts(N, H, R, 256, a.reps, "dos_kane_mele_256") for R in (1, 4)]
+        for r in rs:
+            print(json.dumps(r))
+        return
     else:
-        r = run_spin(64, 8, 512, 1024, a.reps)
+        r = run_spin(a.cells, a.vectors, a.moments, max(1024, a.moments), a.reps)
     print(json.dumps(r))
 
 

@@ -101,3 +101,30 @@ def test_large_operator_rows_not_cached(oracle_lib):
     assert rel(mu, oracle_lib.moments1d(Ho, None, st, 48)) < TOL
     mu2 = lq.moments2d(Hg, None, None, st, 12)
     assert rel(mu2, oracle_lib.moments2d(Ho, None, None, st, 12)) < TOL
+
+
+@pytest.mark.parametrize("fmt", [1, 2])  # SELL-C-sigma (C = 32), autotuned
+def test_sell_layout_matches_csr(oracle_lib, fmt):
+    """The persistent recursions on the SELL-C-sigma layout: the row sums keep their order
+    (padding adds exact zeros), so the 2D tables are those of CSR bit for bit; the 1D moments
+    sum their dot products over rows in another order (1e-13)."""
+    N, H, V = lattices.kane_mele(8, 6, seed=31)  # rows of 9 to 13 non-zeros
+    bw, bc, Hg, Ho, ((Vg, Vo),) = ops(oracle_lib, N, H, [V])
+    st = lattices.random_phase_states(N, 5, seed=34)
+    o = lq.make_opts(fmt=fmt)
+    csr2 = lq.moments2d(Hg, Vg, Vg, st, 40)
+    sell2 = lq.moments2d(Hg, Vg, Vg, st, 40, opts=o)
+    assert np.array_equal(csr2, sell2) or fmt == 2
+    assert rel(sell2, oracle_lib.moments2d(Ho, Vo, Vo, st, 40)) < TOL
+    csr1 = lq.moments1d(Hg, None, st, 100)
+    sell1 = lq.moments1d(Hg, None, st, 100, opts=o)
+    assert rel(sell1, csr1) < 1e-13
+    assert rel(sell1, oracle_lib.moments1d(Ho, None, st, 100)) < TOL
+
+
+def test_sell_layout_large_operator(oracle_lib):
+    N, H = lattices.cubic_lattice(100, t=1.0, W=2.0, seed=43)
+    bw, bc, Hg, Ho, _ = ops(oracle_lib, N, H)
+    st = lattices.random_phase_states(N, 2, seed=47)
+    mu = lq.moments1d(Hg, None, st, 32, opts=lq.make_opts(fmt=1))
+    assert rel(mu, oracle_lib.moments1d(Ho, None, st, 32)) < TOL

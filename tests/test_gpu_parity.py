@@ -276,12 +276,15 @@ def test_errors_are_reported(honey):
     assert e.value.code == -1 and "nump" in str(e.value)
     with pytest.raises(lq.LinqtError):
         lq.Operator.from_csr(3, [0, 1, 2, 3], [0, 1, 5], [1.0, 1.0, 1.0])
+    with pytest.raises(lq.LinqtError) as e:  # unknown sparse format
+        lq.moments1d(honey["Hg"], None, np.ones((1, honey["N"])), 8, opts=lq.make_opts(fmt=7))
+    assert e.value.code == -1 and "format" in str(e.value)
 
 
 # ---------------------------------------------------------------------------
 # precision modes: FP32 recursion + FP64 contraction (PREC_FP32) and FP32 recursion +
 # tcgen05 3xTF32 contraction (PREC_MIXED).  Bounds are the measured accuracy of the
-# modes (stated in DESIGN.md), checked against the FP64 path.
+# modes, checked against the FP64 path.
 # ---------------------------------------------------------------------------
 @pytest.mark.parametrize("R,M", [(2, 32), (3, 100), (8, 130)])
 def test_mixed_precision_moments2d(honey, R, M):
