@@ -129,6 +129,18 @@ int linqt_moments1d(linqt_session *s, const linqt_op *H, const linqt_op *op, con
 int linqt_moments1d_dev(linqt_session *s, const linqt_op *H, const linqt_op *op, const double *states_dev, int R,
                         int M, const linqt_opts *opts, double *mu_dev);
 
+/* Disorder realisations batched in one recursion (no reference counterpart: LinQT runs
+ * one Hamiltonian per process).  H[0..S) share one sparsity pattern (e.g. Anderson disorder
+ * seeds); states are R x N with R = S * Rs, the Rs states of realisation r in rows
+ * [r Rs, (r+1) Rs).  All run as one R-wide block in one persistent launch, the grid split into
+ * S groups of CTAs, each reading its realisation's values and columns.  mu[2*S*M]: the
+ * SpectralMoments of each realisation (identity operator) with its Rs states.  Rs a power of
+ * two <= 256. */
+int linqt_moments1d_realisations(linqt_session *s, const linqt_op *const *H, int S, const double *states, int R,
+                                 int M, const linqt_opts *opts, double *mu);
+int linqt_moments1d_realisations_dev(linqt_session *s, const linqt_op *const *H, int S, const double *states_dev,
+                                     int R, int M, const linqt_opts *opts, double *mu_dev);
+
 /* chebyshev::CorrelationExpansionMoments (src/chebyshev_solver.cpp:86-172) with the
  * default BATCH_SIZE: mu[2*M*M] row-major mu(mL, mR), symmetrised and scaled by
  * (4/R)(1/2)^{[mL=0]}(1/2)^{[mR=0]}.  opl/opr = NULL are identities. */

@@ -62,6 +62,10 @@ SIGNATURES = {
     "linqt_spectral_bounds": (c_int, [c_void_p, c_void_p, P_double, P_double]),
     "linqt_moments1d": (c_int, [c_void_p, c_void_p, c_void_p, P_double, c_int, c_int, ctypes.POINTER(Opts),
                                 P_double]),
+    "linqt_moments1d_realisations": (c_int, [c_void_p, ctypes.POINTER(c_void_p), c_int, P_double, c_int, c_int,
+                                             ctypes.POINTER(Opts), P_double]),
+    "linqt_moments1d_realisations_dev": (c_int, [c_void_p, ctypes.POINTER(c_void_p), c_int, c_void_p, c_int, c_int,
+                                                 ctypes.POINTER(Opts), c_void_p]),
     "linqt_moments1d_dev": (c_int, [c_void_p, c_void_p, c_void_p, c_void_p, c_int, c_int, ctypes.POINTER(Opts),
                                     c_void_p]),
     "linqt_moments2d": (c_int, [c_void_p, c_void_p, c_void_p, c_void_p, P_double, c_int, c_int,

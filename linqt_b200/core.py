@@ -211,6 +211,28 @@ def random_phase_states_dev(N, R, seed, out_dev, session=None):
     check(load().linqt_random_phase_states_dev(_sh(session), N, R, seed, ctypes.c_void_p(_ptr(out_dev))))
 
 
+def _handles(Hs):
+    return (ctypes.c_void_p * len(Hs))(*[H.h.value if isinstance(H.h, ctypes.c_void_p) else H.h for H in Hs])
+
+
+def moments1d_realisations(Hs, states, M, opts=None, session=None):
+    """mu[S, M]: SpectralMoments of S Hamiltonians with one sparsity pattern (disorder
+    realisations), the R/S consecutive rows of `states` per realisation, in one recursion."""
+    st = np.atleast_2d(_c128(states))
+    R, S = st.shape[0], len(Hs)
+    mu = np.zeros((S, M), np.complex128)
+    o = opts or make_opts()
+    check(load().linqt_moments1d_realisations(_sh(session), _handles(Hs), S, _dp(st.view(np.float64)), R, M,
+                                              ctypes.byref(o), _dp(mu.view(np.float64))))
+    return mu
+
+
+def moments1d_realisations_dev(Hs, states_dev, R, M, mu_dev, opts=None, session=None):
+    o = opts or make_opts()
+    check(load().linqt_moments1d_realisations_dev(_sh(session), _handles(Hs), len(Hs), ctypes.c_void_p(_ptr(states_dev)),
+                                                  R, M, ctypes.byref(o), ctypes.c_void_p(_ptr(mu_dev))))
+
+
 def moments1d_dev(H, op, states_dev, R, M, mu_dev, opts=None, session=None):
     o = opts or make_opts()
     check(load().linqt_moments1d_dev(_sh(session), H.h, _oph(op), ctypes.c_void_p(_ptr(states_dev)), R, M,

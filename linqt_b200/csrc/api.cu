@@ -498,6 +498,48 @@ static void moments1d_dev(Session *s, const DeviceOp &H, const DeviceOp *op, con
 }
 
 // ---------------------------------------------------------------------------
+// Disorder realisations in one block: S Hamiltonians with the same pattern (e.g. Anderson
+// disorder seeds), Rs random vectors each, run as one R = S*Rs wide persistent recursion in
+// which each realisation has its own group of CTAs, reading its own values (stacked [S][nnz]
+// on the device) and its own Rs columns.  Moments per realisation (identity operator,
+// doubling identities): mu[S][M].
+// ---------------------------------------------------------------------------
+static void moments1d_realisations_dev(Session *s, const DeviceOp *const *Hs, int S, const double2 *states, int R,
+                                       int M, const linqt_opts &o, double2 *mu) {
+  LQ_REQUIRE(S >= 1 && R > 0 && M > 0 && R % S == 0, "realisations: R must be a positive multiple of S");
+  const DeviceOp &H0 = *Hs[0];
+  for (int r = 1; r < S; ++r)
+    LQ_REQUIRE(Hs[r]->n == H0.n && Hs[r]->rowptr == H0.rowptr && Hs[r]->col == H0.col,
+               "realisations: every Hamiltonian must have the sparsity pattern of the first");
+  const int Rs = R / S;
+  LQ_REQUIRE(Rs <= 256 && (Rs & (Rs - 1)) == 0, "realisations: R/S must be a power of two <= 256");
+  const bool fp32 = o.precision != LINQT_PREC_FP64;
+  const int N = H0.n;
+  const size_t esz = fp32 ? sizeof(float2) : sizeof(double2);
+  char *vals = (char *)s->get("real_vals", esz * (size_t)S * std::max(1L, H0.nnz));
+  for (int r = 0; r < S; ++r) {
+    if (fp32) const_cast<DeviceOp *>(Hs[r])->ensure_fp32();
+    const void *src = fp32 ? (const void *)Hs[r]->d_val32 : (const void *)Hs[r]->d_val64;
+    LQ_CUDA(cudaMemcpyAsync(vals + esz * (size_t)r * H0.nnz, src, esz * H0.nnz, cudaMemcpyDeviceToDevice, s->stream));
+  }
+  const int steps = (M + 1) / 2;  // doubling identities
+  const size_t blk = esz * (size_t)N * R;
+  char *T = (char *)s->get("m1_T", 3 * blk);
+  double2 *dots = (double2 *)s->get("m1_dots", sizeof(double2) * 2 * (size_t)steps * S);
+  void *b0 = T, *b1 = T + blk, *phi = T + 2 * blk;
+  {
+    PhaseScope ph(s, PH_RECURSION);
+    chunk_block(s, states, N, R, 0, R, phi, fp32);
+    LQ_CUDA(cudaMemcpyAsync(b0, phi, blk, cudaMemcpyDeviceToDevice, s->stream));
+    recur_1d(s, H0, phi, b0, b1, steps, M, 2, R, fp32, dots, 0, vals, S);
+    ph.launches(3);
+  }
+  PhaseScope p3(s, PH_OTHER);
+  for (int r = 0; r < S; ++r)
+    moments1d_from_dots(s, dots + (size_t)2 * steps * r, steps, M, Rs, 2, mu + (size_t)M * r);
+}
+
+// ---------------------------------------------------------------------------
 // L/R Chebyshev vector blocks (shared by the 2D moments and the FFT solver)
 //   L_m = T_m(H) OPL phi  (Moments::SetInitVectors(OP, phi) + Vectors::IterateAll,
 //                          src/chebyshev_moments.cpp:5-22, src/chebyshev_vectors.cpp:4-21)
@@ -1030,6 +1072,41 @@ int linqt_moments1d(linqt_session *s, const linqt_op *H, const linqt_op *op, con
     LQ_CUDA(cudaMemcpyAsync(mu, d_mu, sizeof(double2) * (size_t)M, cudaMemcpyDeviceToHost, r->stream));
     LQ_CUDA(cudaStreamSynchronize(r->stream));
     check_device_errors(r);
+  });
+}
+
+int linqt_moments1d_realisations(linqt_session *s, const linqt_op *const *H, int S, const double *states, int R,
+                                 int M, const linqt_opts *opts, double *mu) {
+  return guarded([&] {
+    LQ_REQUIRE(H && states && mu && S >= 1 && R > 0 && M > 0, "bad argument");
+    std::vector<const DeviceOp *> ops(S);
+    for (int r = 0; r < S; ++r) {
+      check_op(H[r], "H[r]");
+      ops[r] = &H[r]->op;
+    }
+    Session *ss = resolve(s);
+    const size_t sb = sizeof(double2) * (size_t)R * ops[0]->n;
+    double2 *d_st = (double2 *)ss->get("io_states", sb);
+    double2 *d_mu = (double2 *)ss->get("io_mu", sizeof(double2) * (size_t)M * S);
+    LQ_CUDA(cudaMemcpyAsync(d_st, states, sb, cudaMemcpyHostToDevice, ss->stream));
+    moments1d_realisations_dev(ss, ops.data(), S, d_st, R, M, defaults(opts), d_mu);
+    LQ_CUDA(cudaMemcpyAsync(mu, d_mu, sizeof(double2) * (size_t)M * S, cudaMemcpyDeviceToHost, ss->stream));
+    LQ_CUDA(cudaStreamSynchronize(ss->stream));
+    check_device_errors(ss);
+  });
+}
+
+int linqt_moments1d_realisations_dev(linqt_session *s, const linqt_op *const *H, int S, const double *states_dev,
+                                     int R, int M, const linqt_opts *opts, double *mu_dev) {
+  return guarded([&] {
+    LQ_REQUIRE(H && states_dev && mu_dev && S >= 1, "bad argument");
+    std::vector<const DeviceOp *> ops(S);
+    for (int r = 0; r < S; ++r) {
+      check_op(H[r], "H[r]");
+      ops[r] = &H[r]->op;
+    }
+    moments1d_realisations_dev(resolve(s), ops.data(), S, (const double2 *)states_dev, R, M, defaults(opts),
+                               (double2 *)mu_dev);
   });
 }
 

@@ -272,8 +272,11 @@ void moments1d_from_dots_stream(cudaStream_t st, const double2 *dots, int steps,
 // sellC = 0: the operator's CSR; sellC > 0: its SELL-C-sigma layout with slice height sellC
 void recur_lr(Session *s, const DeviceOp &H, const DeviceOp *V, void *Lstore, void *Rstore, const void *phi,
               void *tbuf, int M, int R, bool fp32, int sellC);
+// stacked != NULL: nreal realisations sharing H's pattern, values [nreal][nnz]; realisation r
+// owns columns [r R/nreal, (r+1) R/nreal), served by its own group of CTAs, and dots becomes
+// [nreal][steps][2]
 void recur_1d(Session *s, const DeviceOp &H, const void *phi, void *x0, void *b1, int steps, int M, int mode, int R,
-              bool fp32, double2 *dots, int sellC);
+              bool fp32, double2 *dots, int sellC, const void *stacked = nullptr, int nreal = 1);
 // after a stream synchronisation: fail with LINQT_ERR_TIMEOUT if a persistent kernel's barrier gave up
 void check_device_errors(Session *s);
 

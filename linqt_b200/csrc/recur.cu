@@ -268,16 +268,26 @@ __global__ void __launch_bounds__(kThreads)
 // The recursion runs in place: T_{s+1} overwrites T_{s-1}; T_1 goes to b1.
 // partials: [steps][grid][2] per-CTA sums.
 // ---------------------------------------------------------------------------
-template <class T, int TPR, int VPT>
+template <class T, int TPR, int VPT, bool STACKED>
 __global__ void __launch_bounds__(kThreads)
     k_recur_1d(int n, const int *rp, const int *ci, const typename cplx_t<T>::type *hv,
                const typename cplx_t<T>::type *phi, typename cplx_t<T>::type *x0, typename cplx_t<T>::type *b1,
                int steps, int M, int mode, double2 *__restrict__ partials, Barrier *bar, int cache,
-               const int *__restrict__ sperm, const int *__restrict__ soff, int sC) {
+               const int *__restrict__ sperm, const int *__restrict__ soff, int sC, long vstride, int nreal,
+               int ldx_rt) {
   using C = typename cplx_t<T>::type;
-  constexpr int R = TPR * VPT;
+  constexpr int RW = TPR * VPT;  // columns handled by a CTA
   const int lane = threadIdx.x % TPR;
   constexpr int gpb = kThreads / TPR;
+  // STACKED: nreal realisations (value sets at hv + r*vstride) share the sparsity pattern; the
+  // grid is split into nreal equal groups of CTAs, group r serving columns [r*RW, (r+1)*RW) of
+  // rows of ldx_rt columns.  Otherwise one group, rows of RW columns.
+  const int ldx = STACKED ? ldx_rt : RW;
+  const int G1 = STACKED ? (int)gridDim.x / nreal : (int)gridDim.x;
+  const int real = STACKED ? (int)blockIdx.x / G1 : 0;
+  const int bl = STACKED ? (int)blockIdx.x % G1 : (int)blockIdx.x;
+  const int coff = real * RW;
+  if (STACKED) hv += (size_t)real * vstride;
   const int per = (n + gridDim.x - 1) / gridDim.x;
   const int r0 = min(n, blockIdx.x * per), r1 = min(n, r0 + per);
   if (cache) {
@@ -285,8 +295,8 @@ __global__ void __launch_bounds__(kThreads)
     cache_rows<C>(rp, ci, hv, r0, r1, smc1, rp, ci, hv);
     __syncthreads();
   }
-  const int rfirst = cache ? r0 : blockIdx.x * gpb, rend = cache ? r1 : n;  // as in k_recur_lr
-  const int rstep = cache ? gpb : gridDim.x * gpb;
+  const int rfirst = cache ? r0 : bl * gpb, rend = cache ? r1 : n;  // as in k_recur_lr
+  const int rstep = cache ? gpb : G1 * gpb;
   C *prev = nullptr, *cur = x0;
   for (int s = 0; s < steps; ++s) {
     const bool need_y = mode == 2 ? (2 * s + 1 < M) : (s + 1 < M);
@@ -302,11 +312,11 @@ __global__ void __launch_bounds__(kThreads)
       for (int k = b; k < e; k += st) {
         const int j = ci[k];
         const C h = hv[k];
-        const C *xr = cur + (size_t)j * R + lane;
+        const C *xr = cur + (size_t)j * ldx + coff + lane;
 #pragma unroll
         for (int u = 0; u < VPT; ++u) acc[u] = cfma(h, ldv(xr + u * TPR), acc[u]);
       }
-      const size_t base = (size_t)row * R + lane;
+      const size_t base = (size_t)row * ldx + coff + lane;
 #pragma unroll
       for (int u = 0; u < VPT; ++u) {
         const size_t idx = base + u * TPR;
@@ -345,6 +355,18 @@ __global__ void k_reduce_step_partials(const double2 *__restrict__ partials, int
     const int s = t >> 1, i = t & 1;
     double2 acc = make_double2(0, 0);
     for (int b = 0; b < nb; ++b) acc = cadd(acc, partials[((size_t)s * nb + b) * 2 + i]);
+    dots[t] = acc;
+  }
+}
+
+// Stacked realisations: dots[(r*steps + s)*2 + i] = sum over the CTAs b of group r
+// (b in [r*g1, (r+1)*g1)) of partials[s][b][i]  (fixed order)
+__global__ void k_reduce_step_partials_split(const double2 *__restrict__ partials, int steps, int nb, int g1,
+                                             int nreal, double2 *__restrict__ dots) {
+  for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < 2 * steps * nreal; t += gridDim.x * blockDim.x) {
+    const int i = t & 1, s = (t >> 1) % steps, r = (t >> 1) / steps;
+    double2 acc = make_double2(0, 0);
+    for (int b = r * g1; b < (r + 1) * g1; ++b) acc = cadd(acc, partials[((size_t)s * nb + b) * 2 + i]);
     dots[t] = acc;
   }
 }
@@ -468,10 +490,12 @@ struct LRF {
 template <class T, int TPR, int VPT>
 struct OneDF {
   static void run(Session *s, const DeviceOp &H, const void *phi, void *x0, void *b1, int steps, int M, int mode,
-                  double2 *dots, Barrier *bar, int sellC) {
+                  double2 *dots, Barrier *bar, int sellC, const void *stacked, int nreal) {
     using C = typename cplx_t<T>::type;
     const bool fp32 = sizeof(T) == 4;
-    const C *hv = fp32 ? (const C *)H.d_val32 : (const C *)H.d_val64;
+    const C *hv = stacked ? (const C *)stacked : fp32 ? (const C *)H.d_val32 : (const C *)H.d_val64;
+    long vstride = stacked ? H.nnz : 0;
+    LQ_REQUIRE(!stacked || (nreal >= 1 && sellC == 0), "stacked realisations: CSR layout only");
     const int *hci = H.d_col, *sperm = nullptr, *soff = nullptr;
     if (sellC) {
       const DeviceOp::Sell &L = const_cast<DeviceOp &>(H).ensure_sell(sellC, fp32);
@@ -480,20 +504,27 @@ struct OneDF {
       sperm = L.d_perm;
       soff = L.d_off;
     }
-    const void *f = (const void *)k_recur_1d<T, TPR, VPT>;
+    const void *f = stacked ? (const void *)k_recur_1d<T, TPR, VPT, true> : (const void *)k_recur_1d<T, TPR, VPT, false>;
     size_t smem = 0;
-    const int grid = coop_setup(f, s->sm_count, H, nullptr, TPR, sizeof(C), &smem, sellC == 0);
+    // the shared-memory operator cache holds one value set: not with stacked realisations
+    int grid = coop_setup(f, s->sm_count, H, nullptr, TPR, sizeof(C), &smem, sellC == 0 && !stacked);
+    if (stacked) grid = std::max(nreal, grid / nreal * nreal);  // equal CTA groups per realisation
     int cache = smem > 0;
     int sc = sellC;
+    int ldx = TPR * VPT * (stacked ? nreal : 1);
     double2 *partials = (double2 *)s->get("rec1d_part", sizeof(double2) * 2 * (size_t)steps * grid);
     int n = H.n;
     const C *ph = (const C *)phi;
     C *xx = (C *)x0, *bb = (C *)b1;
     void *args[] = {&n,        (void *)&H.d_rowptr, (void *)&hci, (void *)&hv,    (void *)&ph, &xx, &bb, &steps,
                     &M,        &mode,               &partials,    &bar,           &cache,      (void *)&sperm,
-                    (void *)&soff, &sc};
+                    (void *)&soff, &sc, &vstride, &nreal, &ldx};
     coop_launch(s, f, grid, args, smem);
-    k_reduce_step_partials<<<(2 * steps + 255) / 256, 256, 0, s->stream>>>(partials, steps, grid, dots);
+    if (stacked)
+      k_reduce_step_partials_split<<<(2 * steps * nreal + 255) / 256, 256, 0, s->stream>>>(
+          partials, steps, grid, grid / nreal, nreal, dots);
+    else
+      k_reduce_step_partials<<<(2 * steps + 255) / 256, 256, 0, s->stream>>>(partials, steps, grid, dots);
     LQ_LAUNCHED();
   }
 };
@@ -537,12 +568,13 @@ void recur_lr(Session *s, const DeviceOp &H, const DeviceOp *V, void *Lstore, vo
 }
 
 void recur_1d(Session *s, const DeviceOp &H, const void *phi, void *x0, void *b1, int steps, int M, int mode, int R,
-              bool fp32, double2 *dots, int sellC) {
+              bool fp32, double2 *dots, int sellC, const void *stacked, int nreal) {
   Barrier *bar = barrier_for(s);
+  const int Rw = stacked ? R / nreal : R;  // columns per CTA
   if (fp32)
-    dispatch<float, OneDF>(R, s, H, phi, x0, b1, steps, M, mode, dots, bar, sellC);
+    dispatch<float, OneDF>(Rw, s, H, phi, x0, b1, steps, M, mode, dots, bar, sellC, stacked, nreal);
   else
-    dispatch<double, OneDF>(R, s, H, phi, x0, b1, steps, M, mode, dots, bar, sellC);
+    dispatch<double, OneDF>(Rw, s, H, phi, x0, b1, steps, M, mode, dots, bar, sellC, stacked, nreal);
 }
 
 void check_device_errors(Session *s) {

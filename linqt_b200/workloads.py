@@ -6,6 +6,7 @@ Kubo-Bastin graphene workload:
     python -m linqt_b200.workloads spin     # Kane-Mele with spin, 64x64 cells, R=8, M=512, nump=1024
     python -m linqt_b200.workloads spin --moments 1024 --vectors 32 --reps 1   # the full moment and vector counts
     python -m linqt_b200.workloads layouts  # DOS recursion per sparse layout (CSR, SELL-C-sigma, autotuned)
+    python -m linqt_b200.workloads realisations  # 4 disorder seeds in one recursion vs 4 separate solves
 
 Each line gives the device time per solve (CUDA events on the session stream, warm-up
 first), Chebyshev steps*nnz/s, the recursion's algorithmic bytes per second, and for the
@@ -126,9 +127,37 @@ def run_layouts(N, H, R, M, reps, name):
     return out
 
 
+def run_realisations(L, S, Rs, M, reps):
+    """S disorder seeds x Rs vectors: one stacked recursion against S separate solves."""
+    import torch
+    from .core import moments1d_realisations_dev
+    sess = Session()
+    sess.set_stream(torch.cuda.current_stream())
+    ops, sts = [], []
+    for r in range(S):
+        N, H = lattices.cubic_lattice(L, 1.0, 2.0, 41 + r)
+        Hg = Operator.from_csr(N, *H, session=sess)
+        Hg.rescale_to_chebyshev(2 * 1.05 * 7.0, 0.0)
+        ops.append(Hg)
+        sts.append(lattices.random_phase_states(N, Rs, seed=45 + r))
+    st_all = torch.from_numpy(np.concatenate(sts).view(np.float64).copy()).cuda()
+    st_one = [torch.from_numpy(x.view(np.float64).copy()).cuda() for x in sts]
+    out = {"workload": "dos_cubic_%d_%dseeds_x_%d" % (L, S, Rs), "N": ops[0].n, "M": M}
+    for label, prec in (("fp64", PREC_FP64), ("mixed", PREC_MIXED)):
+        o = make_opts(precision=prec)
+        mu = torch.zeros(2 * S * M, dtype=torch.float64, device="cuda")
+        mu1 = torch.zeros(2 * M, dtype=torch.float64, device="cuda")
+        out[label + "_stacked_ms"] = _timed(
+            lambda: moments1d_realisations_dev(ops, st_all, S * Rs, M, mu, opts=o, session=sess), reps, torch)
+        out[label + "_separate_ms"] = _timed(
+            lambda: [moments1d_dev(ops[r], None, st_one[r], Rs, M, mu1, opts=o, session=sess) for r in range(S)],
+            reps, torch)
+    return out
+
+
 def main(argv=None):
     ap = argparse.ArgumentParser()
-    ap.add_argument("workload", choices=["dos", "cubic", "spin", "layouts"])
+    ap.add_argument("workload", choices=["dos", "cubic", "spin", "layouts", "realisations"])
     ap.add_argument("--reps", type=int, default=5)
     ap.add_argument("--cells", type=int, default=64, help="spin: Kane-Mele cells per side")
     ap.add_argument("--moments", type=int, default=512, help="spin: M")
@@ -140,6 +169,11 @@ def main(argv=None):
     elif a.workload == "cubic":
         N, H = lattices.cubic_lattice(100, 1.0, 2.0, 41)
         r = run_1d("dos_cubic_100_seed41", N, H, 64, 1024, a.reps, 45)
+    elif a.workload == "realisations":
+        rs = [run_realisations(100, 4, 64, 1024, a.reps), run_realisations(40, 4, 8, 1024, a.reps)]
+        for r in rs:
+            print(json.dumps(r))
+        return
     elif a.workload == "layouts":
         N, H = lattices.cubic_lattice(100, 1.0, 2.0, 41)
         rs = [run_layouts(N, H, R, 256, a.reps, "dos_cubic_100") for R in (1, 4, 64)]

@@ -128,3 +128,36 @@ def test_sell_layout_large_operator(oracle_lib):
     st = lattices.random_phase_states(N, 2, seed=47)
     mu = lq.moments1d(Hg, None, st, 32, opts=lq.make_opts(fmt=1))
     assert rel(mu, oracle_lib.moments1d(Ho, None, st, 32)) < TOL
+
+
+@pytest.mark.parametrize("S,Rs", [(4, 32), (2, 64), (3, 8)])
+def test_disorder_realisations_in_one_block(oracle_lib, S, Rs):
+    """S Anderson disorder seeds x Rs vectors in one persistent recursion: each realisation's
+    moments equal its own single-Hamiltonian solve and the oracle's."""
+    L, M = 10, 200
+    ops_g, ops_o, states = [], [], []
+    bw, bc = 2 * 1.05 * (6.0 + 1.0), 0.0  # common bounds for all seeds: |E| <= 6t + W/2
+    for r in range(S):
+        N, H = lattices.cubic_lattice(L, t=1.0, W=2.0, seed=41 + r)
+        Hg = lq.Operator.from_csr(N, *H)
+        Hg.rescale_to_chebyshev(bw, bc)
+        ops_g.append(Hg)
+        ops_o.append(oracle_lib.Op(*H).rescale(2 / bw, -bc / (bw / 2)))
+        states.append(lattices.random_phase_states(N, Rs, seed=100 + r))
+    mu = lq.moments1d_realisations(ops_g, np.concatenate(states), M)
+    assert mu.shape == (S, M)
+    for r in range(S):
+        alone = lq.moments1d(ops_g[r], None, states[r], M)
+        assert rel(mu[r], alone) < 1e-12
+        assert rel(mu[r], oracle_lib.moments1d(ops_o[r], None, states[r], M)) < TOL
+    mx = lq.moments1d_realisations(ops_g, np.concatenate(states), M, opts=lq.make_opts(precision=lq.PREC_MIXED))
+    assert rel(mx, mu) < 1e-5
+
+
+def test_disorder_realisations_reject_mismatched_patterns():
+    N, H = lattices.cubic_lattice(6, seed=41)
+    N2, H2 = lattices.cubic_lattice(7, seed=41)
+    a = lq.Operator.from_csr(N, *H)
+    b = lq.Operator.from_csr(N2, *H2)
+    with pytest.raises(lq.LinqtError):
+        lq.moments1d_realisations([a, b], np.ones((64, N)), 16)
