@@ -71,7 +71,9 @@ typedef struct linqt_opts {
                        (autotuned among CSR and SELL with C = 8, 32; cached per operator) */
   int block_width;  /* vector columns per recursion block (0 = all R, or the autotuned chunk) */
   int doubling;     /* 1D: 0 = doubling identities when the operator is the identity, 1 = force them, 2 = direct <r|T_n r> */
-  int use_graphs;   /* reserved (0) */
+  int use_graphs;   /* 1: *_dev solves replay an instantiated CUDA graph from the second call with the same
+                       pointers, sizes and operators on (first call eager, second captured); workspace
+                       reallocations drop the session's graphs; not for sessions on the legacy stream */
   int step_launches; /* 1 = one kernel launch per recursion step instead of one persistent cooperative launch */
   int reserved[10];
 } linqt_opts;
@@ -94,6 +96,8 @@ int linqt_session_trim(linqt_session *s);
  * reconstruction, [3] other; launches[0..3] the kernel launches per phase. */
 int linqt_session_phase_times(linqt_session *s, double ms[4], long launches[4], int reset);
 int linqt_session_enable_timing(linqt_session *s, int on);
+/* Instantiated CUDA graphs held by the session (opts.use_graphs) and solves launched from them. */
+int linqt_session_graph_stats(linqt_session *s, int *graphs, long *replays);
 
 /* ---- operators: SparseMatrixType (include/sparse_matrix.hpp:45-88) ------ */
 /* ConvertFromCSR (src/mkl_sparse_matrix.cpp:39-54) + BuildOPFromCSRFile (include/sparse_matrix.hpp:100-108) */

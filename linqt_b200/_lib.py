@@ -54,6 +54,7 @@ SIGNATURES = {
     "linqt_session_trim": (c_int, [c_void_p]),
     "linqt_session_phase_times": (c_int, [c_void_p, P_double, P_long, c_int]),
     "linqt_session_enable_timing": (c_int, [c_void_p, c_int]),
+    "linqt_session_graph_stats": (c_int, [c_void_p, P_int, P_long]),
     "linqt_csr_create": (c_int, [c_void_p, c_int, P_int, P_int, P_double, c_int, ctypes.POINTER(c_void_p)]),
     "linqt_op_destroy": (c_int, [c_void_p]),
     "linqt_op_info": (c_int, [c_void_p, P_int, P_long]),

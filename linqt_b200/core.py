@@ -44,12 +44,14 @@ def _ptr(x):
     return x.data_ptr()
 
 
-def make_opts(precision=PREC_FP64, fmt=0, block_width=0, doubling=0, step_launches=0):
+def make_opts(precision=PREC_FP64, fmt=0, block_width=0, doubling=0, step_launches=0, use_graphs=0):
     """Solver options (linqt_opts).  doubling: 0 auto, 1 force, 2 off.  step_launches: 1 = one launch per
-    recursion step instead of the persistent cooperative kernel."""
+    recursion step instead of the persistent cooperative kernel.  use_graphs: 1 = *_dev solves replayed
+    from CUDA graphs after their first call."""
     o = Opts()
     o.precision, o.format, o.block_width, o.doubling, o.step_launches = (precision, fmt, block_width, doubling,
                                                                          step_launches)
+    o.use_graphs = use_graphs
     return o
 
 
@@ -92,6 +94,12 @@ class Session:
 
     def enable_timing(self, on=True):
         check(load().linqt_session_enable_timing(self.h, 1 if on else 0))
+
+    def graph_stats(self):
+        """(instantiated graphs, solves launched from graphs) under opts.use_graphs."""
+        g, r = ctypes.c_int(), ctypes.c_long()
+        check(load().linqt_session_graph_stats(self.h, ctypes.byref(g), ctypes.byref(r)))
+        return g.value, r.value
 
     def phase_times(self, reset=False):
         """(ms[4], launches[4]) for recursion, contraction, FFT, other."""

@@ -3,6 +3,7 @@
 // Every entry point catches linqt::Error (and std::exception) and turns it into a
 // negative status plus a thread-local message; nothing aborts across the ABI.
 #include <algorithm>
+#include <atomic>
 #include <cmath>
 #include <cstring>
 #include <functional>
@@ -61,7 +62,9 @@ void *Session::get(const std::string &name, size_t bytes) {
   if (bytes == 0) bytes = 16;
   auto it = ws.find(name);
   if (it != ws.end() && it->second.second >= bytes) return it->second.first;
+  if (capturing) fail(LINQT_ERR_INTERNAL, "workspace '" + name + "' would be allocated inside a graph capture");
   if (it != ws.end()) {
+    drop_graphs();  // they hold the old address
     LQ_CUDA(cudaFreeAsync(it->second.first, stream));
     ws.erase(it);
   }
@@ -83,7 +86,14 @@ void *Session::get(const std::string &name, size_t bytes) {
   return p;
 }
 
+void Session::drop_graphs() {
+  for (auto &kv : graphs) cudaGraphExecDestroy(kv.second);
+  graphs.clear();
+  graph_calls.clear();
+}
+
 void Session::trim() {
+  drop_graphs();
   for (auto &kv : ws) cudaFreeAsync(kv.second.first, stream);
   ws.clear();
   if (stream) cudaStreamSynchronize(stream);
@@ -230,6 +240,8 @@ void DeviceOp::upload() {
   }
   nnz = rowptr[n];
   free_device();
+  static std::atomic<unsigned long> next_uid{1};
+  uid = next_uid++;
   LQ_CUDA(cudaSetDevice(device));
   LQ_CUDA(cudaMalloc(&d_rowptr, sizeof(int) * (n + 1)));
   LQ_CUDA(cudaMalloc(&d_col, sizeof(int) * std::max(1L, nnz)));
@@ -338,6 +350,79 @@ static linqt_opts defaults(const linqt_opts *o) {
   LQ_REQUIRE(d.format == LINQT_FORMAT_CSR || d.format == LINQT_FORMAT_SELL || d.format == LINQT_FORMAT_AUTO,
              "opts.format: unknown sparse format");
   return d;
+}
+
+// ---------------------------------------------------------------------------
+// opts.use_graphs: a *_dev solve is enqueued eagerly on its first call with a given key (so
+// that every workspace is allocated and any autotuning is done), captured into a CUDA graph
+// on the second and replayed from the instantiated graph afterwards.  The key holds every
+// pointer and size of the call and the operators' upload ids and versions; a workspace
+// reallocation drops all graphs of the session.  While capturing, cooperative launches go on
+// the session stream itself rather than the device lane.  Sessions on the legacy default
+// stream, sessions with phase timing on, and keys whose capture failed run eagerly.
+// ---------------------------------------------------------------------------
+static std::string call_key(const char *name, std::initializer_list<const void *> ptrs,
+                            std::initializer_list<const DeviceOp *> ops, std::initializer_list<double> nums,
+                            const linqt_opts &o) {
+  std::string k(name);
+  char buf[64];
+  for (const void *p : ptrs) {
+    snprintf(buf, sizeof(buf), ":%p", p);
+    k += buf;
+  }
+  for (const DeviceOp *d : ops) {
+    snprintf(buf, sizeof(buf), ":%lu.%u", d ? d->uid : 0ul, d ? d->version : 0u);
+    k += buf;
+  }
+  for (double x : nums) {
+    snprintf(buf, sizeof(buf), ":%a", x);
+    k += buf;
+  }
+  snprintf(buf, sizeof(buf), ":%d.%d.%d.%d.%d", o.precision, o.format, o.block_width, o.doubling, o.step_launches);
+  return k + buf;
+}
+
+template <class F>
+static void with_graph(Session *s, const linqt_opts &o, const std::string &key, F &&enqueue) {
+  if (!o.use_graphs || s->timing || s->stream == nullptr) {
+    enqueue();
+    return;
+  }
+  auto g = s->graphs.find(key);
+  if (g != s->graphs.end()) {
+    LQ_CUDA(cudaGraphLaunch(g->second, s->stream));
+    ++s->graph_replays;
+    return;
+  }
+  int &calls = s->graph_calls[key];
+  if (calls <= 0) {  // first call, or a capture that failed: eagerly
+    if (calls == 0) calls = 1;
+    enqueue();
+    return;
+  }
+  cudaGraph_t graph = nullptr;
+  cudaGraphExec_t exec = nullptr;
+  LQ_CUDA(cudaStreamBeginCapture(s->stream, cudaStreamCaptureModeThreadLocal));
+  s->capturing = true;
+  bool ok = true;
+  try {
+    enqueue();
+  } catch (const Error &) {
+    ok = false;
+  }
+  s->capturing = false;
+  cudaError_t e = cudaStreamEndCapture(s->stream, &graph);
+  if (ok && e == cudaSuccess && graph) e = cudaGraphInstantiate(&exec, graph, 0);
+  if (graph) cudaGraphDestroy(graph);
+  if (!ok || e != cudaSuccess || !exec) {
+    cudaGetLastError();
+    s->graph_calls[key] = -1;
+    enqueue();
+    return;
+  }
+  s->graphs[key] = exec;
+  LQ_CUDA(cudaGraphLaunch(exec, s->stream));
+  ++s->graph_replays;
 }
 
 // ---------------------------------------------------------------------------
@@ -882,6 +967,14 @@ int linqt_session_enable_timing(linqt_session *s, int on) {
   return guarded([&] { resolve(s)->timing = on != 0; });
 }
 
+int linqt_session_graph_stats(linqt_session *s, int *graphs, long *replays) {
+  return guarded([&] {
+    Session *r = resolve(s);
+    if (graphs) *graphs = (int)r->graphs.size();
+    if (replays) *replays = r->graph_replays;
+  });
+}
+
 int linqt_session_phase_times(linqt_session *s, double ms[4], long launches[4], int reset) {
   return guarded([&] {
     Session *r = resolve(s);
@@ -1054,7 +1147,11 @@ int linqt_moments1d_dev(linqt_session *s, const linqt_op *H, const linqt_op *op,
   return guarded([&] {
     check_op(H, "H");
     LQ_REQUIRE(states_dev && mu_dev, "NULL pointer");
-    moments1d_dev(resolve(s), H->op, dop(op), (const double2 *)states_dev, R, M, defaults(opts), (double2 *)mu_dev);
+    Session *ss = resolve(s);
+    const linqt_opts o = defaults(opts);
+    with_graph(ss, o, call_key("m1", {states_dev, mu_dev}, {&H->op, dop(op)}, {(double)R, (double)M}, o), [&] {
+      moments1d_dev(ss, H->op, dop(op), (const double2 *)states_dev, R, M, o, (double2 *)mu_dev);
+    });
   });
 }
 
@@ -1115,8 +1212,10 @@ int linqt_moments2d_dev(linqt_session *s, const linqt_op *H, const linqt_op *opl
   return guarded([&] {
     check_op(H, "H");
     LQ_REQUIRE(states_dev && mu_dev, "NULL pointer");
-    moments2d_dev(resolve(s), H->op, dop(opl), dop(opr), (const double2 *)states_dev, R, M, defaults(opts),
-                  (double2 *)mu_dev);
+    Session *ss = resolve(s);
+    const linqt_opts o = defaults(opts);
+    with_graph(ss, o, call_key("m2", {states_dev, mu_dev}, {&H->op, dop(opl), dop(opr)}, {(double)R, (double)M}, o),
+               [&] { moments2d_dev(ss, H->op, dop(opl), dop(opr), (const double2 *)states_dev, R, M, o, (double2 *)mu_dev); });
   });
 }
 
@@ -1144,8 +1243,15 @@ int linqt_kubo_fft_dev(linqt_session *s, const linqt_op *H, const linqt_op *opl,
   return guarded([&] {
     check_op(H, "H");
     LQ_REQUIRE(states_dev && out_dev, "NULL pointer");
-    kubo_fft_dev(resolve(s), H->op, dop(opl), dop(opr), (const double2 *)states_dev, R, M, nump, formula,
-                 band_width, band_center, defaults(opts), out_dev);
+    Session *ss = resolve(s);
+    const linqt_opts o = defaults(opts);
+    with_graph(ss, o,
+               call_key("kf", {states_dev, out_dev}, {&H->op, dop(opl), dop(opr)},
+                        {(double)R, (double)M, (double)nump, (double)formula, band_width, band_center}, o),
+               [&] {
+                 kubo_fft_dev(ss, H->op, dop(opl), dop(opr), (const double2 *)states_dev, R, M, nump, formula,
+                              band_width, band_center, o, out_dev);
+               });
   });
 }
 
@@ -1178,8 +1284,15 @@ int linqt_kubo_bastin_dev(linqt_session *s, const linqt_op *H, const linqt_op *o
   return guarded([&] {
     check_op(H, "H");
     LQ_REQUIRE(states_dev && (mu_dev || out_dev), "NULL pointer");
-    kubo_bastin_dev(resolve(s), H->op, dop(opl), dop(opr), (const double2 *)states_dev, R, M, nump, band_width,
-                    band_center, defaults(opts), (double2 *)mu_dev, out_dev);
+    Session *ss = resolve(s);
+    const linqt_opts o = defaults(opts);
+    with_graph(ss, o,
+               call_key("kb", {states_dev, mu_dev, out_dev}, {&H->op, dop(opl), dop(opr)},
+                        {(double)R, (double)M, (double)nump, band_width, band_center}, o),
+               [&] {
+                 kubo_bastin_dev(ss, H->op, dop(opl), dop(opr), (const double2 *)states_dev, R, M, nump, band_width,
+                                 band_center, o, (double2 *)mu_dev, out_dev);
+               });
   });
 }
 

@@ -128,6 +128,7 @@ struct DeviceOp {
   double2 *d_val64 = nullptr;
   float2 *d_val32 = nullptr;  // created on first mixed-precision use
   unsigned version = 0;  // bumped by rescale
+  unsigned long uid = 0;  // distinct for every upload (keys the replayable graphs)
   // SELL-C-sigma copies of the expanded operator, by slice height C (built on first use)
   struct Sell {
     int *d_perm = nullptr, *d_off = nullptr, *d_col = nullptr;
@@ -174,6 +175,13 @@ struct Session {
   int sm_count = 148;
   size_t hbm_budget = 0;  // chunking budget; 0 = what the device has free
   bool barrier_used = false;  // a persistent kernel ran since the last error check
+  // opts.use_graphs: solves replayed from instantiated CUDA graphs, by call key.  A graph holds
+  // the workspace addresses it was captured with, so every workspace reallocation drops them.
+  bool capturing = false;
+  std::map<std::string, cudaGraphExec_t> graphs;
+  std::map<std::string, int> graph_calls;  // calls seen per key (the first runs eagerly); -1: capture failed
+  long graph_replays = 0;
+  void drop_graphs();
 
   void *get(const std::string &name, size_t bytes);  // cached device buffer, >= bytes
   void trim();

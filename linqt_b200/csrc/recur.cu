@@ -430,6 +430,10 @@ struct CoopLane {
 };
 
 void coop_launch(Session *s, const void *f, int grid, void **args, size_t smem) {
+  if (s->capturing) {  // a graph capture of this session's stream (api.cu, with_graph)
+    LQ_CUDA(cudaLaunchCooperativeKernel(f, dim3(grid), dim3(kThreads), args, smem, s->stream));
+    return;
+  }
   static std::mutex table_mu;
   static std::unordered_map<int, std::unique_ptr<CoopLane>> lanes;
   CoopLane *lane;
