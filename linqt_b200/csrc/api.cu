@@ -215,16 +215,13 @@ void DeviceOp::free_device() {
   cudaFree(d_rowptr);
   cudaFree(d_col);
   cudaFree(d_val64);
-  cudaFree(d_val32);
   d_rowptr = d_col = nullptr;
   d_val64 = nullptr;
-  d_val32 = nullptr;
   for (auto &kv : sell) {
     cudaFree(kv.second.d_perm);
     cudaFree(kv.second.d_off);
     cudaFree(kv.second.d_col);
     cudaFree(kv.second.d_val64);
-    cudaFree(kv.second.d_val32);
   }
   sell.clear();
   tuned.clear();
@@ -257,7 +254,7 @@ void DeviceOp::upload() {
 // SELL-C-sigma: rows sorted by decreasing length inside windows of sigma = 8C rows
 // (stable), slices of C rows, each slice stored column-major with width = its longest
 // row; padding entries point at the row itself with value zero.
-const DeviceOp::Sell &DeviceOp::ensure_sell(int C, bool fp32) {
+const DeviceOp::Sell &DeviceOp::ensure_sell(int C) {
   std::lock_guard<std::mutex> g(mu);
   Sell &L = sell[C];
   if (!L.d_perm) {
@@ -302,24 +299,7 @@ const DeviceOp::Sell &DeviceOp::ensure_sell(int C, bool fp32) {
     LQ_CUDA(cudaMemcpy(L.d_col, sc.data(), sizeof(int) * L.len, cudaMemcpyHostToDevice));
     LQ_CUDA(cudaMemcpy(L.d_val64, sv.data(), sizeof(double2) * L.len, cudaMemcpyHostToDevice));
   }
-  if (fp32 && !L.d_val32) {
-    std::vector<double2> sv(L.len);
-    LQ_CUDA(cudaMemcpy(sv.data(), L.d_val64, sizeof(double2) * L.len, cudaMemcpyDeviceToHost));
-    std::vector<float2> v32(L.len);
-    for (size_t q = 0; q < L.len; ++q) v32[q] = make_float2((float)sv[q].x, (float)sv[q].y);
-    LQ_CUDA(cudaMalloc(&L.d_val32, sizeof(float2) * L.len));
-    LQ_CUDA(cudaMemcpy(L.d_val32, v32.data(), sizeof(float2) * L.len, cudaMemcpyHostToDevice));
-  }
   return L;
-}
-
-void DeviceOp::ensure_fp32() {
-  std::lock_guard<std::mutex> g(mu);
-  if (d_val32) return;
-  std::vector<float2> v(std::max(1L, nnz));
-  for (long k = 0; k < nnz; ++k) v[k] = make_float2((float)val[k].x, (float)val[k].y);
-  LQ_CUDA(cudaMalloc(&d_val32, sizeof(float2) * v.size()));
-  LQ_CUDA(cudaMemcpy(d_val32, v.data(), sizeof(float2) * v.size(), cudaMemcpyHostToDevice));
 }
 
 // ---------------------------------------------------------------------------
@@ -482,10 +462,6 @@ static void moments1d_dev(Session *s, const DeviceOp &H, const DeviceOp *op, con
   LQ_REQUIRE(!op || op->n == H.n, "moments1d: operator dimension mismatch");
   const int N = H.n;
   const bool fp32 = o.precision != LINQT_PREC_FP64;
-  if (fp32) {
-    const_cast<DeviceOp &>(H).ensure_fp32();
-    if (op) const_cast<DeviceOp &>(*op).ensure_fp32();
-  }
   const bool doubling = (o.doubling == 0 && op == nullptr) || o.doubling == 1;
   LQ_REQUIRE(!(doubling && op), "moments1d: the doubling identities need the identity operator");
   int Rc = o.block_width > 0 ? o.block_width : std::min(256, pow2_at_least(R));
@@ -601,12 +577,11 @@ static void moments1d_realisations_dev(Session *s, const DeviceOp *const *Hs, in
   const bool fp32 = o.precision != LINQT_PREC_FP64;
   const int N = H0.n;
   const size_t esz = fp32 ? sizeof(float2) : sizeof(double2);
-  char *vals = (char *)s->get("real_vals", esz * (size_t)S * std::max(1L, H0.nnz));
-  for (int r = 0; r < S; ++r) {
-    if (fp32) const_cast<DeviceOp *>(Hs[r])->ensure_fp32();
-    const void *src = fp32 ? (const void *)Hs[r]->d_val32 : (const void *)Hs[r]->d_val64;
-    LQ_CUDA(cudaMemcpyAsync(vals + esz * (size_t)r * H0.nnz, src, esz * H0.nnz, cudaMemcpyDeviceToDevice, s->stream));
-  }
+  // the S value sets side by side (FP64 for either precision of the vectors)
+  char *vals = (char *)s->get("real_vals", sizeof(double2) * (size_t)S * std::max(1L, H0.nnz));
+  for (int r = 0; r < S; ++r)
+    LQ_CUDA(cudaMemcpyAsync(vals + sizeof(double2) * (size_t)r * H0.nnz, Hs[r]->d_val64, sizeof(double2) * H0.nnz,
+                            cudaMemcpyDeviceToDevice, s->stream));
   const int steps = (M + 1) / 2;  // doubling identities
   const size_t blk = esz * (size_t)N * R;
   char *T = (char *)s->get("m1_T", 3 * blk);
@@ -737,15 +712,11 @@ static Chunking pick_chunks(Session *s, int N, int R, int M, size_t esz, const l
   return {Rc, (R + Rc - 1) / Rc};
 }
 
-// FP32 recursions need FP32 copies of the operators; returns whether the blocks are FP32.
-static bool prepare_precision(const linqt_opts &o, const DeviceOp &H, const DeviceOp *a, const DeviceOp *b) {
+// Whether the vector blocks are FP32 (the operators stay FP64 in every mode).
+static bool prepare_precision(const linqt_opts &o, const DeviceOp &, const DeviceOp *, const DeviceOp *) {
   LQ_REQUIRE(o.precision == LINQT_PREC_FP64 || o.precision == LINQT_PREC_MIXED || o.precision == LINQT_PREC_FP32,
              "unknown precision");
-  if (o.precision == LINQT_PREC_FP64) return false;
-  const_cast<DeviceOp &>(H).ensure_fp32();
-  if (a) const_cast<DeviceOp &>(*a).ensure_fp32();
-  if (b) const_cast<DeviceOp &>(*b).ensure_fp32();
-  return true;
+  return o.precision != LINQT_PREC_FP64;
 }
 
 // ---------------------------------------------------------------------------

@@ -93,6 +93,21 @@ __host__ __device__ __forceinline__ double2 cconj(double2 a) { return make_doubl
 __device__ __forceinline__ double2 to_d2(double2 a) { return a; }
 __device__ __forceinline__ double2 to_d2(float2 a) { return make_double2(a.x, a.y); }
 
+// FP64 operator entry times a vector entry of either precision, accumulated in FP64: the
+// recursions keep H and V in FP64 whatever the precision of their vector blocks (an FP32
+// copy of H perturbs its spectrum coherently, and that error grows with the moment index).
+__device__ __forceinline__ double2 cfma(double2 a, float2 b, double2 c) { return cfma(a, to_d2(b), c); }
+template <class C>
+__device__ __forceinline__ C from_d2(double2 v);
+template <>
+__device__ __forceinline__ double2 from_d2<double2>(double2 v) {
+  return v;
+}
+template <>
+__device__ __forceinline__ float2 from_d2<float2>(double2 v) {
+  return make_float2((float)v.x, (float)v.y);
+}
+
 // ---------------------------------------------------------------------------
 // device operator: Hermitian-expanded CSR (plus optional FP32 copy and SELL-C)
 // ---------------------------------------------------------------------------
@@ -126,24 +141,21 @@ struct DeviceOp {
   long nnz = 0;
   int *d_rowptr = nullptr, *d_col = nullptr;
   double2 *d_val64 = nullptr;
-  float2 *d_val32 = nullptr;  // created on first mixed-precision use
   unsigned version = 0;  // bumped by rescale
   unsigned long uid = 0;  // distinct for every upload (keys the replayable graphs)
   // SELL-C-sigma copies of the expanded operator, by slice height C (built on first use)
   struct Sell {
     int *d_perm = nullptr, *d_off = nullptr, *d_col = nullptr;
     double2 *d_val64 = nullptr;
-    float2 *d_val32 = nullptr;
     size_t len = 0;
   };
   std::map<int, Sell> sell;
-  const Sell &ensure_sell(int C, bool fp32);
+  const Sell &ensure_sell(int C);
   // format chosen by the autotuner, per (recursion kind, block width, precision, second operator)
   std::map<std::string, int> tuned;
   std::mutex mu;
 
   CsrView csr64() const { return CsrView{n, nnz, d_rowptr, d_col, d_val64}; }
-  void ensure_fp32();
   void free_device();
   void upload();
 };

@@ -14,8 +14,13 @@
 // recursion with the dot products of every step written as per-CTA partials, reduced
 // afterwards in a fixed order.
 //
-// Vectors written in one step are read by other CTAs in the next, so vector loads use
-// ld.global.cg (L2, bypassing the non-coherent L1); the operators use the read-only path.
+// Vectors written in one step are read by other CTAs in the next.  The grid barrier
+// orders those writes before the next step's reads (release: bar.sync, fence, atomic;
+// acquire: poll, fence, bar.sync) and its gpu-scope fence invalidates stale L1 lines, so
+// vector loads may go through L1 (ld.global.ca), where a row's neighbours read by nearby
+// rows of the same CTA hit.  Operators (read-only for the whole launch) use the
+// read-only path.  The operators are FP64 for either vector precision: FP32 blocks are
+// accumulated in FP64 and rounded once per entry and step.
 #include <memory>
 #include <unordered_map>
 
@@ -37,11 +42,8 @@ struct Barrier {
 
 template <class C>
 __device__ __forceinline__ C ldv(const C *p) {
-  return __ldcg(p);
+  return __ldca(p);
 }
-
-__device__ __forceinline__ double2 zero2(double2) { return make_double2(0, 0); }
-__device__ __forceinline__ float2 zero2(float2) { return make_float2(0, 0); }
 
 // Grid barrier (all CTAs co-resident: cooperative launch).  Returns false if the wait gave up.
 __device__ bool grid_barrier(Barrier *bar, unsigned nblocks) {
@@ -160,8 +162,8 @@ __device__ size_t cache_rows(const int *__restrict__ rp, const int *__restrict__
 // ---------------------------------------------------------------------------
 template <class T, int TPR, int VPT, bool HAS_V>
 __global__ void __launch_bounds__(kThreads)
-    k_recur_lr(int n, const int *rp, const int *ci, const typename cplx_t<T>::type *hv, const int *vrp,
-               const int *vci, const typename cplx_t<T>::type *vv, typename cplx_t<T>::type *Lst,
+    k_recur_lr(int n, const int *rp, const int *ci, const double2 *hv, const int *vrp, const int *vci,
+               const double2 *vv, typename cplx_t<T>::type *Lst,
                typename cplx_t<T>::type *Rst, const typename cplx_t<T>::type *phi, typename cplx_t<T>::type *tb, int M,
                size_t blk, Barrier *bar, int cache, const int *__restrict__ sperm, const int *__restrict__ soff,
                int sC) {
@@ -174,8 +176,8 @@ __global__ void __launch_bounds__(kThreads)
   if (cache) {
     // the operators do not change during the recursion: keep this CTA's rows on chip
     extern __shared__ __align__(16) unsigned char smc[];
-    size_t off = cache_rows<C>(rp, ci, hv, r0, r1, smc, rp, ci, hv);
-    if (HAS_V) cache_rows<C>(vrp, vci, vv, r0, r1, smc + off, vrp, vci, vv);
+    size_t off = cache_rows<double2>(rp, ci, hv, r0, r1, smc, rp, ci, hv);
+    if (HAS_V) cache_rows<double2>(vrp, vci, vv, r0, r1, smc + off, vrp, vci, vv);
     __syncthreads();
   }
   // Rows: with the operators cached, this CTA's contiguous range; otherwise tiles of gpb
@@ -202,13 +204,13 @@ __global__ void __launch_bounds__(kThreads)
     for (int pos = rfirst + threadIdx.x / TPR; pos < rend; pos += rstep) {
       int row, b, e, st;
       sell_or_csr(pos, sperm, soff, sC, rp, row, b, e, st);
-      C aL[VPT], aR[VPT];
+      double2 aL[VPT], aR[VPT];
 #pragma unroll
-      for (int u = 0; u < VPT; ++u) aL[u] = aR[u] = zero2(C());
+      for (int u = 0; u < VPT; ++u) aL[u] = aR[u] = make_double2(0, 0);
 #pragma unroll 4
       for (int k = b; k < e; k += st) {
         const int j = ci[k];
-        const C h = hv[k];
+        const double2 h = hv[k];
         const size_t off = (size_t)j * R + lane;
 #pragma unroll
         for (int u = 0; u < VPT; ++u) {
@@ -218,42 +220,42 @@ __global__ void __launch_bounds__(kThreads)
       }
       const size_t base = (size_t)row * R + lane;
       if (HAS_V) {
-        C aV[VPT];
+        double2 aV[VPT];
 #pragma unroll
-        for (int u = 0; u < VPT; ++u) aV[u] = zero2(C());
+        for (int u = 0; u < VPT; ++u) aV[u] = make_double2(0, 0);
         const int vb = vrp[row], ve = vrp[row + 1];
 #pragma unroll 4
         for (int k = vb; k < ve; ++k) {
           const int j = vci[k];
-          const C h = vv[k];
+          const double2 h = vv[k];
           const size_t off = (size_t)j * R + lane;
 #pragma unroll
           for (int u = 0; u < VPT; ++u) aV[u] = cfma(h, ldv(xR + off + u * TPR), aV[u]);
         }
         C *vo = Rst + (size_t)m * blk;
 #pragma unroll
-        for (int u = 0; u < VPT; ++u) vo[base + u * TPR] = aV[u];
+        for (int u = 0; u < VPT; ++u) vo[base + u * TPR] = from_d2<C>(aV[u]);
       }
 #pragma unroll
       for (int u = 0; u < VPT; ++u) {
         const size_t idx = base + u * TPR;
         if (doL) {
-          C y = aL[u];
+          double2 y = aL[u];
           if (pL) {
-            const C p = ldv(pL + idx);
+            const double2 p = to_d2(ldv(pL + idx));
             y.x = 2 * y.x - p.x;
             y.y = 2 * y.y - p.y;
           }
-          yL[idx] = y;
+          yL[idx] = from_d2<C>(y);
         }
         if (yR) {
-          C y = aR[u];
+          double2 y = aR[u];
           if (pR) {
-            const C p = ldv(pR + idx);
+            const double2 p = to_d2(ldv(pR + idx));
             y.x = 2 * y.x - p.x;
             y.y = 2 * y.y - p.y;
           }
-          yR[idx] = y;
+          yR[idx] = from_d2<C>(y);
         }
       }
     }
@@ -270,8 +272,7 @@ __global__ void __launch_bounds__(kThreads)
 // ---------------------------------------------------------------------------
 template <class T, int TPR, int VPT, bool STACKED>
 __global__ void __launch_bounds__(kThreads)
-    k_recur_1d(int n, const int *rp, const int *ci, const typename cplx_t<T>::type *hv,
-               const typename cplx_t<T>::type *phi, typename cplx_t<T>::type *x0, typename cplx_t<T>::type *b1,
+    k_recur_1d(int n, const int *rp, const int *ci, const double2 *hv, const typename cplx_t<T>::type *phi, typename cplx_t<T>::type *x0, typename cplx_t<T>::type *b1,
                int steps, int M, int mode, double2 *__restrict__ partials, Barrier *bar, int cache,
                const int *__restrict__ sperm, const int *__restrict__ soff, int sC, long vstride, int nreal,
                int ldx_rt) {
@@ -292,7 +293,7 @@ __global__ void __launch_bounds__(kThreads)
   const int r0 = min(n, blockIdx.x * per), r1 = min(n, r0 + per);
   if (cache) {
     extern __shared__ __align__(16) unsigned char smc1[];
-    cache_rows<C>(rp, ci, hv, r0, r1, smc1, rp, ci, hv);
+    cache_rows<double2>(rp, ci, hv, r0, r1, smc1, rp, ci, hv);
     __syncthreads();
   }
   const int rfirst = cache ? r0 : bl * gpb, rend = cache ? r1 : n;  // as in k_recur_lr
@@ -305,13 +306,13 @@ __global__ void __launch_bounds__(kThreads)
     for (int pos = rfirst + threadIdx.x / TPR; pos < rend; pos += rstep) {
       int row, b, e, st;
       sell_or_csr(pos, sperm, soff, sC, rp, row, b, e, st);
-      C acc[VPT];
+      double2 acc[VPT];
 #pragma unroll
-      for (int u = 0; u < VPT; ++u) acc[u] = zero2(C());
+      for (int u = 0; u < VPT; ++u) acc[u] = make_double2(0, 0);
 #pragma unroll 4
       for (int k = b; k < e; k += st) {
         const int j = ci[k];
-        const C h = hv[k];
+        const double2 h = hv[k];
         const C *xr = cur + (size_t)j * ldx + coff + lane;
 #pragma unroll
         for (int u = 0; u < VPT; ++u) acc[u] = cfma(h, ldv(xr + u * TPR), acc[u]);
@@ -320,12 +321,13 @@ __global__ void __launch_bounds__(kThreads)
 #pragma unroll
       for (int u = 0; u < VPT; ++u) {
         const size_t idx = base + u * TPR;
-        C yn = acc[u];
+        double2 ya = acc[u];
         if (prev) {
-          const C p = ldv(prev + idx);
-          yn.x = 2 * yn.x - p.x;
-          yn.y = 2 * yn.y - p.y;
+          const double2 p = to_d2(ldv(prev + idx));
+          ya.x = 2 * ya.x - p.x;
+          ya.y = 2 * ya.y - p.y;
         }
+        const C yn = from_d2<C>(ya);  // the value stored and used in the dot products
         if (y) y[idx] = yn;
         const double2 xi = to_d2(ldv(cur + idx));
         if (mode == 1) {
@@ -464,24 +466,23 @@ struct LRF {
   static void run(Session *s, const DeviceOp &H, const DeviceOp *V, void *Lst, void *Rst, const void *phi, void *tb,
                   int M, size_t blk, Barrier *bar, int sellC) {
     using C = typename cplx_t<T>::type;
-    const bool fp32 = sizeof(T) == 4;
-    const C *hv = fp32 ? (const C *)H.d_val32 : (const C *)H.d_val64;
+    const double2 *hv = H.d_val64;
     const int *hci = H.d_col, *sperm = nullptr, *soff = nullptr;
     if (sellC) {
-      const DeviceOp::Sell &L = const_cast<DeviceOp &>(H).ensure_sell(sellC, fp32);
-      hv = fp32 ? (const C *)L.d_val32 : (const C *)L.d_val64;
+      const DeviceOp::Sell &L = const_cast<DeviceOp &>(H).ensure_sell(sellC);
+      hv = L.d_val64;
       hci = L.d_col;
       sperm = L.d_perm;
       soff = L.d_off;
     }
     const int *vrp = V ? V->d_rowptr : nullptr, *vci = V ? V->d_col : nullptr;
-    const C *vv = V ? (fp32 ? (const C *)V->d_val32 : (const C *)V->d_val64) : nullptr;
+    const double2 *vv = V ? V->d_val64 : nullptr;
     int n = H.n;
     C *L = (C *)Lst, *Rs = (C *)Rst, *tbuf = (C *)tb;
     const C *ph = (const C *)phi;
     const void *f = V ? (const void *)k_recur_lr<T, TPR, VPT, true> : (const void *)k_recur_lr<T, TPR, VPT, false>;
     size_t smem = 0;
-    const int grid = coop_setup(f, s->sm_count, H, V, TPR, sizeof(C), &smem, sellC == 0);
+    const int grid = coop_setup(f, s->sm_count, H, V, TPR, sizeof(double2), &smem, sellC == 0);
     int cache = smem > 0;
     int sc = sellC;
     void *args[] = {&n,    (void *)&H.d_rowptr, (void *)&hci, (void *)&hv, (void *)&vrp, (void *)&vci,
@@ -496,14 +497,13 @@ struct OneDF {
   static void run(Session *s, const DeviceOp &H, const void *phi, void *x0, void *b1, int steps, int M, int mode,
                   double2 *dots, Barrier *bar, int sellC, const void *stacked, int nreal) {
     using C = typename cplx_t<T>::type;
-    const bool fp32 = sizeof(T) == 4;
-    const C *hv = stacked ? (const C *)stacked : fp32 ? (const C *)H.d_val32 : (const C *)H.d_val64;
+    const double2 *hv = stacked ? (const double2 *)stacked : H.d_val64;
     long vstride = stacked ? H.nnz : 0;
     LQ_REQUIRE(!stacked || (nreal >= 1 && sellC == 0), "stacked realisations: CSR layout only");
     const int *hci = H.d_col, *sperm = nullptr, *soff = nullptr;
     if (sellC) {
-      const DeviceOp::Sell &L = const_cast<DeviceOp &>(H).ensure_sell(sellC, fp32);
-      hv = fp32 ? (const C *)L.d_val32 : (const C *)L.d_val64;
+      const DeviceOp::Sell &L = const_cast<DeviceOp &>(H).ensure_sell(sellC);
+      hv = L.d_val64;
       hci = L.d_col;
       sperm = L.d_perm;
       soff = L.d_off;
@@ -511,7 +511,7 @@ struct OneDF {
     const void *f = stacked ? (const void *)k_recur_1d<T, TPR, VPT, true> : (const void *)k_recur_1d<T, TPR, VPT, false>;
     size_t smem = 0;
     // the shared-memory operator cache holds one value set: not with stacked realisations
-    int grid = coop_setup(f, s->sm_count, H, nullptr, TPR, sizeof(C), &smem, sellC == 0 && !stacked);
+    int grid = coop_setup(f, s->sm_count, H, nullptr, TPR, sizeof(double2), &smem, sellC == 0 && !stacked);
     if (stacked) grid = std::max(nreal, grid / nreal * nreal);  // equal CTA groups per realisation
     int cache = smem > 0;
     int sc = sellC;

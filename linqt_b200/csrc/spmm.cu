@@ -25,17 +25,6 @@ namespace {
 
 constexpr int kThreads = 256;
 
-template <class C>
-__device__ __forceinline__ C czero();
-template <>
-__device__ __forceinline__ double2 czero<double2>() {
-  return make_double2(0.0, 0.0);
-}
-template <>
-__device__ __forceinline__ float2 czero<float2>() {
-  return make_float2(0.f, 0.f);
-}
-
 __device__ __forceinline__ double2 shfl_down2(double2 v, int o) {
   v.x = __shfl_down_sync(0xffffffffu, v.x, o);
   v.y = __shfl_down_sync(0xffffffffu, v.y, o);
@@ -100,13 +89,13 @@ __device__ __forceinline__ C ld(const C *p) {
   return __ldg(p);
 }
 
-// One recursion step on a CSR operator.  FUSE_V adds a second CSR operator applied
+// One recursion step on a CSR operator (FP64 values and accumulation for either vector
+// precision; FP32 results are rounded once).  FUSE_V adds a second CSR operator applied
 // to the same x.  dot_mode: 0 none, 1 <phi|x>, 2 <x|x> and <y|x>.
 template <class T, int TPR, int VPT, bool FUSE_V>
 __global__ void __launch_bounds__(kThreads)
-    k_step_csr(int n, const int *__restrict__ rp, const int *__restrict__ ci,
-               const typename cplx_t<T>::type *__restrict__ hv, const int *__restrict__ vrp,
-               const int *__restrict__ vci, const typename cplx_t<T>::type *__restrict__ vv,
+    k_step_csr(int n, const int *__restrict__ rp, const int *__restrict__ ci, const double2 *__restrict__ hv,
+               const int *__restrict__ vrp, const int *__restrict__ vci, const double2 *__restrict__ vv,
                const typename cplx_t<T>::type *__restrict__ x, const typename cplx_t<T>::type *yprev,
                typename cplx_t<T>::type *y, typename cplx_t<T>::type *__restrict__ vout,
                const typename cplx_t<T>::type *__restrict__ phi, int first, int dot_mode,
@@ -117,15 +106,15 @@ __global__ void __launch_bounds__(kThreads)
   const int gpb = kThreads / TPR;
   double2 d0 = make_double2(0, 0), d1 = make_double2(0, 0);
   for (int row = blockIdx.x * gpb + threadIdx.x / TPR; row < n; row += gridDim.x * gpb) {
-    C acc[VPT];
+    double2 acc[VPT];
 #pragma unroll
-    for (int u = 0; u < VPT; ++u) acc[u] = czero<C>();
+    for (int u = 0; u < VPT; ++u) acc[u] = make_double2(0, 0);
     {
       const int b = rp[row], e = rp[row + 1];
 #pragma unroll 4
       for (int k = b; k < e; ++k) {
         const int j = __ldg(ci + k);
-        const C h = ld(hv + k);
+        const double2 h = ld(hv + k);
         const C *xr = x + (size_t)j * R + lane;
 #pragma unroll
         for (int u = 0; u < VPT; ++u) acc[u] = cfma(h, ld(xr + u * TPR), acc[u]);
@@ -133,30 +122,31 @@ __global__ void __launch_bounds__(kThreads)
     }
     const size_t base = (size_t)row * R + lane;
     if (FUSE_V) {
-      C accv[VPT];
+      double2 accv[VPT];
 #pragma unroll
-      for (int u = 0; u < VPT; ++u) accv[u] = czero<C>();
+      for (int u = 0; u < VPT; ++u) accv[u] = make_double2(0, 0);
       const int b = vrp[row], e = vrp[row + 1];
 #pragma unroll 4
       for (int k = b; k < e; ++k) {
         const int j = __ldg(vci + k);
-        const C h = ld(vv + k);
+        const double2 h = ld(vv + k);
         const C *xr = x + (size_t)j * R + lane;
 #pragma unroll
         for (int u = 0; u < VPT; ++u) accv[u] = cfma(h, ld(xr + u * TPR), accv[u]);
       }
 #pragma unroll
-      for (int u = 0; u < VPT; ++u) vout[base + u * TPR] = accv[u];
+      for (int u = 0; u < VPT; ++u) vout[base + u * TPR] = from_d2<C>(accv[u]);
     }
 #pragma unroll
     for (int u = 0; u < VPT; ++u) {
       const size_t idx = base + u * TPR;
-      C yn = acc[u];
+      double2 ya = acc[u];
       if (!first) {
-        const C p = yprev[idx];
-        yn.x = 2 * yn.x - p.x;
-        yn.y = 2 * yn.y - p.y;
+        const double2 p = to_d2(yprev[idx]);
+        ya.x = 2 * ya.x - p.x;
+        ya.y = 2 * ya.y - p.y;
       }
+      const C yn = from_d2<C>(ya);
       if (y) y[idx] = yn;
       if (dot_mode == 1) {
         d0 = cfma_conj(to_d2(ld(phi + idx)), to_d2(ld(x + idx)), d0);
@@ -173,22 +163,22 @@ __global__ void __launch_bounds__(kThreads)
 // y = alpha*A*x + beta*y  (general SpMM on a site-major block)
 template <class T, int TPR, int VPT>
 __global__ void __launch_bounds__(kThreads)
-    k_spmm_csr(int n, const int *__restrict__ rp, const int *__restrict__ ci,
-               const typename cplx_t<T>::type *__restrict__ av, const typename cplx_t<T>::type *__restrict__ x,
+    k_spmm_csr(int n, const int *__restrict__ rp, const int *__restrict__ ci, const double2 *__restrict__ av,
+               const typename cplx_t<T>::type *__restrict__ x,
                typename cplx_t<T>::type *y, double2 alpha, double2 beta) {
   using C = typename cplx_t<T>::type;
   constexpr int R = TPR * VPT;
   const int lane = threadIdx.x % TPR;
   const int gpb = kThreads / TPR;
   for (int row = blockIdx.x * gpb + threadIdx.x / TPR; row < n; row += gridDim.x * gpb) {
-    C acc[VPT];
+    double2 acc[VPT];
 #pragma unroll
-    for (int u = 0; u < VPT; ++u) acc[u] = czero<C>();
+    for (int u = 0; u < VPT; ++u) acc[u] = make_double2(0, 0);
     const int b = rp[row], e = rp[row + 1];
 #pragma unroll 4
     for (int k = b; k < e; ++k) {
       const int j = __ldg(ci + k);
-      const C h = __ldg(av + k);
+      const double2 h = __ldg(av + k);
       const C *xr = x + (size_t)j * R + lane;
 #pragma unroll
       for (int u = 0; u < VPT; ++u) acc[u] = cfma(h, __ldg(xr + u * TPR), acc[u]);
@@ -196,8 +186,7 @@ __global__ void __launch_bounds__(kThreads)
     const size_t base = (size_t)row * R + lane;
 #pragma unroll
     for (int u = 0; u < VPT; ++u) {
-      const double2 a = to_d2(acc[u]);
-      double2 r = cmul(alpha, a);
+      double2 r = cmul(alpha, acc[u]);
       if (beta.x != 0.0 || beta.y != 0.0) r = cadd(r, cmul(beta, to_d2(y[base + u * TPR])));
       y[base + u * TPR] = typename cplx_t<T>::type{(T)r.x, (T)r.y};
     }
@@ -225,8 +214,7 @@ int grid_for(Session *s, long rows, int tpr) {
 template <class T, int TPR, int VPT>
 void launch_step(Session *s, const DeviceOp &H, const StepArgs &a) {
   using C = typename cplx_t<T>::type;
-  const bool fp32 = sizeof(T) == 4;
-  const C *hv = fp32 ? (const C *)H.d_val32 : (const C *)H.d_val64;
+  const double2 *hv = H.d_val64;
   const int grid = grid_for(s, H.n, TPR);
   double2 *partials = nullptr;
   unsigned *counter = nullptr;
@@ -237,7 +225,7 @@ void launch_step(Session *s, const DeviceOp &H, const StepArgs &a) {
   const int first = a.yprev == nullptr;
   if (a.V) {
     const DeviceOp &V = *a.V;
-    const C *vv = fp32 ? (const C *)V.d_val32 : (const C *)V.d_val64;
+    const double2 *vv = V.d_val64;
     k_step_csr<T, TPR, VPT, true><<<grid, kThreads, 0, s->stream>>>(
         H.n, H.d_rowptr, H.d_col, hv, V.d_rowptr, V.d_col, vv, (const C *)a.x, (const C *)a.yprev, (C *)a.y,
         (C *)a.vout, (const C *)a.phi, first, a.dot_mode, partials, counter, a.dots);
@@ -252,7 +240,7 @@ void launch_step(Session *s, const DeviceOp &H, const StepArgs &a) {
 template <class T, int TPR, int VPT>
 void launch_spmm(Session *s, const DeviceOp &A, double2 alpha, const void *x, double2 beta, void *y) {
   using C = typename cplx_t<T>::type;
-  const C *av = sizeof(T) == 4 ? (const C *)A.d_val32 : (const C *)A.d_val64;
+  const double2 *av = A.d_val64;
   const int grid = grid_for(s, A.n, TPR);
   k_spmm_csr<T, TPR, VPT><<<grid, kThreads, 0, s->stream>>>(A.n, A.d_rowptr, A.d_col, av, (const C *)x, (C *)y,
                                                             alpha, beta);
