@@ -75,7 +75,9 @@ typedef struct linqt_opts {
                        pointers, sizes and operators on (first call eager, second captured); workspace
                        reallocations drop the session's graphs; not for sessions on the legacy stream */
   int step_launches; /* 1 = one kernel launch per recursion step instead of one persistent cooperative launch */
-  int reserved[10];
+  int realisations; /* linqt_moments1d_realisations: 0 = autotuned (short timed trials of both, cached per
+                       operator pattern, S, R/S and precision), 1 = stacked in one launch, 2 = one solve each */
+  int reserved[9];
 } linqt_opts;
 
 /* ---- library / sessions ------------------------------------------------ */

@@ -44,14 +44,17 @@ def _ptr(x):
     return x.data_ptr()
 
 
-def make_opts(precision=PREC_FP64, fmt=0, block_width=0, doubling=0, step_launches=0, use_graphs=0):
+def make_opts(precision=PREC_FP64, fmt=0, block_width=0, doubling=0, step_launches=0, use_graphs=0,
+              realisations=0):
     """Solver options (linqt_opts).  doubling: 0 auto, 1 force, 2 off.  step_launches: 1 = one launch per
     recursion step instead of the persistent cooperative kernel.  use_graphs: 1 = *_dev solves replayed
-    from CUDA graphs after their first call."""
+    from CUDA graphs after their first call.  realisations: 0 autotuned, 1 stacked in one launch,
+    2 one solve per realisation."""
     o = Opts()
     o.precision, o.format, o.block_width, o.doubling, o.step_launches = (precision, fmt, block_width, doubling,
                                                                          step_launches)
     o.use_graphs = use_graphs
+    o.realisations = realisations
     return o
 
 

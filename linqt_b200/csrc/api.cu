@@ -255,6 +255,7 @@ void DeviceOp::upload() {
 // (stable), slices of C rows, each slice stored column-major with width = its longest
 // row; padding entries point at the row itself with value zero.
 const DeviceOp::Sell &DeviceOp::ensure_sell(int C) {
+  LQ_REQUIRE(C > 0, "SELL slice height must be positive");
   std::lock_guard<std::mutex> g(mu);
   Sell &L = sell[C];
   if (!L.d_perm) {
@@ -428,7 +429,9 @@ static int pick_layout(Session *s, const DeviceOp &H, const std::string &key, in
   LQ_CUDA(cudaEventCreate(&b));
   float best = 0;
   int bestC = 0;
-  for (int C : {0, 8, 32}) {
+  // 0: CSR, its row slices cached in shared memory when they fit; -1: CSR without the
+  // cache (more resident CTAs per SM); 8, 32: SELL-C-sigma
+  for (int C : {0, -1, 8, 32}) {
     trial(C);
     LQ_CUDA(cudaEventRecord(a, s->stream));
     trial(C);
@@ -565,15 +568,11 @@ static void moments1d_dev(Session *s, const DeviceOp &H, const DeviceOp *op, con
 // on the device) and its own Rs columns.  Moments per realisation (identity operator,
 // doubling identities): mu[S][M].
 // ---------------------------------------------------------------------------
-static void moments1d_realisations_dev(Session *s, const DeviceOp *const *Hs, int S, const double2 *states, int R,
-                                       int M, const linqt_opts &o, double2 *mu) {
-  LQ_REQUIRE(S >= 1 && R > 0 && M > 0 && R % S == 0, "realisations: R must be a positive multiple of S");
+// S realisations stacked in one persistent launch (S CTA groups, rows of R = S * Rs columns).
+static void realisations_stacked(Session *s, const DeviceOp *const *Hs, int S, const double2 *states, int R, int M,
+                                 const linqt_opts &o, double2 *mu) {
   const DeviceOp &H0 = *Hs[0];
-  for (int r = 1; r < S; ++r)
-    LQ_REQUIRE(Hs[r]->n == H0.n && Hs[r]->rowptr == H0.rowptr && Hs[r]->col == H0.col,
-               "realisations: every Hamiltonian must have the sparsity pattern of the first");
   const int Rs = R / S;
-  LQ_REQUIRE(Rs <= 256 && (Rs & (Rs - 1)) == 0, "realisations: R/S must be a power of two <= 256");
   const bool fp32 = o.precision != LINQT_PREC_FP64;
   const int N = H0.n;
   const size_t esz = fp32 ? sizeof(float2) : sizeof(double2);
@@ -597,6 +596,77 @@ static void moments1d_realisations_dev(Session *s, const DeviceOp *const *Hs, in
   PhaseScope p3(s, PH_OTHER);
   for (int r = 0; r < S; ++r)
     moments1d_from_dots(s, dots + (size_t)2 * steps * r, steps, M, Rs, 2, mu + (size_t)M * r);
+}
+
+// One 1D solve per realisation (each with its own autotuned layout).
+static void realisations_separate(Session *s, const DeviceOp *const *Hs, int S, const double2 *states, int R, int M,
+                                  const linqt_opts &o, double2 *mu) {
+  const int Rs = R / S, N = Hs[0]->n;
+  for (int r = 0; r < S; ++r)
+    moments1d_dev(s, *Hs[r], nullptr, states + (size_t)r * Rs * N, Rs, M, o, mu + (size_t)r * M);
+}
+
+// linqt_moments1d_realisations: stacked or separate.  Stacking saves launches and barriers and
+// fills the GPU when one realisation's block is narrow; on large lattices with wide blocks each
+// separate solve already streams HBM with the whole GPU and the stacked rows (S times wider)
+// cost more in the gathers.  opts.realisations = 0 times a 32-moment trial of both (after one
+// untimed run each) and caches the faster per pattern owner, S, R/S and precision.
+static void moments1d_realisations_dev(Session *s, const DeviceOp *const *Hs, int S, const double2 *states, int R,
+                                       int M, const linqt_opts &o, double2 *mu) {
+  LQ_REQUIRE(S >= 1 && R > 0 && M > 0 && R % S == 0, "realisations: R must be a positive multiple of S");
+  const DeviceOp &H0 = *Hs[0];
+  for (int r = 1; r < S; ++r)
+    LQ_REQUIRE(Hs[r]->n == H0.n && Hs[r]->rowptr == H0.rowptr && Hs[r]->col == H0.col,
+               "realisations: every Hamiltonian must have the sparsity pattern of the first");
+  const int Rs = R / S;
+  LQ_REQUIRE(Rs <= 256 && (Rs & (Rs - 1)) == 0, "realisations: R/S must be a power of two <= 256");
+  LQ_REQUIRE(o.realisations >= 0 && o.realisations <= 2, "opts.realisations must be 0, 1 or 2");
+  int mode = S == 1 ? 2 : o.realisations;
+  if (mode == 0) {
+    DeviceOp &Hm = const_cast<DeviceOp &>(H0);
+    const std::string key = "real:" + std::to_string(S) + ":" + std::to_string(Rs) + ":" +
+                            (o.precision != LINQT_PREC_FP64 ? "f32" : "f64");
+    {
+      std::lock_guard<std::mutex> g(Hm.mu);
+      auto it = Hm.tuned.find(key);
+      if (it != Hm.tuned.end()) mode = it->second;
+    }
+    if (mode == 0) {
+      const int Mt = std::min(M, 32);
+      double2 *tmu = (double2 *)s->get("real_trial_mu", sizeof(double2) * (size_t)S * Mt);
+      cudaEvent_t a, b;
+      LQ_CUDA(cudaEventCreate(&a));
+      LQ_CUDA(cudaEventCreate(&b));
+      float best = 0;
+      for (int c : {1, 2}) {
+        auto run = [&] {
+          if (c == 1)
+            realisations_stacked(s, Hs, S, states, R, Mt, o, tmu);
+          else
+            realisations_separate(s, Hs, S, states, R, Mt, o, tmu);
+        };
+        run();
+        LQ_CUDA(cudaEventRecord(a, s->stream));
+        run();
+        LQ_CUDA(cudaEventRecord(b, s->stream));
+        LQ_CUDA(cudaEventSynchronize(b));
+        float ms = 0;
+        LQ_CUDA(cudaEventElapsedTime(&ms, a, b));
+        if (c == 1 || ms < best) {
+          best = ms;
+          mode = c;
+        }
+      }
+      cudaEventDestroy(a);
+      cudaEventDestroy(b);
+      std::lock_guard<std::mutex> g(Hm.mu);
+      Hm.tuned[key] = mode;
+    }
+  }
+  if (mode == 1)
+    realisations_stacked(s, Hs, S, states, R, M, o, mu);
+  else
+    realisations_separate(s, Hs, S, states, R, M, o, mu);
 }
 
 // ---------------------------------------------------------------------------

@@ -468,7 +468,7 @@ struct LRF {
     using C = typename cplx_t<T>::type;
     const double2 *hv = H.d_val64;
     const int *hci = H.d_col, *sperm = nullptr, *soff = nullptr;
-    if (sellC) {
+    if (sellC > 0) {
       const DeviceOp::Sell &L = const_cast<DeviceOp &>(H).ensure_sell(sellC);
       hv = L.d_val64;
       hci = L.d_col;
@@ -483,6 +483,7 @@ struct LRF {
     const void *f = V ? (const void *)k_recur_lr<T, TPR, VPT, true> : (const void *)k_recur_lr<T, TPR, VPT, false>;
     size_t smem = 0;
     const int grid = coop_setup(f, s->sm_count, H, V, TPR, sizeof(double2), &smem, sellC == 0);
+    sellC = std::max(sellC, 0);  // -1: CSR without the shared-memory cache
     int cache = smem > 0;
     int sc = sellC;
     void *args[] = {&n,    (void *)&H.d_rowptr, (void *)&hci, (void *)&hv, (void *)&vrp, (void *)&vci,
@@ -499,9 +500,9 @@ struct OneDF {
     using C = typename cplx_t<T>::type;
     const double2 *hv = stacked ? (const double2 *)stacked : H.d_val64;
     long vstride = stacked ? H.nnz : 0;
-    LQ_REQUIRE(!stacked || (nreal >= 1 && sellC == 0), "stacked realisations: CSR layout only");
+    LQ_REQUIRE(!stacked || (nreal >= 1 && sellC <= 0), "stacked realisations: CSR layout only");
     const int *hci = H.d_col, *sperm = nullptr, *soff = nullptr;
-    if (sellC) {
+    if (sellC > 0) {
       const DeviceOp::Sell &L = const_cast<DeviceOp &>(H).ensure_sell(sellC);
       hv = L.d_val64;
       hci = L.d_col;
@@ -512,6 +513,7 @@ struct OneDF {
     size_t smem = 0;
     // the shared-memory operator cache holds one value set: not with stacked realisations
     int grid = coop_setup(f, s->sm_count, H, nullptr, TPR, sizeof(double2), &smem, sellC == 0 && !stacked);
+    sellC = std::max(sellC, 0);  // -1: CSR without the shared-memory cache
     if (stacked) grid = std::max(nreal, grid / nreal * nreal);  // equal CTA groups per realisation
     int cache = smem > 0;
     int sc = sellC;

@@ -7,6 +7,7 @@ Kubo-Bastin graphene workload:
     python -m linqt_b200.workloads spin --moments 1024 --vectors 32 --reps 1   # the full moment and vector counts
     python -m linqt_b200.workloads layouts  # DOS recursion per sparse layout (CSR, SELL-C-sigma, autotuned)
     python -m linqt_b200.workloads realisations  # 4 disorder seeds in one recursion vs 4 separate solves
+    python -m linqt_b200.workloads cubic_full    # cubic L=200 (N=8e6), 4 seeds x 64 vectors, M=4096 (full size)
 
 Each line gives the device time per solve (CUDA events on the session stream, warm-up
 first), Chebyshev steps*nnz/s, the recursion's algorithmic bytes per second, and for the
@@ -155,13 +156,63 @@ def run_realisations(L, S, Rs, M, reps):
     return out
 
 
+def run_cubic_full(L, S, Rs, M, mode=0):
+    """Large DOS batching at full size: cubic Anderson L^3, S disorder seeds x Rs vectors in one
+    persistent recursion (stacked realisations), FP64 and mixed.  The states come from the device
+    generator (S*Rs*N complex values would be 33 GB on the host at L = 200).  Each precision is
+    warmed up with a short solve (allocations, module loads, the stacked-or-separate choice of
+    opts.realisations = mode) and then timed once."""
+    import time
+    import torch
+    from .core import moments1d_realisations_dev, random_phase_states_dev
+    sess = Session()
+    sess.set_stream(torch.cuda.current_stream())
+    ops = []
+    t0 = time.time()
+    for r in range(S):
+        N, H = lattices.cubic_lattice(L, 1.0, 2.0, 41 + r)
+        Hg = Operator.from_csr(N, *H, session=sess)
+        Hg.rescale_to_chebyshev(2 * 1.05 * 7.0, 0.0)
+        ops.append(Hg)
+        del H
+    setup_s = time.time() - t0
+    R = S * Rs
+    st = torch.empty(2 * R * N, dtype=torch.float64, device="cuda")
+    random_phase_states_dev(N, R, 45, st, session=sess)
+    nnz = ops[0].nnz
+    steps = (M + 1) // 2  # recursion steps with the doubling identities
+    out = {"workload": "dos_cubic_%d_%dseeds_x_%d" % (L, S, Rs), "N": N, "nnz_full": nnz, "R_total": R,
+           "M": M, "realisations": ["autotuned", "stacked", "separate"][mode], "host_setup_s": round(setup_s, 1)}
+    mus = {}
+    for label, prec, esz in (("fp64", PREC_FP64, 16), ("mixed", PREC_MIXED, 8)):
+        o = make_opts(precision=prec, realisations=mode)
+        mu = torch.zeros(2 * S * M, dtype=torch.float64, device="cuda")
+        moments1d_realisations_dev(ops, st, R, 64, mu, opts=o, session=sess)  # warm-up
+        torch.cuda.synchronize()
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record()
+        moments1d_realisations_dev(ops, st, R, M, mu, opts=o, session=sess)
+        b.record()
+        torch.cuda.synchronize()
+        ms = a.elapsed_time(b)
+        bytes_step = S * (nnz * (16 + 4) + 4 * (N + 1)) + 3 * esz * N * R
+        gbs = steps * bytes_step / (ms * 1e-3) / 1e9
+        mus[label] = mu.cpu().numpy().view(np.complex128).reshape(S, M)
+        out[label] = {"ms_per_solve": ms, "steps_nnz_per_s": M * R * nnz / (ms * 1e-3),
+                      "recursion_GBps": gbs, "hbm_frac_of_measured_6549": gbs / 6549.1}
+    e = np.abs(mus["mixed"] - mus["fp64"]).max(axis=1) / np.abs(mus["fp64"]).max(axis=1)
+    out["mixed"]["err_mu_vs_fp64_per_seed"] = [float(x) for x in e]
+    return out
+
+
 def main(argv=None):
     ap = argparse.ArgumentParser()
-    ap.add_argument("workload", choices=["dos", "cubic", "spin", "layouts", "realisations"])
+    ap.add_argument("workload", choices=["dos", "cubic", "cubic_full", "spin", "layouts", "realisations"])
     ap.add_argument("--reps", type=int, default=5)
     ap.add_argument("--cells", type=int, default=64, help="spin: Kane-Mele cells per side")
     ap.add_argument("--moments", type=int, default=512, help="spin: M")
     ap.add_argument("--vectors", type=int, default=8, help="spin: R")
+    ap.add_argument("--realisations", type=int, default=0, help="cubic_full: 0 autotuned, 1 stacked, 2 separate")
     a = ap.parse_args(argv)
     if a.workload == "dos":
         N, H = lattices.square_lattice(256, 1.0, 1.0, 11)
@@ -169,6 +220,8 @@ def main(argv=None):
     elif a.workload == "cubic":
         N, H = lattices.cubic_lattice(100, 1.0, 2.0, 41)
         r = run_1d("dos_cubic_100_seed41", N, H, 64, 1024, a.reps, 45)
+    elif a.workload == "cubic_full":
+        r = run_cubic_full(200, 4, 64, 4096, a.realisations)
     elif a.workload == "realisations":
         rs = [run_realisations(100, 4, 64, 1024, a.reps), run_realisations(40, 4, 8, 1024, a.reps)]
         for r in rs:

@@ -144,14 +144,25 @@ def test_disorder_realisations_in_one_block(oracle_lib, S, Rs):
         ops_g.append(Hg)
         ops_o.append(oracle_lib.Op(*H).rescale(2 / bw, -bc / (bw / 2)))
         states.append(lattices.random_phase_states(N, Rs, seed=100 + r))
-    mu = lq.moments1d_realisations(ops_g, np.concatenate(states), M)
+    mu = lq.moments1d_realisations(ops_g, np.concatenate(states), M, opts=lq.make_opts(realisations=1))
     assert mu.shape == (S, M)
+    for mode in (0, 2):  # autotuned, one solve per realisation
+        other = lq.moments1d_realisations(ops_g, np.concatenate(states), M, opts=lq.make_opts(realisations=mode))
+        assert rel(other, mu) < 1e-12
     for r in range(S):
         alone = lq.moments1d(ops_g[r], None, states[r], M)
         assert rel(mu[r], alone) < 1e-12
         assert rel(mu[r], oracle_lib.moments1d(ops_o[r], None, states[r], M)) < TOL
     mx = lq.moments1d_realisations(ops_g, np.concatenate(states), M, opts=lq.make_opts(precision=lq.PREC_MIXED))
     assert rel(mx, mu) < 1e-5
+
+
+def test_disorder_realisations_reject_unknown_mode():
+    N, H = lattices.cubic_lattice(6, seed=41)
+    a = lq.Operator.from_csr(N, *H)
+    with pytest.raises(lq.LinqtError) as e:
+        lq.moments1d_realisations([a, a], np.ones((2, N)), 16, opts=lq.make_opts(realisations=3))
+    assert "realisations" in str(e.value)
 
 
 def test_disorder_realisations_reject_mismatched_patterns():
