@@ -68,7 +68,10 @@ typedef struct linqt_opts {
   int precision;    /* LINQT_PREC_* */
   int format;       /* sparse layout of H in the persistent recursions: LINQT_FORMAT_CSR (default),
                        LINQT_FORMAT_SELL (SELL-C-sigma, C = 32, sigma = 8C) or LINQT_FORMAT_AUTO
-                       (autotuned among CSR and SELL with C = 8, 32; cached per operator) */
+                       (autotuned among CSR with and without its shared-memory row cache and SELL
+                       with C = 8, 32, times the thread shapes of the block (threads per row
+                       min(R, 32) >> s, s = 0..3), and for 1D moments without a fixed block_width
+                       the block width (R, R/2, R/4, R/8); cached per operator, width and precision) */
   int block_width;  /* vector columns per recursion block (0 = all R, or the autotuned chunk) */
   int doubling;     /* 1D: 0 = doubling identities when the operator is the identity, 1 = force them, 2 = direct <r|T_n r> */
   int use_graphs;   /* 1: *_dev solves replay an instantiated CUDA graph from the second call with the same

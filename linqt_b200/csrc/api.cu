@@ -407,48 +407,58 @@ static void with_graph(Session *s, const linqt_opts &o, const std::string &key, 
 }
 
 // ---------------------------------------------------------------------------
-// Sparse layout of a persistent recursion.  LINQT_FORMAT_CSR: the operator's CSR (whose
-// per-CTA row slices the kernels keep in shared memory when they fit); LINQT_FORMAT_SELL:
-// SELL-C-sigma with C = 32; LINQT_FORMAT_AUTO: the autotuner times a short run of the same
-// recursion (trial(C) with C = 0 for CSR, else the slice height) for CSR and SELL with
-// C in {8, 32}, keeps the fastest per operator pair, block width and precision, and returns
-// it.  Each candidate runs once untimed (building its layout) and once timed.
+// Sparse layout and thread shape of a persistent recursion.  LINQT_FORMAT_CSR: the
+// operator's CSR (whose per-CTA row slices the kernels keep in shared memory when they fit),
+// thread shape 0; LINQT_FORMAT_SELL: SELL-C-sigma with C = 32, shape 0; LINQT_FORMAT_AUTO:
+// the autotuner times a short run of the same recursion (trial(C, shape)) for every layout
+// (CSR cached, CSR uncached, SELL with C = 8 and 32) and thread shape, keeps the fastest per
+// operator pair, block width and precision, and returns it.  Each candidate runs once
+// untimed (building its layout) and once timed.
 // ---------------------------------------------------------------------------
-static int pick_layout(Session *s, const DeviceOp &H, const std::string &key, int format,
-                       const std::function<void(int)> &trial) {
-  if (format == LINQT_FORMAT_CSR) return 0;
-  if (format == LINQT_FORMAT_SELL) return 32;
+struct RecCfg {
+  int sellC = 0, shape = 0;
+};
+
+static RecCfg pick_layout(Session *s, const DeviceOp &H, const std::string &key, int format, int Rc,
+                          const std::function<void(int, int)> &trial, float *best_ms = nullptr) {
+  if (best_ms) *best_ms = -1;
+  if (format == LINQT_FORMAT_CSR) return RecCfg{0, 0};
+  if (format == LINQT_FORMAT_SELL) return RecCfg{32, 0};
   DeviceOp &Hm = const_cast<DeviceOp &>(H);
   {
     std::lock_guard<std::mutex> g(Hm.mu);
     auto it = Hm.tuned.find(key);
-    if (it != Hm.tuned.end()) return it->second;
+    if (it != Hm.tuned.end()) return RecCfg{it->second / 16 - 1, it->second % 16};
   }
   cudaEvent_t a, b;
   LQ_CUDA(cudaEventCreate(&a));
   LQ_CUDA(cudaEventCreate(&b));
   float best = 0;
-  int bestC = 0;
+  RecCfg pick;
+  bool first = true;
   // 0: CSR, its row slices cached in shared memory when they fit; -1: CSR without the
   // cache (more resident CTAs per SM); 8, 32: SELL-C-sigma
-  for (int C : {0, -1, 8, 32}) {
-    trial(C);
-    LQ_CUDA(cudaEventRecord(a, s->stream));
-    trial(C);
-    LQ_CUDA(cudaEventRecord(b, s->stream));
-    LQ_CUDA(cudaEventSynchronize(b));
-    float ms = 0;
-    LQ_CUDA(cudaEventElapsedTime(&ms, a, b));
-    if (C == 0 || ms < best) {
-      best = ms;
-      bestC = C;
+  for (int C : {0, -1, 8, 32})
+    for (int sh = 0; sh < recur_shapes(Rc); ++sh) {
+      trial(C, sh);
+      LQ_CUDA(cudaEventRecord(a, s->stream));
+      trial(C, sh);
+      LQ_CUDA(cudaEventRecord(b, s->stream));
+      LQ_CUDA(cudaEventSynchronize(b));
+      float ms = 0;
+      LQ_CUDA(cudaEventElapsedTime(&ms, a, b));
+      if (first || ms < best) {
+        best = ms;
+        pick = RecCfg{C, sh};
+        first = false;
+      }
     }
-  }
   cudaEventDestroy(a);
   cudaEventDestroy(b);
+  if (best_ms) *best_ms = best;
   std::lock_guard<std::mutex> g(Hm.mu);
-  Hm.tuned[key] = bestC;
-  return bestC;
+  Hm.tuned[key] = (pick.sellC + 1) * 16 + pick.shape;
+  return pick;
 }
 
 static std::string layout_key(const char *kind, const DeviceOp *V, int Rc, bool fp32) {
@@ -469,31 +479,68 @@ static void moments1d_dev(Session *s, const DeviceOp &H, const DeviceOp *op, con
   LQ_REQUIRE(!(doubling && op), "moments1d: the doubling identities need the identity operator");
   int Rc = o.block_width > 0 ? o.block_width : std::min(256, pow2_at_least(R));
   Rc = std::min(256, pow2_at_least(Rc));
-  const int nchunks = (R + Rc - 1) / Rc;
   const int steps = doubling ? (M + 1) / 2 : M;
   const size_t esz = fp32 ? sizeof(float2) : sizeof(double2);
-  const size_t blk = esz * (size_t)N * Rc;
-  char *T = (char *)s->get("m1_T", 3 * blk);
-  double2 *dots = (double2 *)s->get("m1_dots", sizeof(double2) * 2 * (size_t)steps * nchunks);
+  char *T = (char *)s->get("m1_T", 3 * esz * (size_t)N * Rc);
   PhaseScope ph(s, PH_RECURSION);
   long launches = 0;
-  int sellC = 0;
-  if (!o.step_launches)
-    sellC = pick_layout(s, H, layout_key("1d", op, Rc, fp32), o.format, [&](int C) {
-      // a short recursion on the first chunk (the real run below starts from scratch)
-      const int Mt = std::min(M, 32), st = doubling ? (Mt + 1) / 2 : Mt;
-      void *b0 = T, *b1 = T + blk, *b2 = T + 2 * blk;
-      chunk_block(s, states, N, R, 0, Rc, b2, fp32);
-      void *x0 = b2;
-      if (!doubling) {
-        if (op)
-          spmm(s, *op, make_double2(1, 0), b2, make_double2(0, 0), b0, Rc, fp32);
-        else
-          LQ_CUDA(cudaMemcpyAsync(b0, b2, blk, cudaMemcpyDeviceToDevice, s->stream));
-        x0 = b0;
+  // layout and thread shape for block width w, from short trials on the first w vectors
+  auto tune = [&](int w, float *best_ms) {
+    const size_t bw = esz * (size_t)N * w;
+    const int Mt = std::min(M, 32), st = doubling ? (Mt + 1) / 2 : Mt;
+    double2 *tdots = (double2 *)s->get("m1_trial_dots", sizeof(double2) * 2 * (size_t)st);
+    return pick_layout(
+        s, H, layout_key("1d", op, w, fp32), o.format, w,
+        [&](int C, int shape) {
+          // a short recursion on the first chunk (the real run below starts from scratch)
+          void *b0 = T, *b1 = T + bw, *b2 = T + 2 * bw;
+          chunk_block(s, states, N, R, 0, w, b2, fp32);
+          void *x0 = b2;
+          if (!doubling) {
+            if (op)
+              spmm(s, *op, make_double2(1, 0), b2, make_double2(0, 0), b0, w, fp32);
+            else
+              LQ_CUDA(cudaMemcpyAsync(b0, b2, bw, cudaMemcpyDeviceToDevice, s->stream));
+            x0 = b0;
+          }
+          recur_1d(s, H, b2, x0, b1, st, Mt, doubling ? 2 : 1, w, fp32, tdots, C, shape);
+        },
+        best_ms);
+  };
+  // LINQT_FORMAT_AUTO without a fixed block width: also the block width, among Rc, Rc/2, Rc/4
+  // and Rc/8, by trial time per vector (a narrower block streams fewer bytes per row, which
+  // can keep a large lattice's neighbour rows in L2), cached per operator pair, R and precision
+  if (o.format == LINQT_FORMAT_AUTO && o.block_width <= 0 && !o.step_launches && Rc > 1) {
+    DeviceOp &Hm = const_cast<DeviceOp &>(H);
+    const std::string wkey = "1dw:" + std::to_string(R) + ":" + layout_key("", op, Rc, fp32) + (doubling ? ":d" : "");
+    int w = 0;
+    {
+      std::lock_guard<std::mutex> g(Hm.mu);
+      auto it = Hm.tuned.find(wkey);
+      if (it != Hm.tuned.end()) w = it->second;
+    }
+    if (!w) {
+      float best = 0;
+      for (int c = Rc; c >= std::max(1, Rc / 8); c /= 2) {
+        float ms = -1;
+        tune(c, &ms);
+        if (ms < 0) continue;  // tuned before at this width (another R): keep the widest so far
+        if (!w || ms / c < 0.97f * best) {
+          best = ms / c;
+          w = c;
+        }
       }
-      recur_1d(s, H, b2, x0, b1, st, Mt, doubling ? 2 : 1, Rc, fp32, dots, C);
-    });
+      if (!w) w = Rc;
+      std::lock_guard<std::mutex> g(Hm.mu);
+      Hm.tuned[wkey] = w;
+    }
+    Rc = w;
+  }
+  const int nchunks = (R + Rc - 1) / Rc;
+  const size_t blk = esz * (size_t)N * Rc;
+  double2 *dots = (double2 *)s->get("m1_dots", sizeof(double2) * 2 * (size_t)steps * nchunks);
+  RecCfg cfg;
+  if (!o.step_launches) cfg = tune(Rc, nullptr);
   LQ_CUDA(cudaMemsetAsync(dots, 0, sizeof(double2) * 2 * (size_t)steps * nchunks, s->stream));
   for (int c = 0; c < nchunks; ++c) {
     void *b0 = T, *b1 = T + blk, *b2 = T + 2 * blk;
@@ -512,7 +559,7 @@ static void moments1d_dev(Session *s, const DeviceOp &H, const DeviceOp *op, con
         }
         x0 = b0;
       }
-      recur_1d(s, H, phi, x0, b1, steps, M, doubling ? 2 : 1, Rc, fp32, cd, sellC);
+      recur_1d(s, H, phi, x0, b1, steps, M, doubling ? 2 : 1, Rc, fp32, cd, cfg.sellC, cfg.shape);
       launches += 2;
       continue;
     }
@@ -590,7 +637,7 @@ static void realisations_stacked(Session *s, const DeviceOp *const *Hs, int S, c
     PhaseScope ph(s, PH_RECURSION);
     chunk_block(s, states, N, R, 0, R, phi, fp32);
     LQ_CUDA(cudaMemcpyAsync(b0, phi, blk, cudaMemcpyDeviceToDevice, s->stream));
-    recur_1d(s, H0, phi, b0, b1, steps, M, 2, R, fp32, dots, 0, vals, S);
+    recur_1d(s, H0, phi, b0, b1, steps, M, 2, R, fp32, dots, 0, 0, vals, S);
     ph.launches(3);
   }
   PhaseScope p3(s, PH_OTHER);
@@ -690,12 +737,12 @@ static long lr_vectors(Session *s, const DeviceOp &H, const DeviceOp *opl, const
         LQ_CUDA(cudaMemcpyAsync(Lstore, phi, blk, cudaMemcpyDeviceToDevice, s->stream));
       if (!opr) LQ_CUDA(cudaMemcpyAsync(Rstore, phi, blk, cudaMemcpyDeviceToDevice, s->stream));
     };
-    const int sellC = pick_layout(s, H, layout_key("lr", opr, Rc, fp32), format, [&](int C) {
+    const RecCfg cfg = pick_layout(s, H, layout_key("lr", opr, Rc, fp32), format, Rc, [&](int C, int shape) {
       start();
-      recur_lr(s, H, opr, Lstore, Rstore, phi, tmp3, std::min(M, 16), Rc, fp32, C);
+      recur_lr(s, H, opr, Lstore, Rstore, phi, tmp3, std::min(M, 16), Rc, fp32, C, shape);
     });
     start();
-    recur_lr(s, H, opr, Lstore, Rstore, phi, tmp3, M, Rc, fp32, sellC);
+    recur_lr(s, H, opr, Lstore, Rstore, phi, tmp3, M, Rc, fp32, cfg.sellC, cfg.shape);
     return opl ? 2 : 1;
   }
   // ---- L side: the recursion runs in place inside the store

@@ -289,14 +289,17 @@ void moments1d_from_dots_stream(cudaStream_t st, const double2 *dots, int steps,
                                 double2 *mu);
 
 // persistent recursions (recur.cu): one cooperative launch per recursion
-// sellC = 0: the operator's CSR; sellC > 0: its SELL-C-sigma layout with slice height sellC
+// sellC = 0: the operator's CSR (row slices cached in shared memory when they fit); -1: CSR
+// without the cache; sellC > 0: its SELL-C-sigma layout with slice height sellC.
+// shape < recur_shapes(R): thread shape (shape s: min(R, 32) >> s threads per row)
+int recur_shapes(int R);
 void recur_lr(Session *s, const DeviceOp &H, const DeviceOp *V, void *Lstore, void *Rstore, const void *phi,
-              void *tbuf, int M, int R, bool fp32, int sellC);
+              void *tbuf, int M, int R, bool fp32, int sellC, int shape = 0);
 // stacked != NULL: nreal realisations sharing H's pattern, values [nreal][nnz]; realisation r
 // owns columns [r R/nreal, (r+1) R/nreal), served by its own group of CTAs, and dots becomes
 // [nreal][steps][2]
 void recur_1d(Session *s, const DeviceOp &H, const void *phi, void *x0, void *b1, int steps, int M, int mode, int R,
-              bool fp32, double2 *dots, int sellC, const void *stacked = nullptr, int nreal = 1);
+              bool fp32, double2 *dots, int sellC, int shape = 0, const void *stacked = nullptr, int nreal = 1);
 // after a stream synchronisation: fail with LINQT_ERR_TIMEOUT if a persistent kernel's barrier gave up
 void check_device_errors(Session *s);
 

@@ -535,20 +535,27 @@ struct OneDF {
   }
 };
 
+// Thread shape of a block of R columns: TPR threads per row, VPT = R / TPR columns per
+// thread.  Shape 0 has TPR = min(R, 32); shape s halves TPR s times (VPT <= 8), so a warp
+// serves 2^s times more rows at once with 2^s times more loads in flight per thread.
 template <class T, template <class, int, int> class F, class... Args>
-void dispatch(int R, Args &&...args) {
-  switch (R) {
-    case 1: return F<T, 1, 1>::run(args...);
-    case 2: return F<T, 2, 1>::run(args...);
-    case 4: return F<T, 4, 1>::run(args...);
-    case 8: return F<T, 8, 1>::run(args...);
-    case 16: return F<T, 16, 1>::run(args...);
-    case 32: return F<T, 32, 1>::run(args...);
-    case 64: return F<T, 32, 2>::run(args...);
-    case 128: return F<T, 32, 4>::run(args...);
-    case 256: return F<T, 32, 8>::run(args...);
-    default: fail(LINQT_ERR_UNSUPPORTED, "block width must be a power of two <= 256");
+void dispatch(int R, int shape, Args &&...args) {
+#define LQ_SHAPE(r, s, tpr, vpt) \
+  case (r) * 8 + (s): return F<T, tpr, vpt>::run(args...);
+  switch (R * 8 + shape) {
+    LQ_SHAPE(1, 0, 1, 1)
+    LQ_SHAPE(2, 0, 2, 1) LQ_SHAPE(2, 1, 1, 2)
+    LQ_SHAPE(4, 0, 4, 1) LQ_SHAPE(4, 1, 2, 2) LQ_SHAPE(4, 2, 1, 4)
+    LQ_SHAPE(8, 0, 8, 1) LQ_SHAPE(8, 1, 4, 2) LQ_SHAPE(8, 2, 2, 4) LQ_SHAPE(8, 3, 1, 8)
+    LQ_SHAPE(16, 0, 16, 1) LQ_SHAPE(16, 1, 8, 2) LQ_SHAPE(16, 2, 4, 4) LQ_SHAPE(16, 3, 2, 8)
+    LQ_SHAPE(32, 0, 32, 1) LQ_SHAPE(32, 1, 16, 2) LQ_SHAPE(32, 2, 8, 4) LQ_SHAPE(32, 3, 4, 8)
+    LQ_SHAPE(64, 0, 32, 2) LQ_SHAPE(64, 1, 16, 4) LQ_SHAPE(64, 2, 8, 8)
+    LQ_SHAPE(128, 0, 32, 4) LQ_SHAPE(128, 1, 16, 8)
+    LQ_SHAPE(256, 0, 32, 8)
+    default: fail(LINQT_ERR_UNSUPPORTED, "block width must be a power of two <= 256 (thread shape " +
+                                             std::to_string(shape) + ")");
   }
+#undef LQ_SHAPE
 }
 
 // The barrier's count/generation restart at zero for every launch; its error flag is
@@ -562,25 +569,37 @@ Barrier *barrier_for(Session *s) {
 
 }  // namespace
 
+int recur_shapes(int R) {
+  switch (R) {
+    case 1: return 1;
+    case 2: return 2;
+    case 4: return 3;
+    case 8: case 16: case 32: return 4;
+    case 64: return 3;
+    case 128: return 2;
+    default: return 1;
+  }
+}
+
 void recur_lr(Session *s, const DeviceOp &H, const DeviceOp *V, void *Lstore, void *Rstore, const void *phi,
-              void *tbuf, int M, int R, bool fp32, int sellC) {
+              void *tbuf, int M, int R, bool fp32, int sellC, int shape) {
   const size_t blk = (size_t)H.n * R;
   Barrier *bar = barrier_for(s);
   if (fp32)
-    dispatch<float, LRF>(R, s, H, V, Lstore, Rstore, phi, tbuf, M, blk, bar, sellC);
+    dispatch<float, LRF>(R, shape, s, H, V, Lstore, Rstore, phi, tbuf, M, blk, bar, sellC);
   else
-    dispatch<double, LRF>(R, s, H, V, Lstore, Rstore, phi, tbuf, M, blk, bar, sellC);
+    dispatch<double, LRF>(R, shape, s, H, V, Lstore, Rstore, phi, tbuf, M, blk, bar, sellC);
   LQ_LAUNCHED();
 }
 
 void recur_1d(Session *s, const DeviceOp &H, const void *phi, void *x0, void *b1, int steps, int M, int mode, int R,
-              bool fp32, double2 *dots, int sellC, const void *stacked, int nreal) {
+              bool fp32, double2 *dots, int sellC, int shape, const void *stacked, int nreal) {
   Barrier *bar = barrier_for(s);
   const int Rw = stacked ? R / nreal : R;  // columns per CTA
   if (fp32)
-    dispatch<float, OneDF>(Rw, s, H, phi, x0, b1, steps, M, mode, dots, bar, sellC, stacked, nreal);
+    dispatch<float, OneDF>(Rw, shape, s, H, phi, x0, b1, steps, M, mode, dots, bar, sellC, stacked, nreal);
   else
-    dispatch<double, OneDF>(Rw, s, H, phi, x0, b1, steps, M, mode, dots, bar, sellC, stacked, nreal);
+    dispatch<double, OneDF>(Rw, shape, s, H, phi, x0, b1, steps, M, mode, dots, bar, sellC, stacked, nreal);
 }
 
 void check_device_errors(Session *s) {
