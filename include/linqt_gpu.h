@@ -51,9 +51,16 @@ enum {
 enum { LINQT_STORAGE_HERMITIAN_UPPER = 0, LINQT_STORAGE_GENERAL = 1 };
 
 enum {
-  LINQT_PREC_FP64 = 0,  /* FP64 recursion, FP64 moment contraction */
-  LINQT_PREC_MIXED = 1, /* FP32 recursion, split-TF32 tensor-core contraction, FP64 accumulation */
-  LINQT_PREC_FP32 = 2   /* FP32 recursion, FP32 contraction (diagnostic) */
+  LINQT_PREC_FP64 = 0,       /* FP64 recursion, FP64 moment contraction */
+  LINQT_PREC_MIXED = 1,      /* FP32 Chebyshev vectors (FP64 operators and accumulation in the recursion),
+                                moment contraction on the INT8 tensor cores from 4-digit (28-bit) splits
+                                of the FP32 blocks with exact INT32 accumulation, FP64 across chunks */
+  LINQT_PREC_FP32 = 2,       /* FP32 vectors, FP64 MMA contraction of the FP32 blocks (diagnostic) */
+  LINQT_PREC_MIXED_TF32 = 3, /* FP32 vectors, 3xTF32 tensor-core contraction with FP32 accumulation over
+                                2048-float chunks (the split-precision form; its truncating FP32
+                                accumulation costs about 4e-5 of max|mu|) */
+  LINQT_PREC_MIXED_FAST = 4  /* as LINQT_PREC_MIXED with 3-digit (21-bit) splits: 6 instead of 10 INT8
+                                products, ~1e-7 of max|mu| */
 };
 
 enum { LINQT_KUBO_GREENWOOD = 0, LINQT_KUBO_BASTIN = 1 }; /* chebyshev::formula, include/Kubo_solver_FFT.hpp:17-21 */

@@ -18,7 +18,7 @@ import numpy as np
 
 from ._lib import Opts, check, load
 
-PREC_FP64, PREC_MIXED, PREC_FP32 = 0, 1, 2
+PREC_FP64, PREC_MIXED, PREC_FP32, PREC_MIXED_TF32, PREC_MIXED_FAST = 0, 1, 2, 3, 4
 KUBO_GREENWOOD, KUBO_BASTIN = 0, 1
 STORAGE_HERMITIAN_UPPER, STORAGE_GENERAL = 0, 1
 

@@ -802,8 +802,12 @@ struct Chunking {
   int Rc, nchunks;
 };
 
-// pick the vector-chunk width so that 2 stores of M*N*Rc + buffers fit in memory
-static Chunking pick_chunks(Session *s, int N, int R, int M, size_t esz, const linqt_opts &o, size_t extra) {
+// pick the vector-chunk width so that 2 stores of M*N*Rc + buffers fit in memory, with the
+// digit planes of the INT8 contraction (`digits` per value: 3 digits per float on the L side
+// and 6 on the R side per digit, i.e. 3 * digits bytes per complex entry of each store)
+static Chunking pick_chunks(Session *s, int N, int R, int M, size_t esz, const linqt_opts &o, size_t extra,
+                            int digits = 0) {
+  esz += 3 * (size_t)digits;
   int Rc = o.block_width > 0 ? pow2_at_least(o.block_width) : pow2_at_least(R);
   Rc = std::min(Rc, 256);
   size_t avail;
@@ -831,8 +835,7 @@ static Chunking pick_chunks(Session *s, int N, int R, int M, size_t esz, const l
 
 // Whether the vector blocks are FP32 (the operators stay FP64 in every mode).
 static bool prepare_precision(const linqt_opts &o, const DeviceOp &, const DeviceOp *, const DeviceOp *) {
-  LQ_REQUIRE(o.precision == LINQT_PREC_FP64 || o.precision == LINQT_PREC_MIXED || o.precision == LINQT_PREC_FP32,
-             "unknown precision");
+  LQ_REQUIRE(o.precision >= LINQT_PREC_FP64 && o.precision <= LINQT_PREC_MIXED_FAST, "unknown precision");
   return o.precision != LINQT_PREC_FP64;
 }
 
@@ -846,7 +849,7 @@ static void moments2d_dev(Session *s, const DeviceOp &H, const DeviceOp *opl, co
   const bool fp32 = prepare_precision(o, H, opl, opr);
   const int N = H.n;
   const size_t esz = fp32 ? sizeof(float2) : sizeof(double2);
-  const Chunking ch = pick_chunks(s, N, R, M, esz, o, sizeof(double2) * (size_t)M * M * 66);
+  const Chunking ch = pick_chunks(s, N, R, M, esz, o, sizeof(double2) * (size_t)M * M * 66, i8_digits(o.precision));
   const size_t blk = esz * (size_t)N * ch.Rc;
   char *Ls = (char *)s->get("lr_L", blk * M);
   char *Rs = (char *)s->get("lr_R", blk * M);
@@ -909,7 +912,7 @@ static void kubo_solve(Session *s, const DeviceOp &H, const DeviceOp *opl, const
   size_t extra = 0;
   if (mu) extra += sizeof(double2) * (size_t)M * M * 66;
   if (out) extra += sizeof(double2) * 2 * (size_t)std::max(nump, 1) * 1024;
-  const Chunking ch = pick_chunks(s, N, R, M, esz, o, extra);
+  const Chunking ch = pick_chunks(s, N, R, M, esz, o, extra, mu ? i8_digits(o.precision) : 0);
   const size_t blk = esz * (size_t)N * ch.Rc;
   char *Ls = (char *)s->get("lr_L", blk * M);
   char *Rs = (char *)s->get("lr_R", blk * M);

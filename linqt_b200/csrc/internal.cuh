@@ -252,6 +252,12 @@ void random_phase_states(Session *s, int N, int R, unsigned long long seed, doub
 bool mu_tc_supported(long K);
 void mu_contract_tc(Session *s, const void *L, const void *Rv, int M, long K, double2 *mu_raw);
 int mu_tc_check_error(Session *s);
+// tcgen05 INT8 contraction of FP32 Chebyshev blocks split into 3 or 4 digits, exact accumulation (mu_i8.cu)
+void mu_contract_i8(Session *s, const void *L, const void *Rv, int M, long K, int digits, double2 *mu_raw);
+// digits per value of the INT8 contraction a precision mode uses (0: none)
+inline int i8_digits(int precision) {
+  return precision == LINQT_PREC_MIXED ? 4 : precision == LINQT_PREC_MIXED_FAST ? 3 : 0;
+}
 
 // FFT path: accumulate p/w over all sites into acc[2*nump] (complex)
 // prefactors pf_m of Kubo_solver_FFT (kubo_fft.cu)

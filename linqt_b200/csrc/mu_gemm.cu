@@ -248,7 +248,9 @@ void mu_contract(Session *s, const void *L, const void *Rv, int M, long K, bool 
                  double2 *mu_raw) {
   if (!fp32_inputs) {
     zgemm_cn_t<double2>(s, (const double2 *)L, M, (const double2 *)Rv, M, K, mu_raw, true);
-  } else if (precision == LINQT_PREC_MIXED && mu_tc_supported(K)) {
+  } else if (i8_digits(precision)) {
+    mu_contract_i8(s, L, Rv, M, K, i8_digits(precision), mu_raw);  // tcgen05 INT8 digits, exact sums (mu_i8.cu)
+  } else if (precision == LINQT_PREC_MIXED_TF32 && mu_tc_supported(K)) {
     mu_contract_tc(s, L, Rv, M, K, mu_raw);  // tcgen05 3xTF32 (mu_tc.cu)
   } else {
     zgemm_cn_t<float2>(s, (const float2 *)L, M, (const float2 *)Rv, M, K, mu_raw, true);  // FP64 MMA on FP32 data

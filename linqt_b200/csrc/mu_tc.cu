@@ -28,10 +28,13 @@
 #include <cstdint>
 
 #include "internal.cuh"
+#include "tc_common.cuh"
 
 namespace linqt {
 
 namespace {
+
+using namespace tc;
 
 constexpr int TC_BM = 128;           // output rows (m0) per CTA
 constexpr int TC_BN = 128;           // output columns (m1) per CTA; MMA N = 2 * TC_BN
@@ -42,7 +45,6 @@ constexpr int TILE = 128 * TC_BK * 4;  // 16 KB: 128 rows x 128 B
 constexpr int OFF_AHI = 0, OFF_ALO = TILE, OFF_BHI = 2 * TILE, OFF_BLO = 4 * TILE;
 constexpr int STAGE_BYTES = 6 * TILE;
 constexpr int TMEM_COLS = 256;
-constexpr long kWaitLimit = 1L << 22;
 
 struct TcShared {
   alignas(1024) uint8_t stage[TC_STAGES][STAGE_BYTES];
@@ -50,61 +52,6 @@ struct TcShared {
   uint32_t tmem_base;
   int abort;
 };
-
-__device__ __forceinline__ uint32_t smem_u32(const void *p) { return (uint32_t)__cvta_generic_to_shared(p); }
-
-__device__ __forceinline__ void mbar_init(unsigned long long *b, uint32_t count) {
-  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;\n" ::"r"(smem_u32(b)), "r"(count));
-}
-__device__ __forceinline__ void mbar_arrive_expect_tx(unsigned long long *b, uint32_t bytes) {
-  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;\n" ::"r"(smem_u32(b)), "r"(bytes)
-               : "memory");
-}
-__device__ __forceinline__ void mbar_arrive(unsigned long long *b) {
-  asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];\n" ::"r"(smem_u32(b)) : "memory");
-}
-__device__ __forceinline__ bool mbar_try_wait(unsigned long long *b, uint32_t parity) {
-  uint32_t done;
-  asm volatile(
-      "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}\n"
-      : "=r"(done)
-      : "r"(smem_u32(b)), "r"(parity)
-      : "memory");
-  return done != 0;
-}
-// bounded wait; false (and the error flag raised) if the phase never completed
-__device__ __forceinline__ bool mbar_wait(unsigned long long *b, uint32_t parity, int *err) {
-  for (long i = 0; i < kWaitLimit; ++i)
-    if (mbar_try_wait(b, parity)) return true;
-  atomicExch(err, 1);
-  return false;
-}
-
-__device__ __forceinline__ void tma_load_2d(void *dst, const CUtensorMap *map, int x, int y,
-                                            unsigned long long *bar) {
-  asm volatile(
-      "cp.async.bulk.tensor.2d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%3, %4}], [%2];\n" ::"r"(
-          smem_u32(dst)),
-      "l"(map), "r"(smem_u32(bar)), "r"(x), "r"(y)
-      : "memory");
-}
-
-__device__ __forceinline__ void fence_proxy_async() { asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory"); }
-__device__ __forceinline__ void tc_fence_before() { asm volatile("tcgen05.fence::before_thread_sync;\n" ::: "memory"); }
-__device__ __forceinline__ void tc_fence_after() { asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory"); }
-
-// K-major operand tile, 128-byte swizzle: 8-row groups 1024 B apart (SBO), LBO unused (1),
-// descriptor version 1, layout type 2 (SWIZZLE_128B).
-__device__ __forceinline__ uint64_t smem_desc_sw128(const void *p) {
-  const uint64_t addr = smem_u32(p);
-  uint64_t d = 0;
-  d |= (addr >> 4) & 0x3FFFull;          // start address, bits [0,14)
-  d |= (uint64_t)1 << 16;                // leading byte offset (unused for swizzled K-major)
-  d |= (uint64_t)(1024 >> 4) << 32;      // stride byte offset, bits [32,46)
-  d |= (uint64_t)1 << 46;                // version = 1
-  d |= (uint64_t)2 << 61;                // SWIZZLE_128B
-  return d;
-}
 
 // instruction descriptor: D F32, A/B TF32, both K-major, N = 256, M = 128
 constexpr uint32_t kIdesc = (1u << 4) | (2u << 7) | (2u << 10) | ((uint32_t)(2 * TC_BN >> 3) << 17) |
@@ -118,25 +65,7 @@ __device__ __forceinline__ void umma_tf32(uint32_t tmem_d, uint64_t adesc, uint6
       "l"(adesc), "l"(bdesc), "r"(kIdesc), "r"(accumulate), "r"(z), "r"(z), "r"(z), "r"(z));
 }
 
-__device__ __forceinline__ void umma_commit(unsigned long long *bar) {
-  asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];\n" ::"r"(smem_u32(bar))
-               : "memory");
-}
-
 __device__ __forceinline__ float tf32_hi(float x) { return __uint_as_float(__float_as_uint(x) & 0xFFFFE000u); }
-
-// 16 consecutive FP32 accumulator columns of this thread's TMEM lane
-__device__ __forceinline__ void tmem_ld16(uint32_t taddr, float (&v)[16]) {
-  uint32_t r[16];
-  asm volatile(
-      "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15}, [%16];\n"
-      : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]), "=r"(r[8]),
-        "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15])
-      : "r"(taddr));
-  asm volatile("tcgen05.wait::ld.sync.aligned;\n" ::: "memory");
-#pragma unroll
-  for (int i = 0; i < 16; ++i) v[i] = __uint_as_float(r[i]);
-}
 
 __global__ void __launch_bounds__(192, 1)
     k_mu_tf32x3(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUtensorMap tmB, int M0, int M1,
@@ -284,26 +213,6 @@ __global__ void __launch_bounds__(192, 1)
     tc_fence_after();
     asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;\n" ::"r"(tmem), "r"(TMEM_COLS));
   }
-}
-
-// ---------------------------------------------------------------------------
-// host side: tensor maps through the driver entry point (the runtime is linked
-// statically; cuTensorMapEncodeTiled lives in the driver)
-// ---------------------------------------------------------------------------
-typedef CUresult (*EncodeTiledFn)(CUtensorMap *, CUtensorMapDataType, cuuint32_t, void *, const cuuint64_t *,
-                                  const cuuint64_t *, const cuuint32_t *, const cuuint32_t *, CUtensorMapInterleave,
-                                  CUtensorMapSwizzle, CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
-
-EncodeTiledFn encode_fn() {
-  static EncodeTiledFn fn = nullptr;
-  if (!fn) {
-    void *p = nullptr;
-    cudaDriverEntryPointQueryResult q;
-    LQ_CUDA(cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q));
-    if (q != cudaDriverEntryPointSuccess || !p) fail(LINQT_ERR_CUDA, "cuTensorMapEncodeTiled is not available");
-    fn = (EncodeTiledFn)p;
-  }
-  return fn;
 }
 
 // rows x kf floats, row-major (kf contiguous); box 32 floats x 128 rows, 128-byte swizzle

@@ -59,7 +59,9 @@ size_t estimate_footprint(const linqt_request &r, int n, int sm_count, int Rc) {
     return io + esz * (size_t)n * Rc * 3 +
            sizeof(double2) * (2 * steps * ((size_t)sm_count * 32 + 1) + 2 * steps * chunks) + (1 << 20);
   }
-  return io + esz * (size_t)n * Rc * (2 * (size_t)r.M + 4) + sizeof(double2) * (size_t)r.M * r.M * 66 + (1 << 20);
+  const size_t digits = 6 * (size_t)i8_digits(r.precision) * n * Rc * r.M;  // INT8 contraction planes
+  return io + esz * (size_t)n * Rc * (2 * (size_t)r.M + 4) + digits + sizeof(double2) * (size_t)r.M * r.M * 66 +
+         (1 << 20);
 }
 
 // Vector-block width of a request: the widest power of two up to R whose footprint fits in
