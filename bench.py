@@ -398,12 +398,13 @@ def main():
                  "phases_ms": {k: round(v / args.steps, 4) for k, v in zip(("recursion", "contraction", "fft", "other"),
                                                                            o_phase)},
                  "err_mu_vs_fp64": err_mu, "err_sigma_vs_fp64_interior90": err_sigma,
-                 "dtype": "f32 recursion + 3xTF32 tcgen05 contraction (FP32 TMEM accumulation over 2048-float "
-                          "chunks, FP64 across chunks) + FP64 FFT" if name == "mixed" else "f64"}
-        # tensor-pipe view of the tcgen05 contraction: 3 split products x real GEMM (2M x M x 4K flops)
+                 "dtype": "f32 recursion vectors (f64 operators and accumulation) + tcgen05 INT8 contraction of "
+                          "4-digit splits with exact INT32 accumulation, FP64 across chunks + FP64 FFT"
+                          if name == "mixed" else "f64"}
+        # tensor-pipe view of the tcgen05 contraction: 10 digit products x real GEMM (2M x M x 2K MACs)
         if name == "mixed" and o_phase[1] > 0:
-            tc_flops = 3 * 2.0 * (2 * M) * M * (2 * K)
-            other["contraction_tf32_tflops"] = tc_flops / (o_phase[1] / args.steps * 1e-3) / 1e12
+            tc_ops = 10 * 2.0 * (2 * M) * M * (2 * K)
+            other["contraction_int8_tops"] = tc_ops / (o_phase[1] / args.steps * 1e-3) / 1e12
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
@@ -419,7 +420,7 @@ def main():
                    nnz_full=nnz, N=N)
         line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
                 "warmup": args.warmup, "ms_per_step": dev_ms, "higher_is_better": True, "scaling": "weak",
-                "vs_baseline": None, "dtype": "f64" if prec == lq.PREC_FP64 else "f32+tf32x3",
+                "vs_baseline": None, "dtype": "f64" if prec == lq.PREC_FP64 else "f32+int8x4",
                 "data": "synthetic (seeded lattice, random-phase states)", "config": cfg,
                 "e2e": {"value": e2e, "unit": UNIT, "ms_per_step": e2e_ms,
                         "h2d_bytes_per_step": int(st.nbytes), "d2h_bytes_per_step": int(16 * M * M + 16 * nump)},
