@@ -203,7 +203,7 @@ def run_cubic_full(L, S, Rs, M, mode=0):
            "M": M, "realisations": ["autotuned", "stacked", "separate"][mode], "host_setup_s": round(setup_s, 1)}
     mus = {}
     for label, prec, esz in (("fp64", PREC_FP64, 16), ("mixed", PREC_MIXED, 8)):
-        o = make_opts(precision=prec, realisations=mode)
+        o = make_opts(precision=prec, fmt=2, realisations=mode)
         mu = torch.zeros(2 * S * M, dtype=torch.float64, device="cuda")
         moments1d_realisations_dev(ops, st, R, 64, mu, opts=o, session=sess)  # warm-up
         torch.cuda.synchronize()
