@@ -34,6 +34,8 @@
 // flag, stops issuing, drains what it issued, frees TMEM and returns.  No TMA multicast.
 #include <cuda.h>
 
+#include <cooperative_groups.h>
+
 #include <cstdint>
 
 #include "internal.cuh"
@@ -44,6 +46,7 @@ namespace linqt {
 namespace {
 
 using namespace tc;
+namespace cg = cooperative_groups;
 
 constexpr int I8_BM = 128;         // A rows (m0) per CTA
 constexpr int I8_BN = 64;          // complex output columns (m1) per CTA
@@ -252,35 +255,71 @@ __device__ __forceinline__ uint32_t pack4(int a, int b, int c, int d) {
 // Digit planes of both sides: z = 0 the L side (ND planes), z = 1 the R side (ND planes of b,
 // then ND of b'' = (Bi, -Br)).  src: rows of kf floats; dig: [planes][rows][kfp] int8 (K
 // padded with zeros to kfp); expo[row][chunk]: the exponent e with max |x| over the chunk
-// < 2^e.  Grid (nchunk, rows, 2), 256 threads: a pass for the maximum, then one for the
-// digits (its reads mostly hit L2).
+// < 2^e.  Grid (4 nchunk, rows, 2) in clusters of 4 CTAs: each CTA stages a quarter of a
+// (row, chunk) in shared memory (kchunk / 4 floats, up to 64 KB), the cluster exchanges the
+// quarter maxima through distributed shared memory, and the digits are written from the
+// staged copy, so every value is read from HBM once.
+constexpr int kDigitCluster = 4;
+
 template <int ND>
-__global__ void __launch_bounds__(256)
+__global__ void __cluster_dims__(kDigitCluster, 1, 1) __launch_bounds__(256)
     k_digits(const float *__restrict__ srcA, const float *__restrict__ srcB, long kf, long kfp, long kchunk,
              int rows, int nchunk, int8_t *__restrict__ digA, int8_t *__restrict__ digB, int *__restrict__ expA,
              int *__restrict__ expB) {
+  extern __shared__ float4 stage_q[];
   __shared__ float red[8];
+  __shared__ float qmax;
+  cg::cluster_group cl = cg::this_cluster();
   const bool b_side = blockIdx.z == 1;
-  const int row = blockIdx.y, c = blockIdx.x;
-  const long k0 = (long)c * kchunk, k1 = min(kfp, k0 + kchunk), kd = min(k1, kf);
+  const int row = blockIdx.y, c = blockIdx.x / kDigitCluster, quarter = blockIdx.x % kDigitCluster;
+  const long q = kchunk / kDigitCluster;  // a multiple of 32 floats
+  const long k0 = (long)c * kchunk + quarter * q, k1 = min(kfp, k0 + q), kd = min(k1, kf);
   const float *x = (b_side ? srcB : srcA) + (size_t)row * kf;
+  // stage this quarter (kf is even: a pair (k, k+1) is all in or all out of [k0, kd))
   float mx = 0.f;
-  for (long k = k0 + threadIdx.x; k < kd; k += blockDim.x) mx = fmaxf(mx, fabsf(x[k]));
+  const int nquad = (int)max(0L, (k1 - k0) / 4);
+  for (int i = threadIdx.x; i < nquad; i += blockDim.x) {
+    const long k = k0 + 4L * i;
+    float4 t = make_float4(0.f, 0.f, 0.f, 0.f);
+    if (k < kd) {
+      const float2 p = *reinterpret_cast<const float2 *>(x + k);
+      t.x = p.x;
+      t.y = p.y;
+      if (k + 2 < kd) {
+        const float2 r = *reinterpret_cast<const float2 *>(x + k + 2);
+        t.z = r.x;
+        t.w = r.y;
+      }
+    }
+    stage_q[i] = t;
+    mx = fmaxf(mx, fmaxf(fmaxf(fabsf(t.x), fabsf(t.y)), fmaxf(fabsf(t.z), fabsf(t.w))));
+  }
   for (int o = 16; o > 0; o >>= 1) mx = fmaxf(mx, __shfl_xor_sync(0xffffffffu, mx, o));
   if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = mx;
   __syncthreads();
+  if (threadIdx.x == 0) {
+    float m = 0.f;
+    for (int w = 0; w < 8; ++w) m = fmaxf(m, red[w]);
+    qmax = m;
+  }
+  cl.sync();  // every quarter's maximum is written
   mx = 0.f;
 #pragma unroll
-  for (int w = 0; w < 8; ++w) mx = fmaxf(mx, red[w]);
+  for (int r = 0; r < kDigitCluster; ++r) mx = fmaxf(mx, *cl.map_shared_rank(&qmax, r));
+  cl.sync();  // no CTA leaves while another may still read its maximum
   int e = 0;
   if (mx > 0.f) (void)frexpf(mx, &e);  // mx = f 2^e, f in [0.5, 1): every |x| < 2^e
-  if (threadIdx.x == 0) (b_side ? expB : expA)[(size_t)row * nchunk + c] = e;
+  if (threadIdx.x == 0 && quarter == 0) (b_side ? expB : expA)[(size_t)row * nchunk + c] = e;
   const size_t plane = (size_t)rows * kfp;
   int8_t *drow = (b_side ? digB : digA) + (size_t)row * kfp;
-  for (long k = k0 + 4 * (long)threadIdx.x; k < k1; k += 4 * (long)blockDim.x) {
+  for (int i = threadIdx.x; i < nquad; i += blockDim.x) {
+    const long k = k0 + 4L * i;
+    const float4 t = stage_q[i];
     int d[4][ND];
-#pragma unroll
-    for (int i = 0; i < 4; ++i) digits<ND>(k + i < kd ? ldexpf(x[k + i], 6 - e) : 0.f, d[i]);
+    digits<ND>(ldexpf(t.x, 6 - e), d[0]);
+    digits<ND>(ldexpf(t.y, 6 - e), d[1]);
+    digits<ND>(ldexpf(t.z, 6 - e), d[2]);
+    digits<ND>(ldexpf(t.w, 6 - e), d[3]);
 #pragma unroll
     for (int p = 0; p < ND; ++p) {
       *reinterpret_cast<uint32_t *>(drow + p * plane + k) = pack4(d[0][p], d[1][p], d[2][p], d[3][p]);
@@ -339,8 +378,10 @@ void contract_i8(Session *s, const void *L, const void *Rv, int M, long K, doubl
   double2 *part = (double2 *)s->get("mu_i8_parts", sizeof(double2) * (size_t)S * M * M);
   int *err = (int *)s->get("mu_tc_err_barrier", sizeof(int) * 4);  // read by mu_tc_check_error
   s->barrier_used = true;
-  k_digits<ND><<<dim3(nchunk, M, 2), 256, 0, s->stream>>>((const float *)L, (const float *)Rv, kf, kfp, kchunk, M,
-                                                           nchunk, dA, dB, eA, eB);
+  const size_t qsmem = sizeof(float) * (size_t)(kchunk / kDigitCluster);
+  LQ_CUDA(cudaFuncSetAttribute(k_digits<ND>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)qsmem));
+  k_digits<ND><<<dim3(kDigitCluster * nchunk, M, 2), 256, qsmem, s->stream>>>(
+      (const float *)L, (const float *)Rv, kf, kfp, kchunk, M, nchunk, dA, dB, eA, eB);
   LQ_LAUNCHED();
   const CUtensorMap ta = make_map_i8(dA, M, kfp, ND, I8_BM, Cfg::BK),
                     tb = make_map_i8(dB, M, kfp, 2 * ND, I8_BN, Cfg::BK);
