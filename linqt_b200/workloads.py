@@ -8,6 +8,9 @@ Kubo-Bastin graphene workload:
     python -m linqt_b200.workloads layouts  # DOS recursion per sparse layout (CSR, SELL-C-sigma, autotuned)
     python -m linqt_b200.workloads realisations  # 4 disorder seeds in one recursion vs 4 separate solves
     python -m linqt_b200.workloads cubic_full    # cubic L=200 (N=8e6), 4 seeds x 64 vectors, M=4096 (full size)
+    python -m linqt_b200.workloads lr_layouts    # L/R recursion of the 2D moments: CSR vs autotuned
+    python -m linqt_b200.workloads cubic_width   # cubic L=200 DOS recursion GB/s: CSR vs autotuned, R = 64, 8
+    python -m linqt_b200.workloads moments2d --cells 32 --moments 1024 --vectors 32   # one profiled 2D solve
 
 Each line gives the device time per solve (CUDA events on the session stream, warm-up
 first), Chebyshev steps*nnz/s, the recursion's algorithmic bytes per second, and for the
@@ -223,9 +226,84 @@ def run_cubic_full(L, S, Rs, M, mode=0):
     return out
 
 
+def run_lr_layouts(name, N, H, V, R, M, reps):
+    """Recursion phase of the 2D moments (L and R recursions with V fused) per precision,
+    the operator's CSR (shape 0) against the autotuned layout / thread shape."""
+    import torch
+    from .core import moments2d_dev
+    sess, bw, bc, Hg, (Vg,) = _ops(N, H, [V])
+    st = torch.from_numpy(lattices.random_phase_states(N, R, seed=32).view(np.float64).copy()).cuda()
+    mu = torch.zeros(2 * M * M, dtype=torch.float64, device="cuda")
+    out = {"workload": "lr_" + name, "N": N, "R": R, "M": M}
+    for lab, prec in (("fp64", PREC_FP64), ("mixed", PREC_MIXED)):
+        for fl, fmt in (("csr", 0), ("auto", 2)):
+            o = make_opts(precision=prec, fmt=fmt)
+            f = lambda: moments2d_dev(Hg, Vg, Vg, st, R, M, mu, opts=o, session=sess)
+            f()
+            f()
+            torch.cuda.synchronize()
+            sess.enable_timing(True)
+            sess.phase_times(reset=True)
+            for _ in range(reps):
+                f()
+            torch.cuda.synchronize()
+            ph, _ = sess.phase_times(reset=True)
+            sess.enable_timing(False)
+            out[lab + "_" + fl + "_recursion_ms"] = ph[0] / reps
+    return out
+
+
+def run_cubic_width(L, R, M, reps):
+    """1D recursion on a large cubic lattice: algorithmic GB/s with the operator's CSR and
+    with the autotuned layout, thread shape and block width."""
+    import torch
+    from .core import random_phase_states_dev
+    N, H = lattices.cubic_lattice(L, 1.0, 2.0, 41)
+    sess = Session()
+    sess.set_stream(torch.cuda.current_stream())
+    Hg = Operator.from_csr(N, *H, session=sess)
+    Hg.rescale_to_chebyshev(2 * 1.05 * 7.0, 0.0)
+    del H
+    st = torch.empty(2 * R * N, dtype=torch.float64, device="cuda")
+    random_phase_states_dev(N, R, 45, st, session=sess)
+    mu = torch.zeros(2 * M, dtype=torch.float64, device="cuda")
+    out = {"workload": "dos_cubic_%d" % L, "N": N, "R": R, "M": M}
+    for lab, prec, esz in (("fp64", PREC_FP64, 16), ("mixed", PREC_MIXED, 8)):
+        for fl, fmt in (("csr", 0), ("auto", 2)):
+            o = make_opts(precision=prec, fmt=fmt)
+            ms = _timed(lambda: moments1d_dev(Hg, None, st, R, M, mu, opts=o, session=sess), reps, torch)
+            by = Hg.nnz * 20 + 4 * (N + 1) + 3 * esz * N * R
+            out[lab + "_" + fl + "_GBps"] = (M + 1) // 2 * by / (ms * 1e-3) / 1e9
+    return out
+
+
+def run_moments2d_once(Lc, R, M, prec):
+    """One warm-up and one timed Kane-Mele spin 2D-moment solve with per-phase times (the
+    case the contraction kernels are profiled on)."""
+    import torch
+    from .core import moments2d_dev
+    N, H, J = lattices.kane_mele(Lc, Lc, seed=31)
+    sess, bw, bc, Hg, (Jg,) = _ops(N, H, [J])
+    st = torch.from_numpy(lattices.random_phase_states(N, R, seed=32).view(np.float64).copy()).cuda()
+    mu = torch.zeros(2 * M * M, dtype=torch.float64, device="cuda")
+    o = make_opts(precision=prec)
+    f = lambda: moments2d_dev(Hg, Jg, Jg, st, R, M, mu, opts=o, session=sess)
+    f()
+    torch.cuda.synchronize()
+    sess.enable_timing(True)
+    sess.phase_times(reset=True)
+    f()
+    torch.cuda.synchronize()
+    ph, ln = sess.phase_times(reset=True)
+    return {"workload": "moments2d_kane_mele_%dx%d" % (Lc, Lc), "N": N, "R": R, "M": M, "precision": prec,
+            "phases_ms": ph, "launches": ln}
+
+
 def main(argv=None):
     ap = argparse.ArgumentParser()
-    ap.add_argument("workload", choices=["dos", "cubic", "cubic_full", "spin", "layouts", "realisations"])
+    ap.add_argument("workload", choices=["dos", "cubic", "cubic_full", "spin", "layouts", "realisations",
+                                         "lr_layouts", "cubic_width", "moments2d"])
+    ap.add_argument("--precision", type=int, default=PREC_MIXED, help="moments2d: LINQT_PREC_* value")
     ap.add_argument("--reps", type=int, default=5)
     ap.add_argument("--cells", type=int, default=64, help="spin: Kane-Mele cells per side")
     ap.add_argument("--moments", type=int, default=512, help="spin: M")
@@ -238,6 +316,16 @@ def main(argv=None):
     elif a.workload == "cubic":
         N, H = lattices.cubic_lattice(100, 1.0, 2.0, 41)
         r = run_1d("dos_cubic_100_seed41", N, H, 64, 1024, a.reps, 45)
+    elif a.workload == "lr_layouts":
+        N, H, J = lattices.kane_mele(64, 64, seed=31)
+        print(json.dumps(run_lr_layouts("kane_mele_64", N, H, J, 32, 1024, a.reps)))
+        N, H, V = lattices.honeycomb(128, 128, t=-2.7, W=1.0, seed=21)
+        r = run_lr_layouts("graphene_128", N, H, V, 8, 512, a.reps)
+    elif a.workload == "cubic_width":
+        print(json.dumps(run_cubic_width(200, 64, 64, a.reps)))
+        r = run_cubic_width(200, 8, 64, a.reps)
+    elif a.workload == "moments2d":
+        r = run_moments2d_once(a.cells, a.vectors, a.moments, a.precision)
     elif a.workload == "cubic_full":
         r = run_cubic_full(200, 4, 64, 4096, a.realisations)
     elif a.workload == "realisations":
