@@ -74,6 +74,29 @@ def read_chebmom2d(path):
     return n, bw, bc, (v[0::2] + 1j * v[1::2]).reshape(m0, m1)
 
 
+def write_chebmomtd(path, system_size, band_width, band_center, dt, mu):
+    """MomentsTD::saveIn (src/chebyshev_momentsTD.cpp:86-99): header `N bw bc NT dt`, then
+    `M NT`, then mu(m, n) row-major, one `re im` per line, 15 digits."""
+    mu = np.asarray(mu, dtype=np.complex128)
+    m, nt = mu.shape
+    with open(path, "w") as f:
+        f.write("%d %s %s %d %s \n" % (system_size, _g(band_width), _g(band_center), nt, _g(dt)))
+        f.write("%d %d \n" % (m, nt))
+        for z in mu.reshape(-1):
+            f.write("%s %s\n" % (_g(z.real), _g(z.imag)))
+
+
+def read_chebmomtd(path):
+    """(N, band_width, band_center, dt, mu[M, NT]) of a .chebmomTD file."""
+    if ".chebmomTD" not in path:
+        raise ValueError("not a .chebmomTD file: %s" % path)
+    tok = open(path).read().split()
+    n, bw, bc, nt, dt = int(tok[0]), float(tok[1]), float(tok[2]), int(tok[3]), float(tok[4])
+    m, nt2 = int(tok[5]), int(tok[6])
+    v = np.array(tok[7:7 + 2 * m * nt2], dtype=np.float64)
+    return n, bw, bc, dt, (v[0::2] + 1j * v[1::2]).reshape(m, nt2)
+
+
 def write_vector_states(path, states):
     st = np.atleast_2d(np.asarray(states, dtype=np.complex128))
     R, N = st.shape

@@ -217,6 +217,84 @@ int lo_moments1d(const lo_op *H, const lo_op *op, const double *states, int R, i
   return 0;
 }
 
+/* chebyshev::besselJ (src/special_functions.cpp:3-17): libm's j0 / j1 / jn. */
+static double bessel_j(int n, double x) { return n == 0 ? j0(x) : n == 1 ? j1(x) : jn(n, x); }
+
+/* MomentsTD::Evolve (src/chebyshev_momentsTD.cpp:4-46): Phi <- exp(-i w0 dt) *
+ * sum_n c_n (-i)^n J_n(x) T_n(H) Phi, x = dt * w, c_0 = 1, c_n = 2; the series stops before
+ * the first n whose |J_n(x)| <= 1e-10.  T0/T1 are scratch. */
+static void evolve(const lo_op *H, cplx *phi, cplx *T0, cplx *T1, double x, cplx exp0) {
+  const int n = H->n;
+  const double tol = 1e-10;
+  memcpy(T0, phi, sizeof(cplx) * (size_t)n);
+  op_mv(H, 1.0, T0, 0.0, T1);
+  int k = 0;
+  cplx nIp = 1.0;
+  double Jn = 0.5 * bessel_j(k, x);
+  double cut = 2.0 * tol;
+  memset(phi, 0, sizeof(cplx) * (size_t)n);
+  while (cut > tol) {
+    const cplx c = nIp * 2.0 * Jn;
+    for (int i = 0; i < n; i++) phi[i] += c * T0[i];
+    op_mv(H, 2.0, T1, -1.0, T0);
+    cplx *t = T0;
+    T0 = T1;
+    T1 = t;
+    nIp *= -I;
+    k++;
+    Jn = bessel_j(k, x);
+    cut = fabs(Jn);
+  }
+  for (int i = 0; i < n; i++) phi[i] *= exp0;
+}
+
+/* chebyshev::TimeDependentCorrelations (src/chebyshev_solver.cpp:231-275): per state,
+ * PhiL = OPL Phi, PhiR = Phi; for each time step n: mu(m, n) += (2/R)(1/2)^[m=0]
+ * <PhiL|T_m(H) OPR PhiR>, then both vectors evolve by dt.  mu_out: M x NT complex,
+ * row-major (MomentsTD::operator(), include/chebyshev_moments.hpp:346-351).
+ * w = (band_width / 2) / hbar, w0 = band_center / hbar (ChebyshevFreq / ChebyshevFreq_0,
+ * include/chebyshev_moments.hpp:290-326, hbar = 0.6582119624 eV fs). */
+int lo_moments_td(const lo_op *H, const lo_op *opl, const lo_op *opr, const double *states, int R, int M, int NT,
+                  double dt, double band_width, double band_center, double *mu_out) {
+  if (!H || R <= 0 || M <= 0 || NT <= 0) return -1;
+  const int n = H->n;
+  const double hbar = 0.6582119624;
+  const double x = dt * (0.5 * band_width) / hbar;
+  const cplx exp0 = cexp(-I * (band_center / hbar) * dt);
+  cplx *mu = calloc((size_t)M * NT, sizeof(cplx));
+  cplx *pl = malloc(sizeof(cplx) * (size_t)n), *pr = malloc(sizeof(cplx) * (size_t)n);
+  cplx *a = malloc(sizeof(cplx) * (size_t)n), *b = malloc(sizeof(cplx) * (size_t)n);
+  for (int r = 0; r < R; r++) {
+    memcpy(pr, (const cplx *)states + (long)r * n, sizeof(cplx) * (size_t)n);
+    if (opl)
+      op_mv(opl, 1.0, pr, 0.0, pl);
+    else
+      memcpy(pl, pr, sizeof(cplx) * (size_t)n);
+    for (int t = 0; t < NT; t++) {
+      cplx *T0 = a, *T1 = b;
+      set_init_vectors(H, opr, pr, T0, T1);
+      for (int m = 0; m < M; m++) {
+        double scal = 2.0 / R;
+        if (m == 0) scal *= 0.5;
+        mu[(size_t)m * NT + t] += scal * vdot(n, pl, T0);
+        iterate(H, &T0, &T1);
+      }
+      evolve(H, pl, a, b, x, exp0);
+      evolve(H, pr, a, b, x, exp0);
+    }
+  }
+  for (size_t q = 0; q < (size_t)M * NT; q++) {
+    mu_out[2 * q] = creal(mu[q]);
+    mu_out[2 * q + 1] = cimag(mu[q]);
+  }
+  free(a);
+  free(b);
+  free(pl);
+  free(pr);
+  free(mu);
+  return 0;
+}
+
 /* Vectors::IterateAll (src/chebyshev_vectors.cpp:4-21): store T_0..T_{M-1}. */
 static void iterate_all(const lo_op *H, cplx *T0, cplx *T1, cplx *store, int M) {
   const int n = H->n;

@@ -50,6 +50,8 @@ def lib():
         L.lo_op_export.argtypes = [vp, ip, ip, dp]
         L.lo_moments1d.argtypes = [vp, vp, dp, ctypes.c_int, ctypes.c_int, dp]
         L.lo_moments2d.argtypes = [vp, vp, vp, dp, ctypes.c_int, ctypes.c_int, dp]
+        L.lo_moments_td.argtypes = [vp, vp, vp, dp, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_double,
+                                    ctypes.c_double, ctypes.c_double, dp]
         L.lo_jackson1d.argtypes = [dp, ctypes.c_int, ctypes.c_double, ctypes.c_double]
         L.lo_jackson2d.argtypes = [dp, ctypes.c_int, ctypes.c_int, ctypes.c_double, ctypes.c_double,
                                    ctypes.c_double, ip, ip]
@@ -133,6 +135,18 @@ def moments1d(H, op, states, M):
     rc = lib().lo_moments1d(H.h, _h(op), _dp(st.view(np.float64)), R, M, _dp(mu.view(np.float64)))
     if rc:
         raise RuntimeError("lo_moments1d failed: %d" % rc)
+    return mu
+
+
+def moments_td(H, opl, opr, states, M, NT, dt, band_width, band_center):
+    """TimeDependentCorrelations: mu[m, n] (M x NT) for time steps n*dt."""
+    st = np.ascontiguousarray(states, dtype=np.complex128)
+    R = st.shape[0]
+    mu = np.zeros((M, NT), np.complex128)
+    rc = lib().lo_moments_td(H.h, _h(opl), _h(opr), _dp(st.view(np.float64)), R, M, NT, ctypes.c_double(dt),
+                             ctypes.c_double(band_width), ctypes.c_double(band_center), _dp(mu.view(np.float64)))
+    if rc:
+        raise RuntimeError("lo_moments_td failed: %d" % rc)
     return mu
 
 

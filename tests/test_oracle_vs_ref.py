@@ -142,3 +142,24 @@ def test_kubo_fft_operator_order_vs_ref(oracle_lib, tmp_path, formula):
     st = formats.read_state_file(os.path.join(d, "states.txt"))
     E, s, integ, _ = oracle_lib.kubo_fft(Ho, ops["VX"], ops["DG"], st, M, nump, formula, N, bw, bc)
     assert np.abs(s - ref[:, 1]).max() < 2e-6 * np.abs(s).max()
+
+
+def test_time_correlations_vs_ref(oracle_lib, tmp_path):
+    """TimeDependentCorrelations through the reference's own inline_compute-kpm-CorrOp
+    (its default state, a delta at N/2, with OPL != OPR) against the C restatement."""
+    N, d, ops, (bw, bc) = _graphene_with_diagonal(tmp_path, oracle_lib, 1, 3)
+    M, NT, tmax = 32, 5, 10.0
+    exe = os.path.join(os.path.dirname(__file__), "..", "oracle", "_ref", "inline_compute-kpm-CorrOp")
+    subprocess.run([exe, "gr", "VX", "DG", str(M), str(NT), str(tmax)], cwd=d, check=True, capture_output=True,
+                   timeout=600)
+    n, bw_f, bc_f, dt, mu_ref = formats.read_chebmomtd(os.path.join(d, "TimeCorrVX-DGgrKPM_M%d_statedefault.chebmomTD"
+                                                                    % M))
+    assert n == N and mu_ref.shape == (M, NT) and abs(dt - tmax / (NT - 1)) < 1e-14
+    lo, hi = [float(x) for x in open(os.path.join(d, "BOUNDS")).read().split()]
+    bw, bc = hi - lo, (hi + lo) / 2
+    Ho = oracle_lib.Op(*formats.read_csr(os.path.join(d, "operators", "gr.HAM.CSR"))[1:])
+    Ho.rescale(2 / bw, -bc / (bw / 2))
+    delta = np.zeros((1, N), np.complex128)
+    delta[0, N // 2] = 1.0
+    mu = oracle_lib.moments_td(Ho, ops["VX"], ops["DG"], delta, M, NT, tmax / (NT - 1), bw, bc)
+    assert rel(mu, mu_ref) < 1e-12
