@@ -157,6 +157,21 @@ int linqt_moments1d_realisations(linqt_session *s, const linqt_op *const *H, int
 int linqt_moments1d_realisations_dev(linqt_session *s, const linqt_op *const *H, int S, const double *states_dev,
                                      int R, int M, const linqt_opts *opts, double *mu_dev);
 
+/* chebyshev::TimeDependentCorrelations (src/chebyshev_solver.cpp:231-275) with
+ * MomentsTD::Evolve (src/chebyshev_momentsTD.cpp:4-46): for each state, PhiL = OPL phi and
+ * PhiR = phi; at time step n (t = n dt, fs) mu[m*NT + n] += (2/R)(1/2)^{[m=0]}
+ * <PhiL|T_m(H) OPR PhiR>, then PhiL and PhiR evolve by exp(-i H dt / hbar), hbar =
+ * 0.6582119624 eV fs, as the series sum_k (2 - [k=0]) (-i)^k J_k(dt w) T_k(H), w =
+ * band_width / 2 / hbar, times exp(-i band_center dt / hbar), truncated before the first
+ * |J_k| <= 1e-10.  H must already be rescaled with band_width / band_center (eV).
+ * mu: 2*M*NT doubles (MomentsTD layout).  FP64 only.  opl/opr = NULL are identities. */
+int linqt_moments_td(linqt_session *s, const linqt_op *H, const linqt_op *opl, const linqt_op *opr,
+                     const double *states, int R, int M, int NT, double dt, double band_width, double band_center,
+                     const linqt_opts *opts, double *mu);
+int linqt_moments_td_dev(linqt_session *s, const linqt_op *H, const linqt_op *opl, const linqt_op *opr,
+                         const double *states_dev, int R, int M, int NT, double dt, double band_width,
+                         double band_center, const linqt_opts *opts, double *mu_dev);
+
 /* chebyshev::CorrelationExpansionMoments (src/chebyshev_solver.cpp:86-172) with the
  * default BATCH_SIZE: mu[2*M*M] row-major mu(mL, mR), symmetrised and scaled by
  * (4/R)(1/2)^{[mL=0]}(1/2)^{[mR=0]}.  opl/opr = NULL are identities. */

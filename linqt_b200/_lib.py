@@ -71,6 +71,10 @@ SIGNATURES = {
                                     c_void_p]),
     "linqt_moments2d": (c_int, [c_void_p, c_void_p, c_void_p, c_void_p, P_double, c_int, c_int,
                                 ctypes.POINTER(Opts), P_double]),
+    "linqt_moments_td": (c_int, [c_void_p, c_void_p, c_void_p, c_void_p, P_double, c_int, c_int, c_int, c_double,
+                                 c_double, c_double, ctypes.POINTER(Opts), P_double]),
+    "linqt_moments_td_dev": (c_int, [c_void_p, c_void_p, c_void_p, c_void_p, c_void_p, c_int, c_int, c_int,
+                                     c_double, c_double, c_double, ctypes.POINTER(Opts), c_void_p]),
     "linqt_moments2d_dev": (c_int, [c_void_p, c_void_p, c_void_p, c_void_p, c_void_p, c_int, c_int,
                                     ctypes.POINTER(Opts), c_void_p]),
     "linqt_kubo_fft": (c_int, [c_void_p, c_void_p, c_void_p, c_void_p, P_double, c_int, c_int, c_int, c_int,

@@ -257,6 +257,24 @@ def moments1d_noalloc(H, states_dev, R, M, mu_dev, stream=0):
                                          ctypes.c_void_p(stream)))
 
 
+def moments_td(H, opl, opr, states, M, NT, dt, band_width, band_center, opts=None, session=None):
+    """TimeDependentCorrelations: mu[m, n] (M x NT) at times n*dt (fs); H rescaled with
+    band_width / band_center (eV)."""
+    st = _c128(np.atleast_2d(states))
+    R = st.shape[0]
+    mu = np.zeros((M, NT), np.complex128)
+    o = opts or make_opts()
+    check(load().linqt_moments_td(_sh(session), H.h, _oph(opl), _oph(opr), _dp(st.view(np.float64)), R, M, NT, dt,
+                                  band_width, band_center, ctypes.byref(o), _dp(mu.view(np.float64))))
+    return mu
+
+
+def moments_td_dev(H, opl, opr, states_dev, R, M, NT, dt, band_width, band_center, mu_dev, opts=None, session=None):
+    o = opts or make_opts()
+    check(load().linqt_moments_td_dev(_sh(session), H.h, _oph(opl), _oph(opr), ctypes.c_void_p(_ptr(states_dev)), R, M,
+                                      NT, dt, band_width, band_center, ctypes.byref(o), ctypes.c_void_p(_ptr(mu_dev))))
+
+
 def moments2d(H, opl, opr, states, M, opts=None, session=None):
     """mu[M, M] of chebyshev::CorrelationExpansionMoments (row index follows OPL)."""
     st = np.atleast_2d(_c128(states))

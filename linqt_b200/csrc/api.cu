@@ -952,6 +952,83 @@ static void kubo_solve(Session *s, const DeviceOp &H, const DeviceOp *opl, const
   ph.launches((mu ? 1 : 0) + (out ? 1 : 0));
 }
 
+// ---------------------------------------------------------------------------
+// Time-domain correlations: chebyshev::TimeDependentCorrelations
+// (src/chebyshev_solver.cpp:231-275) with MomentsTD::Evolve (src/chebyshev_momentsTD.cpp:4-46).
+// Per block of states: PhiL = OPL Phi, PhiR = Phi; at time step n the 1D recursion from
+// T_0 = OPR PhiR gives mu(m, n) = (2/R)(1/2)^[m=0] sum_r <PhiL|T_m>; both blocks then evolve
+// by dt through one Chebyshev-Bessel series launch each.
+// ---------------------------------------------------------------------------
+// Coefficients of the evolution series: the reference's loop adds the terms n = 0, 1, ...
+// and stops before the first n with |J_n(x)| <= 1e-10; c_n = e^{-i w0 dt} (2 - [n=0]) (-i)^n J_n(x).
+static std::vector<double2> td_coefficients(double dt, double band_width, double band_center) {
+  const double hbar = 0.6582119624;  // eV fs (MomentsTD::HBAR)
+  const double x = dt * (0.5 * band_width) / hbar, w0dt = band_center / hbar * dt;
+  const double2 e0 = make_double2(std::cos(w0dt), -std::sin(w0dt));
+  auto J = [](int n, double z) { return n == 0 ? ::j0(z) : n == 1 ? ::j1(z) : ::jn(n, z); };
+  std::vector<double2> c;
+  double2 ip = make_double2(1, 0);  // (-i)^n
+  double jn = 0.5 * J(0, x);
+  for (int n = 0;; ++n) {
+    const double a = 2.0 * jn;
+    c.push_back(cmul(e0, make_double2(a * ip.x, a * ip.y)));
+    ip = make_double2(ip.y, -ip.x);
+    jn = J(n + 1, x);
+    LQ_REQUIRE(n < 100000, "time correlations: the evolution series does not converge");
+    if (!(std::fabs(jn) > 1e-10)) break;
+  }
+  return c;
+}
+
+static void moments_td_dev(Session *s, const DeviceOp &H, const DeviceOp *opl, const DeviceOp *opr,
+                           const double2 *states, int R, int M, int NT, double dt, double band_width,
+                           double band_center, const linqt_opts &o, double2 *mu) {
+  LQ_REQUIRE(R > 0 && M > 0 && NT > 0, "time correlations: R, M and NT must be positive");
+  LQ_REQUIRE((!opl || opl->n == H.n) && (!opr || opr->n == H.n), "time correlations: operator dimension mismatch");
+  LQ_REQUIRE(band_width > 0 && dt >= 0, "time correlations: band_width > 0 and dt >= 0");
+  LQ_REQUIRE(o.precision == LINQT_PREC_FP64, "time correlations: FP64 only");
+  const int N = H.n;
+  int Rc = o.block_width > 0 ? o.block_width : std::min(256, pow2_at_least(R));
+  Rc = std::min(256, pow2_at_least(Rc));
+  const int nchunks = (R + Rc - 1) / Rc;
+  const size_t blk = sizeof(double2) * (size_t)N * Rc;
+  char *W = (char *)s->get("td_blocks", 4 * blk);
+  void *PR = W, *PL = W + blk, *X0 = W + 2 * blk, *X1 = W + 3 * blk;
+  double2 *dots = (double2 *)s->get("td_dots", sizeof(double2) * 2 * (size_t)M * nchunks * NT);
+  const std::vector<double2> c = td_coefficients(dt, band_width, band_center);
+  double2 *coef = (double2 *)s->get("td_coef", sizeof(double2) * c.size());
+  LQ_CUDA(cudaMemcpyAsync(coef, c.data(), sizeof(double2) * c.size(), cudaMemcpyHostToDevice, s->stream));
+  const int sellC = o.format == LINQT_FORMAT_SELL ? 32 : 0;
+  {
+    PhaseScope ph(s, PH_RECURSION);
+    for (int ch = 0; ch < nchunks; ++ch) {
+      chunk_block(s, states, N, R, ch * Rc, Rc, PR, false);
+      if (opl)
+        spmm(s, *opl, make_double2(1, 0), PR, make_double2(0, 0), PL, Rc, false);
+      else
+        LQ_CUDA(cudaMemcpyAsync(PL, PR, blk, cudaMemcpyDeviceToDevice, s->stream));
+      for (int t = 0; t < NT; ++t) {
+        if (opr)
+          spmm(s, *opr, make_double2(1, 0), PR, make_double2(0, 0), X0, Rc, false);
+        else
+          LQ_CUDA(cudaMemcpyAsync(X0, PR, blk, cudaMemcpyDeviceToDevice, s->stream));
+        recur_1d(s, H, PL, X0, X1, M, M, 1, Rc, false, dots + ((size_t)t * nchunks + ch) * 2 * M, sellC);
+        if (t + 1 < NT) {  // the reference also evolves after the last step; nothing reads that
+          cheb_series(s, H, PL, X0, X1, coef, (int)c.size(), Rc);
+          cheb_series(s, H, PR, X0, X1, coef, (int)c.size(), Rc);
+        }
+      }
+    }
+    ph.launches((long)nchunks * (2 + (long)NT * 4));
+  }
+  PhaseScope p3(s, PH_OTHER);
+  for (int t = 0; t < NT; ++t) {
+    double2 *dt_dots = dots + (size_t)t * nchunks * 2 * M;
+    if (nchunks > 1) sum_chunks(s, dt_dots, 2 * M, nchunks);
+    moments1d_from_dots(s, dt_dots, M, M, R, 1, mu + t, NT);
+  }
+}
+
 static void kubo_fft_dev(Session *s, const DeviceOp &H, const DeviceOp *opl, const DeviceOp *opr,
                          const double2 *states, int R, int M, int nump, int formula, double bw, double bc,
                          const linqt_opts &o, double *out) {
@@ -1322,6 +1399,37 @@ int linqt_moments2d(linqt_session *s, const linqt_op *H, const linqt_op *opl, co
     double2 *d_mu = (double2 *)r->get("io_mu", mb);
     LQ_CUDA(cudaMemcpyAsync(d_st, states, sb, cudaMemcpyHostToDevice, r->stream));
     moments2d_dev(r, H->op, dop(opl), dop(opr), d_st, R, M, defaults(opts), d_mu);
+    LQ_CUDA(cudaMemcpyAsync(mu, d_mu, mb, cudaMemcpyDeviceToHost, r->stream));
+    LQ_CUDA(cudaStreamSynchronize(r->stream));
+    check_device_errors(r);
+  });
+}
+
+int linqt_moments_td_dev(linqt_session *s, const linqt_op *H, const linqt_op *opl, const linqt_op *opr,
+                         const double *states_dev, int R, int M, int NT, double dt, double band_width,
+                         double band_center, const linqt_opts *opts, double *mu_dev) {
+  return guarded([&] {
+    check_op(H, "H");
+    LQ_REQUIRE(states_dev && mu_dev, "NULL pointer");
+    moments_td_dev(resolve(s), H->op, dop(opl), dop(opr), (const double2 *)states_dev, R, M, NT, dt, band_width,
+                   band_center, defaults(opts), (double2 *)mu_dev);
+  });
+}
+
+int linqt_moments_td(linqt_session *s, const linqt_op *H, const linqt_op *opl, const linqt_op *opr,
+                     const double *states, int R, int M, int NT, double dt, double band_width, double band_center,
+                     const linqt_opts *opts, double *mu) {
+  return guarded([&] {
+    check_op(H, "H");
+    LQ_REQUIRE(states && mu, "NULL pointer");
+    LQ_REQUIRE(R > 0 && M > 0 && NT > 0, "time correlations: R, M and NT must be positive");
+    Session *r = resolve(s);
+    const int N = H->op.n;
+    const size_t sb = sizeof(double2) * (size_t)R * N, mb = sizeof(double2) * (size_t)M * NT;
+    double2 *d_st = (double2 *)r->get("td_io_states", sb);
+    double2 *d_mu = (double2 *)r->get("td_io_mu", mb);
+    LQ_CUDA(cudaMemcpyAsync(d_st, states, sb, cudaMemcpyHostToDevice, r->stream));
+    moments_td_dev(r, H->op, dop(opl), dop(opr), d_st, R, M, NT, dt, band_width, band_center, defaults(opts), d_mu);
     LQ_CUDA(cudaMemcpyAsync(mu, d_mu, mb, cudaMemcpyDeviceToHost, r->stream));
     LQ_CUDA(cudaStreamSynchronize(r->stream));
     check_device_errors(r);

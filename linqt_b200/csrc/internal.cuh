@@ -237,7 +237,8 @@ void cheb_step(Session *s, const DeviceOp &H, const StepArgs &a, int R, bool fp3
 void states_to_block(Session *s, const double2 *states, void *block, int N, int R, int Rpad, bool fp32);
 
 // 1D moments assembly from per-step dots
-void moments1d_from_dots(Session *s, const double2 *dots, int steps, int M, int R, int mode, double2 *mu);
+void moments1d_from_dots(Session *s, const double2 *dots, int steps, int M, int R, int mode, double2 *mu,
+                         long stride = 1);
 
 // mu_raw[M x M] += sum_k conj(L[m0][k]) * Rv[m1][k], FP64 (or FP32-input) operands
 // C(i,j) (+)= sum_k conj(A[i][k]) B[j][k], FP64
@@ -306,6 +307,9 @@ void recur_lr(Session *s, const DeviceOp &H, const DeviceOp *V, void *Lstore, vo
 // [nreal][steps][2]
 void recur_1d(Session *s, const DeviceOp &H, const void *phi, void *x0, void *b1, int steps, int M, int mode, int R,
               bool fp32, double2 *dots, int sellC, int shape = 0, const void *stacked = nullptr, int nreal = 1);
+// X <- sum_{s<K} coef[s] T_s(H) X on an FP64 block of R columns (a, b: scratch blocks), one
+// persistent launch (recur.cu)
+void cheb_series(Session *s, const DeviceOp &H, void *X, void *a, void *b, const double2 *coef, int K, int R);
 // after a stream synchronisation: fail with LINQT_ERR_TIMEOUT if a persistent kernel's barrier gave up
 void check_device_errors(Session *s);
 

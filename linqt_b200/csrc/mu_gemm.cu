@@ -189,7 +189,7 @@ __global__ void k_mu_finalize(const double2 *__restrict__ raw, int M, double R, 
 // src/chebyshev_solver.cpp:190-195: (2/R)(1/2)^{[m=0]}).
 // mode 1: dots[2m] = <phi|T_m>; mode 2: dots[2s] = <T_s|T_s>, dots[2s+1] = <T_{s+1}|T_s>.
 __global__ void k_moments1d(const double2 *__restrict__ dots, int steps, int M, double R, int mode,
-                            double2 *__restrict__ mu) {
+                            double2 *__restrict__ mu, long stride) {
   for (int m = blockIdx.x * blockDim.x + threadIdx.x; m < M; m += gridDim.x * blockDim.x) {
     double2 v;
     if (mode == 1) {
@@ -203,7 +203,7 @@ __global__ void k_moments1d(const double2 *__restrict__ dots, int steps, int M, 
     }
     double scal = 2.0 / R;
     if (m == 0) scal *= 0.5;
-    mu[m] = cscale(v, scal);
+    mu[(size_t)m * stride] = cscale(v, scal);
   }
 }
 
@@ -266,12 +266,13 @@ void mu_finalize(Session *s, const double2 *mu_raw, int M, int R, double2 *mu) {
 
 void moments1d_from_dots_stream(cudaStream_t st, const double2 *dots, int steps, int M, int R, int mode,
                                 double2 *mu) {
-  k_moments1d<<<(M + 255) / 256, 256, 0, st>>>(dots, steps, M, (double)R, mode, mu);
+  k_moments1d<<<(M + 255) / 256, 256, 0, st>>>(dots, steps, M, (double)R, mode, mu, 1);
   LQ_LAUNCHED();
 }
 
-void moments1d_from_dots(Session *s, const double2 *dots, int steps, int M, int R, int mode, double2 *mu) {
-  k_moments1d<<<(M + 255) / 256, 256, 0, s->stream>>>(dots, steps, M, (double)R, mode, mu);
+void moments1d_from_dots(Session *s, const double2 *dots, int steps, int M, int R, int mode, double2 *mu,
+                         long stride) {
+  k_moments1d<<<(M + 255) / 256, 256, 0, s->stream>>>(dots, steps, M, (double)R, mode, mu, stride);
   LQ_LAUNCHED();
 }
 

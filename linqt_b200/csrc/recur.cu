@@ -350,6 +350,73 @@ __global__ void __launch_bounds__(kThreads)
   }
 }
 
+// ---------------------------------------------------------------------------
+// Chebyshev series of H applied to a block (MomentsTD::Evolve, src/chebyshev_momentsTD.cpp:4-46):
+//   X <- sum_{s < K} coef[s] T_s(H) X
+// T_0 = X is copied to a, T_1 = H T_0 goes to b, then T_{s+1} = 2 H T_s - T_{s-1} in place
+// over T_{s-1}; X accumulates coef[s] T_s as each T_s is produced (FP64).
+// ---------------------------------------------------------------------------
+template <int TPR, int VPT>
+__global__ void __launch_bounds__(kThreads)
+    k_cheb_series(int n, const int *rp, const int *ci, const double2 *hv, double2 *X, double2 *a, double2 *b,
+                  const double2 *__restrict__ coef, int K, Barrier *bar, int cache) {
+  constexpr int RW = TPR * VPT;
+  const int lane = threadIdx.x % TPR;
+  constexpr int gpb = kThreads / TPR;
+  const int per = (n + gridDim.x - 1) / gridDim.x;
+  const int r0 = min(n, blockIdx.x * per), r1 = min(n, r0 + per);
+  if (cache) {
+    extern __shared__ __align__(16) unsigned char smc2[];
+    cache_rows<double2>(rp, ci, hv, r0, r1, smc2, rp, ci, hv);
+    __syncthreads();
+  }
+  const int rfirst = cache ? r0 : blockIdx.x * gpb, rend = cache ? r1 : n;  // as in k_recur_lr
+  const int rstep = cache ? gpb : gridDim.x * gpb;
+  const double2 c0 = coef[0];
+  for (int pos = rfirst + threadIdx.x / TPR; pos < rend; pos += rstep)
+#pragma unroll
+    for (int u = 0; u < VPT; ++u) {
+      const size_t idx = (size_t)pos * RW + lane + u * TPR;
+      const double2 x = X[idx];
+      a[idx] = x;
+      X[idx] = cmul(c0, x);
+    }
+  double2 *prev = nullptr, *cur = a;
+  for (int s = 1; s < K; ++s) {
+    if (!grid_barrier(bar, gridDim.x)) return;
+    double2 *y = prev ? prev : b;
+    const double2 cs = coef[s];
+    for (int pos = rfirst + threadIdx.x / TPR; pos < rend; pos += rstep) {
+      double2 acc[VPT];
+#pragma unroll
+      for (int u = 0; u < VPT; ++u) acc[u] = make_double2(0, 0);
+      const int kb = rp[pos], ke = rp[pos + 1];
+#pragma unroll 4
+      for (int k = kb; k < ke; ++k) {
+        const int j = ci[k];
+        const double2 h = hv[k];
+        const double2 *xr = cur + (size_t)j * RW + lane;
+#pragma unroll
+        for (int u = 0; u < VPT; ++u) acc[u] = cfma(h, ldv(xr + u * TPR), acc[u]);
+      }
+#pragma unroll
+      for (int u = 0; u < VPT; ++u) {
+        const size_t idx = (size_t)pos * RW + lane + u * TPR;
+        double2 yn = acc[u];
+        if (prev) {
+          const double2 p = ldv(prev + idx);
+          yn.x = 2 * yn.x - p.x;
+          yn.y = 2 * yn.y - p.y;
+        }
+        y[idx] = yn;
+        X[idx] = cadd(X[idx], cmul(cs, yn));  // X rows are this thread's own: no barrier needed
+      }
+    }
+    prev = cur;
+    cur = y;
+  }
+}
+
 // dots[2s + i] = sum_b partials[s][b][i]  (fixed order)
 __global__ void k_reduce_step_partials(const double2 *__restrict__ partials, int steps, int nb,
                                        double2 *__restrict__ dots) {
@@ -538,6 +605,22 @@ struct OneDF {
 // Thread shape of a block of R columns: TPR threads per row, VPT = R / TPR columns per
 // thread.  Shape 0 has TPR = min(R, 32); shape s halves TPR s times (VPT <= 8), so a warp
 // serves 2^s times more rows at once with 2^s times more loads in flight per thread.
+template <class T, int TPR, int VPT>
+struct SeriesF {
+  static void run(Session *s, const DeviceOp &H, void *X, void *a, void *b, const double2 *coef, int K, Barrier *bar) {
+    const void *f = (const void *)k_cheb_series<TPR, VPT>;
+    size_t smem = 0;
+    const int grid = coop_setup(f, s->sm_count, H, nullptr, TPR, sizeof(double2), &smem, true);
+    int cache = smem > 0;
+    int n = H.n;
+    const double2 *hv = H.d_val64;
+    double2 *x = (double2 *)X, *pa = (double2 *)a, *pb = (double2 *)b;
+    void *args[] = {&n, (void *)&H.d_rowptr, (void *)&H.d_col, (void *)&hv, &x, &pa, &pb, (void *)&coef, &K, &bar,
+                    &cache};
+    coop_launch(s, f, grid, args, smem);
+  }
+};
+
 template <class T, template <class, int, int> class F, class... Args>
 void dispatch(int R, int shape, Args &&...args) {
 #define LQ_SHAPE(r, s, tpr, vpt) \
@@ -600,6 +683,13 @@ void recur_1d(Session *s, const DeviceOp &H, const void *phi, void *x0, void *b1
     dispatch<float, OneDF>(Rw, shape, s, H, phi, x0, b1, steps, M, mode, dots, bar, sellC, stacked, nreal);
   else
     dispatch<double, OneDF>(Rw, shape, s, H, phi, x0, b1, steps, M, mode, dots, bar, sellC, stacked, nreal);
+}
+
+void cheb_series(Session *s, const DeviceOp &H, void *X, void *a, void *b, const double2 *coef, int K, int R) {
+  LQ_REQUIRE(K >= 1, "Chebyshev series: at least one term");
+  Barrier *bar = barrier_for(s);
+  dispatch<double, SeriesF>(R, 0, s, H, X, a, b, coef, K, bar);
+  LQ_LAUNCHED();
 }
 
 void check_device_errors(Session *s) {
