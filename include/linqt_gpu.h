@@ -172,6 +172,15 @@ int linqt_moments_td_dev(linqt_session *s, const linqt_op *H, const linqt_op *op
                          const double *states_dev, int R, int M, int NT, double dt, double band_width,
                          double band_center, const linqt_opts *opts, double *mu_dev);
 
+/* timeCorrelationsFromChebmom (src/timeCorrelationsFromChebmom.cpp:17-68) with
+ * MomentsTD::ApplyJacksonKernel (src/chebyshev_momentsTD.cpp:135-154): the Jackson kernel over
+ * m (broad_meV), then corr[n] = N/(band_width/2) sum_m delta_chebF(x, m) Re mu(m, n) at the
+ * energy x = (energy - band_center)/(band_width/2), t[n] = n dt.  mu: M x NT (MomentsTD
+ * layout); M_used (may be NULL) gets the moments kept. */
+int linqt_time_correlation_from_moments(linqt_session *s, const double *mu, int M, int NT, int N, double band_width,
+                                        double band_center, double dt, double broad_meV, double energy, double *t,
+                                        double *corr, int *M_used);
+
 /* chebyshev::CorrelationExpansionMoments (src/chebyshev_solver.cpp:86-172) with the
  * default BATCH_SIZE: mu[2*M*M] row-major mu(mL, mR), symmetrised and scaled by
  * (4/R)(1/2)^{[mL=0]}(1/2)^{[mR=0]}.  opl/opr = NULL are identities. */

@@ -71,6 +71,8 @@ SIGNATURES = {
                                     c_void_p]),
     "linqt_moments2d": (c_int, [c_void_p, c_void_p, c_void_p, c_void_p, P_double, c_int, c_int,
                                 ctypes.POINTER(Opts), P_double]),
+    "linqt_time_correlation_from_moments": (c_int, [c_void_p, P_double, c_int, c_int, c_int, c_double, c_double,
+                                                    c_double, c_double, c_double, P_double, P_double, P_int]),
     "linqt_moments_td": (c_int, [c_void_p, c_void_p, c_void_p, c_void_p, P_double, c_int, c_int, c_int, c_double,
                                  c_double, c_double, ctypes.POINTER(Opts), P_double]),
     "linqt_moments_td_dev": (c_int, [c_void_p, c_void_p, c_void_p, c_void_p, c_void_p, c_int, c_int, c_int,

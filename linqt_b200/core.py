@@ -269,6 +269,18 @@ def moments_td(H, opl, opr, states, M, NT, dt, band_width, band_center, opts=Non
     return mu
 
 
+def time_correlation_from_moments(mu, N, band_width, band_center, dt, broad_meV, energy, session=None):
+    """timeCorrelationsFromChebmom: (t, C(t)) from a TD moment table mu[M, NT]."""
+    m = _c128(mu)
+    M, NT = m.shape
+    t, c = np.zeros(NT), np.zeros(NT)
+    used = ctypes.c_int()
+    check(load().linqt_time_correlation_from_moments(_sh(session), _dp(m.view(np.float64)), M, NT, N, band_width,
+                                                     band_center, dt, broad_meV, energy, _dp(t), _dp(c),
+                                                     ctypes.byref(used)))
+    return t, c
+
+
 def moments_td_dev(H, opl, opr, states_dev, R, M, NT, dt, band_width, band_center, mu_dev, opts=None, session=None):
     o = opts or make_opts()
     check(load().linqt_moments_td_dev(_sh(session), H.h, _oph(opl), _oph(opr), ctypes.c_void_p(_ptr(states_dev)), R, M,

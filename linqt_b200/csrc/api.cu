@@ -1436,6 +1436,24 @@ int linqt_moments_td(linqt_session *s, const linqt_op *H, const linqt_op *opl, c
   });
 }
 
+int linqt_time_correlation_from_moments(linqt_session *s, const double *mu, int M, int NT, int N, double band_width,
+                                        double band_center, double dt, double broad_meV, double energy, double *t,
+                                        double *corr, int *M_used) {
+  return guarded([&] {
+    LQ_REQUIRE(mu && t && corr && M > 0 && NT > 0 && band_width > 0 && broad_meV > 0, "bad argument");
+    Session *r = resolve(s);
+    double2 *d_mu = (double2 *)r->get("tc_mu", sizeof(double2) * (size_t)M * NT);
+    double *d_out = (double *)r->get("tc_out", sizeof(double) * 2 * (size_t)NT);
+    LQ_CUDA(cudaMemcpyAsync(d_mu, mu, sizeof(double2) * (size_t)M * NT, cudaMemcpyHostToDevice, r->stream));
+    int T = 0;
+    time_correlation(r, d_mu, M, NT, N, band_width, band_center, dt, broad_meV, energy, d_out, d_out + NT, &T);
+    LQ_CUDA(cudaMemcpyAsync(t, d_out, sizeof(double) * NT, cudaMemcpyDeviceToHost, r->stream));
+    LQ_CUDA(cudaMemcpyAsync(corr, d_out + NT, sizeof(double) * NT, cudaMemcpyDeviceToHost, r->stream));
+    LQ_CUDA(cudaStreamSynchronize(r->stream));
+    if (M_used) *M_used = T;
+  });
+}
+
 int linqt_kubo_fft_dev(linqt_session *s, const linqt_op *H, const linqt_op *opl, const linqt_op *opr,
                        const double *states_dev, int R, int M, int nump, int formula, double band_width,
                        double band_center, const linqt_opts *opts, double *out_dev) {

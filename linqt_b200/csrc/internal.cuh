@@ -284,6 +284,9 @@ void gershgorin(Session *s, const DeviceOp &A, double *lo, double *hi);
 // Jackson kernel helpers (reconstruct.cu)
 int jackson_cut(int M, double band_width, double broad);
 double jackson_factor(int m, int Mom);
+// timeCorrelationsFromChebmom on a device TD table mu[M x NT] (reconstruct.cu)
+void time_correlation(Session *s, const double2 *mu, int M, int NT, int N, double band_width, double band_center,
+                      double dt, double broad_meV, double energy, double *t_out, double *c_out, int *T_out);
 void jackson2d_dev(Session *s, const double2 *mu, int M0, int M1, int M0t, int M1t, double2 *out);
 
 // explicit-stream / caller-scratch launchers (spmm.cu, mu_gemm.cu) for the no-alloc entry point

@@ -188,6 +188,33 @@ __global__ void k_minmax(const double2 *__restrict__ part, int nb, double2 *__re
 
 }  // namespace
 
+namespace {
+// C(t_n) = scale * sum_{m < T} delta(x, m) (g_m Re mu(m, n)), one thread per time step
+__global__ void k_time_correlation(const double2 *__restrict__ mu, int NT, int T, double x, double scale, double dt,
+                                   double *__restrict__ t_out, double *__restrict__ c_out) {
+  const double phi = M_PI / (double)(T + 1.0);
+  for (int n = blockIdx.x * blockDim.x + threadIdx.x; n < NT; n += gridDim.x * blockDim.x) {
+    double out = 0.0;
+    for (int m = 0; m < T; ++m) {
+      const double g = ((T - m + 1) * cos(phi * m) + sin(phi * m) * cos(phi) / sin(phi)) * phi / M_PI;
+      out += coef(COEF_DELTA, x, m).x * (mu[(size_t)m * NT + n].x * g);
+    }
+    t_out[n] = n * dt;
+    c_out[n] = out * scale;
+  }
+}
+}  // namespace
+
+void time_correlation(Session *s, const double2 *mu, int M, int NT, int N, double band_width, double band_center,
+                      double dt, double broad_meV, double energy, double *t_out, double *c_out, int *T_out) {
+  const int T = jackson_cut(M, band_width, broad_meV);
+  const double hw = band_width / 2;
+  k_time_correlation<<<(NT + 127) / 128, 128, 0, s->stream>>>(mu, NT, T, (energy - band_center) / hw, N / hw, dt,
+                                                               t_out, c_out);
+  LQ_LAUNCHED();
+  *T_out = T;
+}
+
 int jackson_cut(int M, double band_width, double broad) {
   const double eta = 2.0 * broad / 1000 / band_width;
   const int maxMom = (int)ceil(M_PI / eta);

@@ -197,6 +197,57 @@ void Moments1D::ApplyJacksonKernel(const double broad) {
 
 void Moments1D::Print() { print_info(*this, "CHEBYSHEV 1D MOMENTS INFO", std::to_string(HighestMomentNumber())); }
 
+// .chebmomTD: "N BW BC NT dt", "M NT", then mu(m, n) row-major (src/chebyshev_momentsTD.cpp:49-99)
+MomentsTD::MomentsTD(std::string momfilename) : _numMoms(0), _maxTimeStep(0), _timeStep(0), _dt(0) {
+  std::ifstream f = open_moments(*this, momfilename, ".chebmomTD");
+  f >> _maxTimeStep >> _dt >> _numMoms >> _maxTimeStep;
+  MomentVector(Moments::vector_t(_numMoms * _maxTimeStep, 0.0));
+  for (size_t q = 0; q < _numMoms * _maxTimeStep; q++) {
+    double re = 0, im = 0;
+    f >> re >> im;
+    MomentVector((int)q) = value_t(re, im);
+  }
+}
+
+void MomentsTD::MomentNumber(const size_t numMoms) {
+  assert(numMoms <= _numMoms);
+  vector_t mu(numMoms * _maxTimeStep, 0.0);
+  for (size_t m = 0; m < numMoms; m++)
+    for (size_t n = 0; n < _maxTimeStep; n++) mu[m * _maxTimeStep + n] = (*this)(m, n);
+  _numMoms = numMoms;
+  MomentVector(mu);
+}
+
+// Jackson factors over m for every time step (src/chebyshev_momentsTD.cpp:135-154)
+void MomentsTD::ApplyJacksonKernel(const double broad) {
+  assert(broad > 0);
+  const double eta = 2.0 * broad / 1000 / BandWidth();
+  size_t maxMom = (size_t)ceil(M_PI / eta);
+  if (maxMom > HighestMomentNumber()) maxMom = HighestMomentNumber();
+  std::cout << "Kernel reduced the number of moments to " << maxMom << " for a broadening of " << M_PI / maxMom
+            << std::endl;
+  MomentNumber(maxMom);
+  const double phi_J = M_PI / (double)(maxMom + 1.0);
+  for (size_t m = 0; m < maxMom; m++) {
+    const double g = ((maxMom - m + 1) * cos(phi_J * m) + sin(phi_J * m) * cos(phi_J) / sin(phi_J)) * phi_J / M_PI;
+    for (size_t n = 0; n < MaxTimeStep(); n++) (*this)(m, n) *= g;
+  }
+}
+
+void MomentsTD::saveIn(std::string filename) {
+  std::ofstream f(filename.c_str());
+  f.precision(std::numeric_limits<double>::digits10);
+  f << SystemSize() << " " << BandWidth() << " " << BandCenter() << " " << MaxTimeStep() << " " << TimeDiff() << " "
+    << std::endl;
+  f << HighestMomentNumber() << " " << MaxTimeStep() << " " << std::endl;
+  for (auto mom : MomentVector()) f << mom.real() << " " << mom.imag() << std::endl;
+}
+
+void MomentsTD::Print() {
+  print_info(*this, "CHEBYSHEV TD MOMENTS INFO",
+             std::to_string(HighestMomentNumber()) + " x " + std::to_string(MaxTimeStep()));
+}
+
 Moments2D::Moments2D(std::string momfilename) {
   std::ifstream f = open_moments(*this, momfilename, ".chebmom2D");
   f >> numMoms[0] >> numMoms[1];
@@ -251,6 +302,24 @@ std::array<double, 2> utility::SpectralBounds(SparseMatrixType &) {
   std::ifstream f("BOUNDS");
   if (f.is_open()) f >> lowest >> highest;
   return {lowest, highest};
+}
+
+int TimeDependentCorrelations(SparseMatrixType &OPL, SparseMatrixType &OPR, chebyshev::MomentsTD &chebMoms,
+                              qstates::generator &gen) {
+  const int N = (int)chebMoms.SystemSize(), M = (int)chebMoms.HighestMomentNumber();
+  const int NT = (int)chebMoms.MaxTimeStep();
+  int R = 0;
+  std::vector<std::complex<double> > st = qstates::collect_states(gen, N, &R);
+  if (R == 0 || M == 0 || NT == 0) return 0;
+  std::vector<std::complex<double> > mu((size_t)M * NT);
+  check(linqt_moments_td(nullptr, need_op(chebMoms.Hamiltonian(), "TimeDependentCorrelations"),
+                         OPL.isIdentity() ? nullptr : need_op(OPL, "TimeDependentCorrelations"),
+                         OPR.isIdentity() ? nullptr : need_op(OPR, "TimeDependentCorrelations"), dp(st.data()), R, M,
+                         NT, chebMoms.TimeDiff(), chebMoms.BandWidth(), chebMoms.BandCenter(), nullptr,
+                         dp(mu.data())),
+        "linqt_moments_td");
+  for (size_t q = 0; q < mu.size(); q++) chebMoms.MomentVector((int)q) += mu[q];  // accumulates, as the reference
+  return 0;
 }
 
 int SpectralMoments(SparseMatrixType &OP, chebyshev::Moments1D &chebMoms, qstates::generator &gen) {

@@ -129,6 +129,43 @@ class Moments2D : public Moments {
   array<int, 2> numMoms;
 };
 
+// Time-domain moment table mu(m, n), m < numMoms, n < maxTimeStep (MomentsTD of LinQT's
+// include/chebyshev_moments.hpp:287-360), with LinQT's .chebmomTD file.  The evolution runs
+// inside chebyshev::TimeDependentCorrelations on the GPU.
+class MomentsTD : public Moments {
+ public:
+  const double HBAR = 0.6582119624;  // eV fs
+
+  MomentsTD() : _numMoms(1), _maxTimeStep(1), _timeStep(0), _dt(0) {}
+  MomentsTD(const size_t m, const size_t n) : _numMoms(m), _maxTimeStep(n), _timeStep(0), _dt(0) {
+    MomentVector(Moments::vector_t(m * n, 0.0));
+  }
+  MomentsTD(std::string momfilename);
+
+  size_t MomentNumber() const { return _numMoms; }
+  size_t HighestMomentNumber() const { return _numMoms; }
+  size_t CurrentTimeStep() const { return _timeStep; }
+  size_t MaxTimeStep() const { return _maxTimeStep; }
+  double TimeDiff() const { return _dt; }
+  double ChebyshevFreq() const { return HalfWidth() / chebyshev::CUTOFF / HBAR; }
+  double ChebyshevFreq_0() const { return BandCenter() / HBAR; }
+
+  void MomentNumber(const size_t mom);
+  void MaxTimeStep(const size_t maxTimeStep) { _maxTimeStep = maxTimeStep; }
+  void IncreaseTimeStep() { _timeStep++; }
+  void ResetTime() { _timeStep = 0; }
+  void TimeDiff(const double dt) { _dt = dt; }
+
+  Moments::value_t &operator()(const size_t m, const size_t n) { return MomentVector(m * MaxTimeStep() + n); }
+  void ApplyJacksonKernel(const double broad);
+  void saveIn(std::string filename);
+  void Print();
+
+ private:
+  size_t _numMoms, _maxTimeStep, _timeStep;
+  double _dt;
+};
+
 // Parameters of Kubo_solver_FFT's recursion (number of moments, sections).  The vectors
 // themselves are device buffers of the solver.
 class Vectors_sliced : public Moments {

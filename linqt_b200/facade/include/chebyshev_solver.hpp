@@ -34,6 +34,10 @@ int CorrelationExpansionMoments(SparseMatrixType &OPL, SparseMatrixType &OPR, ch
 
 int SpectralMoments(SparseMatrixType &OP, chebyshev::Moments1D &chebMoms, qstates::generator &gen);
 
+// all states of the generator as one block through linqt_moments_td
+int TimeDependentCorrelations(SparseMatrixType &OPL, SparseMatrixType &OPR, chebyshev::MomentsTD &chebMoms,
+                              qstates::generator &gen);
+
 }  // namespace chebyshev
 
 #endif

@@ -295,6 +295,31 @@ int lo_moments_td(const lo_op *H, const lo_op *opl, const lo_op *opr, const doub
   return 0;
 }
 
+/* timeCorrelationsFromChebmom (src/timeCorrelationsFromChebmom.cpp:17-68) with
+ * MomentsTD::ApplyJacksonKernel (src/chebyshev_momentsTD.cpp:135-154): Jackson factors over
+ * m < T (T = min(M, ceil(pi/eta)), eta = 2 broad/1000/bw), then
+ * C(t_n) = N/halfwidth sum_m delta_chebF(x, m) Re mu(m, n), x = (energy - bc)/halfwidth. */
+static double delta_chebF(double x, double m);
+int lo_time_correlation(const double *mu, int M, int NT, int N, double band_width, double band_center, double dt,
+                        double broad_meV, double energy, double *t_out, double *c_out) {
+  if (M <= 0 || NT <= 0 || broad_meV <= 0) return -1;
+  const double eta = 2.0 * broad_meV / 1000 / band_width;
+  int T = (int)ceil(M_PI / eta);
+  if (T > M) T = M;
+  const double phi = M_PI / (double)(T + 1.0);
+  const double hw = band_width / 2, x = (energy - band_center) / hw;
+  for (int n = 0; n < NT; n++) {
+    double out = 0.0;
+    for (int m = 0; m < T; m++) {
+      const double g = ((T - m + 1) * cos(phi * m) + sin(phi * m) * cos(phi) / sin(phi)) * phi / M_PI;
+      out += delta_chebF(x, m) * (mu[2 * ((size_t)m * NT + n)] * g);
+    }
+    t_out[n] = n * dt;
+    c_out[n] = out * N / hw;
+  }
+  return T;
+}
+
 /* Vectors::IterateAll (src/chebyshev_vectors.cpp:4-21): store T_0..T_{M-1}. */
 static void iterate_all(const lo_op *H, cplx *T0, cplx *T1, cplx *store, int M) {
   const int n = H->n;

@@ -40,6 +40,8 @@ void lo_op_export(const lo_op *op, int *rowptr, int *col, double *val);
 int lo_moments1d(const lo_op *H, const lo_op *op, const double *states, int R, int M, double *mu);
 int lo_moments_td(const lo_op *H, const lo_op *opl, const lo_op *opr, const double *states, int R, int M, int NT,
                   double dt, double band_width, double band_center, double *mu_out);
+int lo_time_correlation(const double *mu, int M, int NT, int N, double band_width, double band_center, double dt,
+                        double broad_meV, double energy, double *t_out, double *c_out);
 
 /* mu[2*M*M] = chebyshev::CorrelationExpansionMoments with BATCH_SIZE = M
  * (src/chebyshev_solver.cpp:45-82, 86-172), row-major mu(mL, mR) */

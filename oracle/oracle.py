@@ -50,6 +50,9 @@ def lib():
         L.lo_op_export.argtypes = [vp, ip, ip, dp]
         L.lo_moments1d.argtypes = [vp, vp, dp, ctypes.c_int, ctypes.c_int, dp]
         L.lo_moments2d.argtypes = [vp, vp, vp, dp, ctypes.c_int, ctypes.c_int, dp]
+        L.lo_time_correlation.restype = ctypes.c_int
+        L.lo_time_correlation.argtypes = [dp, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_double,
+                                          ctypes.c_double, ctypes.c_double, ctypes.c_double, ctypes.c_double, dp, dp]
         L.lo_moments_td.argtypes = [vp, vp, vp, dp, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_double,
                                     ctypes.c_double, ctypes.c_double, dp]
         L.lo_jackson1d.argtypes = [dp, ctypes.c_int, ctypes.c_double, ctypes.c_double]
@@ -148,6 +151,18 @@ def moments_td(H, opl, opr, states, M, NT, dt, band_width, band_center):
     if rc:
         raise RuntimeError("lo_moments_td failed: %d" % rc)
     return mu
+
+
+def time_correlation(mu, N, band_width, band_center, dt, broad_meV, energy):
+    """timeCorrelationsFromChebmom: (t, C(t)) from a TD moment table mu[M, NT]."""
+    m = np.ascontiguousarray(mu, dtype=np.complex128)
+    M, NT = m.shape
+    t, c = np.zeros(NT), np.zeros(NT)
+    rc = lib().lo_time_correlation(_dp(m.view(np.float64)), M, NT, N, band_width, band_center, dt, broad_meV, energy,
+                                   _dp(t), _dp(c))
+    if rc < 0:
+        raise RuntimeError("lo_time_correlation failed: %d" % rc)
+    return t, c
 
 
 def moments2d(H, opl, opr, states, M):

@@ -1,7 +1,8 @@
 """Drop-in check: LinQT's own driver programs (src/inline_compute-kpm-spectralOp.cpp,
 inline_compute-kpm-nonEqOp.cpp, inline_compute-Kubo-kpm-FFT.cpp), compiled unchanged against
 the C++ facade (linqt_b200/facade) and so running on the GPU library, write the same files as
-the same programs built from the reference's sources on the CPU (oracle/_ref).
+the same programs built from the reference's sources on the CPU (oracle/_ref); also
+inline_compute-kpm-CorrOp (time-domain correlations).
 
 Inputs: the golden linear chain (N = 20000, upper-triangle CSR), a second diagonal operator
 DG so that OPL != OPR, ./BOUNDS, and either the default state (delta at N/2) or a `vector`
@@ -21,7 +22,8 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 ROOT = os.path.dirname(HERE)
 FACADE = os.path.join(ROOT, "linqt_b200", "facade", "_drivers")
 REFBIN = os.path.join(ROOT, "oracle", "_ref")
-DRIVERS = ["inline_compute-kpm-spectralOp", "inline_compute-kpm-nonEqOp", "inline_compute-Kubo-kpm-FFT"]
+DRIVERS = ["inline_compute-kpm-spectralOp", "inline_compute-kpm-nonEqOp", "inline_compute-Kubo-kpm-FFT",
+           "inline_compute-kpm-CorrOp"]
 
 
 def _need(path):
@@ -104,3 +106,15 @@ def test_kubo_fft_driver(workdir, tmp_path, opr, opl):
     # both write 6 significant digits (default stream precision)
     assert np.abs(a[:, 0] - b[:, 0]).max() <= 1e-5 * np.abs(b[:, 0]).max()
     assert np.abs(a[:, 1] - b[:, 1]).max() <= 2e-6 * np.abs(b[:, 1]).max()
+
+
+@pytest.mark.parametrize("opl,opr,M,NT,tmax", [("VX", "VX", 64, 6, 20.0), ("VX", "DG", 48, 4, 6.0)])
+def test_time_correlation_driver(workdir, tmp_path, opl, opr, M, NT, tmax):
+    """inline_compute-kpm-CorrOp (its default state, a delta at N/2): the .chebmomTD tables."""
+    args = ["linear_chain", opl, opr, M, NT, tmax]
+    gpu, cpu, files = _both("inline_compute-kpm-CorrOp", args, workdir, tmp_path)
+    (f,) = files
+    n1, bw1, bc1, dt1, mu1 = formats.read_chebmomtd(str(gpu / f))
+    n2, bw2, bc2, dt2, mu2 = formats.read_chebmomtd(str(cpu / f))
+    assert (n1, bw1, bc1, dt1) == (n2, bw2, bc2, dt2) and mu1.shape == mu2.shape == (M, NT)
+    assert _rel(mu1, mu2) < 1e-12  # 15 printed digits

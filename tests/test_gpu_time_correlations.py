@@ -72,3 +72,15 @@ def test_time_correlations_reject_mixed_precision(graphene):
         lq.moments_td(g["Hg"], None, None, np.ones((1, g["N"])), 8, 2, 1.0, g["bw"], g["bc"],
                       opts=lq.make_opts(precision=lq.PREC_MIXED))
     assert "FP64" in str(e.value)
+
+
+def test_time_correlation_from_moments_matches_oracle(oracle_lib, graphene):
+    g = graphene
+    st = lattices.random_phase_states(g["N"], 3, seed=11)
+    M, NT, dt = 128, 6, 1.0
+    mu = lq.moments_td(g["Hg"], g["Vg"], g["Vg"], st, M, NT, dt, g["bw"], g["bc"])
+    for broad, ef in ((150.0, 0.3), (40.0, -2.0)):
+        t, c = lq.time_correlation_from_moments(mu, g["N"], g["bw"], g["bc"], dt, broad, ef)
+        to, co = oracle_lib.time_correlation(mu, g["N"], g["bw"], g["bc"], dt, broad, ef)
+        assert np.array_equal(t, to)
+        assert rel(c, co) < 1e-12

@@ -163,3 +163,26 @@ def test_time_correlations_vs_ref(oracle_lib, tmp_path):
     delta[0, N // 2] = 1.0
     mu = oracle_lib.moments_td(Ho, ops["VX"], ops["DG"], delta, M, NT, tmax / (NT - 1), bw, bc)
     assert rel(mu, mu_ref) < 1e-12
+
+
+def test_time_correlation_postprocessor_vs_ref(oracle_lib, tmp_path):
+    """timeCorrelationsFromChebmom built from the reference's sources against the C
+    restatement, on a TD table the restatement computed (6 printed digits)."""
+    N, H, V = lattices.honeycomb(6, 5, t=-2.7, W=1.0, seed=21)
+    lo, hi = lattices.gershgorin_bounds(N, *H)
+    bw, bc = 1.05 * (hi - lo), 1.05 * (hi + lo) / 2
+    Ho = oracle_lib.Op(*H)
+    Ho.rescale(2 / bw, -bc / (bw / 2))
+    st = lattices.random_phase_states(N, 2, seed=8)
+    M, NT, dt = 96, 7, 1.5
+    mu = oracle_lib.moments_td(Ho, oracle_lib.Op(*V), oracle_lib.Op(*V), st, M, NT, dt, bw, bc)
+    formats.write_chebmomtd(str(tmp_path / "tdchain.chebmomTD"), N, bw, bc, dt, mu)
+    exe = os.path.join(os.path.dirname(__file__), "..", "oracle", "_ref", "inline_timeCorrelationsFromChebmom")
+    for broad, ef in ((200.0, 0.5), (60.0, -1.25)):
+        subprocess.run([exe, "tdchain.chebmomTD", str(broad), str(ef)], cwd=str(tmp_path), check=True,
+                       capture_output=True, timeout=600)
+        ref = np.loadtxt(str(tmp_path / ("meantdchainEF%.6fJACKSON.dat" % ef)))
+        mu_f = formats.read_chebmomtd(str(tmp_path / "tdchain.chebmomTD"))[4]
+        t, c = oracle_lib.time_correlation(mu_f, N, bw, bc, dt, broad, ef)
+        assert np.abs(t - ref[:, 0]).max() < 1e-5 * max(1.0, np.abs(t).max())
+        assert np.abs(c - ref[:, 1]).max() < 2e-6 * np.abs(c).max()
