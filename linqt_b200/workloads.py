@@ -11,6 +11,7 @@ Kubo-Bastin graphene workload:
     python -m linqt_b200.workloads lr_layouts    # L/R recursion of the 2D moments: CSR vs autotuned
     python -m linqt_b200.workloads cubic_width   # cubic L=200 DOS recursion GB/s: CSR vs autotuned, R = 64, 8
     python -m linqt_b200.workloads moments2d --cells 32 --moments 1024 --vectors 32   # one profiled 2D solve
+    python -m linqt_b200.workloads time_corr     # <V(t)V> of graphene 128x128, R=16, M=512, 40 time steps
 
 Each line gives the device time per solve (CUDA events on the session stream, warm-up
 first), Chebyshev steps*nnz/s, the recursion's algorithmic bytes per second, and for the
@@ -299,10 +300,35 @@ def run_moments2d_once(Lc, R, M, prec):
             "phases_ms": ph, "launches": ln}
 
 
+def run_time_corr(Lc, R, M, NT, dt, reps):
+    """Time-domain correlations <V(t) V> of graphene (TimeDependentCorrelations): per time step a
+    1D recursion of M steps and two evolution series of K steps each."""
+    import torch
+    from .core import moments_td_dev, random_phase_states_dev
+    N, H, V = lattices.honeycomb(Lc, Lc, t=-2.7, W=1.0, seed=21)
+    sess, bw, bc, Hg, (Vg,) = _ops(N, H, [V])
+    st = torch.empty(2 * R * N, dtype=torch.float64, device="cuda")
+    random_phase_states_dev(N, R, 22, st, session=sess)
+    mu = torch.zeros(2 * M * NT, dtype=torch.float64, device="cuda")
+    ms = _timed(lambda: moments_td_dev(Hg, Vg, Vg, st, R, M, NT, dt, bw, bc, mu, session=sess), reps, torch)
+    x = dt * (0.5 * bw) / 0.6582119624
+    K = 0
+    from math import fabs
+    from scipy.special import jv
+    while True:  # the series length the library uses (terms until |J_k(x)| <= 1e-10)
+        K += 1
+        if not fabs(jv(K, x)) > 1e-10:
+            break
+    steps = NT * M + 2 * (NT - 1) * K
+    return {"workload": "time_corr_graphene_%dx%d" % (Lc, Lc), "N": N, "nnz_full": Hg.nnz, "R": R, "M": M, "NT": NT,
+            "dt_fs": dt, "series_terms": K, "ms_per_solve": ms, "ms_per_time_step": ms / NT,
+            "steps_nnz_per_s": steps * R * Hg.nnz / (ms * 1e-3)}
+
+
 def main(argv=None):
     ap = argparse.ArgumentParser()
     ap.add_argument("workload", choices=["dos", "cubic", "cubic_full", "spin", "layouts", "realisations",
-                                         "lr_layouts", "cubic_width", "moments2d"])
+                                         "lr_layouts", "cubic_width", "moments2d", "time_corr"])
     ap.add_argument("--precision", type=int, default=PREC_MIXED, help="moments2d: LINQT_PREC_* value")
     ap.add_argument("--reps", type=int, default=5)
     ap.add_argument("--cells", type=int, default=64, help="spin: Kane-Mele cells per side")
@@ -324,6 +350,8 @@ def main(argv=None):
     elif a.workload == "cubic_width":
         print(json.dumps(run_cubic_width(200, 64, 64, a.reps)))
         r = run_cubic_width(200, 8, 64, a.reps)
+    elif a.workload == "time_corr":
+        r = run_time_corr(128, 16, 512, 40, 1.0, a.reps)
     elif a.workload == "moments2d":
         r = run_moments2d_once(a.cells, a.vectors, a.moments, a.precision)
     elif a.workload == "cubic_full":
