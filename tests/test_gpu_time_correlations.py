@@ -84,3 +84,24 @@ def test_time_correlation_from_moments_matches_oracle(oracle_lib, graphene):
         to, co = oracle_lib.time_correlation(mu, g["N"], g["bw"], g["bc"], dt, broad, ef)
         assert np.array_equal(t, to)
         assert rel(c, co) < 1e-12
+
+
+@pytest.mark.parametrize("R,NT,dt", [(300, 2, 0.7), (5, 1, 1.0), (4, 3, 0.0)])
+def test_time_correlations_edge_cases(oracle_lib, R, NT, dt):
+    """R > 256 (two vector chunks), a single time step, dt = 0 (the series is the identity:
+    every time step repeats t = 0)."""
+    N, H, V = lattices.honeycomb(4, 4, t=-2.7, W=1.0, seed=21)
+    lo, hi = lattices.gershgorin_bounds(N, *H)
+    bw, bc = 1.05 * (hi - lo), 1.05 * (hi + lo) / 2
+    Hg = lq.Operator.from_csr(N, *H)
+    Hg.rescale_to_chebyshev(bw, bc)
+    Ho = oracle_lib.Op(*H)
+    Ho.rescale(2 / bw, -bc / (bw / 2))
+    st = lattices.random_phase_states(N, R, seed=13)
+    M = 20
+    mu = lq.moments_td(Hg, lq.Operator.from_csr(N, *V), None, st, M, NT, dt, bw, bc)
+    ref = oracle_lib.moments_td(Ho, oracle_lib.Op(*V), None, st, M, NT, dt, bw, bc)
+    assert rel(mu, ref) < TOL
+    if dt == 0.0:
+        for t in range(1, NT):
+            assert rel(mu[:, t], mu[:, 0]) < 1e-13
