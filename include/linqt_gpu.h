@@ -310,6 +310,39 @@ int linqt_server_wait_all(linqt_server *srv);
 int linqt_server_release(linqt_server *srv, long ticket);
 int linqt_server_destroy(linqt_server *srv);
 
+/* ---- operator builder: utilities/wannier2sparse -------------------------- */
+/* A Wannier90 tight-binding model, read like tbmodel::readOrbitalPositions / readUnitCell /
+ * readWannierModel (utilities/wannier2sparse/src/tbmodel.cpp:5-22, wannier_parser.cpp:45-117):
+ * LABEL.xyz (orbital count, then "label x y z" per orbital; spin-down orbitals in the second
+ * half), LABEL.uc (3 lattice vectors), LABEL_hr.dat (Wannier90 hoppings).  A LABEL.stdis
+ * static-disorder file is rejected with LINQT_ERR_UNSUPPORTED (the reference draws it from
+ * std::random_device). */
+typedef struct linqt_tbmodel linqt_tbmodel;
+int linqt_tbmodel_load(const char *label, linqt_tbmodel **out);
+int linqt_tbmodel_destroy(linqt_tbmodel *m);
+int linqt_tbmodel_info(const linqt_tbmodel *m, int *num_orbitals, long *num_hoppings);
+/* The CSR file hopping_list::save_hopping_list_as_csr writes for
+ * tbmodel::WannierOperator(op).wrap_in_supercell(cell_dim) (src/main.cpp:46-53,
+ * hopping_list.cpp:158-285): the upper triangle (col >= row) of the operator on a supercell
+ * of cell_dim[0] x cell_dim[1] x cell_dim[2] unit cells, rows sorted by column, entries of
+ * equal (row, col) summed, 0-based int32 indices.  op: "HAM", one of VX VY VZ, V{X,Y,Z}S{X,Y,Z},
+ * SX SY SZ, TX TY TZ (include/operator_utils.hpp:31-35), or NAME with a spinorial NAME.OP file
+ * in the working directory (tbmodel.cpp:331-354).  Built on the session's device.
+ *   linqt_supercell_csr:     host arrays; rowptr == NULL asks for *n and *nnz only;
+ *                            capacity = room in col and val (entries)
+ *   linqt_supercell_csr_dev: device arrays (rowptr_dev of *n + 1 entries, from a size query),
+ *                            filled on the session stream
+ *   linqt_supercell_write_csr: the text file itself (same bytes as the reference writes)
+ *   linqt_supercell_operator:  a device operator with the file's (Hermitian-upper) meaning */
+int linqt_supercell_csr(linqt_session *s, linqt_tbmodel *m, const char *op, const int cell_dim[3], int *n, long *nnz,
+                        int *rowptr, int *col, double *val, long capacity);
+int linqt_supercell_csr_dev(linqt_session *s, linqt_tbmodel *m, const char *op, const int cell_dim[3], int *n,
+                            long *nnz, int *rowptr_dev, int *col_dev, double *val_dev, long capacity);
+int linqt_supercell_write_csr(linqt_session *s, linqt_tbmodel *m, const char *op, const int cell_dim[3],
+                              const char *path);
+int linqt_supercell_operator(linqt_session *s, linqt_tbmodel *m, const char *op, const int cell_dim[3],
+                             linqt_op **out);
+
 #ifdef __cplusplus
 }
 #endif

@@ -102,6 +102,15 @@ SIGNATURES = {
     "linqt_server_wait_all": (c_int, [c_void_p]),
     "linqt_server_release": (c_int, [c_void_p, c_long]),
     "linqt_server_destroy": (c_int, [c_void_p]),
+    "linqt_tbmodel_load": (c_int, [ctypes.c_char_p, ctypes.POINTER(c_void_p)]),
+    "linqt_tbmodel_destroy": (c_int, [c_void_p]),
+    "linqt_tbmodel_info": (c_int, [c_void_p, P_int, P_long]),
+    "linqt_supercell_csr": (c_int, [c_void_p, c_void_p, ctypes.c_char_p, P_int, P_int, P_long, P_int, P_int, P_double,
+                                    c_long]),
+    "linqt_supercell_csr_dev": (c_int, [c_void_p, c_void_p, ctypes.c_char_p, P_int, P_int, P_long, c_void_p, c_void_p,
+                                        c_void_p, c_long]),
+    "linqt_supercell_write_csr": (c_int, [c_void_p, c_void_p, ctypes.c_char_p, P_int, ctypes.c_char_p]),
+    "linqt_supercell_operator": (c_int, [c_void_p, c_void_p, ctypes.c_char_p, P_int, ctypes.POINTER(c_void_p)]),
 }
 
 _lib = None

@@ -4,8 +4,8 @@
 
 The GPU library is compiled from linqt_b200/csrc/*.cu with the CUDA runtime linked
 statically, so the .so carries no dependency on a particular libcudart.  The facade
-library (linqt_b200/facade: LinQT's C++ classes on the C ABI) is plain C++ linked
-against it.
+library (linqt_b200/facade: LinQT's C++ classes on the C ABI) and the wannier2sparse
+command line (linqt_b200/w2s) are plain C++ linked against it.
 """
 import glob
 import os
@@ -18,6 +18,8 @@ CSRC = os.path.join(HERE, "csrc")
 LIB = os.path.join(HERE, "liblinqt_gpu.so")
 FACADE = os.path.join(HERE, "facade")
 FACADE_LIB = os.path.join(HERE, "liblinqt_facade.so")
+W2S_SRC = os.path.join(HERE, "w2s", "wannier2sparse.cpp")
+W2S_BIN = os.path.join(HERE, "w2s", "_bin", "wannier2sparse")
 ROOT = os.path.dirname(HERE)
 
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
@@ -61,6 +63,22 @@ def build_facade(force=False, verbose=False):
     return FACADE_LIB
 
 
+def build_w2s(force=False, verbose=False):
+    """The wannier2sparse command line on liblinqt_gpu.so (linqt_b200/w2s/_bin/wannier2sparse)."""
+    deps = [W2S_SRC, LIB, os.path.join(ROOT, "include", "linqt_gpu.h")]
+    if not force and os.path.exists(W2S_BIN) and all(os.path.getmtime(p) <= os.path.getmtime(W2S_BIN) for p in deps):
+        return W2S_BIN
+    os.makedirs(os.path.dirname(W2S_BIN), exist_ok=True)
+    cmd = ["g++", "-std=c++17", "-O2", "-I", os.path.join(ROOT, "include"), "-o", W2S_BIN, W2S_SRC, "-L", HERE,
+           "-llinqt_gpu", "-Wl,-rpath,$ORIGIN/../.."]
+    if verbose:
+        print(" ".join(cmd))
+    p = subprocess.run(cmd, capture_output=True, text=True)
+    if p.returncode != 0:
+        raise RuntimeError("g++ (wannier2sparse) failed:\n" + p.stdout + p.stderr)
+    return W2S_BIN
+
+
 def build(force=False, verbose=False, extra=()):
     if force or needs_build():
         cmd = [nvcc()] + ARCH + FLAGS + list(extra) + ["-I", os.path.join(ROOT, "include"), "-o", LIB] + sources()
@@ -70,6 +88,7 @@ def build(force=False, verbose=False, extra=()):
         if p.returncode != 0:
             raise RuntimeError("nvcc failed:\n" + p.stdout + p.stderr)
     build_facade(force=force, verbose=verbose)
+    build_w2s(force=force, verbose=verbose)
     return LIB
 
 

@@ -414,3 +414,87 @@ def jackson2d(mu, band_width, b0, b1):
     check(load().linqt_jackson2d(_dp(m.view(np.float64)), M0, M1, band_width, b0, b1, ctypes.byref(a),
                                  ctypes.byref(b)))
     return m.reshape(-1)[: a.value * b.value].reshape(a.value, b.value)
+
+
+# --- operator builder (LinQT's utilities/wannier2sparse) ---------------------------------------
+W2S_OPERATORS = ["VX", "VY", "VZ", "VXSX", "VXSY", "VXSZ", "VYSX", "VYSY", "VYSZ", "VZSX", "VZSY", "VZSZ",
+                 "SX", "SY", "SZ", "TX", "TY", "TZ"]
+
+
+class TBModel:
+    """A Wannier90 tight-binding model (LABEL.xyz, LABEL.uc, LABEL_hr.dat) and the supercell
+    operators wannier2sparse builds from it, assembled on the GPU (linqt_supercell_*)."""
+
+    def __init__(self, handle):
+        self.h = handle
+
+    @classmethod
+    def load(cls, label):
+        h = ctypes.c_void_p()
+        check(load().linqt_tbmodel_load(label.encode(), ctypes.byref(h)))
+        return cls(h)
+
+    def close(self):
+        if getattr(self, "h", None):
+            check(load().linqt_tbmodel_destroy(self.h))
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def info(self):
+        """(orbitals per cell, hoppings kept from the _hr.dat file)."""
+        n, k = ctypes.c_int(), ctypes.c_long()
+        check(load().linqt_tbmodel_info(self.h, ctypes.byref(n), ctypes.byref(k)))
+        return n.value, k.value
+
+    @staticmethod
+    def _dims(cell_dim):
+        d = np.ascontiguousarray(cell_dim, dtype=np.int32)
+        if d.shape != (3,):
+            raise ValueError("cell_dim must hold 3 integers")
+        return d
+
+    def csr_size(self, op, cell_dim, session=None):
+        """(n, nnz) of the upper-triangle CSR of `op` on the supercell."""
+        d = self._dims(cell_dim)
+        n, nnz = ctypes.c_int(), ctypes.c_long()
+        check(load().linqt_supercell_csr(_sh(session), self.h, op.encode(), _ip(d), ctypes.byref(n),
+                                         ctypes.byref(nnz), None, None, None, 0))
+        return n.value, nnz.value
+
+    def supercell_csr(self, op, cell_dim, session=None):
+        """(n, rowptr, col, val complex128): the matrix of LABEL.op.CSR as wannier2sparse writes it."""
+        d = self._dims(cell_dim)
+        n, nnz = self.csr_size(op, cell_dim, session)
+        rp = np.zeros(n + 1, dtype=np.int32)
+        cl = np.zeros(max(nnz, 1), dtype=np.int32)
+        vl = np.zeros(max(nnz, 1), dtype=np.complex128)
+        n2, nnz2 = ctypes.c_int(), ctypes.c_long()
+        check(load().linqt_supercell_csr(_sh(session), self.h, op.encode(), _ip(d), ctypes.byref(n2),
+                                         ctypes.byref(nnz2), _ip(rp), _ip(cl), _dp(vl.view(np.float64)), len(cl)))
+        return n2.value, rp, cl[: nnz2.value], vl[: nnz2.value]
+
+    def supercell_csr_dev(self, op, cell_dim, rowptr_dev, col_dev, val_dev, capacity, session=None):
+        """Fill device buffers (torch tensors or pointers) on the session stream; returns (n, nnz)."""
+        d = self._dims(cell_dim)
+        n, nnz = ctypes.c_int(), ctypes.c_long()
+        check(load().linqt_supercell_csr_dev(_sh(session), self.h, op.encode(), _ip(d), ctypes.byref(n),
+                                             ctypes.byref(nnz), _ptr(rowptr_dev), _ptr(col_dev), _ptr(val_dev),
+                                             capacity))
+        return n.value, nnz.value
+
+    def write_csr(self, op, cell_dim, path, session=None):
+        """Write LABEL.op.CSR (the bytes wannier2sparse writes)."""
+        d = self._dims(cell_dim)
+        check(load().linqt_supercell_write_csr(_sh(session), self.h, op.encode(), _ip(d), path.encode()))
+
+    def operator(self, op, cell_dim, session=None):
+        """The supercell operator as a device Operator (Hermitian-upper, like the file)."""
+        d = self._dims(cell_dim)
+        h = ctypes.c_void_p()
+        check(load().linqt_supercell_operator(_sh(session), self.h, op.encode(), _ip(d), ctypes.byref(h)))
+        return Operator(h, session)

@@ -19,22 +19,6 @@ void set_last_error(const std::string &msg) { g_last_error = msg; }
 
 [[noreturn]] void fail(int code, const std::string &msg) { throw Error(code, msg); }
 
-template <class F>
-static int guarded(F &&f) {
-  try {
-    f();
-    return LINQT_OK;
-  } catch (const Error &e) {
-    set_last_error(e.what());
-    return e.code;
-  } catch (const std::bad_alloc &) {
-    set_last_error("host allocation failed");
-    return LINQT_ERR_NOMEM;
-  } catch (const std::exception &e) {
-    set_last_error(e.what());
-    return LINQT_ERR_INTERNAL;
-  }
-}
 
 // ---------------------------------------------------------------------------
 // sessions

@@ -25,6 +25,24 @@ struct Error : std::runtime_error {
 [[noreturn]] void fail(int code, const std::string &msg);
 void set_last_error(const std::string &msg);
 
+// body of a C entry point: runs f, turns an exception into a status and a message
+template <class F>
+inline int guarded(F &&f) {
+  try {
+    f();
+    return LINQT_OK;
+  } catch (const Error &e) {
+    set_last_error(e.what());
+    return e.code;
+  } catch (const std::bad_alloc &) {
+    set_last_error("host allocation failed");
+    return LINQT_ERR_NOMEM;
+  } catch (const std::exception &e) {
+    set_last_error(e.what());
+    return LINQT_ERR_INTERNAL;
+  }
+}
+
 #define LQ_CUDA(x)                                                                                    \
   do {                                                                                                \
     cudaError_t e_ = (x);                                                                             \
