@@ -9,7 +9,7 @@ sites), t = -2.7 eV, Anderson disorder W = 1.0 eV (seed 21), V_x = i (x_i - x_j)
 in for operators read from files.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl linqt|reference]
-                    [--precision fp64|mixed]
+                    [--precision fp64|mixed] [--workload kubo|supercell]
 
 metric = (recursion steps per vector column: 2M) x (columns: R) x nnz(H, Hermitian-
 expanded, diagonal included) / seconds.  value: device time of K solves with operators
@@ -17,6 +17,13 @@ and states resident in HBM (CUDA events on the launching stream, max over ranks)
 e2e: the same through the host-pointer C ABI call with the states copied from pinned
 host memory and mu / sigma(E) copied back inside the timed region.  Multi-GPU: one
 independent solve per rank (different random vectors), no collective on the data path.
+
+--workload supercell times the operator builder instead (LinQT's wannier2sparse): the
+Hamiltonian of a synthetic 18-orbital Wannier model (hoppings to |R_i| <= 3, seed 7) on a
+128 x 128 x 1 supercell, written as the upper-triangle CSR of LABEL.HAM.CSR.  metric =
+stored entries / second; value: the device build into HBM-resident buffers; e2e: the model
+files read and the CSR returned in host arrays (linqt_supercell_csr) every step; the
+reference arm runs the reference tool built from its sources on a bounded supercell.
 """
 import argparse
 import json
@@ -207,6 +214,176 @@ def cpu_baseline_sample():
                       "Kubo_solver_FFT %.2fs)" % (a["seconds"], b["seconds"])}
 
 
+SC_WORKLOAD = dict(workload="supercell_wannier18_r3_128x128", model="synthetic Wannier90 model", orbitals=18, reach=3,
+                   seed=7, cell_dim=[128, 128, 1], op="HAM", reference_cell_dim=[16, 16, 1])
+SC_METRIC = "supercell_csr_entries_per_s"
+SC_UNIT = "entries/s"
+
+
+def supercell_inputs():
+    from linqt_b200 import lattices
+    d = tempfile.mkdtemp(prefix="linqt_w2s_")
+    label = os.path.join(d, "syn")
+    lattices.wannier_model(label, SC_WORKLOAD["orbitals"], SC_WORKLOAD["reach"], SC_WORKLOAD["seed"])
+    return d, label
+
+
+def supercell_reference_sample():
+    """The reference tool (oracle/_ref/wannier2sparse, LinQT's utilities/wannier2sparse built
+    here) on the bounded supercell: (entries/s, seconds, entries)."""
+    tool = os.path.join(ROOT, "oracle", "_ref", "wannier2sparse")
+    if not os.path.exists(tool):
+        return None
+    d, label = supercell_inputs()
+    cd = [str(x) for x in SC_WORKLOAD["reference_cell_dim"]]
+    t0 = time.perf_counter()
+    subprocess.run([tool, "syn"] + cd, cwd=d, check=True, stdout=subprocess.DEVNULL)
+    secs = time.perf_counter() - t0
+    with open(os.path.join(d, "syn.HAM.CSR")) as f:
+        nnz = int(f.readline().split()[1])
+    return nnz / secs, secs, nnz
+
+
+def run_supercell_reference(args):
+    first = supercell_reference_sample()
+    if first is None:
+        print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref/wannier2sparse is not built "
+                                                              "(needs the reference checkout)"}))
+        return
+    secs = 0.0
+    ents = 0
+    for it in range(args.warmup + args.steps - 1):
+        r = supercell_reference_sample()
+        if it >= args.warmup - 1:
+            secs += r[1]
+            ents += r[2]
+    value = ents / secs
+    sample = "supercell %s of the same model (one thread: the tool is serial), text file included" % (
+        "x".join(str(x) for x in SC_WORKLOAD["reference_cell_dim"]))
+    print(json.dumps({"impl": "reference", "metric": SC_METRIC, "value": value, "unit": SC_UNIT, "n_gpus": args.gpus,
+                      "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * secs / args.steps,
+                      "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+                      "data": "synthetic (seeded model files)", "config": dict(SC_WORKLOAD, parallelism="cpu"),
+                      "cpu_baseline": {"value": value, "unit": SC_UNIT, "cores": 1, "kind": "reference",
+                                       "sample": sample},
+                      "e2e": {"value": value, "unit": SC_UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}))
+
+
+def run_supercell(args, rank, world, local):
+    import torch
+    import linqt_b200 as lq
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300), device_id=torch.device("cuda", local))
+
+    def barrier():
+        if dist is not None:
+            dist.barrier()
+
+    w = SC_WORKLOAD
+    d, label = supercell_inputs()
+    stream = torch.cuda.current_stream()
+    sess = lq.Session(local)
+    sess.set_stream(stream)
+    m = lq.TBModel.load(label)
+    dims, op = w["cell_dim"], w["op"]
+    n, nnz = m.csr_size(op, dims, session=sess)
+    rp = torch.empty(n + 1, dtype=torch.int32, device="cuda")
+    cl = torch.empty(nnz, dtype=torch.int32, device="cuda")
+    vl = torch.empty(2 * nnz, dtype=torch.float64, device="cuda")
+
+    def build():
+        m.supercell_csr_dev(op, dims, rp, cl, vl, nnz, session=sess)
+
+    for _ in range(args.warmup):
+        build()
+    torch.cuda.synchronize()
+    sess.enable_timing(True)
+    sess.phase_times(reset=True)
+    with ClockSampler(local) as clocks:
+        barrier()
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(args.steps):
+            build()
+        e1.record(stream)
+        torch.cuda.synchronize()
+        barrier()
+    dev_ms = e0.elapsed_time(e1) / args.steps
+    phase_ms, phase_launches = sess.phase_times(reset=True)
+    sess.enable_timing(False)
+    clk = clocks.summary()
+
+    # end to end: read the model files and return the CSR in host arrays, every step
+    out_rp = np.empty(n + 1, dtype=np.int32)
+    out_cl = np.empty(nnz, dtype=np.int32)
+    out_vl = np.empty(nnz, dtype=np.complex128)
+
+    def build_host():
+        mm = lq.TBModel.load(label)
+        nn, kk = ctypes.c_int(), ctypes.c_long()
+        dd = np.ascontiguousarray(dims, dtype=np.int32)
+        lq.load().linqt_supercell_csr(sess.h, mm.h, op.encode(), dd.ctypes.data_as(ctypes.POINTER(ctypes.c_int)),
+                                      ctypes.byref(nn), ctypes.byref(kk),
+                                      out_rp.ctypes.data_as(ctypes.POINTER(ctypes.c_int)),
+                                      out_cl.ctypes.data_as(ctypes.POINTER(ctypes.c_int)),
+                                      out_vl.ctypes.data_as(ctypes.POINTER(ctypes.c_double)), nnz)
+        mm.close()
+
+    import ctypes
+    build_host()
+    barrier()
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        build_host()
+    torch.cuda.synchronize()
+    barrier()
+    e2e_ms = 1e3 * (time.perf_counter() - t0) / args.steps
+    assert np.array_equal(out_rp, rp.cpu().numpy()) and np.array_equal(out_cl, cl.cpu().numpy())
+
+    dev_ms = max_over_ranks(dev_ms, dist, "cuda")
+    e2e_ms = max_over_ranks(e2e_ms, dist, "cuda")
+    value, e2e = whole_job_rates(nnz, world, dev_ms, e2e_ms)
+    hbm_peak, _, peak_src = measured_peaks()
+    out_bytes = 20 * nnz + 4 * (n + 1)
+    ach = out_bytes / (dev_ms * 1e-3) / 1e9
+    roof = {"kernel": "k_row_totals + k_scan_totals + k_rowptr + k_fill (whole build)", "bound": "hbm",
+            "achieved": ach, "peak": hbm_peak, "unit": "GB/s", "frac": ach / hbm_peak, "peak_source": peak_src,
+            "algorithmic_bytes": "20 B per stored entry (int32 column + complex128 value) + 4 B per row pointer",
+            "traffic": None}
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        try:
+            r = supercell_reference_sample()
+            if r:
+                cpu = {"value": r[0], "unit": SC_UNIT, "cores": 1, "kind": "reference",
+                       "sample": "reference tool on the %s supercell of the same model (%.1f s, %d entries, "
+                                 "text file included)" % ("x".join(str(x) for x in w["reference_cell_dim"]), r[1],
+                                                          r[2])}
+        except Exception as ex:
+            cpu = {"error": str(ex)[:200]}
+    if rank == 0:
+        cfg = dict(w, parallelism="replicas%d" % world if world > 1 else "single", N=n, nnz_upper=nnz,
+                   l2="output larger than L2: %.1f GB written per build" % (out_bytes / 1e9))
+        print(json.dumps({"metric": SC_METRIC, "value": value, "unit": SC_UNIT, "n_gpus": world, "steps": args.steps,
+                          "warmup": args.warmup, "ms_per_step": dev_ms, "higher_is_better": True, "scaling": "weak",
+                          "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded model files)",
+                          "config": cfg,
+                          "e2e": {"value": e2e, "unit": SC_UNIT, "ms_per_step": e2e_ms,
+                                  "h2d_bytes_per_step": int(os.path.getsize(label + "_hr.dat")),
+                                  "d2h_bytes_per_step": int(out_bytes)},
+                          "gpu_launches": int(sum(phase_launches)), "roofline": roof,
+                          "build_phases_ms": round(phase_ms[3] / args.steps, 4), "clocks": clk,
+                          "cpu_baseline": cpu}))
+    if dist is not None:
+        dist.destroy_process_group()
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -216,6 +393,8 @@ def main():
     ap.add_argument("--precision", default="fp64", choices=["fp64", "mixed", "fp32"])
     ap.add_argument("--no-compare", action="store_true", help="skip the mixed-vs-FP64 accuracy run")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--workload", default="kubo", choices=["kubo", "supercell"])
+    ap.add_argument("--sc-cells", type=int, default=None, help="supercell: L x L x 1 cells (profiling captures)")
     # size overrides, for profiling captures on a smaller case of the same kernels
     ap.add_argument("--lx", type=int, default=None)
     ap.add_argument("--ly", type=int, default=None)
@@ -232,6 +411,17 @@ def main():
     rank = int(os.environ.get("RANK", "0"))
     world = int(os.environ.get("WORLD_SIZE", "1"))
     local = int(os.environ.get("LOCAL_RANK", "0"))
+
+    if args.workload == "supercell":
+        if args.sc_cells:
+            SC_WORKLOAD["cell_dim"] = [args.sc_cells, args.sc_cells, 1]
+            SC_WORKLOAD["workload"] = "supercell_wannier18_r3_%dx%d" % (args.sc_cells, args.sc_cells)
+        if args.impl == "reference":
+            if rank == 0:
+                run_supercell_reference(args)
+            return
+        run_supercell(args, rank, world, local)
+        return
 
     if args.impl == "reference":
         if rank == 0:

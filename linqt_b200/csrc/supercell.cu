@@ -303,20 +303,21 @@ int linqt_supercell_csr(linqt_session *s, linqt_tbmodel *m, const char *op, cons
       *nnz = w2s::count_rows(r, v, nullptr);
       return;
     }
-    long N;
-    std::vector<int> rp, cl;
-    std::vector<double2> vl;
-    to_host(m, r, op, cell_dim, N, rp, cl, vl);
+    int *rp, *cl;
+    double2 *vl;
+    const long k = build_on_device(m, r, op, cell_dim, &rp, &cl, &vl);
+    const long N = m->dev.v.n;
     *n = (int)N;
-    *nnz = (long)cl.size();
-    LQ_REQUIRE(capacity >= (long)cl.size(), "capacity " + std::to_string(capacity) + " is below the " +
-                                                std::to_string(cl.size()) + " stored entries");
-    LQ_REQUIRE(cl.empty() || (col && val), "NULL col/val");
-    std::memcpy(rowptr, rp.data(), sizeof(int) * (N + 1));
-    if (!cl.empty()) {
-      std::memcpy(col, cl.data(), sizeof(int) * cl.size());
-      std::memcpy(val, vl.data(), sizeof(double2) * vl.size());
+    *nnz = k;
+    LQ_REQUIRE(capacity >= k, "capacity " + std::to_string(capacity) + " is below the " + std::to_string(k) +
+                                  " stored entries");
+    LQ_REQUIRE(k == 0 || (col && val), "NULL col/val");
+    LQ_CUDA(cudaMemcpyAsync(rowptr, rp, sizeof(int) * (N + 1), cudaMemcpyDeviceToHost, r->stream));
+    if (k) {
+      LQ_CUDA(cudaMemcpyAsync(col, cl, sizeof(int) * k, cudaMemcpyDeviceToHost, r->stream));
+      LQ_CUDA(cudaMemcpyAsync(val, vl, sizeof(double2) * k, cudaMemcpyDeviceToHost, r->stream));
     }
+    LQ_CUDA(cudaStreamSynchronize(r->stream));
   });
 }
 

@@ -225,3 +225,37 @@ def gershgorin_bounds(n, rowptr, col, val):
     np.add.at(rad, rows[off], np.abs(val[off]))
     np.add.at(rad, col[off], np.abs(val[off]))
     return float((diag - rad).min()), float((diag + rad).max())
+
+
+def wannier_model(label, orbitals=18, reach=3, seed=7, three_d=False):
+    """Write a synthetic Wannier90 model LABEL_hr.dat / LABEL.xyz / LABEL.uc and return its
+    number of hopping lines.  `orbitals` spinful orbitals (spin-down block second, labels
+    _s+_ / _s-_) on a hexagonal cell; a hopping between every orbital pair for every cell
+    vector with |R_i| <= reach (R_z = 0 unless three_d), magnitudes decaying as exp(-|R|),
+    Hermitian (t(-R) = t(R)^H) and printed with 6 decimals as Wannier90 does."""
+    rng = np.random.default_rng(seed)
+    rz = reach if three_d else 0
+    Rs = [(x, y, z) for x in range(-reach, reach + 1) for y in range(-reach, reach + 1) for z in range(-rz, rz + 1)]
+    A = {R: (rng.normal(size=(orbitals, orbitals)) + 1j * rng.normal(size=(orbitals, orbitals)))
+         * np.exp(-np.sqrt(R[0] ** 2 + R[1] ** 2 + R[2] ** 2)) for R in Rs}
+    lines = []
+    for R in Rs:
+        mR = (-R[0], -R[1], -R[2])
+        t = 0.5 * (A[R] + A[mR].conj().T)
+        for n in range(orbitals):
+            for m in range(orbitals):
+                v = t[m, n]
+                lines.append("%5d%5d%5d%5d%5d%12.6f%12.6f" % (R[0], R[1], R[2], m + 1, n + 1, v.real, v.imag))
+    deg = ["    1" * min(15, len(Rs) - i) for i in range(0, len(Rs), 15)]
+    with open(label + "_hr.dat", "w") as f:
+        f.write(" synthetic model (seed %d)\n%12d\n%12d\n%s\n%s\n" % (seed, orbitals, len(Rs), "\n".join(deg),
+                                                                     "\n".join(lines)))
+    with open(label + ".uc", "w") as f:
+        f.write(" 2.46 0.0 0.0\n 1.23 2.130422 0.0\n 0.0 0.0 %s\n" % ("2.46" if three_d else "20.0"))
+    pos = rng.uniform(0.0, 1.0, size=(orbitals // 2, 3)) * np.array([2.0, 1.7, 0.5])
+    with open(label + ".xyz", "w") as f:
+        f.write("%d\n" % orbitals)
+        for s in ("+", "-"):
+            for i, p in enumerate(pos):
+                f.write("o%d_s%s_ %.8f %.8f %.8f\n" % (i, s, *p))
+    return len(lines)

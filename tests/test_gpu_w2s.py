@@ -84,8 +84,10 @@ def scipy_upper(o, op, dims):
     cells = np.stack(np.meshgrid(np.arange(D[0]), np.arange(D[1]), np.arange(D[2]), indexing="ij"), -1).reshape(-1, 3)
     idx = lambda c: (c[:, 2] * D[1] + c[:, 1]) * D[0] + c[:, 0]  # noqa: E731
     norms = np.array([np.hypot(*v) for _, _, v in uc])
-    keep = norms / norms.mean() > 1e-10
-    rows, cols, vals = [], [], []
+    mean = norms.mean() if len(norms) else 0.0
+    keep = norms > 1e-10 * mean if mean > 0 else np.zeros(len(norms), dtype=bool)
+    n = wbb * len(cells)
+    rows, cols, vals = [np.zeros(0, np.int64)], [np.zeros(0, np.int64)], [np.zeros(0, np.complex128)]
     for (cell, (e0, e1), v), k in zip(uc, keep):
         if not k:
             continue
@@ -95,7 +97,6 @@ def scipy_upper(o, op, dims):
         vals.append(np.full(len(cells), complex(*v)))
     r, c, v = np.concatenate(rows), np.concatenate(cols), np.concatenate(vals)
     up = c >= r
-    n = wbb * len(cells)
     A = sp.csr_matrix((v[up], (r[up], c[up])), shape=(n, n))
     A.sort_indices()
     return n, A.indptr, A.indices, A.data
@@ -156,7 +157,12 @@ def test_device_operator_reproduces_shipped_moments():
     m = lq.TBModel.load(os.path.join(W2S, "linear_chain_example", "linear_chain"))
     H = m.operator("HAM", (100, 100, 1))
     V = m.operator("VX", (100, 100, 1))
-    assert H.info() == (20000, 40000) and V.info()[0] == 20000
+    # the same operators as the ones read from the shipped files
+    for op, X in (("HAM", H), ("VX", V)):
+        F = lq.Operator.from_csr(20000, g[op + "_rowptr"], g[op + "_col"],
+                                 g[op + "_val"][0::2] + 1j * g[op + "_val"][1::2])
+        assert F.info() == X.info()
+    assert H.info() == (20000, 40000)
     bw, bc = 10.0, 0.0  # BOUNDS -5 5
     H.rescale_to_chebyshev(bw, bc)
     st = np.zeros((1, 20000), dtype=np.complex128)
@@ -164,7 +170,3 @@ def test_device_operator_reproduces_shipped_moments():
     mu = lq.moments2d(H, V, V, st, 100)
     want = g["mu100"][..., 0] + 1j * g["mu100"][..., 1]
     assert np.abs(mu - want).max() <= 1e-13 * np.abs(want).max()
-    # and the operator equals the one read from the shipped files
-    for op, X in (("HAM", H), ("VX", V)):
-        F = lq.Operator.from_csr(20000, g[op + "_rowptr"], g[op + "_col"], g[op + "_val"][0::2] + 1j * g[op + "_val"][1::2])
-        assert F.info() == X.info()
