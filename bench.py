@@ -22,7 +22,7 @@ independent solve per rank (different random vectors), no collective on the data
 Hamiltonian of a synthetic 18-orbital Wannier model (hoppings to |R_i| <= 3, seed 7) on a
 128 x 128 x 1 supercell, written as the upper-triangle CSR of LABEL.HAM.CSR.  metric =
 stored entries / second; value: the device build into HBM-resident buffers; e2e: the model
-files read and the CSR returned in host arrays (linqt_supercell_csr) every step; the
+files read and the CSR returned in pinned host arrays (linqt_supercell_csr) every step; the
 reference arm runs the reference tool built from its sources on a bounded supercell.
 """
 import argparse
@@ -272,6 +272,7 @@ def run_supercell_reference(args):
 def run_supercell(args, rank, world, local):
     import torch
     import linqt_b200 as lq
+    from linqt_b200._lib import check
     torch.cuda.set_device(local)
     dist = None
     if world > 1:
@@ -318,20 +319,20 @@ def run_supercell(args, rank, world, local):
     sess.enable_timing(False)
     clk = clocks.summary()
 
-    # end to end: read the model files and return the CSR in host arrays, every step
-    out_rp = np.empty(n + 1, dtype=np.int32)
-    out_cl = np.empty(nnz, dtype=np.int32)
-    out_vl = np.empty(nnz, dtype=np.complex128)
+    # end to end: read the model files and return the CSR in (pinned) host arrays, every step
+    out_rp = torch.empty(n + 1, dtype=torch.int32).pin_memory()
+    out_cl = torch.empty(nnz, dtype=torch.int32).pin_memory()
+    out_vl = torch.empty(2 * nnz, dtype=torch.float64).pin_memory()
 
     def build_host():
         mm = lq.TBModel.load(label)
         nn, kk = ctypes.c_int(), ctypes.c_long()
         dd = np.ascontiguousarray(dims, dtype=np.int32)
-        lq.load().linqt_supercell_csr(sess.h, mm.h, op.encode(), dd.ctypes.data_as(ctypes.POINTER(ctypes.c_int)),
-                                      ctypes.byref(nn), ctypes.byref(kk),
-                                      out_rp.ctypes.data_as(ctypes.POINTER(ctypes.c_int)),
-                                      out_cl.ctypes.data_as(ctypes.POINTER(ctypes.c_int)),
-                                      out_vl.ctypes.data_as(ctypes.POINTER(ctypes.c_double)), nnz)
+        check(lq.load().linqt_supercell_csr(sess.h, mm.h, op.encode(),
+                                               dd.ctypes.data_as(ctypes.POINTER(ctypes.c_int)), ctypes.byref(nn),
+                                               ctypes.byref(kk), ctypes.cast(out_rp.data_ptr(), ctypes.POINTER(ctypes.c_int)),
+                                               ctypes.cast(out_cl.data_ptr(), ctypes.POINTER(ctypes.c_int)),
+                                               ctypes.cast(out_vl.data_ptr(), ctypes.POINTER(ctypes.c_double)), nnz))
         mm.close()
 
     import ctypes
@@ -344,7 +345,7 @@ def run_supercell(args, rank, world, local):
     torch.cuda.synchronize()
     barrier()
     e2e_ms = 1e3 * (time.perf_counter() - t0) / args.steps
-    assert np.array_equal(out_rp, rp.cpu().numpy()) and np.array_equal(out_cl, cl.cpu().numpy())
+    assert torch.equal(out_rp, rp.cpu()) and torch.equal(out_cl, cl.cpu()) and torch.equal(out_vl, vl.cpu())
 
     dev_ms = max_over_ranks(dev_ms, dist, "cuda")
     e2e_ms = max_over_ranks(e2e_ms, dist, "cuda")

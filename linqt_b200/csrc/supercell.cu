@@ -38,8 +38,10 @@ struct DevPlan {
 namespace {
 
 constexpr int kScanThreads = 256;
-constexpr int kScanItems = 16;
-constexpr int kRowsPerBlock = kScanThreads * kScanItems;
+constexpr int kFillThreads = 256;
+// shared memory per CTA of the fill, below the default dynamic limit; a sweep of 16-48 KB
+// and of 2-8 cells per CTA (18-orbital model, 128 x 128 cells) moved the build by < 5 %
+constexpr long kFillSmem = 48 * 1024;
 
 // inclusive scan across the block (kScanThreads threads); returns the block total in *tot
 __device__ long long block_inclusive_scan(long long x, long long *tot) {
@@ -66,11 +68,13 @@ __device__ long long block_inclusive_scan(long long x, long long *tot) {
   return x + before;
 }
 
+// ITEMS consecutive rows per thread, ITEMS * kScanThreads per block
+template <int ITEMS>
 __global__ void __launch_bounds__(kScanThreads) k_row_totals(PlanView p, long long *bsum) {
-  const long base = (long)blockIdx.x * kRowsPerBlock + (long)threadIdx.x * kScanItems;
+  const long base = (long)blockIdx.x * kScanThreads * ITEMS + (long)threadIdx.x * ITEMS;
   long long s = 0;
 #pragma unroll 4
-  for (int i = 0; i < kScanItems; ++i)
+  for (int i = 0; i < ITEMS; ++i)
     if (base + i < p.n) s += row_count(p, base + i);
   long long tot;
   block_inclusive_scan(s, &tot);
@@ -91,23 +95,24 @@ __global__ void __launch_bounds__(kScanThreads) k_scan_totals(long long *bsum, i
   if (threadIdx.x == 0) bsum[nb] = carry;
 }
 
+template <int ITEMS>
 __global__ void __launch_bounds__(kScanThreads) k_rowptr(PlanView p, const long long *boff, int *rowptr) {
-  const long base = (long)blockIdx.x * kRowsPerBlock + (long)threadIdx.x * kScanItems;
-  int c[kScanItems];
+  const long base = (long)blockIdx.x * kScanThreads * ITEMS + (long)threadIdx.x * ITEMS;
+  int c[ITEMS];
   long long s = 0;
 #pragma unroll
-  for (int i = 0; i < kScanItems; ++i) {
+  for (int i = 0; i < ITEMS; ++i) {
     c[i] = base + i < p.n ? row_count(p, base + i) : 0;
     s += c[i];
   }
   long long tot;
   long long run = boff[blockIdx.x] + block_inclusive_scan(s, &tot) - s;
 #pragma unroll
-  for (int i = 0; i < kScanItems; ++i) {
+  for (int i = 0; i < ITEMS; ++i) {
     if (base + i < p.n) rowptr[base + i] = (int)run;
     run += c[i];
   }
-  if (base <= p.n - 1 && p.n - 1 < base + kScanItems) rowptr[p.n] = (int)boff[gridDim.x];
+  if (base <= p.n - 1 && p.n - 1 < base + ITEMS) rowptr[p.n] = (int)boff[gridDim.x];
 }
 
 // one thread per (cell, key): items i = s * K + t
@@ -126,6 +131,76 @@ __global__ void __launch_bounds__(256) k_fill(PlanView p, const int *__restrict_
   }
 }
 
+// one CTA per group of cpb cells: the cells' tables go to shared memory (their coordinates
+// first), then every key of every cell is placed.  With at least as many keys per cell as
+// threads, a thread loads a key once and places it in all cpb cells; otherwise the
+// (cell, key) items are walked with a fixed stride (no division per item).
+__global__ void __launch_bounds__(kFillThreads) k_fill_cells(PlanView p, const int *__restrict__ rowptr,
+                                                             int *__restrict__ col, double2 *__restrict__ val,
+                                                             int cpb) {
+  extern __shared__ int tabs[];
+  int *xyz = tabs;               // 3 per cell
+  int *tab0 = tabs + 3 * cpb;    // cell tables
+  const int per_cell = cell_table_size(p), NN = cell_table_items(p), K = p.K;
+  const int qn = blockDim.x / NN, rn = blockDim.x % NN;
+  const int c0n = threadIdx.x / NN, j0 = threadIdx.x % NN;
+  for (long base = (long)blockIdx.x * cpb; base < p.ncells; base += (long)gridDim.x * cpb) {
+    const int ncell = (int)min((long)cpb, p.ncells - base);
+    for (int c = threadIdx.x; c < ncell; c += blockDim.x)
+      cell_coords(p, base + c, xyz[3 * c], xyz[3 * c + 1], xyz[3 * c + 2]);
+    __syncthreads();
+    for (int c = c0n, j = j0; c < ncell;) {
+      cell_table_entry(p, base + c, xyz[3 * c], xyz[3 * c + 1], xyz[3 * c + 2], j, rowptr, tab0 + c * per_cell);
+      c += qn;
+      j += rn;
+      if (j >= NN) {
+        j -= NN;
+        c++;
+      }
+    }
+    __syncthreads();
+    if (K >= (int)blockDim.x) {
+      // the next key's data is requested before this key is placed
+      int t = threadIdx.x;
+      int4 k = __ldg(&p.kpack[t]);
+      int go = __ldg(&p.kgo[t]);
+      double2 v = __ldg(&p.kval[t]);
+      for (; t < K; t += blockDim.x) {
+        const int tn = t + blockDim.x < K ? t + blockDim.x : t;
+        const int4 kn = __ldg(&p.kpack[tn]);
+        const int gon = __ldg(&p.kgo[tn]);
+        const double2 vn = __ldg(&p.kval[tn]);
+        for (int c = 0; c < ncell; ++c) {
+          long pos, cc;
+          if (key_place(p, k, go, tab0 + c * per_cell, pos, cc)) {
+            col[pos] = (int)cc;
+            val[pos] = v;
+          }
+        }
+        k = kn;
+        go = gon;
+        v = vn;
+      }
+    } else {
+      const int qk = blockDim.x / K, rk = blockDim.x % K;
+      for (int c = threadIdx.x / K, t = threadIdx.x % K; c < ncell;) {
+        long pos, cc;
+        if (key_entry(p, t, tab0 + c * per_cell, pos, cc)) {
+          col[pos] = (int)cc;
+          val[pos] = __ldg(&p.kval[t]);
+        }
+        c += qk;
+        t += rk;
+        if (t >= K) {
+          t -= K;
+          c++;
+        }
+      }
+    }
+    __syncthreads();
+  }
+}
+
 template <class T>
 size_t put(std::vector<char> &blob, const std::vector<T> &v) {
   const size_t off = (blob.size() + 255) & ~(size_t)255;
@@ -139,7 +214,7 @@ void upload(const Plan &pl, int device, DevPlan &d) {
   const size_t o_gk = put(blob, pl.grp_key0), o_gz = put(blob, pl.grp_z0), o_kz = put(blob, pl.kz),
                o_ky = put(blob, pl.ky), o_kx = put(blob, pl.kx), o_kl = put(blob, pl.kleaf), o_ko = put(blob, pl.ko1),
                o_kg = put(blob, pl.kgrp), o_zn = put(blob, pl.zn), o_yn = put(blob, pl.yn), o_xn = put(blob, pl.xn),
-               o_kv = put(blob, pl.kval);
+               o_kv = put(blob, pl.kval), o_kp = put(blob, pl.kpack), o_kgo = put(blob, pl.kgo);
   d.release();
   d.device = device;
   LQ_CUDA(cudaSetDevice(device));
@@ -166,17 +241,24 @@ void upload(const Plan &pl, int device, DevPlan &d) {
   v.yn = (const Node *)(b + o_yn);
   v.xn = (const Node *)(b + o_xn);
   v.kval = (const double2 *)(b + o_kv);
+  v.kpack = (const int4 *)(b + o_kp);
+  v.kgo = (const int *)(b + o_kgo);
+  v.nz = (int)pl.zn.size();
+  v.ny = (int)pl.yn.size();
+  v.nx = (int)pl.xn.size();
 }
 
 }  // namespace
 
 // rowptr pass: returns nnz (rowptr left in rowptr_dev when it is not null)
-static long count_rows(Session *s, const PlanView &v, int *rowptr_dev) {
-  const long nb = (v.n + kRowsPerBlock - 1) / kRowsPerBlock;
+template <int ITEMS>
+static long count_rows_t(Session *s, const PlanView &v, int *rowptr_dev) {
+  const long rows_per_block = (long)kScanThreads * ITEMS;
+  const long nb = (v.n + rows_per_block - 1) / rows_per_block;
   LQ_REQUIRE(nb < 0x7fffffffL, "supercell too large");
   long long *bsum = (long long *)s->get("w2s_block_sums", sizeof(long long) * (nb + 1));
   PhaseScope ph(s, PH_OTHER);
-  k_row_totals<<<(unsigned)nb, kScanThreads, 0, s->stream>>>(v, bsum);
+  k_row_totals<ITEMS><<<(unsigned)nb, kScanThreads, 0, s->stream>>>(v, bsum);
   LQ_LAUNCHED();
   k_scan_totals<<<1, kScanThreads, 0, s->stream>>>(bsum, (int)nb);
   LQ_LAUNCHED();
@@ -185,7 +267,7 @@ static long count_rows(Session *s, const PlanView &v, int *rowptr_dev) {
   LQ_CUDA(cudaStreamSynchronize(s->stream));
   LQ_REQUIRE(total <= 0x7fffffffLL, "the supercell operator has more than 2^31-1 stored entries");
   if (rowptr_dev) {
-    k_rowptr<<<(unsigned)nb, kScanThreads, 0, s->stream>>>(v, bsum, rowptr_dev);
+    k_rowptr<ITEMS><<<(unsigned)nb, kScanThreads, 0, s->stream>>>(v, bsum, rowptr_dev);
     LQ_LAUNCHED();
     ph.launches(3);
   } else {
@@ -194,16 +276,35 @@ static long count_rows(Session *s, const PlanView &v, int *rowptr_dev) {
   return (long)total;
 }
 
+// rowptr pass: returns nnz (rowptr left in rowptr_dev when it is not null).  16 rows per
+// thread, or 2 when that would leave SMs idle.
+static long count_rows(Session *s, const PlanView &v, int *rowptr_dev) {
+  if (v.n >= (long)kScanThreads * 16 * 2 * s->sm_count) return count_rows_t<16>(s, v, rowptr_dev);
+  return count_rows_t<2>(s, v, rowptr_dev);
+}
+
 static void fill_rows(Session *s, const PlanView &v, const int *rowptr_dev, int *col_dev, double2 *val_dev) {
   if (v.K == 0 || v.ncells == 0) return;
   PhaseScope ph(s, PH_OTHER);
-  const long total = v.ncells * (long)v.K;
-  const long want = (total + 255) / 256;
-  const unsigned grid = (unsigned)std::min<long>(want, (long)s->sm_count * 16);
-  if (total < 0x7fffffffL)
-    k_fill<unsigned><<<grid, 256, 0, s->stream>>>(v, rowptr_dev, col_dev, val_dev);
-  else
-    k_fill<unsigned long long><<<grid, 256, 0, s->stream>>>(v, rowptr_dev, col_dev, val_dev);
+  const long table = 4L * (cell_table_size(v) + 3);
+  if (table <= kFillSmem) {
+    // cells per CTA: enough keys to keep the threads busy (4 cells when a thread places one
+    // key in every cell), within the shared-memory budget
+    const long by_smem = kFillSmem / table;
+    const long want = v.K >= kFillThreads ? 4L : std::max(1L, (16L * kFillThreads + v.K - 1) / v.K);
+    const int cpb = (int)std::max(1L, std::min(std::min(by_smem, want), v.ncells));
+    const long blocks = (v.ncells + cpb - 1) / cpb;
+    const unsigned grid = (unsigned)std::min<long>(blocks, (long)s->sm_count * 8);
+    k_fill_cells<<<grid, kFillThreads, (size_t)(table * cpb), s->stream>>>(v, rowptr_dev, col_dev, val_dev, cpb);
+  } else {
+    const long total = v.ncells * (long)v.K;
+    const long want = (total + 255) / 256;
+    const unsigned grid = (unsigned)std::min<long>(want, (long)s->sm_count * 16);
+    if (total < 0x7fffffffL)
+      k_fill<unsigned><<<grid, 256, 0, s->stream>>>(v, rowptr_dev, col_dev, val_dev);
+    else
+      k_fill<unsigned long long><<<grid, 256, 0, s->stream>>>(v, rowptr_dev, col_dev, val_dev);
+  }
   LQ_LAUNCHED();
   ph.launches(1);
 }

@@ -343,6 +343,7 @@ Plan make_plan(const std::vector<Hop> &uc, int wbb, const int dims[3]) {
     LQ_REQUIRE(dims[d] > 0, "supercell dimensions must be positive");
     p.dims[d] = dims[d];
   }
+  LQ_REQUIRE(wbb < 65536, "more than 65535 orbitals per cell");
   p.ncells = (long)dims[0] * dims[1] * dims[2];
   p.n = p.ncells * wbb;
   LQ_REQUIRE(p.n <= 0x7fffffffL, "the supercell has more than 2^31-1 orbitals");
@@ -380,16 +381,16 @@ Plan make_plan(const std::vector<Hop> &uc, int wbb, const int dims[3]) {
       first = false;
       if (nz) {
         zs = K;
-        p.zn.push_back(Node{k[1], K - g0, 0, (int)p.yn.size(), 0});
+        p.zn.push_back(Node{k[1], K - g0, 0, (int)p.yn.size(), 0, g});
       }
       if (ny) {
         ys = K;
-        p.yn.push_back(Node{k[2], K - zs, 0, (int)p.xn.size(), 0});
+        p.yn.push_back(Node{k[2], K - zs, 0, (int)p.xn.size(), 0, (int)p.zn.size() - 1});
         p.zn.back().nc++;
       }
       if (nx) {
         xs = K;
-        p.xn.push_back(Node{k[3], K - ys, 0, K, 0});
+        p.xn.push_back(Node{k[3], K - ys, 0, K, 0, (int)p.yn.size() - 1});
         p.yn.back().nc++;
       }
       p.zn.back().size++;
@@ -402,6 +403,8 @@ Plan make_plan(const std::vector<Hop> &uc, int wbb, const int dims[3]) {
       p.ko1.push_back(k[4]);
       p.kgrp.push_back(g);
       p.kval.push_back(make_double2(it->second.real(), it->second.imag()));
+      p.kpack.push_back(make_int4(p.kz.back(), p.ky.back(), p.kx.back(), p.kleaf.back()));
+      p.kgo.push_back(g << 16 | k[4]);
     }
   }
   p.grp_key0[wbb] = p.keys();

@@ -50,8 +50,9 @@ bool is_builtin_op(const std::string &op);  // HAM or one of the 18 names
 //   size  keys in the run
 //   c0    first child run (next level) or, on the x level, the first key
 //   nc    number of child runs
+//   par   parent: the group (z runs), the z run (y runs) or the y run (x runs)
 struct Node {
-  int val, pre, size, c0, nc;
+  int val, pre, size, c0, nc, par;
 };
 
 struct Plan {
@@ -65,6 +66,8 @@ struct Plan {
   // per key: its z, y, x runs, index inside the x run, target orbital, group
   std::vector<int> kz, ky, kx, kleaf, ko1, kgrp;
   std::vector<double2> kval;
+  std::vector<int4> kpack;  // per key {z run, y run, x run, index in the x run}
+  std::vector<int> kgo;     // per key group << 16 | target orbital
   int keys() const { return (int)ko1.size(); }
 };
 

@@ -12,6 +12,7 @@ Kubo-Bastin graphene workload:
     python -m linqt_b200.workloads cubic_width   # cubic L=200 DOS recursion GB/s: CSR vs autotuned, R = 64, 8
     python -m linqt_b200.workloads moments2d --cells 32 --moments 1024 --vectors 32   # one profiled 2D solve
     python -m linqt_b200.workloads time_corr     # <V(t)V> of graphene 128x128, R=16, M=512, 40 time steps
+    python -m linqt_b200.workloads supercell     # supercell CSR assembly (wannier2sparse) of two Wannier models
 
 Each line gives the device time per solve (CUDA events on the session stream, warm-up
 first), Chebyshev steps*nnz/s, the recursion's algorithmic bytes per second, and for the
@@ -325,10 +326,34 @@ def run_time_corr(Lc, R, M, NT, dt, reps):
             "steps_nnz_per_s": steps * R * Hg.nnz / (ms * 1e-3)}
 
 
+def run_supercell(orbitals, reach, L, op, reps):
+    """The operator builder on the device: the upper-triangle CSR of `op` for a synthetic
+    Wannier model on an L x L x 1 supercell, written into HBM-resident buffers."""
+    import os
+    import tempfile
+    import torch
+    from .core import TBModel
+    d = tempfile.mkdtemp(prefix="linqt_w2s_")
+    label = os.path.join(d, "m")
+    lattices.wannier_model(label, orbitals, reach, seed=7)
+    sess = Session(0)
+    sess.set_stream(torch.cuda.current_stream())
+    m = TBModel.load(label)
+    n, nnz = m.csr_size(op, (L, L, 1), session=sess)
+    rp = torch.empty(n + 1, dtype=torch.int32, device="cuda")
+    cl = torch.empty(nnz, dtype=torch.int32, device="cuda")
+    vl = torch.empty(2 * nnz, dtype=torch.float64, device="cuda")
+    ms = _timed(lambda: m.supercell_csr_dev(op, (L, L, 1), rp, cl, vl, nnz, session=sess), reps, torch)
+    out_bytes = 20 * nnz + 4 * (n + 1)
+    return {"workload": "supercell_wannier%d_r%d_%dx%d_%s" % (orbitals, reach, L, L, op), "N": n, "nnz_upper": nnz,
+            "hoppings_per_cell": m.info()[1], "ms_per_build": ms, "entries_per_s": nnz / (ms * 1e-3),
+            "output_GBps": out_bytes / (ms * 1e-3) / 1e9}
+
+
 def main(argv=None):
     ap = argparse.ArgumentParser()
     ap.add_argument("workload", choices=["dos", "cubic", "cubic_full", "spin", "layouts", "realisations",
-                                         "lr_layouts", "cubic_width", "moments2d", "time_corr"])
+                                         "lr_layouts", "cubic_width", "moments2d", "time_corr", "supercell"])
     ap.add_argument("--precision", type=int, default=PREC_MIXED, help="moments2d: LINQT_PREC_* value")
     ap.add_argument("--reps", type=int, default=5)
     ap.add_argument("--cells", type=int, default=64, help="spin: Kane-Mele cells per side")
@@ -350,6 +375,10 @@ def main(argv=None):
     elif a.workload == "cubic_width":
         print(json.dumps(run_cubic_width(200, 64, 64, a.reps)))
         r = run_cubic_width(200, 8, 64, a.reps)
+    elif a.workload == "supercell":
+        print(json.dumps(run_supercell(18, 3, 128, "HAM", a.reps)))
+        print(json.dumps(run_supercell(18, 3, 128, "VXSY", a.reps)))
+        r = run_supercell(4, 1, 2048, "HAM", a.reps)
     elif a.workload == "time_corr":
         r = run_time_corr(128, 16, 512, 40, 1.0, a.reps)
     elif a.workload == "moments2d":
