@@ -138,14 +138,17 @@ __global__ void __launch_bounds__(192, 1)
           break;
         }
         mbar_arrive_expect_tx(&sm.full[s], Cfg::STAGE);
-        const int x = (int)(kbeg + (long)kb * Cfg::BK);
+        // planes are stored per K chunk and this CTA's range starts on a chunk boundary
+        // (koff is a multiple of kchunk), so x counts from the start of the chunk
+        const int x = kb * Cfg::BK;
+        const int za = chunk * ND, zb = chunk * 2 * ND;
         uint8_t *st = sm.stage[s];
 #pragma unroll
         for (int d = 0; d < ND; ++d) {
-          tma_load_3d(st + d * Cfg::A_TILE, &tmA, x, m0, d, &sm.full[s]);
+          tma_load_3d(st + d * Cfg::A_TILE, &tmA, x, m0, za + d, &sm.full[s]);
           uint8_t *bt = st + ND * Cfg::A_TILE + d * Cfg::B_TILE;
-          tma_load_3d(bt, &tmB, x, m1, d, &sm.full[s]);                     // digit d of b
-          tma_load_3d(bt + Cfg::B_HALF, &tmB, x, m1, ND + d, &sm.full[s]);  // digit d of b''
+          tma_load_3d(bt, &tmB, x, m1, zb + d, &sm.full[s]);                     // digit d of b
+          tma_load_3d(bt + Cfg::B_HALF, &tmB, x, m1, zb + ND + d, &sm.full[s]);  // digit d of b''
         }
       }
     }
@@ -253,9 +256,11 @@ __device__ __forceinline__ uint32_t pack4(int a, int b, int c, int d) {
 }
 
 // Digit planes of both sides: z = 0 the L side (ND planes), z = 1 the R side (ND planes of b,
-// then ND of b'' = (Bi, -Br)).  src: rows of kf floats; dig: [planes][rows][kfp] int8 (K
-// padded with zeros to kfp); expo[row][chunk]: the exponent e with max |x| over the chunk
-// < 2^e.  Grid (4 nchunk, rows, 2) in clusters of 4 CTAs: each CTA stages a quarter of a
+// then ND of b'' = (Bi, -Br)).  src: rows of kf floats; dig: [nchunk][planes][rows][kchunk]
+// int8, chunk-major so that the rows one K chunk's CTAs read at the same time lie kchunk
+// bytes apart rather than the whole K apart (K padded with zeros to kfp; the part of the
+// last chunk past kfp is never read); expo[row][chunk]: the exponent e with max |x| over
+// the chunk < 2^e.  Grid (4 nchunk, rows, 2) in clusters of 4 CTAs: each CTA stages a quarter of a
 // (row, chunk) in shared memory (kchunk / 4 floats, up to 64 KB), the cluster exchanges the
 // quarter maxima through distributed shared memory, and the digits are written from the
 // staged copy, so every value is read from HBM once.
@@ -310,10 +315,11 @@ __global__ void __cluster_dims__(kDigitCluster, 1, 1) __launch_bounds__(256)
   int e = 0;
   if (mx > 0.f) (void)frexpf(mx, &e);  // mx = f 2^e, f in [0.5, 1): every |x| < 2^e
   if (threadIdx.x == 0 && quarter == 0) (b_side ? expB : expA)[(size_t)row * nchunk + c] = e;
-  const size_t plane = (size_t)rows * kfp;
-  int8_t *drow = (b_side ? digB : digA) + (size_t)row * kfp;
+  const size_t plane = (size_t)rows * kchunk;  // one digit plane of one K chunk
+  const int nplanes = b_side ? 2 * ND : ND;
+  int8_t *drow = (b_side ? digB : digA) + (size_t)c * nplanes * plane + (size_t)row * kchunk;
   for (int i = threadIdx.x; i < nquad; i += blockDim.x) {
-    const long k = k0 + 4L * i;
+    const long k = k0 + 4L * i - (long)c * kchunk;  // offset inside the chunk
     const float4 t = stage_q[i];
     int d[4][ND];
     digits<ND>(ldexpf(t.x, 6 - e), d[0]);
@@ -329,12 +335,12 @@ __global__ void __cluster_dims__(kDigitCluster, 1, 1) __launch_bounds__(256)
   }
 }
 
-// [planes][rows][kfp] int8, box bk bytes x box_rows x 1, swizzle of bk bytes; rows past the
-// end of a plane read as zero
-CUtensorMap make_map_i8(const void *base, int rows, long kfp, int planes, int box_rows, int bk) {
+// [planes][rows][kchunk] int8 (planes = chunks x digit planes per chunk), box bk bytes x
+// box_rows x 1, swizzle of bk bytes; rows past the end of a plane read as zero
+CUtensorMap make_map_i8(const void *base, int rows, long kchunk, int planes, int box_rows, int bk) {
   CUtensorMap m;
-  const cuuint64_t dims[3] = {(cuuint64_t)kfp, (cuuint64_t)rows, (cuuint64_t)planes};
-  const cuuint64_t strides[2] = {(cuuint64_t)kfp, (cuuint64_t)kfp * rows};
+  const cuuint64_t dims[3] = {(cuuint64_t)kchunk, (cuuint64_t)rows, (cuuint64_t)planes};
+  const cuuint64_t strides[2] = {(cuuint64_t)kchunk, (cuuint64_t)kchunk * rows};
   const cuuint32_t box[3] = {(cuuint32_t)bk, (cuuint32_t)box_rows, 1};
   const cuuint32_t estr[3] = {1, 1, 1};
   const CUresult r = encode_fn()(&m, CU_TENSOR_MAP_DATA_TYPE_UINT8, 3, const_cast<void *>(base), dims, strides, box,
@@ -371,8 +377,9 @@ void contract_i8(Session *s, const void *L, const void *Rv, int M, long K, doubl
   const int nchunk = (int)((kfp + kchunk - 1) / kchunk);
   const long kMaxSplit = 64;
   const long S = std::min<long>(nchunk, kMaxSplit);
-  int8_t *dA = (int8_t *)s->get("mu_i8_a", (size_t)ND * M * kfp);
-  int8_t *dB = (int8_t *)s->get("mu_i8_b", (size_t)2 * ND * M * kfp);
+  const long kcp = (long)nchunk * kchunk;  // K of the chunk-major planes (>= kfp)
+  int8_t *dA = (int8_t *)s->get("mu_i8_a", (size_t)ND * M * kcp);
+  int8_t *dB = (int8_t *)s->get("mu_i8_b", (size_t)2 * ND * M * kcp);
   int *eA = (int *)s->get("mu_i8_ea", sizeof(int) * (size_t)M * nchunk);
   int *eB = (int *)s->get("mu_i8_eb", sizeof(int) * (size_t)M * nchunk);
   double2 *part = (double2 *)s->get("mu_i8_parts", sizeof(double2) * (size_t)S * M * M);
@@ -383,8 +390,8 @@ void contract_i8(Session *s, const void *L, const void *Rv, int M, long K, doubl
   k_digits<ND><<<dim3(kDigitCluster * nchunk, M, 2), 256, qsmem, s->stream>>>(
       (const float *)L, (const float *)Rv, kf, kfp, kchunk, M, nchunk, dA, dB, eA, eB);
   LQ_LAUNCHED();
-  const CUtensorMap ta = make_map_i8(dA, M, kfp, ND, I8_BM, Cfg::BK),
-                    tb = make_map_i8(dB, M, kfp, 2 * ND, I8_BN, Cfg::BK);
+  const CUtensorMap ta = make_map_i8(dA, M, kchunk, ND * nchunk, I8_BM, Cfg::BK),
+                    tb = make_map_i8(dB, M, kchunk, 2 * ND * nchunk, I8_BN, Cfg::BK);
   const size_t smem = sizeof(I8Shared<ND>) + 1024;
   LQ_CUDA(cudaFuncSetAttribute(k_mu_i8<ND>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
   for (long koff = 0; koff < kfp; koff += S * kchunk) {
