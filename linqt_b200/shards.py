@@ -101,6 +101,8 @@ def _world(group):
 def _my_states(states, group):
     st = np.atleast_2d(np.asarray(states, np.complex128))
     R = st.shape[0]
+    if R == 0 or st.shape[1] == 0:
+        raise ValueError("sharded solve: no states")
     world, rank = _world(group)
     a, b = shard_range(R, world, rank)
     return st[a:b], R
