@@ -89,11 +89,13 @@ def run_spin(Lc, R, M, nump, reps):
     import torch
     from .core import bastin_from_moments, moments2d_dev
     N, H, J = lattices.kane_mele(Lc, Lc, seed=31)
-    sess, bw, bc, Hg, (Jg,) = _ops(N, H, [J])
     st = lattices.random_phase_states(N, R, seed=32)
     st_dev = torch.from_numpy(st.view(np.float64).copy()).cuda()
     res = {}
     for prec in (PREC_FP64, PREC_MIXED):
+        # a session (and operators) of its own per precision, so that neither is timed next
+        # to the other's cached workspaces
+        sess, bw, bc, Hg, (Jg,) = _ops(N, H, [J])
         mu = torch.zeros(2 * M * M, dtype=torch.float64, device="cuda")
         out = torch.zeros(3 * nump, dtype=torch.float64, device="cuda")
         o = make_opts(precision=prec, fmt=2)
@@ -112,7 +114,10 @@ def run_spin(Lc, R, M, nump, reps):
         ms2 = _timed(lambda: moments2d_dev(Hg, Jg, Jg, st_dev, R, M, mu2, opts=o, session=sess), reps, torch)
         E_m, s_mom = bastin_from_moments(mu_h, N, bw, bc, 1e-3, xbound=0.99, session=sess)
         res[prec] = dict(ms=ms, phases=[round(x / reps, 3) for x in ph], mu=mu_h, s_fft=s_fft, ms2=ms2, s_mom=s_mom)
-    nnz = Hg.nnz
+        nnz = Hg.nnz
+        del mu, out, mu2, Hg, Jg
+        sess.close()
+        torch.cuda.synchronize()
     a, b = res[PREC_FP64], res[PREC_MIXED]
     lo, hi = int(0.05 * nump), int(0.95 * nump)
     nd = len(a["s_mom"])
