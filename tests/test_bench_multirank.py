@@ -40,7 +40,7 @@ def _worker(rank, world, port, out):
 
 def test_two_rank_replicas_and_max_over_ranks():
     world, port = 2, _free_port()
-    with mp.Manager() as m:
+    with mp.get_context("spawn").Manager() as m:
         out = m.dict()
         mp.spawn(_worker, args=(world, port, out), nprocs=world, join=True)
         res = dict(out)

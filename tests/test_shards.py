@@ -61,10 +61,11 @@ def _worker(rank, world, port, R, out):
 
 
 def _run(R, world=2):
-    mgr = mp.Manager()
-    out = mgr.dict()
-    mp.spawn(_worker, args=(world, _free_port(), R, out), nprocs=world, join=True)
-    return [out[r] for r in range(world)]
+    # the result store's server process is spawned too: forking a multi-threaded process can deadlock
+    with mp.get_context("spawn").Manager() as mgr:
+        out = mgr.dict()
+        mp.spawn(_worker, args=(world, _free_port(), R, out), nprocs=world, join=True)
+        return [out[r] for r in range(world)]
 
 
 def test_two_ranks_uneven_shards():
