@@ -233,11 +233,16 @@ int linqt_kubo_bastin_dev(linqt_session *s, const linqt_op *H, const linqt_op *o
  * loading the library holds until exit.
  *
  * Limits:
- *   - 3 Chebyshev blocks of N x Rc complex doubles (Rc = min(256, next power of two
- *     >= R)) plus reduction buffers must fit in that array; a larger solve is
- *     rejected with LINQT_ERR_INVALID and a message giving the size it needs.
+ *   - 2 Chebyshev blocks of N x Rc complex doubles (Rc = min(256, next power of two
+ *     >= R); R > 256 runs in chunks of 256 states) plus reduction buffers must fit in
+ *     that array; a larger solve is rejected with LINQT_ERR_INVALID and a message
+ *     giving the size it needs.
+ *   - cuda_stream must belong to H's device (LINQT_ERR_INVALID otherwise).
  *   - The first call on a device resolves the array's device address
- *     (cudaGetSymbolAddress); make that first call before any stream capture.
+ *     (cudaGetSymbolAddress) and keeps it for the life of the process; make that first
+ *     call before any stream capture.  The kept address does not survive a
+ *     cudaDeviceReset or a new primary context on that device: do not call this entry
+ *     point after either.
  *   - All calls share the one array, which keeps the last call's contents.  Calls
  *     that overlap on the GPU (two streams, or two host threads) race on it and must
  *     be serialised by the caller. */
@@ -251,6 +256,17 @@ int linqt_moments1d_noalloc(const linqt_op *H, const double *states_dev, int R, 
  * mu[2*M] in; E, dos of length *num_out (= truncated M) out. */
 int linqt_dos_from_moments(linqt_session *s, const double *mu, int M, int N, double band_width, double band_center,
                            double broad_meV, double *E, double *dos, int *num_out);
+/* Moments1D::ApplyJacksonKernel (src/chebyshev_moments1D.cpp:68-87) followed by the spectral
+ * function N/a sum_m delta_chebF(x_i, m) Re mu_m of
+ *   grid = LINQT_GRID_UNIFORM:   spectralFunctionFromChebmom (src/spectralFunctionFromChebmom.cpp:35-72):
+ *                                x_i = -1 + i 2/(num_div - 1), the sum as it is; num_div <= 0 means 30*M'.
+ *                                The end points x = +-1 divide by zero: non-finite, as in the reference;
+ *   grid = LINQT_GRID_CHEBYSHEV: spectralFunctionFromChebmom_FFTgrid (as linqt_dos_from_moments):
+ *                                x_i = cos(pi (i + 1/2)/num_div), its absolute value; num_div <= 0 means M'.
+ * M' = the moments kept by the Jackson kernel.  E = x a + c.  *num_out = num_div points written. */
+int linqt_spectral_function_from_moments(linqt_session *s, const double *mu, int M, int N, double band_width,
+                                         double band_center, double broad_meV, int grid, int num_div, double *E,
+                                         double *out, int *num_out);
 /* Moments2D::ApplyJacksonKernel (src/chebyshev_moments2D.cpp:87-117) followed by
  * kuboBastinFromChebmom (src/kuboBastinFromChebmom.cpp:35-81): num_div energies in
  * [-xbound, xbound] (num_div <= 0 means 30*M'), *num_out = num_div-1 points written. */

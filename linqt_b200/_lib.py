@@ -90,6 +90,8 @@ SIGNATURES = {
     "linqt_moments1d_noalloc": (c_int, [c_void_p, c_void_p, c_int, c_int, c_void_p, c_void_p]),
     "linqt_dos_from_moments": (c_int, [c_void_p, P_double, c_int, c_int, c_double, c_double, c_double, P_double,
                                        P_double, P_int]),
+    "linqt_spectral_function_from_moments": (c_int, [c_void_p, P_double, c_int, c_int, c_double, c_double, c_double,
+                                                     c_int, c_int, P_double, P_double, P_int]),
     "linqt_bastin_from_moments": (c_int, [c_void_p, P_double, c_int, c_int, c_int, c_double, c_double, c_double,
                                           c_double, c_int, P_double, P_double, P_int]),
     "linqt_kubo_from_moments": (c_int, [c_void_p, P_double, c_int, c_int, c_int, c_double, c_double, c_double, c_int,

@@ -7,6 +7,7 @@ Mirrors the reference operations on the hot path:
     moments2d                                                  chebyshev::CorrelationExpansionMoments
     kubo_fft                                                   chebyshev::Kubo_solver_FFT::compute
     dos_from_moments                                           spectralFunctionFromChebmom_FFTgrid
+    spectral_function_from_moments                             spectralFunctionFromChebmom{,_FFTgrid}
     bastin_from_moments                                        kuboBastinFromChebmom
 
 Host arrays are numpy; *_dev functions take device pointers (ints) or torch CUDA
@@ -366,6 +367,21 @@ def dos_from_moments(mu, N, band_width, band_center, broad_meV, session=None):
     n = ctypes.c_int()
     check(load().linqt_dos_from_moments(_sh(session), _dp(m.view(np.float64)), M, N, band_width, band_center,
                                         broad_meV, _dp(E), _dp(d), ctypes.byref(n)))
+    return E[: n.value], d[: n.value]
+
+
+def spectral_function_from_moments(mu, N, band_width, band_center, broad_meV, grid=0, num_div=0, session=None):
+    """Jackson kernel + spectral function: grid GRID_UNIFORM (spectralFunctionFromChebmom, 30 M'
+    points in [-1, 1], end points non-finite) or GRID_CHEBYSHEV (the _FFTgrid variant, M' points,
+    absolute values)."""
+    m = _c128(mu)
+    M = len(m)
+    n_max = num_div if num_div > 0 else (30 * M if grid == GRID_UNIFORM else M)  # M' <= M
+    E, d = np.zeros(n_max), np.zeros(n_max)
+    n = ctypes.c_int()
+    check(load().linqt_spectral_function_from_moments(_sh(session), _dp(m.view(np.float64)), M, N, band_width,
+                                                      band_center, broad_meV, grid, num_div, _dp(E), _dp(d),
+                                                      ctypes.byref(n)))
     return E[: n.value], d[: n.value]
 
 

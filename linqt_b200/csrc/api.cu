@@ -1575,6 +1575,30 @@ int linqt_dos_from_moments(linqt_session *s, const double *mu, int M, int N, dou
   });
 }
 
+int linqt_spectral_function_from_moments(linqt_session *s, const double *mu, int M, int N, double band_width,
+                                         double band_center, double broad_meV, int grid, int num_div, double *E,
+                                         double *out, int *num_out) {
+  return guarded([&] {
+    LQ_REQUIRE(mu && E && out && M > 0 && band_width > 0 && broad_meV > 0, "bad argument");
+    LQ_REQUIRE(grid == LINQT_GRID_UNIFORM || grid == LINQT_GRID_CHEBYSHEV,
+               "spectral function: grid must be LINQT_GRID_UNIFORM or LINQT_GRID_CHEBYSHEV");
+    Session *r = resolve(s);
+    const int Mt = jackson_cut(M, band_width, broad_meV);
+    const int nd = num_div > 0 ? num_div : (grid == LINQT_GRID_UNIFORM ? 30 * Mt : Mt);
+    LQ_REQUIRE(nd >= 2, "spectral function: at least two energies");
+    double2 *d_mu = (double2 *)r->get("dos_mu", sizeof(double2) * M);
+    double2 *d_muj = (double2 *)r->get("dos_muj", sizeof(double2) * M);
+    double *d_out = (double *)r->get("spec_out", sizeof(double) * 2 * (size_t)nd);
+    LQ_CUDA(cudaMemcpyAsync(d_mu, mu, sizeof(double2) * M, cudaMemcpyHostToDevice, r->stream));
+    jackson2d_dev(r, d_mu, 1, M, 1, Mt, d_muj);  // a 1 x M table: g(0, 1) = 1 on the first axis
+    spectral_grid(r, d_muj, Mt, N, band_width, band_center, grid, nd, d_out, d_out + nd);
+    LQ_CUDA(cudaMemcpyAsync(E, d_out, sizeof(double) * nd, cudaMemcpyDeviceToHost, r->stream));
+    LQ_CUDA(cudaMemcpyAsync(out, d_out + nd, sizeof(double) * nd, cudaMemcpyDeviceToHost, r->stream));
+    LQ_CUDA(cudaStreamSynchronize(r->stream));
+    if (num_out) *num_out = nd;
+  });
+}
+
 int linqt_bastin_from_moments(linqt_session *s, const double *mu, int M0, int M1, int N, double band_width,
                               double band_center, double broad_meV, double xbound, int num_div, double *E,
                               double *sigma, int *num_out) {

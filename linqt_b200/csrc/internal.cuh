@@ -289,6 +289,9 @@ void kubo_postprocess(Session *s, const double2 *acc, int R, int nump, int formu
 // reconstructions
 void dos_grid(Session *s, const double2 *mu, int M, int N, double band_width, double band_center, double *E,
               double *dos);
+// grid 0: num_div uniform points in [-1, 1], raw sums; grid 1: cos(pi (i+1/2)/num_div), |sum|
+void spectral_grid(Session *s, const double2 *mu, int M, int N, double band_width, double band_center, int grid,
+                   int num_div, double *E, double *out);
 // LinQT's post-processor sums (variant 0 Bastin, 1 Greenwood, 2 Bastin I, 3 Bastin II, 4 sea,
 // 5 surface) on a Jackson-damped device table; grid 0 uniform, 1 Chebyshev nodes, 2 ascending
 void energy_sums(Session *s, const double2 *mu, int M0, int M1, int N, double band_width, double band_center,
@@ -335,6 +338,7 @@ void cheb_series(Session *s, const DeviceOp &H, void *X, void *a, void *b, const
 void check_device_errors(Session *s);
 
 // small utilities (util.cu)
+void sum_chunks_stream(cudaStream_t st, double2 *d, int len, int nchunks);
 void sum_chunks(Session *s, double2 *d, int len, int nchunks);       // d[0:len] += sum_{c>0} d[c*len : ...]
 void add_into(Session *s, double2 *dst, const double2 *src, int len); // dst += src
 void block_to_states(Session *s, const void *blk, double2 *states, int N, int R, int Rpad);  // N x Rpad -> R x N

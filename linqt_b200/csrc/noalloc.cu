@@ -52,14 +52,6 @@ const DeviceScratch &setup_device(int dev) {
   return d;
 }
 
-__global__ void k_sum_chunk_dots(double2 *__restrict__ d, int len, int nchunks) {
-  for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < len; t += gridDim.x * blockDim.x) {
-    double2 s = d[t];
-    for (int c = 1; c < nchunks; ++c) s = cadd(s, d[(size_t)c * len + t]);
-    d[t] = s;
-  }
-}
-
 size_t align256(size_t x) { return (x + 255) & ~(size_t)255; }
 
 }  // namespace
@@ -80,6 +72,13 @@ extern "C" int linqt_moments1d_noalloc(const linqt_op *H, const double *states_d
     if (op.device != prev_dev) LQ_CUDA(cudaSetDevice(op.device));
     const DeviceScratch &ds = setup_device(op.device);
     cudaStream_t st = (cudaStream_t)stream;
+    if (st) {
+      int sdev = -1;
+      LQ_CUDA(cudaStreamGetDevice(st, &sdev));
+      if (sdev != op.device)
+        fail(LINQT_ERR_INVALID, "moments1d_noalloc: cuda_stream belongs to device " + std::to_string(sdev) +
+                                    ", the operator to device " + std::to_string(op.device));
+    }
 
     // Same block geometry and step count as linqt_moments1d with the identity operator
     // (doubling identities, block width = min(256, next power of two >= R)).
@@ -90,14 +89,15 @@ extern "C" int linqt_moments1d_noalloc(const linqt_op *H, const double *states_d
     const int N = op.n;
     const int grid = cheb_step_grid(ds.sm_count, N, Rc);
     const size_t blk = sizeof(double2) * (size_t)N * Rc;
+    // two Chebyshev blocks: the starting block (T_0, then every even T) and T_1 (every odd T)
     const size_t off_T = 0;
-    const size_t off_dots = align256(off_T + 3 * blk);
+    const size_t off_dots = align256(off_T + 2 * blk);
     const size_t off_part = align256(off_dots + sizeof(double2) * 2 * (size_t)steps * nchunks);
     const size_t off_cnt = align256(off_part + sizeof(double2) * 2 * (size_t)grid);
     const size_t need = off_cnt + 256;
     if (need > (size_t)LINQT_NOALLOC_SCRATCH_BYTES)
       fail(LINQT_ERR_INVALID, "moments1d_noalloc: this solve needs " + std::to_string(need) +
-                                  " bytes of scratch (3 Chebyshev blocks of N x " + std::to_string(Rc) +
+                                  " bytes of scratch (2 Chebyshev blocks of N x " + std::to_string(Rc) +
                                   " complex doubles plus reductions), above the fixed LINQT_NOALLOC_SCRATCH_BYTES = " +
                                   std::to_string((size_t)LINQT_NOALLOC_SCRATCH_BYTES) +
                                   "; use linqt_moments1d_dev for larger systems");
@@ -111,7 +111,7 @@ extern "C" int linqt_moments1d_noalloc(const linqt_op *H, const double *states_d
     LQ_CUDA(cudaMemsetAsync(dots, 0, sizeof(double2) * 2 * (size_t)steps * nchunks, st));
 
     for (int c = 0; c < nchunks; ++c) {
-      void *b1 = T + blk, *phi = T + 2 * blk;
+      void *phi = T, *b1 = T + blk;
       double2 *cd = dots + (size_t)2 * steps * c;
       const int w = std::min(Rc, R - c * Rc);
       states_to_block_stream(st, ds.sm_count, (const double2 *)states_dev + (size_t)c * Rc * N, phi, N, w, Rc);
@@ -130,10 +130,7 @@ extern "C" int linqt_moments1d_noalloc(const linqt_op *H, const double *states_d
         cur = a.y;
       }
     }
-    if (nchunks > 1) {
-      k_sum_chunk_dots<<<(2 * steps + 255) / 256, 256, 0, st>>>(dots, 2 * steps, nchunks);
-      LQ_LAUNCHED();
-    }
+    if (nchunks > 1) sum_chunks_stream(st, dots, 2 * steps, nchunks);
     moments1d_from_dots_stream(st, dots, steps, M, R, 2, (double2 *)mu_dev);
   } catch (const Error &e) {
     set_last_error(e.what());

@@ -25,13 +25,16 @@ __global__ void k_jackson2d(const double2 *__restrict__ mu, int M1, int M0t, int
   }
 }
 
-// DOS on E_i = cos(pi (i+1/2)/M): |N/a sum_m delta(E_i, m) Re mu_m|
-// (src/spectralFunctionFromChebmom_FFTgrid.cpp:40-75, delta_chebF of
-// include/chebyshev_coefficients.hpp:9-14).  One block per energy.
-__global__ void k_dos(const double2 *__restrict__ mu, int M, double N, double a, double bc, double *__restrict__ E,
-                      double *__restrict__ dos) {
+// The spectral function N/a sum_m delta(E_i, m) Re mu_m (delta_chebF of
+// include/chebyshev_coefficients.hpp:9-14) on num_div energies, one block per energy:
+//   grid 0: x_i = -1 + i 2/(num_div - 1), the sum as it is (src/spectralFunctionFromChebmom.cpp:35-72;
+//           the end points divide by zero and come out non-finite there and here);
+//   grid 1: x_i = cos(pi (i+1/2)/num_div), its absolute value
+//           (src/spectralFunctionFromChebmom_FFTgrid.cpp:35-75).
+__global__ void k_dos(const double2 *__restrict__ mu, int M, double N, double a, double bc, int grid, int num_div,
+                      double *__restrict__ E, double *__restrict__ dos) {
   const int i = blockIdx.x;
-  const double x = cos(M_PI * (i + 0.5) / M);
+  const double x = grid == 0 ? -1.0 + i * (2 * 1.0) / (num_div - 1) : cos(M_PI * (i + 0.5) / num_div);
   const double f0 = sqrt(1.0 - x * x), th = acos(x);
   double acc = 0.0;
   for (int m = threadIdx.x; m < M; m += blockDim.x) acc += cos(m * th) / f0 / M_PI * mu[m].x;
@@ -44,7 +47,8 @@ __global__ void k_dos(const double2 *__restrict__ mu, int M, double N, double a,
   }
   if (threadIdx.x == 0) {
     E[i] = x * a + bc;
-    dos[i] = fabs(sh[0] * N / a);
+    const double v = sh[0] * N / a;
+    dos[i] = grid == 0 ? v : fabs(v);
   }
 }
 
@@ -233,7 +237,13 @@ void jackson2d_dev(Session *s, const double2 *mu, int M0, int M1, int M0t, int M
 
 void dos_grid(Session *s, const double2 *mu, int M, int N, double band_width, double band_center, double *E,
               double *dos) {
-  k_dos<<<M, 256, 0, s->stream>>>(mu, M, (double)N, band_width / 2.0, band_center, E, dos);
+  spectral_grid(s, mu, M, N, band_width, band_center, 1, M, E, dos);
+}
+
+void spectral_grid(Session *s, const double2 *mu, int M, int N, double band_width, double band_center, int grid,
+                   int num_div, double *E, double *out) {
+  LQ_REQUIRE((grid == 0 || grid == 1) && num_div >= 2, "spectral function: bad grid");
+  k_dos<<<num_div, 256, 0, s->stream>>>(mu, M, (double)N, band_width / 2.0, band_center, grid, num_div, E, out);
   LQ_LAUNCHED();
 }
 

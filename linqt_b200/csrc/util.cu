@@ -28,8 +28,10 @@ __global__ void k_block_to_states(const double2 *__restrict__ blk, double2 *__re
 
 }  // namespace
 
-void sum_chunks(Session *s, double2 *d, int len, int nchunks) {
-  k_sum_chunks<<<(len + 255) / 256, 256, 0, s->stream>>>(d, len, nchunks);
+void sum_chunks(Session *s, double2 *d, int len, int nchunks) { sum_chunks_stream(s->stream, d, len, nchunks); }
+
+void sum_chunks_stream(cudaStream_t st, double2 *d, int len, int nchunks) {
+  k_sum_chunks<<<(len + 255) / 256, 256, 0, st>>>(d, len, nchunks);
   LQ_LAUNCHED();
 }
 

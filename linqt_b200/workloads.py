@@ -11,6 +11,7 @@ Kubo-Bastin graphene workload:
     python -m linqt_b200.workloads lr_layouts    # L/R recursion of the 2D moments: CSR vs autotuned
     python -m linqt_b200.workloads cubic_width   # cubic L=200 DOS recursion GB/s: CSR vs autotuned, R = 64, 8
     python -m linqt_b200.workloads moments2d --cells 32 --moments 1024 --vectors 32   # one profiled 2D solve
+    python -m linqt_b200.workloads recur1d --side 100 --vectors 64 --moments 16 --precision 0  # one 1D recursion
     python -m linqt_b200.workloads time_corr     # <V(t)V> of graphene 128x128, R=16, M=512, 40 time steps
     python -m linqt_b200.workloads supercell     # supercell CSR assembly (wannier2sparse) of two Wannier models
 
@@ -284,6 +285,29 @@ def run_cubic_width(L, R, M, reps):
     return out
 
 
+def run_recur1d_once(L, R, M, prec, fmt=0):
+    """One warm-up and one timed 1D DOS recursion on the cubic Anderson lattice L^3 (the
+    case the 1D recursion kernel is profiled on: one persistent launch per solve)."""
+    import torch
+    from .core import random_phase_states_dev
+    N, H = lattices.cubic_lattice(L, 1.0, 2.0, 41)
+    sess = Session()
+    sess.set_stream(torch.cuda.current_stream())
+    Hg = Operator.from_csr(N, *H, session=sess)
+    Hg.rescale_to_chebyshev(2 * 1.05 * 7.0, 0.0)
+    del H
+    st = torch.empty(2 * R * N, dtype=torch.float64, device="cuda")
+    random_phase_states_dev(N, R, 45, st, session=sess)
+    mu = torch.zeros(2 * M, dtype=torch.float64, device="cuda")
+    o = make_opts(precision=prec, fmt=fmt, block_width=R)
+    ms = _timed(lambda: moments1d_dev(Hg, None, st, R, M, mu, opts=o, session=sess), 1, torch)
+    esz = 16 if prec == PREC_FP64 else 8
+    by = Hg.nnz * 20 + 4 * (N + 1) + 3 * esz * N * R
+    return {"workload": "recur1d_cubic_%d" % L, "N": N, "R": R, "M": M, "precision": prec, "format": fmt,
+            "ms_per_solve": ms, "recursion_GBps": (M + 1) // 2 * by / (ms * 1e-3) / 1e9,
+            "bytes_per_step": by}
+
+
 def run_moments2d_once(Lc, R, M, prec):
     """One warm-up and one timed Kane-Mele spin 2D-moment solve with per-phase times (the
     case the contraction kernels are profiled on)."""
@@ -358,13 +382,15 @@ def run_supercell(orbitals, reach, L, op, reps):
 def main(argv=None):
     ap = argparse.ArgumentParser()
     ap.add_argument("workload", choices=["dos", "cubic", "cubic_full", "spin", "layouts", "realisations",
-                                         "lr_layouts", "cubic_width", "moments2d", "time_corr", "supercell"])
+                                         "lr_layouts", "cubic_width", "moments2d", "recur1d", "time_corr", "supercell"])
     ap.add_argument("--precision", type=int, default=PREC_MIXED, help="moments2d: LINQT_PREC_* value")
     ap.add_argument("--reps", type=int, default=5)
     ap.add_argument("--cells", type=int, default=64, help="spin: Kane-Mele cells per side")
     ap.add_argument("--moments", type=int, default=512, help="spin: M")
     ap.add_argument("--vectors", type=int, default=8, help="spin: R")
     ap.add_argument("--realisations", type=int, default=0, help="cubic_full: 0 autotuned, 1 stacked, 2 separate")
+    ap.add_argument("--side", type=int, default=100, help="recur1d: cubic lattice side L")
+    ap.add_argument("--format", type=int, default=0, help="recur1d: LINQT_FORMAT_* value")
     a = ap.parse_args(argv)
     if a.workload == "dos":
         N, H = lattices.square_lattice(256, 1.0, 1.0, 11)
@@ -386,6 +412,8 @@ def main(argv=None):
         r = run_supercell(4, 1, 2048, "HAM", a.reps)
     elif a.workload == "time_corr":
         r = run_time_corr(128, 16, 512, 40, 1.0, a.reps)
+    elif a.workload == "recur1d":
+        r = run_recur1d_once(a.side, a.vectors, a.moments, a.precision, a.format)
     elif a.workload == "moments2d":
         r = run_moments2d_once(a.cells, a.vectors, a.moments, a.precision)
     elif a.workload == "cubic_full":

@@ -471,6 +471,26 @@ int lo_dos_fftgrid(const double *mu, int M, int N, double band_width, double ban
   return 0;
 }
 
+/* src/spectralFunctionFromChebmom.cpp:35-72 (grid 0: num_div points
+ * -1 + i*2/(num_div-1), the value as summed; the end points divide by zero) and
+ * src/spectralFunctionFromChebmom_FFTgrid.cpp:35-75 (grid 1: cos(pi (i+1/2)/num_div), its
+ * absolute value).  mu: the Jackson-damped moments, M of them. */
+int lo_spectral_function(const double *mu, int M, int N, double band_width, double band_center, int grid,
+                         int num_div, double *E, double *out) {
+  if (num_div < 2 || grid < 0 || grid > 1) return -1;
+  const double a = band_width / 2.0;
+#pragma omp parallel for schedule(static)
+  for (int i = 0; i < num_div; i++) {
+    const double x = grid == 0 ? -1.0 + i * (2 * 1.0) / (num_div - 1) : cos(M_PI * (i + 0.5) / num_div);
+    double acc = 0.0;
+    for (int m = 0; m < M; m++) acc += delta_chebF(x, m) * mu[2 * m];
+    acc *= N / a;
+    E[i] = x * a + band_center;
+    out[i] = grid == 0 ? acc : fabs(acc);
+  }
+  return 0;
+}
+
 /* src/kuboBastinFromChebmom.cpp:35-81 (num_div = 30*M there, xbound 0.99; the
  * golden files of the reference were written with xbound 0.9) */
 int lo_bastin_from_moments(const double *mu, int M0, int M1, int N, double band_width, double band_center,

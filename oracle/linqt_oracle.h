@@ -57,6 +57,11 @@ int lo_jackson2d(double *mu, int M0, int M1, double band_width, double b0, doubl
 /* DOS on the Chebyshev grid E_i = cos(pi(i+1/2)/M)  (src/spectralFunctionFromChebmom_FFTgrid.cpp:35-75).
  * E[M] (physical energies), dos[M] = |N/a sum_m delta(E_i,m) Re mu_m| */
 int lo_dos_fftgrid(const double *mu, int M, int N, double band_width, double band_center, double *E, double *dos);
+/* spectralFunctionFromChebmom (grid 0: num_div uniform points in [-1, 1], raw sums) and
+ * spectralFunctionFromChebmom_FFTgrid (grid 1: cos(pi (i+1/2)/num_div), absolute values)
+ * on Jackson-damped moments mu[M]: E[num_div], out[num_div]. */
+int lo_spectral_function(const double *mu, int M, int N, double band_width, double band_center, int grid,
+                         int num_div, double *E, double *out);
 
 /* Kubo-Bastin sigma(E) from a Jackson-damped 2D table (src/kuboBastinFromChebmom.cpp:35-81).
  * num_div energies in [-xbound, xbound]; writes num_div-1 points E[i], sigma[i]. */

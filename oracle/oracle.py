@@ -59,6 +59,8 @@ def lib():
         L.lo_jackson2d.argtypes = [dp, ctypes.c_int, ctypes.c_int, ctypes.c_double, ctypes.c_double,
                                    ctypes.c_double, ip, ip]
         L.lo_dos_fftgrid.argtypes = [dp, ctypes.c_int, ctypes.c_int, ctypes.c_double, ctypes.c_double, dp, dp]
+        L.lo_spectral_function.argtypes = [dp, ctypes.c_int, ctypes.c_int, ctypes.c_double, ctypes.c_double,
+                                           ctypes.c_int, ctypes.c_int, dp, dp]
         L.lo_bastin_from_moments.argtypes = [dp, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_double,
                                              ctypes.c_double, ctypes.c_double, ctypes.c_int, dp, dp]
         L.lo_kubo_from_moments.argtypes = [ctypes.c_int, ctypes.c_int, dp, ctypes.c_int, ctypes.c_int, ctypes.c_int,
@@ -194,6 +196,18 @@ def dos_fftgrid(mu, N, band_width, band_center):
     M = len(m)
     E, d = np.zeros(M), np.zeros(M)
     lib().lo_dos_fftgrid(_dp(m.view(np.float64)), M, N, band_width, band_center, _dp(E), _dp(d))
+    return E, d
+
+
+def spectral_function(mu, N, band_width, band_center, grid=0, num_div=None):
+    """spectralFunctionFromChebmom (grid 0, num_div = 30 M) or its _FFTgrid variant (grid 1,
+    num_div = M) on Jackson-damped moments."""
+    m = np.ascontiguousarray(mu, dtype=np.complex128)
+    M = len(m)
+    n = num_div or (30 * M if grid == 0 else M)
+    E, d = np.zeros(n), np.zeros(n)
+    with np.errstate(all="ignore"):
+        lib().lo_spectral_function(_dp(m.view(np.float64)), M, N, band_width, band_center, grid, n, _dp(E), _dp(d))
     return E, d
 
 

@@ -47,7 +47,9 @@ def read_dat(path):
 
 
 def main():
-    ref = sys.argv[1] if len(sys.argv) > 1 else "/root/reference"
+    ref = sys.argv[1] if len(sys.argv) > 1 else os.environ.get("LINQT_REF")
+    if not ref:
+        sys.exit("usage: python tests/golden/make_golden.py REFERENCE_ROOT  (or set LINQT_REF)")
     d = os.path.join(ref, "examples/utilities/wannier2sparse/linear_chain")
     out = {}
     for op in ("HAM", "VX"):

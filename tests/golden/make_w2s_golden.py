@@ -25,7 +25,9 @@ import tempfile
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 ROOT = os.path.dirname(os.path.dirname(HERE))
-REF = sys.argv[1] if len(sys.argv) > 1 else "/root/reference"
+REF = sys.argv[1] if len(sys.argv) > 1 else os.environ.get("LINQT_REF")
+if not REF:
+    sys.exit("usage: python tests/golden/make_w2s_golden.py REFERENCE_CHECKOUT  (or set LINQT_REF)")
 TOOL = os.path.join(ROOT, "oracle", "_ref", "wannier2sparse")
 OUT = os.path.join(HERE, "w2s")
 

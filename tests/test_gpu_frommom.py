@@ -52,3 +52,24 @@ def test_bastin_entry_point_is_the_bastin_variant(table):
     E1, s1 = lq.bastin_from_moments(mu, N, bw, bc, BROAD, xbound=0.99)
     E2, s2 = lq.kubo_from_moments(mu, N, bw, bc, BROAD, variant="bastin", xbound=0.99)
     assert np.array_equal(E1, E2) and np.array_equal(s1, s2)
+
+
+@pytest.mark.parametrize("grid,num_div", [(0, 0), (1, 0), (0, 777)])
+def test_spectral_function_from_moments(oracle_lib, grid, num_div):
+    """spectralFunctionFromChebmom (uniform grid, raw sums, end points non-finite) and its
+    _FFTgrid variant (absolute values) against the oracle, which is pinned to both reference
+    drivers (tests/test_oracle_frommom_vs_ref.py)."""
+    N, H = lattices.square_lattice(24, t=1.0, W=1.0, seed=11)
+    bw, bc = 2 * 1.05 * 4.5, 0.1
+    Hg = lq.Operator.from_csr(N, *H)
+    Hg.rescale_to_chebyshev(bw, bc)
+    mu = lq.moments1d(Hg, None, lattices.random_phase_states(N, 3, seed=12), 300)
+    E, out = lq.spectral_function_from_moments(mu, N, bw, bc, 40.0, grid=grid, num_div=num_div)
+    muj = oracle_lib.jackson1d(mu, bw, 40.0)
+    Eo, oo = oracle_lib.spectral_function(muj, N, bw, bc, grid=grid, num_div=num_div or None)
+    assert len(E) == len(Eo) == (num_div or (30 * len(muj) if grid == 0 else len(muj)))
+    assert np.abs(E - Eo).max() <= 1e-14 * np.abs(Eo).max()
+    fin = np.isfinite(oo)
+    assert np.array_equal(fin, np.isfinite(out))
+    assert fin.sum() == len(E) - (2 if grid == 0 else 0)
+    assert np.abs(out[fin] - oo[fin]).max() <= 1e-11 * np.abs(oo[fin]).max()

@@ -82,3 +82,47 @@ def test_bastin_II_and_sea_sums_vs_reference(oracle_lib, table, name, variant):
     assert np.all(np.isfinite(o))
     assert np.abs(E - ref[:, 0]).max() <= 1e-12 * np.abs(E).max()
     assert np.abs(o - ref[:, 1]).max() <= 1e-10 * np.abs(ref[:, 1]).max()
+
+
+# spectralFunctionFromChebmom (uniform grid of 30 M' points in [-1, 1], raw sums, the end
+# points divide by zero) and spectralFunctionFromChebmom_FFTgrid (M' Chebyshev points,
+# absolute values): driver, output suffix, grid
+SPECTRAL = [("inline_spectralFunctionFromChebmom", "JACKSON.dat", 0),
+            ("inline_spectralFunctionFromChebmom_FFTgrid", "JACKSON_FFTgrid.dat", 1)]
+
+
+@pytest.fixture(scope="module")
+def table1d(oracle_lib, tmp_path_factory):
+    """Square-lattice DOS moments (R = 2, M = 200) written as LinQT's .chebmom1D."""
+    N, H = lattices.square_lattice(16, t=1.0, W=1.0, seed=11)
+    bw, bc = 2 * 1.05 * 4.5, 0.0
+    Ho = oracle_lib.Op(*H).rescale(2 / bw, -bc / (bw / 2))
+    mu = oracle_lib.moments1d(Ho, None, lattices.random_phase_states(N, 2, seed=12), 200)
+    d = tmp_path_factory.mktemp("frommom1d")
+    path = str(d / "sqDOS.chebmom1D")
+    formats.write_chebmom1d(path, N, bw, bc, mu)
+    n, bw2, bc2, mu2 = formats.read_chebmom1d(path)  # what the drivers read (15 digits)
+    return d, path, n, bw2, bc2, oracle_lib.jackson1d(mu2, bw2, BROAD)
+
+
+@pytest.mark.parametrize("exe,suffix,grid", SPECTRAL)
+def test_spectral_function_vs_reference_driver(oracle_lib, table1d, exe, suffix, grid):
+    d, path, n, bw, bc, muj = table1d
+    _run_driver(exe, d, path)
+    ref = np.loadtxt(str(d / ("meansqDOS" + suffix)))
+    E, out = oracle_lib.spectral_function(muj, n, bw, bc, grid=grid)
+    assert ref.shape == (len(E), 2)
+    assert np.allclose(E, ref[:, 0], rtol=1e-5, atol=1e-5 * np.abs(E).max())
+    fin = np.isfinite(ref[:, 1])
+    assert np.array_equal(fin, np.isfinite(out))  # the same points divide by zero
+    assert fin.sum() >= len(E) - 2
+    scale = np.abs(ref[fin, 1]).max()
+    assert np.abs(out[fin] - ref[fin, 1]).max() <= 2e-6 * scale
+
+
+def test_dos_fftgrid_equals_spectral_function_fftgrid(oracle_lib, table1d):
+    """lo_dos_fftgrid (the checker of linqt_dos_from_moments) is the _FFTgrid driver's sum."""
+    d, path, n, bw, bc, muj = table1d
+    E1, d1 = oracle_lib.dos_fftgrid(muj, n, bw, bc)
+    E2, d2 = oracle_lib.spectral_function(muj, n, bw, bc, grid=1)
+    assert np.array_equal(E1, E2) and np.array_equal(d1, d2)

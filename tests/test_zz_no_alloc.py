@@ -23,7 +23,9 @@ def _rel(a, b):
     return float(np.abs(a - b).max() / np.abs(b).max())
 
 
-@pytest.mark.parametrize("L,R,M", [(24, 3, 200), (64, 16, 101)])
+# (24, 300, 64): R > 256 and not a multiple of 256, so the states run as two chunks of
+# 256 columns, the second zero-padded, and the chunks' dot products are summed.
+@pytest.mark.parametrize("L,R,M", [(24, 3, 200), (64, 16, 101), (24, 300, 64)])
 def test_noalloc_matches_regular_entry_point_twice(L, R, M):
     torch = pytest.importorskip("torch")
     N, Hc = lattices.square_lattice(L, t=1.0, W=1.0, seed=11)
@@ -53,7 +55,7 @@ def test_noalloc_rejects_solves_beyond_its_scratch():
     N, Hc = lattices.square_lattice(300, t=1.0, W=1.0, seed=11)  # 90,000 sites
     H = lq.Operator.from_csr(N, *Hc)
     H.rescale_to_chebyshev(2 * 1.05 * 4.5, 0.0)
-    R, M = 32, 16  # 3 blocks x 90,000 x 32 x 16 B = 138 MB > 32 MiB
+    R, M = 32, 16  # 2 blocks x 90,000 x 32 x 16 B = 92 MB > 32 MiB
     st_dev = torch.zeros(2 * R * N, dtype=torch.float64, device="cuda")
     out = torch.zeros(2 * M, dtype=torch.float64, device="cuda")
     with pytest.raises(lq.LinqtError) as e:
