@@ -108,6 +108,12 @@ int linqt_session_trim(linqt_session *s);
  * reconstruction, [3] other; launches[0..3] the kernel launches per phase. */
 int linqt_session_phase_times(linqt_session *s, double ms[4], long launches[4], int reset);
 int linqt_session_enable_timing(linqt_session *s, int on);
+/* Fault injection for tests of the timeout path (no counterpart in the reference).  From the
+ * next solve on, the grid barriers of the session's persistent kernels wait for
+ * extra_arrivals CTAs that were never launched and give up after spin_limit polls (0: the
+ * normal limit of 2^24); the kernels then return early and the solve reports
+ * LINQT_ERR_TIMEOUT.  (0, 0) restores normal barriers.  No other session is affected. */
+int linqt_session_inject_barrier_timeout(linqt_session *s, int extra_arrivals, long long spin_limit);
 /* Instantiated CUDA graphs held by the session (opts.use_graphs) and solves launched from them. */
 int linqt_session_graph_stats(linqt_session *s, int *graphs, long *replays);
 
@@ -144,6 +150,27 @@ int linqt_moments1d(linqt_session *s, const linqt_op *H, const linqt_op *op, con
                     const linqt_opts *opts, double *mu);
 int linqt_moments1d_dev(linqt_session *s, const linqt_op *H, const linqt_op *op, const double *states_dev, int R,
                         int M, const linqt_opts *opts, double *mu_dev);
+
+/* chebyshev::SpectralMoments_nonOrth (src/chebyshev_solver.cpp:203-229) with
+ * Moments1D_nonOrth::SetInitVectors_nonOrthogonal / Iterate_nonOrthogonal
+ * (src/chebyshev_moments.cpp:63-153): 1D moments in a non-orthogonal basis with overlap
+ * matrix S, mu[2*M] = sum_r (2/R)(1/2)^{[m=0]} <r|T_m> with
+ *   T_0 = S^-1 r (op = NULL) or op S^-1 r,  T_1 = S^-1 H T_0,  T_{m+1} = 2 S^-1 H T_m - T_{m-1}.
+ * Each S^-1 is a BiCGSTAB solve as linalg::orthogonalize (src/mkl_linear_algebra.cpp:100-132)
+ * runs it with Eigen 3.4: Jacobi preconditioner, x0 = 0, stop when |r| <= tol |b| or after
+ * maxit iterations (the reference: tol = 1e-4, maxit = 2000).  S is used as its handle holds
+ * it: the reference hands the solver the CSR arrays as the file stores them (the upper
+ * triangle), so create S with LINQT_STORAGE_GENERAL from those arrays to reproduce it.
+ * FP64 only.  iterations (may be NULL) gets the BiCGSTAB iterations summed over all solves
+ * (the _dev form synchronises the session stream when it is given).  The reference solves
+ * twice more per state after the last moment it uses; those solves do not reach mu and are
+ * not run. */
+int linqt_moments1d_nonorth(linqt_session *s, const linqt_op *H, const linqt_op *op, const linqt_op *S,
+                            const double *states, int R, int M, double tol, int maxit, const linqt_opts *opts,
+                            double *mu, long *iterations);
+int linqt_moments1d_nonorth_dev(linqt_session *s, const linqt_op *H, const linqt_op *op, const linqt_op *S,
+                                const double *states_dev, int R, int M, double tol, int maxit,
+                                const linqt_opts *opts, double *mu_dev, long *iterations);
 
 /* Disorder realisations batched in one recursion (no reference counterpart: LinQT runs
  * one Hamiltonian per process).  H[0..S) share one sparsity pattern (e.g. Anderson disorder
@@ -322,6 +349,9 @@ int linqt_server_submit(linqt_server *srv, const linqt_request *req, long *ticke
 /* status: 0 pending, 1 running, 2 done, <0 error code; latency in ms once done */
 int linqt_server_poll(linqt_server *srv, long ticket, int *status, double *latency_ms);
 int linqt_server_wait_all(linqt_server *srv);
+/* Withdraw a request that has not started: its status becomes LINQT_ERR_CANCELLED and mu_out is
+ * not written.  LINQT_ERR_INVALID (and nothing changes) once it runs or has finished. */
+int linqt_server_cancel(linqt_server *srv, long ticket);
 /* forget a finished request (its ticket becomes unknown); LINQT_ERR_INVALID while it is queued or running */
 int linqt_server_release(linqt_server *srv, long ticket);
 int linqt_server_destroy(linqt_server *srv);

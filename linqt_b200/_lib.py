@@ -87,6 +87,11 @@ SIGNATURES = {
                                   c_double, ctypes.POINTER(Opts), P_double, P_double, P_double, P_double]),
     "linqt_kubo_bastin_dev": (c_int, [c_void_p, c_void_p, c_void_p, c_void_p, c_void_p, c_int, c_int, c_int,
                                       c_double, c_double, ctypes.POINTER(Opts), c_void_p, c_void_p]),
+    "linqt_session_inject_barrier_timeout": (c_int, [c_void_p, c_int, ctypes.c_longlong]),
+    "linqt_moments1d_nonorth": (c_int, [c_void_p, c_void_p, c_void_p, c_void_p, P_double, c_int, c_int, c_double,
+                                        c_int, ctypes.POINTER(Opts), P_double, P_long]),
+    "linqt_moments1d_nonorth_dev": (c_int, [c_void_p, c_void_p, c_void_p, c_void_p, c_void_p, c_int, c_int,
+                                            c_double, c_int, ctypes.POINTER(Opts), c_void_p, P_long]),
     "linqt_moments1d_noalloc": (c_int, [c_void_p, c_void_p, c_int, c_int, c_void_p, c_void_p]),
     "linqt_dos_from_moments": (c_int, [c_void_p, P_double, c_int, c_int, c_double, c_double, c_double, P_double,
                                        P_double, P_int]),
@@ -103,6 +108,7 @@ SIGNATURES = {
     "linqt_server_poll": (c_int, [c_void_p, c_long, P_int, P_double]),
     "linqt_server_wait_all": (c_int, [c_void_p]),
     "linqt_server_release": (c_int, [c_void_p, c_long]),
+    "linqt_server_cancel": (c_int, [c_void_p, c_long]),
     "linqt_server_destroy": (c_int, [c_void_p]),
     "linqt_tbmodel_load": (c_int, [ctypes.c_char_p, ctypes.POINTER(c_void_p)]),
     "linqt_tbmodel_destroy": (c_int, [c_void_p]),

@@ -4,6 +4,7 @@ Mirrors the reference operations on the hot path:
 
     Operator.from_csr / Operator.rescale / Operator.multiply   SparseMatrixType (include/sparse_matrix.hpp)
     moments1d                                                  chebyshev::SpectralMoments
+    moments1d_nonorth                                          chebyshev::SpectralMoments_nonOrth
     moments2d                                                  chebyshev::CorrelationExpansionMoments
     kubo_fft                                                   chebyshev::Kubo_solver_FFT::compute
     dos_from_moments                                           spectralFunctionFromChebmom_FFTgrid
@@ -104,6 +105,11 @@ class Session:
         g, r = ctypes.c_int(), ctypes.c_long()
         check(load().linqt_session_graph_stats(self.h, ctypes.byref(g), ctypes.byref(r)))
         return g.value, r.value
+
+    def inject_barrier_timeout(self, extra_arrivals=1, spin_limit=1024):
+        """Test hook: make this session's grid barriers wait for CTAs never launched (the next
+        solve then fails with LINQT_ERR_TIMEOUT); (0, 0) restores them."""
+        check(load().linqt_session_inject_barrier_timeout(self.h, extra_arrivals, spin_limit))
 
     def phase_times(self, reset=False):
         """(ms[4], launches[4]) for recursion, contraction, FFT, other."""
@@ -215,6 +221,32 @@ def moments1d(H, op, states, M, opts=None, session=None):
     check(load().linqt_moments1d(_sh(session), H.h, _oph(op), _dp(st.view(np.float64)), R, M, ctypes.byref(o),
                                  _dp(mu.view(np.float64))))
     return mu
+
+
+def moments1d_nonorth(H, op, S, states, M, tol=1e-4, maxit=2000, opts=None, session=None):
+    """chebyshev::SpectralMoments_nonOrth: mu[M] in a non-orthogonal basis with overlap S (an
+    Operator; build it with storage=STORAGE_GENERAL from the CSR file's arrays to reproduce
+    the reference, which solves with the stored triangle).  Returns (mu, BiCGSTAB iterations
+    summed over all solves)."""
+    st = np.atleast_2d(_c128(states))
+    R = st.shape[0]
+    mu = np.zeros(M, np.complex128)
+    its = ctypes.c_long()
+    o = opts or make_opts()
+    check(load().linqt_moments1d_nonorth(_sh(session), H.h, _oph(op), S.h, _dp(st.view(np.float64)), R, M, tol,
+                                         maxit, ctypes.byref(o), _dp(mu.view(np.float64)), ctypes.byref(its)))
+    return mu, its.value
+
+
+def moments1d_nonorth_dev(H, op, S, states_dev, R, M, mu_dev, tol=1e-4, maxit=2000, opts=None, session=None,
+                          iterations=False):
+    """Device-pointer form; with iterations=True it synchronises and returns the iteration count."""
+    its = ctypes.c_long()
+    o = opts or make_opts()
+    check(load().linqt_moments1d_nonorth_dev(_sh(session), H.h, _oph(op), S.h, ctypes.c_void_p(_ptr(states_dev)), R,
+                                             M, tol, maxit, ctypes.byref(o), ctypes.c_void_p(_ptr(mu_dev)),
+                                             ctypes.byref(its) if iterations else None))
+    return its.value if iterations else None
 
 
 def random_phase_states_dev(N, R, seed, out_dev, session=None):

@@ -1119,6 +1119,17 @@ int linqt_session_enable_timing(linqt_session *s, int on) {
   return guarded([&] { resolve(s)->timing = on != 0; });
 }
 
+int linqt_session_inject_barrier_timeout(linqt_session *s, int extra_arrivals, long long spin_limit) {
+  return guarded([&] {
+    LQ_REQUIRE(s, "NULL session");
+    LQ_REQUIRE(extra_arrivals >= 0 && spin_limit >= 0, "bad argument");
+    Session *r = resolve(s);
+    r->inject_extra = extra_arrivals;
+    r->inject_limit = spin_limit;
+    r->barrier_cfg_dirty = true;
+  });
+}
+
 int linqt_session_graph_stats(linqt_session *s, int *graphs, long *replays) {
   return guarded([&] {
     Session *r = resolve(s);
@@ -1152,6 +1163,9 @@ int linqt_csr_create(linqt_session *s, int n, const int *rowptr, const int *col,
     LQ_REQUIRE(rowptr[0] == 0, "rowptr[0] must be 0");
     for (int i = 0; i < n; ++i) LQ_REQUIRE(rowptr[i + 1] >= rowptr[i], "rowptr must be non-decreasing");
     const long nnz_in = rowptr[n];
+    for (long k = 0; k < nnz_in; ++k)  // all host-side checks before the device is touched
+      LQ_REQUIRE(col[k] >= 0 && col[k] < n, "column index " + std::to_string(col[k]) + " out of range at entry " +
+                                                std::to_string(k));
     Session *r = resolve(s);
     std::unique_ptr<linqt_op> h(new linqt_op);
     DeviceOp &d = h->op;
@@ -1321,6 +1335,51 @@ int linqt_moments1d(linqt_session *s, const linqt_op *H, const linqt_op *op, con
     LQ_CUDA(cudaMemcpyAsync(mu, d_mu, sizeof(double2) * (size_t)M, cudaMemcpyDeviceToHost, r->stream));
     LQ_CUDA(cudaStreamSynchronize(r->stream));
     check_device_errors(r);
+  });
+}
+
+static void check_nonorth(const linqt_op *H, const linqt_op *S, const linqt_opts *opts, double tol, int maxit) {
+  check_op(H, "H");
+  check_op(S, "S");
+  LQ_REQUIRE(tol > 0 && maxit > 0, "moments1d_nonorth: tolerance and iteration limit must be positive");
+  if (opts && opts->precision != LINQT_PREC_FP64)
+    fail(LINQT_ERR_UNSUPPORTED, "moments1d_nonorth: FP64 only (the BiCGSTAB solves run in FP64)");
+}
+
+int linqt_moments1d_nonorth_dev(linqt_session *s, const linqt_op *H, const linqt_op *op, const linqt_op *S,
+                                const double *states_dev, int R, int M, double tol, int maxit,
+                                const linqt_opts *opts, double *mu_dev, long *iterations) {
+  return guarded([&] {
+    check_nonorth(H, S, opts, tol, maxit);
+    LQ_REQUIRE(states_dev && mu_dev && R > 0 && M > 0, "bad argument");
+    Session *r = resolve(s);
+    long long its = 0;
+    moments1d_nonorth_dev(r, H->op, dop(op), S->op, (const double2 *)states_dev, R, M, tol, maxit,
+                          (double2 *)mu_dev, iterations ? &its : nullptr);
+    if (iterations) {
+      check_device_errors(r);
+      *iterations = (long)its;
+    }
+  });
+}
+
+int linqt_moments1d_nonorth(linqt_session *s, const linqt_op *H, const linqt_op *op, const linqt_op *S,
+                            const double *states, int R, int M, double tol, int maxit, const linqt_opts *opts,
+                            double *mu, long *iterations) {
+  return guarded([&] {
+    check_nonorth(H, S, opts, tol, maxit);
+    LQ_REQUIRE(states && mu && R > 0 && M > 0, "bad argument");
+    Session *r = resolve(s);
+    const size_t sb = sizeof(double2) * (size_t)R * H->op.n;
+    double2 *d_st = (double2 *)r->get("io_states", sb);
+    double2 *d_mu = (double2 *)r->get("io_mu", sizeof(double2) * (size_t)M);
+    LQ_CUDA(cudaMemcpyAsync(d_st, states, sb, cudaMemcpyHostToDevice, r->stream));
+    long long its = 0;
+    moments1d_nonorth_dev(r, H->op, dop(op), S->op, d_st, R, M, tol, maxit, d_mu, &its);
+    LQ_CUDA(cudaMemcpyAsync(mu, d_mu, sizeof(double2) * (size_t)M, cudaMemcpyDeviceToHost, r->stream));
+    LQ_CUDA(cudaStreamSynchronize(r->stream));
+    check_device_errors(r);
+    if (iterations) *iterations = (long)its;
   });
 }
 

@@ -205,6 +205,12 @@ struct Session {
   int sm_count = 148;
   size_t hbm_budget = 0;  // chunking budget; 0 = what the device has free
   bool barrier_used = false;  // a persistent kernel ran since the last error check
+  // fault injection for tests (linqt_session_inject_barrier_timeout): grid barriers await
+  // inject_extra more CTAs than launched and give up after inject_limit polls
+  int inject_extra = 0;
+  long long inject_limit = 0;
+  bool barrier_cfg_dirty = false;
+  void *barrier_cfg_ptr = nullptr;
   // opts.use_graphs: solves replayed from instantiated CUDA graphs, by call key.  A graph holds
   // the workspace addresses it was captured with, so every workspace reallocation drops them.
   bool capturing = false;
@@ -336,6 +342,18 @@ void recur_1d(Session *s, const DeviceOp &H, const void *phi, void *x0, void *b1
 void cheb_series(Session *s, const DeviceOp &H, void *X, void *a, void *b, const double2 *coef, int K, int R);
 // after a stream synchronisation: fail with LINQT_ERR_TIMEOUT if a persistent kernel's barrier gave up
 void check_device_errors(Session *s);
+// chebyshev::SpectralMoments_nonOrth on the device (nonorth.cu): mu[M]; iterations (may be
+// NULL; then nothing synchronises) gets the BiCGSTAB iterations summed over all solves
+void moments1d_nonorth_dev(Session *s, const DeviceOp &H, const DeviceOp *op, const DeviceOp &S,
+                           const double2 *states, int R, int M, double tol, int maxit, double2 *mu,
+                           long long *iterations);
+// the session's grid barrier for the next persistent launch (count and generation reset on
+// the session stream; the error flag stays until check_device_errors reads it)
+struct GridBarrier;
+GridBarrier *barrier_for(Session *s);
+// occupancy-sized cooperative grid and a launch through the device's cooperative lane (recur.cu)
+int coop_grid(const void *func, int sm_count, long max_blocks, size_t smem);
+void coop_launch(Session *s, const void *f, int grid, void **args, size_t smem);
 
 // small utilities (util.cu)
 void sum_chunks_stream(cudaStream_t st, double2 *d, int len, int nchunks);

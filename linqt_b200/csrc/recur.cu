@@ -1,4 +1,5 @@
 // Persistent recursion kernels: a whole Chebyshev recursion in one cooperative launch.
+// (The grid barrier between steps is grid_sync.cuh's.)
 //
 // One launch per recursion step (spmm.cu) costs a launch gap and a cold start per step.
 // At LinQT's sizes a step is 1-10 us of memory traffic, so the gaps are a large part of
@@ -24,6 +25,7 @@
 #include <memory>
 #include <unordered_map>
 
+#include "grid_sync.cuh"
 #include "internal.cuh"
 
 namespace linqt {
@@ -31,53 +33,83 @@ namespace linqt {
 namespace {
 
 constexpr int kThreads = 256;
-constexpr long kSpinLimit = 1L << 24;  // polls of ~0.1 us: well above any step, far below a hang
 
-struct Barrier {
-  unsigned count;
-  unsigned gen;
-  int err;
-  int pad;
-};
+using Barrier = GridBarrier;
 
 template <class C>
 __device__ __forceinline__ C ldv(const C *p) {
   return __ldca(p);
 }
 
-// Grid barrier (all CTAs co-resident: cooperative launch).  Returns false if the wait gave up.
-__device__ bool grid_barrier(Barrier *bar, unsigned nblocks) {
-  __shared__ int ok;
-  __syncthreads();
-  if (threadIdx.x == 0) {
-    ok = 1;
-    volatile unsigned *vgen = &bar->gen;
-    const unsigned g = *vgen;
-    __threadfence();
-    const unsigned arrived = atomicAdd(&bar->count, 1u);
-    if (arrived == nblocks - 1) {
-      bar->count = 0;
-      __threadfence();
-      atomicAdd(&bar->gen, 1u);
-    } else {
-      long spins = 0;
-      while (*vgen == g) {
-        if (*(volatile int *)&bar->err) {
-          ok = 0;
-          break;
-        }
-        if (++spins > kSpinLimit) {
-          atomicExch(&bar->err, 1);
-          ok = 0;
-          break;
-        }
-        __nanosleep(64);
-      }
+// The V adjacent complex values a thread owns in a block row, loaded through L1 with the
+// widest aligned accesses (p is aligned to min(32, V * sizeof(C)) bytes: rows hold a power
+// of two >= V columns and blocks start 256-byte aligned).  One 32-byte access carries two
+// FP64 or four FP32 complex numbers, so a gather of a neighbour row costs V/2 (FP64) or
+// V/4 (FP32) loads per thread instead of V.  The loads are volatile asm so that they stay
+// after the grid barrier that orders the previous step's stores before them.
+template <int V>
+__device__ __forceinline__ void ld_row(const double2 *p, double2 (&o)[V]) {
+  if constexpr (V == 1) {
+    o[0] = __ldca(p);
+  } else {
+#pragma unroll
+    for (int q = 0; q < V; q += 2) {
+      double a, b, c, d;
+      asm volatile("ld.global.ca.v4.f64 {%0, %1, %2, %3}, [%4];"
+                   : "=d"(a), "=d"(b), "=d"(c), "=d"(d)
+                   : "l"(p + q));
+      o[q] = make_double2(a, b);
+      o[q + 1] = make_double2(c, d);
     }
-    __threadfence();
   }
-  __syncthreads();
-  return ok != 0;
+}
+
+template <int V>
+__device__ __forceinline__ void ld_row(const float2 *p, float2 (&o)[V]) {
+  if constexpr (V == 1) {
+    o[0] = __ldca(p);
+  } else if constexpr (V == 2) {
+    const float4 t = __ldca(reinterpret_cast<const float4 *>(p));
+    o[0] = make_float2(t.x, t.y);
+    o[1] = make_float2(t.z, t.w);
+  } else {
+#pragma unroll
+    for (int q = 0; q < V; q += 4) {
+      float a[8];
+      asm volatile("ld.global.ca.v8.f32 {%0, %1, %2, %3, %4, %5, %6, %7}, [%8];"
+                   : "=f"(a[0]), "=f"(a[1]), "=f"(a[2]), "=f"(a[3]), "=f"(a[4]), "=f"(a[5]), "=f"(a[6]),
+                     "=f"(a[7])
+                   : "l"(p + q));
+#pragma unroll
+      for (int w = 0; w < 4; ++w) o[q + w] = make_float2(a[2 * w], a[2 * w + 1]);
+    }
+  }
+}
+
+template <int V>
+__device__ __forceinline__ void st_row(double2 *p, const double2 (&v)[V]) {
+#pragma unroll
+  for (int q = 0; q < V; ++q) p[q] = v[q];
+}
+
+template <int V>
+__device__ __forceinline__ void st_row(float2 *p, const float2 (&v)[V]) {
+  if constexpr (V == 1) {
+    p[0] = v[0];
+  } else {
+#pragma unroll
+    for (int q = 0; q < V; q += 2)
+      *reinterpret_cast<float4 *>(p + q) = make_float4(v[q].x, v[q].y, v[q + 1].x, v[q + 1].y);
+  }
+}
+
+// acc[u] += h * x[u]
+template <class C, int V>
+__device__ __forceinline__ void gather_fma(double2 h, const C *p, double2 (&acc)[V]) {
+  C t[V];
+  ld_row<V>(p, t);
+#pragma unroll
+  for (int u = 0; u < V; ++u) acc[u] = cfma(h, t[u], acc[u]);
 }
 
 __device__ __forceinline__ double2 shfl_down2(double2 v, int o) {
@@ -169,7 +201,7 @@ __global__ void __launch_bounds__(kThreads)
                int sC) {
   using C = typename cplx_t<T>::type;
   constexpr int R = TPR * VPT;
-  const int lane = threadIdx.x % TPR;
+  const int c0 = (threadIdx.x % TPR) * VPT;  // this thread's VPT adjacent columns
   constexpr int gpb = kThreads / TPR;
   const int per = (n + gridDim.x - 1) / gridDim.x;
   const int r0 = min(n, blockIdx.x * per), r1 = min(n, r0 + per);
@@ -211,52 +243,54 @@ __global__ void __launch_bounds__(kThreads)
       for (int k = b; k < e; k += st) {
         const int j = ci[k];
         const double2 h = hv[k];
-        const size_t off = (size_t)j * R + lane;
-#pragma unroll
-        for (int u = 0; u < VPT; ++u) {
-          if (doL) aL[u] = cfma(h, ldv(xL + off + u * TPR), aL[u]);
-          aR[u] = cfma(h, ldv(xR + off + u * TPR), aR[u]);
-        }
+        const size_t off = (size_t)j * R + c0;
+        if (doL) gather_fma<C, VPT>(h, xL + off, aL);
+        gather_fma<C, VPT>(h, xR + off, aR);
       }
-      const size_t base = (size_t)row * R + lane;
+      const size_t base = (size_t)row * R + c0;
       if (HAS_V) {
         double2 aV[VPT];
 #pragma unroll
         for (int u = 0; u < VPT; ++u) aV[u] = make_double2(0, 0);
         const int vb = vrp[row], ve = vrp[row + 1];
 #pragma unroll 4
-        for (int k = vb; k < ve; ++k) {
-          const int j = vci[k];
-          const double2 h = vv[k];
-          const size_t off = (size_t)j * R + lane;
+        for (int k = vb; k < ve; ++k) gather_fma<C, VPT>(vv[k], xR + (size_t)vci[k] * R + c0, aV);
+        C o[VPT];
 #pragma unroll
-          for (int u = 0; u < VPT; ++u) aV[u] = cfma(h, ldv(xR + off + u * TPR), aV[u]);
-        }
-        C *vo = Rst + (size_t)m * blk;
-#pragma unroll
-        for (int u = 0; u < VPT; ++u) vo[base + u * TPR] = from_d2<C>(aV[u]);
+        for (int u = 0; u < VPT; ++u) o[u] = from_d2<C>(aV[u]);
+        st_row<VPT>(Rst + (size_t)m * blk + base, o);
       }
+      if (doL) {
+        C o[VPT];
+        if (pL) {
+          C p[VPT];
+          ld_row<VPT>(pL + base, p);
 #pragma unroll
-      for (int u = 0; u < VPT; ++u) {
-        const size_t idx = base + u * TPR;
-        if (doL) {
-          double2 y = aL[u];
-          if (pL) {
-            const double2 p = to_d2(ldv(pL + idx));
-            y.x = 2 * y.x - p.x;
-            y.y = 2 * y.y - p.y;
+          for (int u = 0; u < VPT; ++u) {
+            const double2 q = to_d2(p[u]);
+            o[u] = from_d2<C>(make_double2(2 * aL[u].x - q.x, 2 * aL[u].y - q.y));
           }
-          yL[idx] = from_d2<C>(y);
+        } else {
+#pragma unroll
+          for (int u = 0; u < VPT; ++u) o[u] = from_d2<C>(aL[u]);
         }
-        if (yR) {
-          double2 y = aR[u];
-          if (pR) {
-            const double2 p = to_d2(ldv(pR + idx));
-            y.x = 2 * y.x - p.x;
-            y.y = 2 * y.y - p.y;
+        st_row<VPT>(yL + base, o);
+      }
+      if (yR) {
+        C o[VPT];
+        if (pR) {
+          C p[VPT];
+          ld_row<VPT>(pR + base, p);
+#pragma unroll
+          for (int u = 0; u < VPT; ++u) {
+            const double2 q = to_d2(p[u]);
+            o[u] = from_d2<C>(make_double2(2 * aR[u].x - q.x, 2 * aR[u].y - q.y));
           }
-          yR[idx] = from_d2<C>(y);
+        } else {
+#pragma unroll
+          for (int u = 0; u < VPT; ++u) o[u] = from_d2<C>(aR[u]);
         }
+        st_row<VPT>(yR + base, o);
       }
     }
     if (m + 1 < M && !grid_barrier(bar, gridDim.x)) return;
@@ -278,7 +312,7 @@ __global__ void __launch_bounds__(kThreads)
                int ldx_rt) {
   using C = typename cplx_t<T>::type;
   constexpr int RW = TPR * VPT;  // columns handled by a CTA
-  const int lane = threadIdx.x % TPR;
+  const int c0 = (threadIdx.x % TPR) * VPT;  // this thread's VPT adjacent columns
   constexpr int gpb = kThreads / TPR;
   // STACKED: nreal realisations (value sets at hv + r*vstride) share the sparsity pattern; the
   // grid is split into nreal equal groups of CTAs, group r serving columns [r*RW, (r+1)*RW) of
@@ -310,31 +344,33 @@ __global__ void __launch_bounds__(kThreads)
 #pragma unroll
       for (int u = 0; u < VPT; ++u) acc[u] = make_double2(0, 0);
 #pragma unroll 4
-      for (int k = b; k < e; k += st) {
-        const int j = ci[k];
-        const double2 h = hv[k];
-        const C *xr = cur + (size_t)j * ldx + coff + lane;
-#pragma unroll
-        for (int u = 0; u < VPT; ++u) acc[u] = cfma(h, ldv(xr + u * TPR), acc[u]);
-      }
-      const size_t base = (size_t)row * ldx + coff + lane;
+      for (int k = b; k < e; k += st) gather_fma<C, VPT>(hv[k], cur + (size_t)ci[k] * ldx + coff + c0, acc);
+      const size_t base = (size_t)row * ldx + coff + c0;
+      C pv[VPT], yv[VPT], xv[VPT];
+      if (prev) ld_row<VPT>(prev + base, pv);
 #pragma unroll
       for (int u = 0; u < VPT; ++u) {
-        const size_t idx = base + u * TPR;
         double2 ya = acc[u];
         if (prev) {
-          const double2 p = to_d2(ldv(prev + idx));
+          const double2 p = to_d2(pv[u]);
           ya.x = 2 * ya.x - p.x;
           ya.y = 2 * ya.y - p.y;
         }
-        const C yn = from_d2<C>(ya);  // the value stored and used in the dot products
-        if (y) y[idx] = yn;
-        const double2 xi = to_d2(ldv(cur + idx));
-        if (mode == 1) {
-          d0 = cfma_conj(to_d2(ldv(phi + idx)), xi, d0);
-        } else {
+        yv[u] = from_d2<C>(ya);  // the value stored and used in the dot products
+      }
+      if (y) st_row<VPT>(y + base, yv);
+      ld_row<VPT>(cur + base, xv);
+      if (mode == 1) {
+        C fv[VPT];
+        ld_row<VPT>(phi + base, fv);
+#pragma unroll
+        for (int u = 0; u < VPT; ++u) d0 = cfma_conj(to_d2(fv[u]), to_d2(xv[u]), d0);
+      } else {
+#pragma unroll
+        for (int u = 0; u < VPT; ++u) {
+          const double2 xi = to_d2(xv[u]);
           d0 = cfma_conj(xi, xi, d0);
-          d1 = cfma_conj(to_d2(yn), xi, d1);
+          d1 = cfma_conj(to_d2(yv[u]), xi, d1);
         }
       }
     }
@@ -361,7 +397,7 @@ __global__ void __launch_bounds__(kThreads)
     k_cheb_series(int n, const int *rp, const int *ci, const double2 *hv, double2 *X, double2 *a, double2 *b,
                   const double2 *__restrict__ coef, int K, Barrier *bar, int cache) {
   constexpr int RW = TPR * VPT;
-  const int lane = threadIdx.x % TPR;
+  const int c0 = (threadIdx.x % TPR) * VPT;  // this thread's VPT adjacent columns
   constexpr int gpb = kThreads / TPR;
   const int per = (n + gridDim.x - 1) / gridDim.x;
   const int r0 = min(n, blockIdx.x * per), r1 = min(n, r0 + per);
@@ -372,14 +408,14 @@ __global__ void __launch_bounds__(kThreads)
   }
   const int rfirst = cache ? r0 : blockIdx.x * gpb, rend = cache ? r1 : n;  // as in k_recur_lr
   const int rstep = cache ? gpb : gridDim.x * gpb;
-  const double2 c0 = coef[0];
+  const double2 coef0 = coef[0];
   for (int pos = rfirst + threadIdx.x / TPR; pos < rend; pos += rstep)
 #pragma unroll
     for (int u = 0; u < VPT; ++u) {
-      const size_t idx = (size_t)pos * RW + lane + u * TPR;
+      const size_t idx = (size_t)pos * RW + c0 + u;
       const double2 x = X[idx];
       a[idx] = x;
-      X[idx] = cmul(c0, x);
+      X[idx] = cmul(coef0, x);
     }
   double2 *prev = nullptr, *cur = a;
   for (int s = 1; s < K; ++s) {
@@ -392,16 +428,10 @@ __global__ void __launch_bounds__(kThreads)
       for (int u = 0; u < VPT; ++u) acc[u] = make_double2(0, 0);
       const int kb = rp[pos], ke = rp[pos + 1];
 #pragma unroll 4
-      for (int k = kb; k < ke; ++k) {
-        const int j = ci[k];
-        const double2 h = hv[k];
-        const double2 *xr = cur + (size_t)j * RW + lane;
-#pragma unroll
-        for (int u = 0; u < VPT; ++u) acc[u] = cfma(h, ldv(xr + u * TPR), acc[u]);
-      }
+      for (int k = kb; k < ke; ++k) gather_fma<double2, VPT>(hv[k], cur + (size_t)ci[k] * RW + c0, acc);
 #pragma unroll
       for (int u = 0; u < VPT; ++u) {
-        const size_t idx = (size_t)pos * RW + lane + u * TPR;
+        const size_t idx = (size_t)pos * RW + c0 + u;
         double2 yn = acc[u];
         if (prev) {
           const double2 p = ldv(prev + idx);
@@ -487,6 +517,17 @@ int coop_setup(const void *func, int sm_count, const DeviceOp &H, const DeviceOp
   return grid0;
 }
 
+}  // namespace
+
+// Co-resident CTAs of kThreads threads for func with smem bytes of dynamic shared memory,
+// at most max_blocks.
+int coop_grid(const void *func, int sm_count, long max_blocks, size_t smem) {
+  int per_sm = 0;
+  LQ_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, func, kThreads, smem));
+  if (per_sm <= 0) fail(LINQT_ERR_UNSUPPORTED, "persistent kernel does not fit on an SM");
+  return (int)std::max(1L, std::min((long)per_sm * sm_count, max_blocks));
+}
+
 // Cooperative kernels of all sessions on a device run one after another on one lane
 // stream.  A grid barrier needs every CTA of its grid resident; two persistent grids
 // that each fill the device, launched from two sessions' streams, could hold half the
@@ -527,6 +568,8 @@ void coop_launch(Session *s, const void *f, int grid, void **args, size_t smem) 
   LQ_CUDA(cudaEventDestroy(in));
   LQ_CUDA(cudaEventDestroy(out));
 }
+
+namespace {
 
 template <class T, int TPR, int VPT>
 struct LRF {
@@ -641,16 +684,24 @@ void dispatch(int R, int shape, Args &&...args) {
 #undef LQ_SHAPE
 }
 
+}  // namespace
+
 // The barrier's count/generation restart at zero for every launch; its error flag is
 // sticky until check_device_errors reads it.
-Barrier *barrier_for(Session *s) {
+GridBarrier *barrier_for(Session *s) {
   Barrier *bar = (Barrier *)s->get("rec_barrier", sizeof(Barrier));
   LQ_CUDA(cudaMemsetAsync(bar, 0, 2 * sizeof(unsigned), s->stream));
+  if (s->barrier_cfg_dirty || (s->barrier_cfg_ptr != bar && (s->inject_extra || s->inject_limit))) {
+    LQ_CUDA(cudaMemcpyAsync(&bar->extra, &s->inject_extra, sizeof(int), cudaMemcpyHostToDevice, s->stream));
+    LQ_CUDA(cudaMemcpyAsync(&bar->spin_limit, &s->inject_limit, sizeof(long long), cudaMemcpyHostToDevice,
+                            s->stream));
+    LQ_CUDA(cudaStreamSynchronize(s->stream));  // the host fields may change after this call
+    s->barrier_cfg_dirty = false;
+  }
+  s->barrier_cfg_ptr = bar;
   s->barrier_used = true;
   return bar;
 }
-
-}  // namespace
 
 int recur_shapes(int R) {
   switch (R) {

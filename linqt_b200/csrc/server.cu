@@ -288,6 +288,41 @@ int linqt_server_wait_all(linqt_server *srv) {
   return LINQT_OK;
 }
 
+int linqt_server_cancel(linqt_server *srv, long ticket) {
+  if (!srv) {
+    set_last_error("server: NULL");
+    return LINQT_ERR_INVALID;
+  }
+  std::shared_ptr<Job> job;
+  {
+    std::lock_guard<std::mutex> g(srv->mu);
+    auto it = srv->jobs.find(ticket);
+    if (it == srv->jobs.end()) {
+      set_last_error("server: unknown ticket");
+      return LINQT_ERR_INVALID;
+    }
+    job = it->second;
+    if (job->status != 0) {
+      set_last_error(job->status == 1 ? "server: the request is running and cannot be cancelled"
+                                      : "server: the request has finished");
+      return LINQT_ERR_INVALID;
+    }
+    for (auto q = srv->queue.begin(); q != srv->queue.end(); ++q)
+      if (q->get() == job.get()) {
+        srv->queue.erase(q);
+        break;
+      }
+    job->status = LINQT_ERR_CANCELLED;
+    job->error = "server: request cancelled before it started";
+    job->latency_ms = std::chrono::duration<double, std::milli>(clk::now() - job->t_submit).count();
+    srv->pinned_put_locked(job->states, job->states_cap);
+    job->states = nullptr;
+  }
+  srv->cv.notify_all();  // the next queued request may fit now
+  srv->done_cv.notify_all();
+  return LINQT_OK;
+}
+
 int linqt_server_release(linqt_server *srv, long ticket) {
   if (!srv) {
     set_last_error("server: NULL");

@@ -47,18 +47,29 @@ bool Sparse::OPERATOR_FromCSRFile(const std::string input, int &dim, vector<int>
     std::cerr << "ERROR: Can not open the matrix file";
     return false;
   }
+  // The reference reads without checks and goes on with whatever a short or malformed file
+  // leaves in the arrays; here a failed read is reported and the file rejected.
   int nnz = 0;
   f >> dim >> nnz;
+  if (!f || dim <= 0 || nnz < 0) {
+    std::cerr << "ERROR: malformed CSR header (dim nnz) in " << input << std::endl;
+    return false;
+  }
   values.assign(nnz, complex<double>(0, 0));
   columns.assign(nnz, 0);
   rowIndex.assign(dim + 1, 0);
-  for (int i = 0; i < nnz; i++) {
+  for (int i = 0; i < nnz && f; i++) {
     double re = 0, im = 0;
     f >> re >> im;
     values[i] = complex<double>(re, im);
   }
-  for (int i = 0; i < nnz; i++) f >> columns[i];
-  for (int i = 0; i <= dim; i++) f >> rowIndex[i];
+  for (int i = 0; i < nnz && f; i++) f >> columns[i];
+  for (int i = 0; i <= dim && f; i++) f >> rowIndex[i];
+  if (!f) {
+    std::cerr << "ERROR: truncated or malformed CSR file " << input << " (expected " << nnz << " values, " << nnz
+              << " columns and " << dim + 1 << " row pointers)" << std::endl;
+    return false;
+  }
   std::cout << "FINISH READING.Status: SUCCEED" << std::endl;
   return true;
 }
@@ -332,6 +343,34 @@ int SpectralMoments(SparseMatrixType &OP, chebyshev::Moments1D &chebMoms, qstate
                         OP.isIdentity() ? nullptr : need_op(OP, "SpectralMoments"), dp(st.data()), R, M, nullptr,
                         dp(mu.data())),
         "linqt_moments1d");
+  for (int m = 0; m < M; m++) chebMoms(m) += mu[m];  // the reference accumulates onto the table
+  return 0;
+}
+
+int SpectralMoments_nonOrth(SparseMatrixType &OP, chebyshev::Moments1D_nonOrth &chebMoms, qstates::generator &gen) {
+  const int N = (int)chebMoms.SystemSize(), M = (int)chebMoms.HighestMomentNumber();
+  SparseMatrixType *S = chebMoms.overlap();
+  if (!S) {
+    std::cerr << "SpectralMoments_nonOrth: no overlap matrix (set_S)" << std::endl;
+    std::abort();
+  }
+  int R = 0;
+  std::vector<std::complex<double> > st = qstates::collect_states(gen, N, &R);
+  if (R == 0 || M == 0) return 0;
+  // the solver sees S's CSR arrays as stored (linalg::orthogonalize maps them into Eigen as
+  // they are, src/mkl_linear_algebra.cpp:100-118): a general-storage operator of the same arrays
+  linqt_op *s_op = nullptr;
+  check(linqt_csr_create(nullptr, S->numRows(), S->rows()->data(), S->cols()->data(), dp(S->vals()->data()),
+                         LINQT_STORAGE_GENERAL, &s_op),
+        "linqt_csr_create (S)");
+  std::vector<std::complex<double> > mu(M);
+  long iters = 0;
+  const int rc = linqt_moments1d_nonorth(nullptr, need_op(chebMoms.Hamiltonian(), "SpectralMoments_nonOrth"),
+                                         OP.isIdentity() ? nullptr : need_op(OP, "SpectralMoments_nonOrth"), s_op,
+                                         dp(st.data()), R, M, 1e-4, 2000, nullptr, dp(mu.data()), &iters);
+  linqt_op_destroy(s_op);
+  check(rc, "linqt_moments1d_nonorth");
+  std::cout << "#BiCGSTAB iterations (all solves): " << iters << std::endl;
   for (int m = 0; m < M; m++) chebMoms(m) += mu[m];  // the reference accumulates onto the table
   return 0;
 }

@@ -95,6 +95,23 @@ class Moments1D : public Moments {
   size_t _numMoms;
 };
 
+// 1D moments in a non-orthogonal basis (Moments1D_nonOrth of LinQT's
+// include/chebyshev_moments.hpp:194-220): a Moments1D plus the overlap matrix S, whose stored
+// CSR arrays chebyshev::SpectralMoments_nonOrth hands to the GPU BiCGSTAB solves.
+class Moments1D_nonOrth : public Moments1D {
+ public:
+  Moments1D_nonOrth(const size_t m0) : Moments1D(m0), S_(NULL) {}
+  Moments1D_nonOrth(SparseMatrixType &S) : Moments1D(), S_(&S) {}
+  Moments1D_nonOrth(const size_t m0, SparseMatrixType &S) : Moments1D(m0), S_(&S) {}
+  Moments1D_nonOrth(std::string &momfilename, SparseMatrixType &S) : Moments1D(momfilename), S_(&S) {}
+
+  void set_S(SparseMatrixType &S) { S_ = &S; }
+  SparseMatrixType *overlap() const { return S_; }
+
+ private:
+  SparseMatrixType *S_;
+};
+
 class Moments2D : public Moments {
  public:
   Moments2D() : numMoms({0, 0}) {}

@@ -34,6 +34,11 @@ int CorrelationExpansionMoments(SparseMatrixType &OPL, SparseMatrixType &OPR, ch
 
 int SpectralMoments(SparseMatrixType &OP, chebyshev::Moments1D &chebMoms, qstates::generator &gen);
 
+// SpectralMoments in a non-orthogonal basis (src/chebyshev_solver.cpp:203-229): every S^-1 a
+// BiCGSTAB solve with the reference's settings (tolerance 1e-4, at most 2000 iterations) on
+// the CSR arrays of S as stored, all states as one block (linqt_moments1d_nonorth)
+int SpectralMoments_nonOrth(SparseMatrixType &OP, chebyshev::Moments1D_nonOrth &chebMoms, qstates::generator &gen);
+
 // all states of the generator as one block through linqt_moments_td
 int TimeDependentCorrelations(SparseMatrixType &OPL, SparseMatrixType &OPR, chebyshev::MomentsTD &chebMoms,
                               qstates::generator &gen);

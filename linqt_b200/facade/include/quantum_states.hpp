@@ -80,13 +80,22 @@ inline StateType String2State(std::string kind) {
   return RANDOM_STATE;
 }
 
+// A state file that ends early or holds something else than numbers: the reference reads on
+// with zeros; here the program stops with a message.
+inline void state_file_error(const std::string &what) {
+  std::cerr << "ERROR: state file: " << what << std::endl;
+  std::abort();
+}
+
 inline void readLocalState(std::ifstream &file, generator &g) {
   int n = 0;
   file >> n;
+  if (!file || n < 0) state_file_error("malformed count of local states");
   g.NumberOfStates(n);
   for (int i = 0; i < n; i++) {
     int site = 0;
     file >> site;
+    if (!file) state_file_error("truncated list of local states");
     g.spos.push_back(site);
   }
 }
@@ -96,12 +105,14 @@ inline void readCustomState(std::ifstream &file, generator &g) {
   file >> n;
   g.NumberOfStates(n);
   file >> dim;
+  if (!file || n < 0 || dim <= 0) state_file_error("malformed vector header (num_states dim)");
   g.SystemSize(dim);
   g.data.assign((size_t)dim * n, scalar(0.0));
   for (int i = 0; i < n; i++) {
     for (int j = 0; j < dim; j++) {
       double re = 0, im = 0;
       file >> re >> im;
+      if (!file) state_file_error("truncated vector states");
       g.data[(size_t)i * dim + j] = scalar(re, im);
     }
     g.spos.push_back(i * dim);

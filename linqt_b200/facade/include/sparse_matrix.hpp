@@ -86,7 +86,10 @@ class SparseMatrixBuilder {
     vector<int> columns, rowIndex;
     vector<complex<double> > values;
     int dim = 0;
-    Sparse::OPERATOR_FromCSRFile(input, dim, columns, rowIndex, values);
+    if (!Sparse::OPERATOR_FromCSRFile(input, dim, columns, rowIndex, values)) {
+      std::cerr << "BuildOPFromCSRFile: cannot build an operator from " << input << std::endl;
+      std::abort();
+    }
     _matrix_type->setDimensions(dim, dim);
     _matrix_type->ConvertFromCSR(rowIndex, columns, values);
     std::cout << "OPERATOR SUCCESSFULLY BUILT" << std::endl;

@@ -51,6 +51,8 @@ def read_chebmom1d(path):
     tok = open(path).read().split()
     n, bw, bc, M = int(tok[0]), float(tok[1]), float(tok[2]), int(tok[3])
     v = np.array(tok[4:4 + 2 * M], dtype=np.float64)
+    if len(v) != 2 * M:
+        raise ValueError("truncated .chebmom1D file: %s" % path)
     return n, bw, bc, v[0::2] + 1j * v[1::2]
 
 
@@ -113,11 +115,15 @@ def read_state_file(path, dim=None):
     if kind == "vector":
         R, N = int(tok[1]), int(tok[2])
         v = np.array(tok[3:3 + 2 * R * N], dtype=np.float64)
+        if len(v) != 2 * R * N:
+            raise ValueError("truncated vector state file: %s" % path)
         return (v[0::2] + 1j * v[1::2]).reshape(R, N)
     if kind == "local":
         R = int(tok[1])
         if dim is None:
             raise ValueError("local states need the system dimension")
+        if len(tok) < 2 + R:
+            raise ValueError("truncated local state file: %s" % path)
         st = np.zeros((R, dim), np.complex128)
         for r in range(R):
             st[r, int(tok[2 + r])] = 1.0

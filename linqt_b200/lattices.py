@@ -214,6 +214,20 @@ def kane_mele(Lx, Ly, t=1.0, lam_so=0.06, lam_r=0.05, W=0.5, seed=31, a=1.0):
     return N, H, J
 
 
+def overlap_matrix(N, H, s=0.08, seed=13):
+    """Upper-triangle CSR of an overlap matrix S = I + (off-diagonal entries on H's bonds) for a
+    non-orthogonal basis: S_ij = s e^{i theta_ij} with theta_ij uniform in [0, 2 pi) (Philox,
+    seed), on every bond (i < j) of H's upper triangle.  Positive definite when s times the
+    bonds per row stays below 1."""
+    rp, col, _ = H
+    rows = np.repeat(np.arange(N), np.diff(rp))
+    off = col > rows
+    r, c = rows[off], col[off].astype(np.int64)
+    th = 2 * np.pi * uniform(seed, len(r))
+    vals = np.concatenate([np.ones(N), s * np.exp(1j * th)])
+    return upper_csr(N, np.concatenate([np.arange(N), r]), np.concatenate([np.arange(N), c]), vals)
+
+
 def gershgorin_bounds(n, rowptr, col, val):
     """Gershgorin interval of the Hermitian matrix stored as upper CSR (host, for tests)."""
     rows = np.repeat(np.arange(n), np.diff(rowptr))

@@ -60,6 +60,10 @@ class Server:
         out, _, _, M, kind = self._keep[ticket]
         return out if kind == REQ_DOS else out.reshape(M, M)
 
+    def cancel(self, ticket):
+        """Withdraw a queued request (LinqtError if it already runs or has finished)."""
+        check(load().linqt_server_cancel(self.h, ticket))
+
     def release(self, ticket):
         """Forget a finished request: the server's record and the Python-side buffers."""
         check(load().linqt_server_release(self.h, ticket))

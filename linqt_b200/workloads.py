@@ -30,6 +30,16 @@ from . import lattices
 from .core import PREC_FP64, PREC_MIXED, Operator, Session, make_opts, kubo_bastin_dev, moments1d_dev
 
 
+def _hbm_peak():
+    """(GB/s, source): the copy bandwidth measured on this GPU model (MEASURED_PEAKS.json at
+    the repository root), else the 6650 GB/s fallback."""
+    import os
+    p = os.path.join(os.path.dirname(os.path.dirname(os.path.abspath(__file__))), "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        return float(json.load(open(p)).get("hbm_gbs", 6650.0)), "measured"
+    return 6650.0, "fallback"
+
+
 def _timed(fn, reps, torch):
     for _ in range(2):
         fn()
@@ -227,8 +237,9 @@ def run_cubic_full(L, S, Rs, M, mode=0):
         bytes_step = S * (nnz * (16 + 4) + 4 * (N + 1)) + 3 * esz * N * R
         gbs = steps * bytes_step / (ms * 1e-3) / 1e9
         mus[label] = mu.cpu().numpy().view(np.complex128).reshape(S, M)
+        peak, src = _hbm_peak()
         out[label] = {"ms_per_solve": ms, "steps_nnz_per_s": M * R * nnz / (ms * 1e-3),
-                      "recursion_GBps": gbs, "hbm_frac_of_measured_6549": gbs / 6549.1}
+                      "recursion_GBps": gbs, "hbm_frac": gbs / peak, "hbm_peak_GBps": peak, "hbm_peak_source": src}
     e = np.abs(mus["mixed"] - mus["fp64"]).max(axis=1) / np.abs(mus["fp64"]).max(axis=1)
     out["mixed"]["err_mu_vs_fp64_per_seed"] = [float(x) for x in e]
     return out

@@ -217,6 +217,159 @@ int lo_moments1d(const lo_op *H, const lo_op *op, const double *states, int R, i
   return 0;
 }
 
+/* ---------------------------------------------------------------------------
+ * Non-orthogonal basis.  linalg::orthogonalize (src/mkl_linear_algebra.cpp:100-132) solves
+ * S x = b with Eigen 3.4.0's BiCGSTAB (a third-party header library the reference includes
+ * from eigen-3.4.0/, not shipped with it), tolerance 1e-4, at most 2000 iterations, and the
+ * default DiagonalPreconditioner; S is Eigen::Map'd over the CSR arrays exactly as the
+ * operator file stores them (SparseMatrixType::rows/cols/vals, no Hermitian expansion),
+ * and solve() starts from x = 0.  bicgstab() restates that published algorithm (van der
+ * Vorst's BiCGSTAB with Eigen's restart when r0 and r become orthogonal):
+ *   r = b - S x, r0 = r, rho = alpha = w = 1, v = p = 0, tol2 = tol^2 |b|^2
+ *   while |r|^2 > tol2 and i < maxit:
+ *     rho_old = rho; rho = <r0, r>
+ *     if |rho| < eps^2 |r0|^2: r = b - S x; r0 = r; rho = |r0|^2 = |r|^2; restart i once
+ *     beta = (rho / rho_old) (alpha / w); p = r + beta (p - w v)
+ *     y = D^-1 p; v = S y; alpha = rho / <r0, v>; s = r - alpha v
+ *     z = D^-1 s; t = S z; w = <t, s> / |t|^2 (0 if |t| = 0)
+ *     x += alpha y + w z; r = s - w t; i++
+ * with <a, b> = sum conj(a_i) b_i, eps = DBL_EPSILON and D the diagonal of S (1 where a
+ * row has no diagonal entry or a zero one).  |b| = 0 gives x = 0.
+ * ------------------------------------------------------------------------- */
+typedef struct {
+  int n;
+  const int *rp, *ci;
+  const cplx *v;
+  cplx *invd;
+} gcsr;
+
+static void gcsr_mv(const gcsr *S, const cplx *x, cplx *y) {
+#pragma omp parallel for schedule(static)
+  for (int i = 0; i < S->n; i++) {
+    cplx acc = 0.0;
+    for (int k = S->rp[i]; k < S->rp[i + 1]; k++) acc += S->v[k] * x[S->ci[k]];
+    y[i] = acc;
+  }
+}
+
+static double sqnorm(int n, const cplx *x) {
+  double acc = 0.0;
+  for (int i = 0; i < n; i++) acc += creal(x[i]) * creal(x[i]) + cimag(x[i]) * cimag(x[i]);
+  return acc;
+}
+
+/* returns the iterations taken; x = S^-1 b to the tolerance */
+static int bicgstab(const gcsr *S, const cplx *b, cplx *x, double tol, int maxit, cplx *work) {
+  const int n = S->n;
+  cplx *r = work, *r0 = work + n, *p = work + 2 * (size_t)n, *v = work + 3 * (size_t)n, *y = work + 4 * (size_t)n,
+       *sv = work + 5 * (size_t)n, *z = work + 6 * (size_t)n, *t = work + 7 * (size_t)n;
+  for (int i = 0; i < n; i++) x[i] = 0.0;
+  for (int i = 0; i < n; i++) r[i] = b[i];  /* b - S*0 */
+  memcpy(r0, r, sizeof(cplx) * (size_t)n);
+  double r0_sq = sqnorm(n, r0);
+  const double rhs_sq = sqnorm(n, b);
+  if (rhs_sq == 0.0) return 0;
+  cplx rho = 1.0, alpha = 1.0, w = 1.0;
+  for (int i = 0; i < n; i++) v[i] = p[i] = 0.0;
+  const double tol2 = tol * tol * rhs_sq, eps = 2.220446049250313e-16, eps2 = eps * eps;
+  int it = 0, restarts = 0;
+  while (sqnorm(n, r) > tol2 && it < maxit) {
+    const cplx rho_old = rho;
+    rho = vdot(n, r0, r);
+    if (cabs(rho) < eps2 * r0_sq) {
+      gcsr_mv(S, x, t);
+      for (int i = 0; i < n; i++) r[i] = b[i] - t[i];
+      memcpy(r0, r, sizeof(cplx) * (size_t)n);
+      rho = r0_sq = sqnorm(n, r);
+      if (restarts++ == 0) it = 0;
+    }
+    const cplx beta = (rho / rho_old) * (alpha / w);
+    for (int i = 0; i < n; i++) p[i] = r[i] + beta * (p[i] - w * v[i]);
+    for (int i = 0; i < n; i++) y[i] = S->invd[i] * p[i];
+    gcsr_mv(S, y, v);
+    alpha = rho / vdot(n, r0, v);
+    for (int i = 0; i < n; i++) sv[i] = r[i] - alpha * v[i];
+    for (int i = 0; i < n; i++) z[i] = S->invd[i] * sv[i];
+    gcsr_mv(S, z, t);
+    const double tt = sqnorm(n, t);
+    w = tt > 0.0 ? vdot(n, t, sv) / tt : 0.0;
+    for (int i = 0; i < n; i++) x[i] += alpha * y[i] + w * z[i];
+    for (int i = 0; i < n; i++) r[i] = sv[i] - w * t[i];
+    ++it;
+  }
+  return it;
+}
+
+/* chebyshev::SpectralMoments_nonOrth (src/chebyshev_solver.cpp:203-229) with
+ * Moments1D_nonOrth::SetInitVectors_nonOrthogonal (src/chebyshev_moments.cpp:63-124) and
+ * Iterate_nonOrthogonal (:129-153):
+ *   identity OP: T_0 = S^-1 phi,            T_1 = S^-1 H T_0
+ *   with OP:     T_0 = OP S^-1 phi,         T_1 = S^-1 H T_0
+ *   T_{m+1} = 2 S^-1 H T_m - T_{m-1};  mu_m += (2/R)(1/2)^{[m=0]} <phi|T_m>.
+ * S: the stored CSR (s_rowptr, s_col, s_val of n rows).  The reference iterates after every
+ * moment, so its last two solves (T_M and T_{M+1}) never reach mu; they are skipped here
+ * (M solves per state instead of M + 2).  *iters: the BiCGSTAB iterations summed over all
+ * solves. */
+int lo_moments1d_nonorth(const lo_op *H, const lo_op *op, const int *s_rowptr, const int *s_col, const double *s_val,
+                         const double *states, int R, int M, double tol, int maxit, double *mu_out, long *iters) {
+  if (!H || R <= 0 || M <= 0) return -1;
+  const int n = H->n;
+  gcsr S = {n, s_rowptr, s_col, (const cplx *)s_val, malloc(sizeof(cplx) * (size_t)n)};
+  for (int i = 0; i < n; i++) {
+    S.invd[i] = 1.0;
+    for (int k = s_rowptr[i]; k < s_rowptr[i + 1]; k++)
+      if (s_col[k] == i) {
+        if (S.v[k] != 0.0) S.invd[i] = 1.0 / S.v[k];
+        break;
+      }
+  }
+  cplx *mu = calloc((size_t)M, sizeof(cplx));
+  cplx *T0 = malloc(sizeof(cplx) * (size_t)n), *T1 = malloc(sizeof(cplx) * (size_t)n);
+  cplx *tmp = malloc(sizeof(cplx) * (size_t)n), *tmp2 = malloc(sizeof(cplx) * (size_t)n);
+  cplx *work = malloc(sizeof(cplx) * 8 * (size_t)n);
+  long its = 0;
+  for (int r = 0; r < R; r++) {
+    const cplx *phi = (const cplx *)states + (long)r * n;
+    if (op) {
+      its += bicgstab(&S, phi, tmp, tol, maxit, work);
+      op_mv(op, 1.0, tmp, 0.0, T0);
+    } else {
+      its += bicgstab(&S, phi, T0, tol, maxit, work);
+    }
+    if (M > 1) {
+      op_mv(H, 1.0, T0, 0.0, tmp);
+      its += bicgstab(&S, tmp, T1, tol, maxit, work);
+    }
+    for (int m = 0; m < M; m++) {
+      double scal = 2.0 / R;
+      if (m == 0) scal *= 0.5;
+      mu[m] += scal * vdot(n, phi, T0);
+      if (m + 1 == M) break;
+      if (m + 2 < M) {  /* T_{m+2} = 2 S^-1 H T_{m+1} - T_m, over T_m */
+        op_mv(H, 1.0, T1, 0.0, tmp);
+        its += bicgstab(&S, tmp, tmp2, tol, maxit, work);
+        for (int i = 0; i < n; i++) T0[i] = 2.0 * tmp2[i] - T0[i];
+      }
+      cplx *t = T0;
+      T0 = T1;
+      T1 = t;
+    }
+  }
+  for (int m = 0; m < M; m++) {
+    mu_out[2 * m] = creal(mu[m]);
+    mu_out[2 * m + 1] = cimag(mu[m]);
+  }
+  if (iters) *iters = its;
+  free(work);
+  free(tmp2);
+  free(tmp);
+  free(T1);
+  free(T0);
+  free(mu);
+  free(S.invd);
+  return 0;
+}
+
 /* chebyshev::besselJ (src/special_functions.cpp:3-17): libm's j0 / j1 / jn. */
 static double bessel_j(int n, double x) { return n == 0 ? j0(x) : n == 1 ? j1(x) : jn(n, x); }
 

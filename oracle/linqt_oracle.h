@@ -56,6 +56,12 @@ int lo_jackson2d(double *mu, int M0, int M1, double band_width, double b0, doubl
 
 /* DOS on the Chebyshev grid E_i = cos(pi(i+1/2)/M)  (src/spectralFunctionFromChebmom_FFTgrid.cpp:35-75).
  * E[M] (physical energies), dos[M] = |N/a sum_m delta(E_i,m) Re mu_m| */
+/* chebyshev::SpectralMoments_nonOrth (src/chebyshev_solver.cpp:203-229): 1D moments in a
+ * non-orthogonal basis, S^-1 applied by BiCGSTAB (tolerance tol, at most maxit iterations,
+ * Jacobi preconditioner, x0 = 0) on the stored CSR of S (no Hermitian expansion).  op = NULL
+ * is the identity.  *iters: the BiCGSTAB iterations summed over all solves. */
+int lo_moments1d_nonorth(const lo_op *H, const lo_op *op, const int *s_rowptr, const int *s_col, const double *s_val,
+                         const double *states, int R, int M, double tol, int maxit, double *mu_out, long *iters);
 int lo_dos_fftgrid(const double *mu, int M, int N, double band_width, double band_center, double *E, double *dos);
 /* spectralFunctionFromChebmom (grid 0: num_div uniform points in [-1, 1], raw sums) and
  * spectralFunctionFromChebmom_FFTgrid (grid 1: cos(pi (i+1/2)/num_div), absolute values)

@@ -59,6 +59,8 @@ def lib():
         L.lo_jackson2d.argtypes = [dp, ctypes.c_int, ctypes.c_int, ctypes.c_double, ctypes.c_double,
                                    ctypes.c_double, ip, ip]
         L.lo_dos_fftgrid.argtypes = [dp, ctypes.c_int, ctypes.c_int, ctypes.c_double, ctypes.c_double, dp, dp]
+        L.lo_moments1d_nonorth.argtypes = [vp, vp, ip, ip, dp, dp, ctypes.c_int, ctypes.c_int, ctypes.c_double,
+                                           ctypes.c_int, dp, ctypes.POINTER(ctypes.c_long)]
         L.lo_spectral_function.argtypes = [dp, ctypes.c_int, ctypes.c_int, ctypes.c_double, ctypes.c_double,
                                            ctypes.c_int, ctypes.c_int, dp, dp]
         L.lo_bastin_from_moments.argtypes = [dp, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_double,
@@ -141,6 +143,23 @@ def moments1d(H, op, states, M):
     if rc:
         raise RuntimeError("lo_moments1d failed: %d" % rc)
     return mu
+
+
+def moments1d_nonorth(H, op, S, states, M, tol=1e-4, maxit=2000):
+    """SpectralMoments_nonOrth: S = (rowptr, col, val) as stored in its CSR file.
+    Returns (mu, BiCGSTAB iterations summed over all solves)."""
+    st = np.ascontiguousarray(states, dtype=np.complex128)
+    R = st.shape[0]
+    rp = np.ascontiguousarray(S[0], dtype=np.int32)
+    cl = np.ascontiguousarray(S[1], dtype=np.int32)
+    vl = _cplx_as_f64(S[2]) if np.iscomplexobj(S[2]) else np.ascontiguousarray(S[2], dtype=np.float64)
+    mu = np.zeros(M, np.complex128)
+    its = ctypes.c_long()
+    rc = lib().lo_moments1d_nonorth(H.h, _h(op), _ip(rp), _ip(cl), _dp(vl), _dp(st.view(np.float64)), R, M, tol, maxit,
+                                    _dp(mu.view(np.float64)), ctypes.byref(its))
+    if rc:
+        raise RuntimeError("lo_moments1d_nonorth failed: %d" % rc)
+    return mu, its.value
 
 
 def moments_td(H, opl, opr, states, M, NT, dt, band_width, band_center):

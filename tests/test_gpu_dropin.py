@@ -118,3 +118,31 @@ def test_time_correlation_driver(workdir, tmp_path, opl, opr, M, NT, tmax):
     n2, bw2, bc2, dt2, mu2 = formats.read_chebmomtd(str(cpu / f))
     assert (n1, bw1, bc1, dt1) == (n2, bw2, bc2, dt2) and mu1.shape == mu2.shape == (M, NT)
     assert _rel(mu1, mu2) < 1e-12  # 15 printed digits
+
+
+@pytest.fixture(scope="module")
+def nonorth_dir(tmp_path_factory):
+    """A square lattice (16 x 16) with an overlap matrix S on its bonds, for
+    inline_compute-kpm-spectralOp-nonOrth (operators/sq.{HAM,S}.CSR, BOUNDS, states)."""
+    d = tmp_path_factory.mktemp("dropin_nonorth")
+    (d / "operators").mkdir()
+    N, H = lattices.square_lattice(16, t=1.0, W=1.0, seed=11)
+    S = lattices.overlap_matrix(N, H, s=0.08, seed=13)
+    formats.write_csr(str(d / "operators" / "sq.HAM.CSR"), N, *H)
+    formats.write_csr(str(d / "operators" / "sq.S.CSR"), N, *S)
+    (d / "BOUNDS").write_text("-4.725 4.725\n")
+    formats.write_vector_states(str(d / "states.txt"), lattices.random_phase_states(N, 3, seed=12))
+    return d
+
+
+@pytest.mark.parametrize("op,state", [("1", "states.txt"), ("HAM", "states.txt"), ("1", None)])
+def test_nonorth_spectral_driver(nonorth_dir, tmp_path, op, state):
+    """inline_compute-kpm-spectralOp-nonOrth: S^-1 by BiCGSTAB (the reference through its Eigen
+    stand-in, the facade on the GPU), the same .chebmom1D-nonOrth file."""
+    args = ["sq", op, 96] + ([state] if state else [])
+    gpu, cpu, files = _both("inline_compute-kpm-spectralOp-nonOrth", args, nonorth_dir, tmp_path)
+    (f,) = files
+    n1, bw1, bc1, mu1 = formats.read_chebmom1d(str(gpu / f))
+    n2, bw2, bc2, mu2 = formats.read_chebmom1d(str(cpu / f))
+    assert (n1, bw1, bc1) == (n2, bw2, bc2)
+    assert _rel(mu1, mu2) < 1e-11

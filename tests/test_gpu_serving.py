@@ -96,3 +96,23 @@ def test_seeded_requests_match_host_states():
     with pytest.raises(lq.LinqtError):
         srv.poll(t1)
     srv.close()
+
+
+def test_cancel_a_queued_request():
+    """A request still queued behind others is withdrawn: status LINQT_ERR_CANCELLED, its
+    result buffer untouched; the others complete; a finished request cannot be cancelled."""
+    N, Hg, _ = _ops("square", 40000, seed=7)
+    st = lattices.random_phase_states(N, 2, seed=8)
+    srv = serve.Server(0, 0, 1)  # one slot: the third request waits for the first two
+    t1 = srv.submit(serve.REQ_DOS, Hg, None, st, 1024, lq.PREC_FP64)
+    t2 = srv.submit(serve.REQ_DOS, Hg, None, st, 1024, lq.PREC_FP64)
+    t3 = srv.submit(serve.REQ_DOS, Hg, None, st, 1024, lq.PREC_FP64)
+    srv.cancel(t3)
+    assert srv.poll(t3)[0] == -7  # LINQT_ERR_CANCELLED
+    srv.wait_all()
+    assert srv.poll(t1)[0] == 2 and srv.poll(t2)[0] == 2
+    assert not np.any(srv.result(t3))
+    assert np.array_equal(srv.result(t1), srv.result(t2))
+    with pytest.raises(lq.LinqtError):
+        srv.cancel(t1)
+    srv.close()

@@ -186,3 +186,38 @@ def test_time_correlation_postprocessor_vs_ref(oracle_lib, tmp_path):
         t, c = oracle_lib.time_correlation(mu_f, N, bw, bc, dt, broad, ef)
         assert np.abs(t - ref[:, 0]).max() < 1e-5 * max(1.0, np.abs(t).max())
         assert np.abs(c - ref[:, 1]).max() < 2e-6 * np.abs(c).max()
+
+
+def _nonorth_dir(oracle_lib, tmp_path, L=8, R=2):
+    N, H = lattices.square_lattice(L, t=1.0, W=1.0, seed=11)
+    S = lattices.overlap_matrix(N, H, s=0.08, seed=13)
+    st = lattices.random_phase_states(N, R, seed=12)
+    d = setup_dir(oracle_lib, tmp_path, "sq", {"HAM": (N, H), "S": (N, S)}, (-4.725, 4.725), st)
+    return d, N
+
+
+@pytest.mark.parametrize("opname", ["1", "HAM"])
+def test_nonorth_moments_vs_reference_driver(oracle_lib, tmp_path, opname):
+    """SpectralMoments_nonOrth: LinQT's own inline_compute-kpm-spectralOp-nonOrth (its Eigen
+    BiCGSTAB solve of S x = b given by the stand-in, tolerance 1e-4) against the restatement,
+    both on the stored upper triangle of S."""
+    d, N = _nonorth_dir(oracle_lib, tmp_path)
+    exe = os.path.join(os.path.dirname(__file__), "..", "oracle", "_ref", "inline_compute-kpm-spectralOp-nonOrth")
+    M = 48
+    p = subprocess.run([exe, "sq", opname, str(M), "states.txt"], cwd=d, capture_output=True, text=True, timeout=300)
+    assert p.returncode == 0, p.stderr[-500:]
+    out = [f for f in os.listdir(d) if f.endswith(".chebmom1D-nonOrth")]
+    assert len(out) == 1
+    n, bw, bc, mu_ref = formats.read_chebmom1d(os.path.join(d, out[0]))
+    assert n == N and abs(bw - 9.45) < 1e-12
+    iters_ref = [int(l.split()[1]) for l in p.stdout.splitlines() if l.startswith("#iterations:")]
+    _, rp, cl, vl = formats.read_csr(os.path.join(d, "operators", "sq.HAM.CSR"))
+    Ho = oracle_lib.Op(rp, cl, vl).rescale(2 / bw, -bc / (bw / 2))
+    OPo = oracle_lib.Op(rp, cl, vl) if opname == "HAM" else None  # the operator file, not rescaled
+    S = formats.read_csr(os.path.join(d, "operators", "sq.S.CSR"))[1:]
+    mu, its = oracle_lib.moments1d_nonorth(Ho, OPo, S, formats.read_state_file(os.path.join(d, "states.txt")), M)
+    # per state the reference solves twice to start and once after every moment; the solves
+    # after moments M-2 and M-1 (T_M, T_{M+1}) never reach mu and the restatement skips them
+    assert len(iters_ref) == 2 * (M + 2)
+    assert its == sum(iters_ref) - sum(iters_ref[(M + 2) * k + M] + iters_ref[(M + 2) * k + M + 1] for k in range(2))
+    assert rel(mu, mu_ref) < 1e-12
