@@ -35,7 +35,7 @@
 extern "C" {
 #endif
 
-#define LINQT_ABI_VERSION 2
+#define LINQT_ABI_VERSION 3
 
 enum {
   LINQT_OK = 0,
@@ -87,7 +87,11 @@ typedef struct linqt_opts {
   int step_launches; /* 1 = one kernel launch per recursion step instead of one persistent cooperative launch */
   int realisations; /* linqt_moments1d_realisations: 0 = autotuned (short timed trials of both, cached per
                        operator pattern, S, R/S and precision), 1 = stacked in one launch, 2 = one solve each */
-  int reserved[9];
+  int operator_precision; /* values of H in the 1D recursions (linqt_moments1d[_dev],
+                       linqt_moments1d_realisations[_dev]): 0 = complex128 (default), 1 = complex64 (each
+                       value rounded once to FP32, products accumulated in FP64; CSR layouts, persistent
+                       recursion); other solvers accept 0 only */
+  int reserved[8];
 } linqt_opts;
 
 /* ---- library / sessions ------------------------------------------------ */
@@ -108,6 +112,15 @@ int linqt_session_trim(linqt_session *s);
  * reconstruction, [3] other; launches[0..3] the kernel launches per phase. */
 int linqt_session_phase_times(linqt_session *s, double ms[4], long launches[4], int reset);
 int linqt_session_enable_timing(linqt_session *s, int on);
+/* Run this session's persistent recursion kernels with at most `share` (0 < share <= 1) of the
+ * device's co-resident CTAs, launched on the session's own stream.  By default (share = 1)
+ * every persistent kernel of every session takes the whole device, one at a time (they queue
+ * on a device-wide cooperative lane, since two full-device grids could not be resident
+ * together).  Sessions whose shares add up to at most 1 can run their recursions at the
+ * same time; a grid that still does not become resident in time ends its solve with
+ * LINQT_ERR_TIMEOUT instead of waiting (the server retries such a request with share 1).
+ * Results depend on the share only through the order of the partial sums (last digits). */
+int linqt_session_set_sm_share(linqt_session *s, double share);
 /* Fault injection for tests of the timeout path (no counterpart in the reference).  From the
  * next solve on, the grid barriers of the session's persistent kernels wait for
  * extra_arrivals CTAs that were never launched and give up after spin_limit polls (0: the
@@ -343,6 +356,11 @@ typedef struct linqt_request {
   int precision;         /* LINQT_PREC_* */
   double *mu_out;        /* host result buffer: 2*M (DOS) or 2*M*M (Kubo) */
   unsigned long long seed; /* states == NULL: as linqt_random_phase_states_dev(N = H's dimension, R, seed) */
+  /* Kubo-Bastin: sigma_xx(E) from the same recursion (linqt_kubo_bastin) when sigma_out != NULL:
+   * 3*nump doubles (E, sigma, integrand), nump >= M; band_width / band_center are H's rescaling */
+  double *sigma_out;
+  int nump;
+  double band_width, band_center;
 } linqt_request;
 int linqt_server_create(int device, size_t hbm_budget_bytes, int max_active, linqt_server **out);
 int linqt_server_submit(linqt_server *srv, const linqt_request *req, long *ticket);
@@ -354,6 +372,11 @@ int linqt_server_wait_all(linqt_server *srv);
 int linqt_server_cancel(linqt_server *srv, long ticket);
 /* forget a finished request (its ticket becomes unknown); LINQT_ERR_INVALID while it is queued or running */
 int linqt_server_release(linqt_server *srv, long ticket);
+/* timeouts_retried: requests whose side-by-side persistent recursion did not become
+ * co-resident in time and were re-run on the device-wide cooperative lane (see
+ * linqt_session_set_sm_share); nomem_retried (may be NULL): requests whose workspaces did not
+ * fit next to the running ones and were re-run alone. */
+int linqt_server_stats(linqt_server *srv, long *timeouts_retried, long *nomem_retried);
 int linqt_server_destroy(linqt_server *srv);
 
 /* ---- operator builder: utilities/wannier2sparse -------------------------- */

@@ -33,12 +33,15 @@ class LinqtError(RuntimeError):
 
 class Opts(ctypes.Structure):
     _fields_ = [("precision", c_int), ("format", c_int), ("block_width", c_int), ("doubling", c_int),
-                ("use_graphs", c_int), ("step_launches", c_int), ("realisations", c_int), ("reserved", c_int * 9)]
+                ("use_graphs", c_int), ("step_launches", c_int), ("realisations", c_int), ("operator_precision", c_int),
+                ("reserved", c_int * 8)]
 
 
 class Request(ctypes.Structure):
     _fields_ = [("kind", c_int), ("H", c_void_p), ("op", c_void_p), ("states", P_double), ("R", c_int),
-                ("M", c_int), ("precision", c_int), ("mu_out", P_double), ("seed", ctypes.c_ulonglong)]
+                ("M", c_int), ("precision", c_int), ("mu_out", P_double), ("seed", ctypes.c_ulonglong),
+                ("sigma_out", P_double), ("nump", c_int), ("band_width", ctypes.c_double),
+                ("band_center", ctypes.c_double)]
 
 
 # name -> (restype, argtypes)
@@ -87,6 +90,7 @@ SIGNATURES = {
                                   c_double, ctypes.POINTER(Opts), P_double, P_double, P_double, P_double]),
     "linqt_kubo_bastin_dev": (c_int, [c_void_p, c_void_p, c_void_p, c_void_p, c_void_p, c_int, c_int, c_int,
                                       c_double, c_double, ctypes.POINTER(Opts), c_void_p, c_void_p]),
+    "linqt_session_set_sm_share": (c_int, [c_void_p, ctypes.c_double]),
     "linqt_session_inject_barrier_timeout": (c_int, [c_void_p, c_int, ctypes.c_longlong]),
     "linqt_moments1d_nonorth": (c_int, [c_void_p, c_void_p, c_void_p, c_void_p, P_double, c_int, c_int, c_double,
                                         c_int, ctypes.POINTER(Opts), P_double, P_long]),
@@ -109,6 +113,7 @@ SIGNATURES = {
     "linqt_server_wait_all": (c_int, [c_void_p]),
     "linqt_server_release": (c_int, [c_void_p, c_long]),
     "linqt_server_cancel": (c_int, [c_void_p, c_long]),
+    "linqt_server_stats": (c_int, [c_void_p, P_long, P_long]),
     "linqt_server_destroy": (c_int, [c_void_p]),
     "linqt_tbmodel_load": (c_int, [ctypes.c_char_p, ctypes.POINTER(c_void_p)]),
     "linqt_tbmodel_destroy": (c_int, [c_void_p]),
@@ -124,7 +129,7 @@ SIGNATURES = {
 _lib = None
 
 
-ABI_VERSION = 2  # LINQT_ABI_VERSION of include/linqt_gpu.h
+ABI_VERSION = 3  # LINQT_ABI_VERSION of include/linqt_gpu.h
 
 
 def load():

@@ -23,6 +23,7 @@ from ._lib import Opts, check, load
 PREC_FP64, PREC_MIXED, PREC_FP32, PREC_MIXED_TF32, PREC_MIXED_FAST = 0, 1, 2, 3, 4
 KUBO_GREENWOOD, KUBO_BASTIN = 0, 1
 STORAGE_HERMITIAN_UPPER, STORAGE_GENERAL = 0, 1
+OP_C128, OP_C64 = 0, 1  # opts.operator_precision: complex128 or complex64 operator values (1D recursions)
 
 
 def _dp(a):
@@ -47,7 +48,7 @@ def _ptr(x):
 
 
 def make_opts(precision=PREC_FP64, fmt=0, block_width=0, doubling=0, step_launches=0, use_graphs=0,
-              realisations=0):
+              realisations=0, operator_precision=OP_C128):
     """Solver options (linqt_opts).  doubling: 0 auto, 1 force, 2 off.  step_launches: 1 = one launch per
     recursion step instead of the persistent cooperative kernel.  use_graphs: 1 = *_dev solves replayed
     from CUDA graphs after their first call.  realisations: 0 autotuned, 1 stacked in one launch,
@@ -57,6 +58,7 @@ def make_opts(precision=PREC_FP64, fmt=0, block_width=0, doubling=0, step_launch
                                                                          step_launches)
     o.use_graphs = use_graphs
     o.realisations = realisations
+    o.operator_precision = operator_precision
     return o
 
 
@@ -105,6 +107,11 @@ class Session:
         g, r = ctypes.c_int(), ctypes.c_long()
         check(load().linqt_session_graph_stats(self.h, ctypes.byref(g), ctypes.byref(r)))
         return g.value, r.value
+
+    def set_sm_share(self, share):
+        """Persistent kernels of this session use at most `share` of the device's co-resident
+        CTAs and run on its stream, next to other sessions' (see linqt_session_set_sm_share)."""
+        check(load().linqt_session_set_sm_share(self.h, share))
 
     def inject_barrier_timeout(self, extra_arrivals=1, spin_limit=1024):
         """Test hook: make this session's grid barriers wait for CTAs never launched (the next

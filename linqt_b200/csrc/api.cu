@@ -199,8 +199,10 @@ void DeviceOp::free_device() {
   cudaFree(d_rowptr);
   cudaFree(d_col);
   cudaFree(d_val64);
+  cudaFree(d_val32);
   d_rowptr = d_col = nullptr;
   d_val64 = nullptr;
+  d_val32 = nullptr;
   for (auto &kv : sell) {
     cudaFree(kv.second.d_perm);
     cudaFree(kv.second.d_off);
@@ -209,6 +211,18 @@ void DeviceOp::free_device() {
   }
   sell.clear();
   tuned.clear();
+}
+
+const float2 *DeviceOp::val32() {
+  std::lock_guard<std::mutex> g(mu);
+  if (!d_val32) {
+    std::vector<float2> v32(std::max(1L, nnz));
+    for (long k = 0; k < nnz; ++k) v32[k] = make_float2((float)val[k].x, (float)val[k].y);
+    LQ_CUDA(cudaSetDevice(device));
+    LQ_CUDA(cudaMalloc(&d_val32, sizeof(float2) * v32.size()));
+    LQ_CUDA(cudaMemcpy(d_val32, v32.data(), sizeof(float2) * v32.size(), cudaMemcpyHostToDevice));
+  }
+  return d_val32;
 }
 
 void DeviceOp::upload() {
@@ -314,7 +328,15 @@ static linqt_opts defaults(const linqt_opts *o) {
   if (o) d = *o;
   LQ_REQUIRE(d.format == LINQT_FORMAT_CSR || d.format == LINQT_FORMAT_SELL || d.format == LINQT_FORMAT_AUTO,
              "opts.format: unknown sparse format");
+  LQ_REQUIRE(d.operator_precision == 0 || d.operator_precision == 1, "opts.operator_precision must be 0 or 1");
   return d;
+}
+
+// complex64 operator values are a 1D-recursion option (persistent CSR kernels)
+static void require_c128_operators(const linqt_opts &o, const char *who) {
+  if (o.operator_precision != 0)
+    fail(LINQT_ERR_UNSUPPORTED, std::string(who) + ": complex64 operators (opts.operator_precision = 1) are "
+                                                   "available for the 1D moments only");
 }
 
 // ---------------------------------------------------------------------------
@@ -404,10 +426,14 @@ struct RecCfg {
 };
 
 static RecCfg pick_layout(Session *s, const DeviceOp &H, const std::string &key, int format, int Rc,
-                          const std::function<void(int, int)> &trial, float *best_ms = nullptr) {
+                          const std::function<void(int, int)> &trial, float *best_ms = nullptr,
+                          bool csr_only = false) {
   if (best_ms) *best_ms = -1;
   if (format == LINQT_FORMAT_CSR) return RecCfg{0, 0};
-  if (format == LINQT_FORMAT_SELL) return RecCfg{32, 0};
+  if (format == LINQT_FORMAT_SELL) {
+    if (csr_only) fail(LINQT_ERR_UNSUPPORTED, "complex64 operators: CSR layouts only");
+    return RecCfg{32, 0};
+  }
   DeviceOp &Hm = const_cast<DeviceOp &>(H);
   {
     std::lock_guard<std::mutex> g(Hm.mu);
@@ -424,6 +450,7 @@ static RecCfg pick_layout(Session *s, const DeviceOp &H, const std::string &key,
   // cache (more resident CTAs per SM); 8, 32: SELL-C-sigma
   for (int C : {0, -1, 8, 32})
     for (int sh = 0; sh < recur_shapes(Rc); ++sh) {
+      if (csr_only && C > 0) continue;
       trial(C, sh);
       LQ_CUDA(cudaEventRecord(a, s->stream));
       trial(C, sh);
@@ -459,6 +486,9 @@ static void moments1d_dev(Session *s, const DeviceOp &H, const DeviceOp *op, con
   LQ_REQUIRE(!op || op->n == H.n, "moments1d: operator dimension mismatch");
   const int N = H.n;
   const bool fp32 = o.precision != LINQT_PREC_FP64;
+  const bool c64 = o.operator_precision == 1;
+  if (c64 && o.step_launches)
+    fail(LINQT_ERR_UNSUPPORTED, "complex64 operators: the persistent recursion only (step_launches = 0)");
   const bool doubling = (o.doubling == 0 && op == nullptr) || o.doubling == 1;
   LQ_REQUIRE(!(doubling && op), "moments1d: the doubling identities need the identity operator");
   int Rc = o.block_width > 0 ? o.block_width : std::min(256, pow2_at_least(R));
@@ -474,7 +504,7 @@ static void moments1d_dev(Session *s, const DeviceOp &H, const DeviceOp *op, con
     const int Mt = std::min(M, 32), st = doubling ? (Mt + 1) / 2 : Mt;
     double2 *tdots = (double2 *)s->get("m1_trial_dots", sizeof(double2) * 2 * (size_t)st);
     return pick_layout(
-        s, H, layout_key("1d", op, w, fp32), o.format, w,
+        s, H, layout_key(c64 ? "1d64" : "1d", op, w, fp32), o.format, w,
         [&](int C, int shape) {
           // a short recursion on the first chunk (the real run below starts from scratch)
           void *b0 = T, *b1 = T + bw, *b2 = T + 2 * bw;
@@ -487,16 +517,17 @@ static void moments1d_dev(Session *s, const DeviceOp &H, const DeviceOp *op, con
               LQ_CUDA(cudaMemcpyAsync(b0, b2, bw, cudaMemcpyDeviceToDevice, s->stream));
             x0 = b0;
           }
-          recur_1d(s, H, b2, x0, b1, st, Mt, doubling ? 2 : 1, w, fp32, tdots, C, shape);
+          recur_1d(s, H, b2, x0, b1, st, Mt, doubling ? 2 : 1, w, fp32, tdots, C, shape, nullptr, 1, c64);
         },
-        best_ms);
+        best_ms, c64);
   };
   // LINQT_FORMAT_AUTO without a fixed block width: also the block width, among Rc, Rc/2, Rc/4
   // and Rc/8, by trial time per vector (a narrower block streams fewer bytes per row, which
   // can keep a large lattice's neighbour rows in L2), cached per operator pair, R and precision
   if (o.format == LINQT_FORMAT_AUTO && o.block_width <= 0 && !o.step_launches && Rc > 1) {
     DeviceOp &Hm = const_cast<DeviceOp &>(H);
-    const std::string wkey = "1dw:" + std::to_string(R) + ":" + layout_key("", op, Rc, fp32) + (doubling ? ":d" : "");
+    const std::string wkey = "1dw:" + std::to_string(R) + ":" + layout_key(c64 ? "c64" : "", op, Rc, fp32) +
+                             (doubling ? ":d" : "");
     int w = 0;
     {
       std::lock_guard<std::mutex> g(Hm.mu);
@@ -543,7 +574,7 @@ static void moments1d_dev(Session *s, const DeviceOp &H, const DeviceOp *op, con
         }
         x0 = b0;
       }
-      recur_1d(s, H, phi, x0, b1, steps, M, doubling ? 2 : 1, Rc, fp32, cd, cfg.sellC, cfg.shape);
+      recur_1d(s, H, phi, x0, b1, steps, M, doubling ? 2 : 1, Rc, fp32, cd, cfg.sellC, cfg.shape, nullptr, 1, c64);
       launches += 2;
       continue;
     }
@@ -607,11 +638,15 @@ static void realisations_stacked(Session *s, const DeviceOp *const *Hs, int S, c
   const bool fp32 = o.precision != LINQT_PREC_FP64;
   const int N = H0.n;
   const size_t esz = fp32 ? sizeof(float2) : sizeof(double2);
-  // the S value sets side by side (FP64 for either precision of the vectors)
-  char *vals = (char *)s->get("real_vals", sizeof(double2) * (size_t)S * std::max(1L, H0.nnz));
+  // the S value sets side by side: complex128, or the complex64 copies with
+  // opts.operator_precision = 1 (for either precision of the vectors)
+  const bool c64 = o.operator_precision == 1;
+  const size_t vsz = c64 ? sizeof(float2) : sizeof(double2);
+  char *vals = (char *)s->get(c64 ? "real_vals32" : "real_vals", vsz * (size_t)S * std::max(1L, H0.nnz));
   for (int r = 0; r < S; ++r)
-    LQ_CUDA(cudaMemcpyAsync(vals + sizeof(double2) * (size_t)r * H0.nnz, Hs[r]->d_val64, sizeof(double2) * H0.nnz,
-                            cudaMemcpyDeviceToDevice, s->stream));
+    LQ_CUDA(cudaMemcpyAsync(vals + vsz * (size_t)r * H0.nnz,
+                            c64 ? (const void *)const_cast<DeviceOp *>(Hs[r])->val32() : (const void *)Hs[r]->d_val64,
+                            vsz * H0.nnz, cudaMemcpyDeviceToDevice, s->stream));
   const int steps = (M + 1) / 2;  // doubling identities
   const size_t blk = esz * (size_t)N * R;
   char *T = (char *)s->get("m1_T", 3 * blk);
@@ -621,7 +656,7 @@ static void realisations_stacked(Session *s, const DeviceOp *const *Hs, int S, c
     PhaseScope ph(s, PH_RECURSION);
     chunk_block(s, states, N, R, 0, R, phi, fp32);
     LQ_CUDA(cudaMemcpyAsync(b0, phi, blk, cudaMemcpyDeviceToDevice, s->stream));
-    recur_1d(s, H0, phi, b0, b1, steps, M, 2, R, fp32, dots, 0, 0, vals, S);
+    recur_1d(s, H0, phi, b0, b1, steps, M, 2, R, fp32, dots, 0, 0, vals, S, c64);
     ph.launches(3);
   }
   PhaseScope p3(s, PH_OTHER);
@@ -656,7 +691,7 @@ static void moments1d_realisations_dev(Session *s, const DeviceOp *const *Hs, in
   if (mode == 0) {
     DeviceOp &Hm = const_cast<DeviceOp &>(H0);
     const std::string key = "real:" + std::to_string(S) + ":" + std::to_string(Rs) + ":" +
-                            (o.precision != LINQT_PREC_FP64 ? "f32" : "f64");
+                            (o.precision != LINQT_PREC_FP64 ? "f32" : "f64") + (o.operator_precision ? ":c64" : "");
     {
       std::lock_guard<std::mutex> g(Hm.mu);
       auto it = Hm.tuned.find(key);
@@ -830,6 +865,7 @@ static void moments2d_dev(Session *s, const DeviceOp &H, const DeviceOp *opl, co
                           const double2 *states, int R, int M, const linqt_opts &o, double2 *mu) {
   LQ_REQUIRE(R > 0 && M > 0, "moments2d: R and M must be positive");
   LQ_REQUIRE((!opl || opl->n == H.n) && (!opr || opr->n == H.n), "moments2d: operator dimension mismatch");
+  require_c128_operators(o, "moments2d");
   const bool fp32 = prepare_precision(o, H, opl, opr);
   const int N = H.n;
   const size_t esz = fp32 ? sizeof(float2) : sizeof(double2);
@@ -887,6 +923,7 @@ static void kubo_solve(Session *s, const DeviceOp &H, const DeviceOp *opl, const
                        const double2 *states, int R, int M, int nump, int formula, double bw, double bc,
                        const linqt_opts &o, double2 *mu, double *out) {
   LQ_REQUIRE(R > 0 && M > 0, "kubo: R and M must be positive");
+  require_c128_operators(o, "kubo");
   LQ_REQUIRE(!out || nump >= M, "kubo: nump must be >= M (pre_factors are indexed m < M, src/Bastin_FFTs.cpp:18-21)");
   LQ_REQUIRE(formula == LINQT_KUBO_BASTIN || formula == LINQT_KUBO_GREENWOOD, "kubo: unknown formula");
   LQ_REQUIRE(bw > 0, "kubo: band_width must be positive");
@@ -968,6 +1005,7 @@ static void moments_td_dev(Session *s, const DeviceOp &H, const DeviceOp *opl, c
                            const double2 *states, int R, int M, int NT, double dt, double band_width,
                            double band_center, const linqt_opts &o, double2 *mu) {
   LQ_REQUIRE(R > 0 && M > 0 && NT > 0, "time correlations: R, M and NT must be positive");
+  require_c128_operators(o, "time correlations");
   LQ_REQUIRE((!opl || opl->n == H.n) && (!opr || opr->n == H.n), "time correlations: operator dimension mismatch");
   LQ_REQUIRE(band_width > 0 && dt >= 0, "time correlations: band_width > 0 and dt >= 0");
   LQ_REQUIRE(o.precision == LINQT_PREC_FP64, "time correlations: FP64 only");
@@ -1023,6 +1061,15 @@ static void kubo_bastin_dev(Session *s, const DeviceOp &H, const DeviceOp *opl, 
                             const double2 *states, int R, int M, int nump, double bw, double bc,
                             const linqt_opts &o, double2 *mu, double *out) {
   kubo_solve(s, H, opl, opr, states, R, M, nump, LINQT_KUBO_BASTIN, bw, bc, o, mu, out);
+}
+
+void kubo_bastin_for_server(Session *s, const DeviceOp &H, const DeviceOp *op, const double2 *states, int R, int M,
+                            int nump, double bw, double bc, int precision, int block_width, double2 *mu,
+                            double *out) {
+  linqt_opts o = defaults(nullptr);
+  o.precision = precision;
+  o.block_width = block_width;
+  kubo_bastin_dev(s, H, op, op, states, R, M, nump, bw, bc, o, mu, out);
 }
 
 // ---------------------------------------------------------------------------
@@ -1117,6 +1164,16 @@ int linqt_session_trim(linqt_session *s) {
 
 int linqt_session_enable_timing(linqt_session *s, int on) {
   return guarded([&] { resolve(s)->timing = on != 0; });
+}
+
+int linqt_session_set_sm_share(linqt_session *s, double share) {
+  return guarded([&] {
+    LQ_REQUIRE(s, "NULL session");
+    LQ_REQUIRE(share > 0.0 && share <= 1.0, "SM share must be in (0, 1]");
+    Session *r = resolve(s);
+    if (r->coop_share != share) r->drop_graphs();  // captured grids have the old size
+    r->coop_share = share;
+  });
 }
 
 int linqt_session_inject_barrier_timeout(linqt_session *s, int extra_arrivals, long long spin_limit) {
@@ -1342,7 +1399,7 @@ static void check_nonorth(const linqt_op *H, const linqt_op *S, const linqt_opts
   check_op(H, "H");
   check_op(S, "S");
   LQ_REQUIRE(tol > 0 && maxit > 0, "moments1d_nonorth: tolerance and iteration limit must be positive");
-  if (opts && opts->precision != LINQT_PREC_FP64)
+  if (opts && (opts->precision != LINQT_PREC_FP64 || opts->operator_precision != 0))
     fail(LINQT_ERR_UNSUPPORTED, "moments1d_nonorth: FP64 only (the BiCGSTAB solves run in FP64)");
 }
 

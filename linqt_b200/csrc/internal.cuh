@@ -173,6 +173,9 @@ struct DeviceOp {
   std::map<std::string, int> tuned;
   std::mutex mu;
 
+  // complex64 copy of the expanded values (each FP64 value rounded once), made on first use
+  float2 *d_val32 = nullptr;
+  const float2 *val32();
   CsrView csr64() const { return CsrView{n, nnz, d_rowptr, d_col, d_val64}; }
   void free_device();
   void upload();
@@ -207,6 +210,9 @@ struct Session {
   bool barrier_used = false;  // a persistent kernel ran since the last error check
   // fault injection for tests (linqt_session_inject_barrier_timeout): grid barriers await
   // inject_extra more CTAs than launched and give up after inject_limit polls
+  // fraction of the device's co-resident CTAs the session's persistent grids may use
+  // (linqt_session_set_sm_share); below 1 they launch on the session stream, not the lane
+  double coop_share = 1.0;
   int inject_extra = 0;
   long long inject_limit = 0;
   bool barrier_cfg_dirty = false;
@@ -335,8 +341,11 @@ void recur_lr(Session *s, const DeviceOp &H, const DeviceOp *V, void *Lstore, vo
 // stacked != NULL: nreal realisations sharing H's pattern, values [nreal][nnz]; realisation r
 // owns columns [r R/nreal, (r+1) R/nreal), served by its own group of CTAs, and dots becomes
 // [nreal][steps][2]
+// c64: the operator's complex64 value copy (FP32 values, FP64 accumulation); CSR layouts only,
+// and `stacked` then holds float2 values
 void recur_1d(Session *s, const DeviceOp &H, const void *phi, void *x0, void *b1, int steps, int M, int mode, int R,
-              bool fp32, double2 *dots, int sellC, int shape = 0, const void *stacked = nullptr, int nreal = 1);
+              bool fp32, double2 *dots, int sellC, int shape = 0, const void *stacked = nullptr, int nreal = 1,
+              bool c64 = false);
 // X <- sum_{s<K} coef[s] T_s(H) X on an FP64 block of R columns (a, b: scratch blocks), one
 // persistent launch (recur.cu)
 void cheb_series(Session *s, const DeviceOp &H, void *X, void *a, void *b, const double2 *coef, int K, int R);
@@ -352,7 +361,7 @@ void moments1d_nonorth_dev(Session *s, const DeviceOp &H, const DeviceOp *op, co
 struct GridBarrier;
 GridBarrier *barrier_for(Session *s);
 // occupancy-sized cooperative grid and a launch through the device's cooperative lane (recur.cu)
-int coop_grid(const void *func, int sm_count, long max_blocks, size_t smem);
+int coop_grid(const void *func, int sm_count, long max_blocks, size_t smem, double share = 1.0);
 void coop_launch(Session *s, const void *f, int grid, void **args, size_t smem);
 
 // small utilities (util.cu)

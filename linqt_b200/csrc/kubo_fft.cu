@@ -13,7 +13,7 @@
 // and ket_m = R_m[l] (= OPR T_m(H) phi).  Products of the transforms are summed over
 // sites into p[k] (and w[k]).
 //
-// Design: one CTA per site at a time (persistent over a contiguous chunk of sites),
+// Design: one CTA per site at a time (persistent, the CTAs interleaved over the sites),
 // all 8 (or 4) transforms of the site in shared memory.  nump = 16 * 16 * R3,
 // R3 in {1, 2, 4, 8}: pass 1 does 16-point DFTs in registers straight from the
 // global loads, pass 2 16-point DFTs, pass 3 R3-point DFTs; every pass reads its
@@ -241,9 +241,13 @@ __global__ void __launch_bounds__(kFftThreads)
   double2 *tw2 = tw1 + 16 * P;
   double2 *pfs = tw2 + 16 * R3;
   Tin *stage = reinterpret_cast<Tin *>(pfs + M);  // 2 buffers of 2M
-  const long lbeg = (long)blockIdx.x * chunk;
-  const long lend = min(K, lbeg + chunk);
-  if (lbeg < lend) stage_site(stage, L, Rv, K, M, lbeg);
+  // Sites blockIdx.x, blockIdx.x + gridDim.x, ...: at any time all CTAs work on neighbouring
+  // sites, so each row m of the stores is read in one place (one page, L2 lines shared by the
+  // CTAs) rather than at gridDim.x places K / gridDim.x sites apart (at K = 4e6 sites the
+  // rows are 64 MB long and a contiguous split touched a different page per CTA and row).
+  (void)chunk;
+  const long lstep = gridDim.x;
+  if ((long)blockIdx.x < K) stage_site(stage, L, Rv, K, M, blockIdx.x);
   for (int t = threadIdx.x; t < 16 * P; t += blockDim.x) {
     const int k2 = t / P, m1 = t % P;
     double sn, cs;
@@ -266,11 +270,11 @@ __global__ void __launch_bounds__(kFftThreads)
   for (int j = 0; j < ND; ++j) accp[j] = accw[j] = make_double2(0, 0);
 
   int cur = 0;
-  for (long l = lbeg; l < lend; ++l) {
+  for (long l = blockIdx.x; l < K; l += lstep) {
     cp_async_wait_all();
     __syncthreads();  // stage[cur] complete and visible; the previous site is fully consumed
     const Tin *bra = stage + cur * 2 * M, *ket = bra + M;
-    if (l + 1 < lend) stage_site(stage + (cur ^ 1) * 2 * M, L, Rv, K, M, l + 1);
+    if (l + lstep < K) stage_site(stage + (cur ^ 1) * 2 * M, L, Rv, K, M, l + lstep);
     // ---- pass 1: x_s[m1 + P m2], m2 < 16 -> 16-point DFT over m2, twiddle w_n^{m1 k2}
     for (int item = threadIdx.x; item < NSEQ * P; item += blockDim.x) {
       const int s = item / P, m1 = item % P;

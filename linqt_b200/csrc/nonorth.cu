@@ -373,7 +373,7 @@ void moments1d_nonorth_dev(Session *s, const DeviceOp &H, const DeviceOp *op, co
   LQ_CUDA(cudaMemcpyAsync(d_invd, invd.data(), sizeof(double2) * N, cudaMemcpyHostToDevice, s->stream));
   char *W = (char *)s->get("no_blocks", 11 * blk);
   const void *f = (const void *)k_nonorth_1d;
-  const int grid = coop_grid(f, s->sm_count, ((long)N * Rb + kT - 1) / kT, 0);
+  const int grid = coop_grid(f, s->sm_count, ((long)N * Rb + kT - 1) / kT, 0, s->coop_share);
   double2 *part = (double2 *)s->get("no_part", sizeof(double2) * 3 * (size_t)grid * Rb);
   double2 *dots = (double2 *)s->get("no_dots", sizeof(double2) * (size_t)M * Rb);
   long long *its = (long long *)s->get("no_iters", sizeof(long long) * kMaxCols);

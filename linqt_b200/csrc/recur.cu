@@ -304,9 +304,9 @@ __global__ void __launch_bounds__(kThreads)
 // The recursion runs in place: T_{s+1} overwrites T_{s-1}; T_1 goes to b1.
 // partials: [steps][grid][2] per-CTA sums.
 // ---------------------------------------------------------------------------
-template <class T, int TPR, int VPT, bool STACKED>
+template <class T, class HV, int TPR, int VPT, bool STACKED>
 __global__ void __launch_bounds__(kThreads)
-    k_recur_1d(int n, const int *rp, const int *ci, const double2 *hv, const typename cplx_t<T>::type *phi, typename cplx_t<T>::type *x0, typename cplx_t<T>::type *b1,
+    k_recur_1d(int n, const int *rp, const int *ci, const HV *hv, const typename cplx_t<T>::type *phi, typename cplx_t<T>::type *x0, typename cplx_t<T>::type *b1,
                int steps, int M, int mode, double2 *__restrict__ partials, Barrier *bar, int cache,
                const int *__restrict__ sperm, const int *__restrict__ soff, int sC, long vstride, int nreal,
                int ldx_rt) {
@@ -327,7 +327,7 @@ __global__ void __launch_bounds__(kThreads)
   const int r0 = min(n, blockIdx.x * per), r1 = min(n, r0 + per);
   if (cache) {
     extern __shared__ __align__(16) unsigned char smc1[];
-    cache_rows<double2>(rp, ci, hv, r0, r1, smc1, rp, ci, hv);
+    cache_rows<HV>(rp, ci, hv, r0, r1, smc1, rp, ci, hv);
     __syncthreads();
   }
   const int rfirst = cache ? r0 : bl * gpb, rend = cache ? r1 : n;  // as in k_recur_lr
@@ -344,7 +344,7 @@ __global__ void __launch_bounds__(kThreads)
 #pragma unroll
       for (int u = 0; u < VPT; ++u) acc[u] = make_double2(0, 0);
 #pragma unroll 4
-      for (int k = b; k < e; k += st) gather_fma<C, VPT>(hv[k], cur + (size_t)ci[k] * ldx + coff + c0, acc);
+      for (int k = b; k < e; k += st) gather_fma<C, VPT>(to_d2(hv[k]), cur + (size_t)ci[k] * ldx + coff + c0, acc);
       const size_t base = (size_t)row * ldx + coff + c0;
       C pv[VPT], yv[VPT], xv[VPT];
       if (prev) ld_row<VPT>(prev + base, pv);
@@ -487,13 +487,16 @@ size_t max_slice_bytes(const DeviceOp &H, const DeviceOp *V, int grid, size_t es
 // Cooperative grid: as many co-resident CTAs as fit (at most one CTA's worth of rows per
 // group of TPR threads).  The operator slices are cached in shared memory when they fit.
 int coop_setup(const void *func, int sm_count, const DeviceOp &H, const DeviceOp *V, int tpr, size_t esz,
-               size_t *smem, bool allow_cache = true) {
+               size_t *smem, bool allow_cache, double share) {
   const int n = H.n;
   const long need = ((long)n * tpr + kThreads - 1) / kThreads;
   int per_sm = 0;
   LQ_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, func, kThreads, 0));
   if (per_sm <= 0) fail(LINQT_ERR_UNSUPPORTED, "persistent recursion: kernel does not fit on an SM");
-  const int grid0 = (int)std::max(1L, std::min((long)per_sm * sm_count, need));
+  // a session with an SM share (linqt_session_set_sm_share) keeps its grid to that fraction
+  // of the co-resident CTAs, so that grids of sessions whose shares add up to 1 fit together
+  const auto cap = [&](int p) { return std::max(1L, (long)(p * (double)sm_count * share)); };
+  const int grid0 = (int)std::max(1L, std::min(cap(per_sm), need));
   const size_t limit = 96 * 1024;
   // the attribute is per function and shared by all threads: always the same value
   LQ_CUDA(cudaFuncSetAttribute(func, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)limit));
@@ -506,7 +509,7 @@ int coop_setup(const void *func, int sm_count, const DeviceOp &H, const DeviceOp
     int p = 0;
     LQ_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&p, func, kThreads, bytes));
     if (p <= 0) break;
-    const int g = (int)std::max(1L, std::min((long)p * sm_count, need));
+    const int g = (int)std::max(1L, std::min(cap(p), need));
     if (g >= grid) {
       *smem = bytes;
       return grid;
@@ -521,11 +524,12 @@ int coop_setup(const void *func, int sm_count, const DeviceOp &H, const DeviceOp
 
 // Co-resident CTAs of kThreads threads for func with smem bytes of dynamic shared memory,
 // at most max_blocks.
-int coop_grid(const void *func, int sm_count, long max_blocks, size_t smem) {
+int coop_grid(const void *func, int sm_count, long max_blocks, size_t smem, double share) {
   int per_sm = 0;
   LQ_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, func, kThreads, smem));
   if (per_sm <= 0) fail(LINQT_ERR_UNSUPPORTED, "persistent kernel does not fit on an SM");
-  return (int)std::max(1L, std::min((long)per_sm * sm_count, max_blocks));
+  const long cap = std::max(1L, (long)(per_sm * (double)sm_count * share));
+  return (int)std::max(1L, std::min(cap, max_blocks));
 }
 
 // Cooperative kernels of all sessions on a device run one after another on one lane
@@ -540,7 +544,9 @@ struct CoopLane {
 };
 
 void coop_launch(Session *s, const void *f, int grid, void **args, size_t smem) {
-  if (s->capturing) {  // a graph capture of this session's stream (api.cu, with_graph)
+  // a graph capture of this session's stream (api.cu, with_graph), or a session whose grids
+  // are sized to its SM share: launched on the session's own stream
+  if (s->capturing || s->coop_share < 1.0) {
     LQ_CUDA(cudaLaunchCooperativeKernel(f, dim3(grid), dim3(kThreads), args, smem, s->stream));
     return;
   }
@@ -592,7 +598,7 @@ struct LRF {
     const C *ph = (const C *)phi;
     const void *f = V ? (const void *)k_recur_lr<T, TPR, VPT, true> : (const void *)k_recur_lr<T, TPR, VPT, false>;
     size_t smem = 0;
-    const int grid = coop_setup(f, s->sm_count, H, V, TPR, sizeof(double2), &smem, sellC == 0);
+    const int grid = coop_setup(f, s->sm_count, H, V, TPR, sizeof(double2), &smem, sellC == 0, s->coop_share);
     sellC = std::max(sellC, 0);  // -1: CSR without the shared-memory cache
     int cache = smem > 0;
     int sc = sellC;
@@ -606,11 +612,13 @@ struct LRF {
 template <class T, int TPR, int VPT>
 struct OneDF {
   static void run(Session *s, const DeviceOp &H, const void *phi, void *x0, void *b1, int steps, int M, int mode,
-                  double2 *dots, Barrier *bar, int sellC, const void *stacked, int nreal) {
+                  double2 *dots, Barrier *bar, int sellC, const void *stacked, int nreal, bool c64) {
     using C = typename cplx_t<T>::type;
-    const double2 *hv = stacked ? (const double2 *)stacked : H.d_val64;
+    // complex64 operator values (FP32, accumulated in FP64) or the complex128 ones
+    const void *hv = stacked ? stacked : (c64 ? (const void *)const_cast<DeviceOp &>(H).val32() : H.d_val64);
     long vstride = stacked ? H.nnz : 0;
     LQ_REQUIRE(!stacked || (nreal >= 1 && sellC <= 0), "stacked realisations: CSR layout only");
+    LQ_REQUIRE(!c64 || sellC <= 0, "complex64 operators: CSR layout only");
     const int *hci = H.d_col, *sperm = nullptr, *soff = nullptr;
     if (sellC > 0) {
       const DeviceOp::Sell &L = const_cast<DeviceOp &>(H).ensure_sell(sellC);
@@ -619,10 +627,14 @@ struct OneDF {
       sperm = L.d_perm;
       soff = L.d_off;
     }
-    const void *f = stacked ? (const void *)k_recur_1d<T, TPR, VPT, true> : (const void *)k_recur_1d<T, TPR, VPT, false>;
+    const void *f = c64 ? (stacked ? (const void *)k_recur_1d<T, float2, TPR, VPT, true>
+                                   : (const void *)k_recur_1d<T, float2, TPR, VPT, false>)
+                        : (stacked ? (const void *)k_recur_1d<T, double2, TPR, VPT, true>
+                                   : (const void *)k_recur_1d<T, double2, TPR, VPT, false>);
     size_t smem = 0;
     // the shared-memory operator cache holds one value set: not with stacked realisations
-    int grid = coop_setup(f, s->sm_count, H, nullptr, TPR, sizeof(double2), &smem, sellC == 0 && !stacked);
+    int grid = coop_setup(f, s->sm_count, H, nullptr, TPR, c64 ? sizeof(float2) : sizeof(double2), &smem,
+                          sellC == 0 && !stacked, s->coop_share);
     sellC = std::max(sellC, 0);  // -1: CSR without the shared-memory cache
     if (stacked) grid = std::max(nreal, grid / nreal * nreal);  // equal CTA groups per realisation
     int cache = smem > 0;
@@ -653,7 +665,7 @@ struct SeriesF {
   static void run(Session *s, const DeviceOp &H, void *X, void *a, void *b, const double2 *coef, int K, Barrier *bar) {
     const void *f = (const void *)k_cheb_series<TPR, VPT>;
     size_t smem = 0;
-    const int grid = coop_setup(f, s->sm_count, H, nullptr, TPR, sizeof(double2), &smem, true);
+    const int grid = coop_setup(f, s->sm_count, H, nullptr, TPR, sizeof(double2), &smem, true, s->coop_share);
     int cache = smem > 0;
     int n = H.n;
     const double2 *hv = H.d_val64;
@@ -690,7 +702,7 @@ void dispatch(int R, int shape, Args &&...args) {
 // sticky until check_device_errors reads it.
 GridBarrier *barrier_for(Session *s) {
   Barrier *bar = (Barrier *)s->get("rec_barrier", sizeof(Barrier));
-  LQ_CUDA(cudaMemsetAsync(bar, 0, 2 * sizeof(unsigned), s->stream));
+  LQ_CUDA(cudaMemsetAsync(bar, 0, kBarrierResetBytes, s->stream));
   if (s->barrier_cfg_dirty || (s->barrier_cfg_ptr != bar && (s->inject_extra || s->inject_limit))) {
     LQ_CUDA(cudaMemcpyAsync(&bar->extra, &s->inject_extra, sizeof(int), cudaMemcpyHostToDevice, s->stream));
     LQ_CUDA(cudaMemcpyAsync(&bar->spin_limit, &s->inject_limit, sizeof(long long), cudaMemcpyHostToDevice,
@@ -727,13 +739,13 @@ void recur_lr(Session *s, const DeviceOp &H, const DeviceOp *V, void *Lstore, vo
 }
 
 void recur_1d(Session *s, const DeviceOp &H, const void *phi, void *x0, void *b1, int steps, int M, int mode, int R,
-              bool fp32, double2 *dots, int sellC, int shape, const void *stacked, int nreal) {
+              bool fp32, double2 *dots, int sellC, int shape, const void *stacked, int nreal, bool c64) {
   Barrier *bar = barrier_for(s);
   const int Rw = stacked ? R / nreal : R;  // columns per CTA
   if (fp32)
-    dispatch<float, OneDF>(Rw, shape, s, H, phi, x0, b1, steps, M, mode, dots, bar, sellC, stacked, nreal);
+    dispatch<float, OneDF>(Rw, shape, s, H, phi, x0, b1, steps, M, mode, dots, bar, sellC, stacked, nreal, c64);
   else
-    dispatch<double, OneDF>(Rw, shape, s, H, phi, x0, b1, steps, M, mode, dots, bar, sellC, stacked, nreal);
+    dispatch<double, OneDF>(Rw, shape, s, H, phi, x0, b1, steps, M, mode, dots, bar, sellC, stacked, nreal, c64);
 }
 
 void cheb_series(Session *s, const DeviceOp &H, void *X, void *a, void *b, const double2 *coef, int K, int R) {

@@ -28,6 +28,9 @@ void moments1d_for_server(Session *s, const DeviceOp &H, const DeviceOp *op, con
                           int precision, int block_width, double2 *mu);
 void moments2d_for_server(Session *s, const DeviceOp &H, const DeviceOp *opl, const DeviceOp *opr,
                           const double2 *states, int R, int M, int precision, int block_width, double2 *mu);
+void kubo_bastin_for_server(Session *s, const DeviceOp &H, const DeviceOp *op, const double2 *states, int R, int M,
+                            int nump, double bw, double bc, int precision, int block_width, double2 *mu,
+                            double *out);
 }  // namespace linqt
 
 using namespace linqt;
@@ -35,6 +38,10 @@ using namespace linqt;
 namespace {
 
 typedef std::chrono::steady_clock clk;
+
+// Fraction of the device the slots' persistent grids share (each slot kSlotShare / slots):
+// a little below 1 leaves room for CTAs of different kernels that do not pack evenly.
+constexpr double kSlotShare = 0.9;
 
 struct Job {
   long ticket = 0;
@@ -44,6 +51,7 @@ struct Job {
   size_t footprint = 0;
   int block_width = 1;
   int status = 0;  // 0 pending, 1 running, 2 done, <0 error
+  bool alone = false;  // ran out of memory next to other requests: runs again with none beside it
   double latency_ms = 0;
   std::string error;
   clk::time_point t_submit;
@@ -59,9 +67,13 @@ size_t estimate_footprint(const linqt_request &r, int n, int sm_count, int Rc) {
     return io + esz * (size_t)n * Rc * 3 +
            sizeof(double2) * (2 * steps * ((size_t)sm_count * 32 + 1) + 2 * steps * chunks) + (1 << 20);
   }
-  const size_t digits = 6 * (size_t)i8_digits(r.precision) * n * Rc * r.M;  // INT8 contraction planes
-  return io + esz * (size_t)n * Rc * (2 * (size_t)r.M + 4) + digits + sizeof(double2) * (size_t)r.M * r.M * 66 +
-         (1 << 20);
+  // INT8 contraction planes: the solver's chunking counts 3 bytes per digit and stored value
+  const size_t digits = 3 * (size_t)i8_digits(r.precision) * n * Rc * (2 * (size_t)r.M + 4);
+  // sigma(E): the per-site transforms' partial sums and the 3*nump outputs
+  const size_t fft = r.sigma_out ? sizeof(double2) * 2 * (size_t)r.nump * 1024 + 3 * sizeof(double) * r.nump : 0;
+  const size_t total = io + esz * (size_t)n * Rc * (2 * (size_t)r.M + 4) + digits +
+                       sizeof(double2) * (size_t)r.M * r.M * 66 + fft + (1 << 20);
+  return total + total / 20;  // 5 % for the buffers the estimate does not itemise
 }
 
 // Vector-block width of a request: the widest power of two up to R whose footprint fits in
@@ -86,6 +98,8 @@ struct linqt_server {
   std::unordered_map<long, std::shared_ptr<Job>> jobs;
   long next_ticket = 1;
   int running = 0;
+  long timeouts_retried = 0;  // requests re-run on the cooperative lane after a co-residency timeout
+  long nomem_retried = 0;     // requests re-run alone after their workspaces did not fit
   bool stop = false;
   std::vector<std::thread> workers;
   // pinned host blocks by power-of-two capacity, recycled across requests
@@ -134,8 +148,15 @@ struct linqt_server {
       std::shared_ptr<Job> job;
       {
         std::unique_lock<std::mutex> g(mu);
-        // admission: the oldest queued job, once its footprint fits next to the running ones
-        cv.wait(g, [&] { return stop || (!queue.empty() && in_use + queue.front()->footprint <= budget); });
+        // admission: the oldest queued job, once its footprint fits next to the running ones;
+        // a job marked `alone` (it ran out of memory next to others) waits until none runs,
+        // and nothing behind it is admitted meanwhile
+        cv.wait(g, [&] {
+          if (stop) return true;
+          if (queue.empty()) return false;
+          const Job &f = *queue.front();
+          return f.alone ? running == 0 : in_use + f.footprint <= budget;
+        });
         if (stop && queue.empty()) return;
         if (queue.empty()) continue;
         job = queue.front();
@@ -144,41 +165,75 @@ struct linqt_server {
         job->status = 1;
         running++;
       }
+      if (job->alone) cudaMemPoolTrimTo(pool, 0);  // the pool's cached blocks back to the device
       int rc = 0;
       std::string err;
       void *res_host = nullptr;
       size_t res_cap = 0;
-      try {
-        Session &s = sess->s;
-        const DeviceOp &H = job->req.H->op;
-        const DeviceOp *op = job->req.op ? &job->req.op->op : nullptr;
-        const int n = H.n, R = job->req.R, M = job->req.M;
-        const size_t sb = sizeof(double2) * (size_t)R * n;
-        const size_t mb = sizeof(double2) * (size_t)M * (job->req.kind == LINQT_REQ_DOS ? 1 : M);
-        s.hbm_budget = job->footprint;  // fixed per request: chunking independent of the other requests
-        double2 *d_st = (double2 *)s.get("io_states", sb);
-        double2 *d_mu = (double2 *)s.get("io_mu", mb);
-        res_host = pinned_get(mb, &res_cap);
-        if (job->states)
-          LQ_CUDA(cudaMemcpyAsync(d_st, job->states, sb, cudaMemcpyHostToDevice, s.stream));
-        else
-          random_phase_states(&s, n, R, job->req.seed, d_st);
-        if (job->req.kind == LINQT_REQ_DOS)
-          moments1d_for_server(&s, H, op, d_st, R, M, job->req.precision, job->block_width, d_mu);
-        else
-          moments2d_for_server(&s, H, op, op, d_st, R, M, job->req.precision, job->block_width, d_mu);
-        LQ_CUDA(cudaMemcpyAsync(res_host, d_mu, mb, cudaMemcpyDeviceToHost, s.stream));
-        LQ_CUDA(cudaStreamSynchronize(s.stream));
-        check_device_errors(&s);
-        s.trim();  // stream-ordered frees back to the pool for the next request
-        std::memcpy(job->req.mu_out, res_host, mb);
-      } catch (const Error &e) {
-        rc = e.code;
-        err = e.what();
-        sess->s.trim();
-      } catch (const std::exception &e) {
-        rc = LINQT_ERR_INTERNAL;
-        err = e.what();
+      // Persistent recursions of the slots run side by side, each grid sized to its share of
+      // the device.  A grid that does not become co-resident in time ends its solve with
+      // LINQT_ERR_TIMEOUT; the request then runs again at once on the device-wide cooperative
+      // lane.  A request whose workspaces did not fit next to the others (LINQT_ERR_NOMEM: the
+      // footprint is an estimate) goes back to the head of the queue to run alone.
+      for (int attempt = 0; attempt < 2; ++attempt) {
+        sess->s.coop_share = (attempt == 0 && max_active > 1 && !job->alone) ? kSlotShare / max_active : 1.0;
+        rc = 0;
+        err.clear();
+        try {
+          Session &s = sess->s;
+          const DeviceOp &H = job->req.H->op;
+          const DeviceOp *op = job->req.op ? &job->req.op->op : nullptr;
+          const int n = H.n, R = job->req.R, M = job->req.M;
+          const size_t sb = sizeof(double2) * (size_t)R * n;
+          const size_t mb = sizeof(double2) * (size_t)M * (job->req.kind == LINQT_REQ_DOS ? 1 : M);
+          s.hbm_budget = job->footprint;  // fixed per request: chunking independent of the other requests
+          double2 *d_st = (double2 *)s.get("io_states", sb);
+          double2 *d_mu = (double2 *)s.get("io_mu", mb);
+          if (!res_host) res_host = pinned_get(mb, &res_cap);
+          if (job->states)
+            LQ_CUDA(cudaMemcpyAsync(d_st, job->states, sb, cudaMemcpyHostToDevice, s.stream));
+          else
+            random_phase_states(&s, n, R, job->req.seed, d_st);
+          const bool sigma = job->req.kind == LINQT_REQ_KUBO_BASTIN && job->req.sigma_out;
+          const size_t ob = sigma ? 3 * sizeof(double) * (size_t)job->req.nump : 0;
+          double *d_out = sigma ? (double *)s.get("io_kubo", ob) : nullptr;
+          if (job->req.kind == LINQT_REQ_DOS)
+            moments1d_for_server(&s, H, op, d_st, R, M, job->req.precision, job->block_width, d_mu);
+          else if (sigma)
+            kubo_bastin_for_server(&s, H, op, d_st, R, M, job->req.nump, job->req.band_width,
+                                   job->req.band_center, job->req.precision, job->block_width, d_mu, d_out);
+          else
+            moments2d_for_server(&s, H, op, op, d_st, R, M, job->req.precision, job->block_width, d_mu);
+          LQ_CUDA(cudaMemcpyAsync(res_host, d_mu, mb, cudaMemcpyDeviceToHost, s.stream));
+          if (sigma)
+            LQ_CUDA(cudaMemcpyAsync(job->req.sigma_out, d_out, ob, cudaMemcpyDeviceToHost, s.stream));
+          LQ_CUDA(cudaStreamSynchronize(s.stream));
+          check_device_errors(&s);
+          s.trim();  // stream-ordered frees back to the pool for the next request
+          std::memcpy(job->req.mu_out, res_host, mb);
+        } catch (const Error &e) {
+          rc = e.code;
+          err = e.what();
+          sess->s.trim();
+        } catch (const std::exception &e) {
+          rc = LINQT_ERR_INTERNAL;
+          err = e.what();
+        }
+        if (rc != LINQT_ERR_TIMEOUT || sess->s.coop_share >= 1.0) break;
+        std::lock_guard<std::mutex> g(mu);
+        timeouts_retried++;
+      }
+      if (rc == LINQT_ERR_NOMEM && !job->alone) {
+        std::lock_guard<std::mutex> g(mu);
+        nomem_retried++;
+        in_use -= job->footprint;
+        running--;
+        pinned_put_locked(res_host, res_cap);
+        job->alone = true;
+        job->status = 0;
+        queue.push_front(job);
+        cv.notify_all();
+        continue;
       }
       {
         std::lock_guard<std::mutex> g(mu);
@@ -232,6 +287,9 @@ int linqt_server_submit(linqt_server *srv, const linqt_request *req, long *ticke
     if (!srv || !req || !ticket || !req->H || !req->mu_out) fail(LINQT_ERR_INVALID, "server: NULL");
     if (req->R <= 0 || req->M <= 0) fail(LINQT_ERR_INVALID, "server: R and M must be positive");
     if (req->kind != LINQT_REQ_DOS && req->kind != LINQT_REQ_KUBO_BASTIN) fail(LINQT_ERR_INVALID, "server: kind");
+    if (req->kind == LINQT_REQ_KUBO_BASTIN && req->sigma_out &&
+        (req->nump < req->M || req->band_width <= 0 || !req->op))
+      fail(LINQT_ERR_INVALID, "server: sigma needs nump >= M, band_width > 0 and a velocity operator");
     auto job = std::make_shared<Job>();
     job->req = *req;
     const int n = req->H->op.n;
@@ -335,6 +393,17 @@ int linqt_server_release(linqt_server *srv, long ticket) {
     return LINQT_ERR_INVALID;
   }
   srv->jobs.erase(it);
+  return LINQT_OK;
+}
+
+int linqt_server_stats(linqt_server *srv, long *timeouts_retried, long *nomem_retried) {
+  if (!srv || !timeouts_retried) {
+    set_last_error("server: NULL");
+    return LINQT_ERR_INVALID;
+  }
+  std::lock_guard<std::mutex> g(srv->mu);
+  *timeouts_retried = srv->timeouts_retried;
+  if (nomem_retried) *nomem_retried = srv->nomem_retried;
   return LINQT_OK;
 }
 

@@ -16,7 +16,7 @@ import numpy as np
 
 from . import lattices
 from ._lib import Request, check, load
-from .core import (PREC_FP64, PREC_MIXED, Operator, Session, make_opts, moments1d_dev, moments2d_dev,
+from .core import (PREC_FP64, PREC_MIXED, Operator, Session, kubo_bastin_dev, make_opts, moments1d_dev,
                    random_phase_states_dev)
 
 REQ_DOS, REQ_KUBO_BASTIN = 0, 1
@@ -29,9 +29,12 @@ class Server:
         self.h = h
         self._keep = {}
 
-    def submit(self, kind, H, op, states, M, precision=PREC_FP64, R=None, seed=None):
+    def submit(self, kind, H, op, states, M, precision=PREC_FP64, R=None, seed=None, nump=0, band_width=None,
+               band_center=0.0):
         """Queue one request.  `states` (R x N, host) are copied at submit; with states=None
-        the server makes R random-phase states on the device from `seed`."""
+        the server makes R random-phase states on the device from `seed`.  A Kubo-Bastin
+        request with nump > 0 (and H's band_width / band_center) also returns sigma_xx(E)
+        (result_sigma) from the same recursion."""
         req = Request()
         if states is not None:
             st = np.ascontiguousarray(np.atleast_2d(states), dtype=np.complex128)
@@ -46,9 +49,16 @@ class Server:
         req.kind, req.H, req.op = kind, H.h, (op.h if op is not None else None)
         req.R, req.M, req.precision = R, M, precision
         req.mu_out = out.view(np.float64).ctypes.data_as(ctypes.POINTER(ctypes.c_double))
+        sig = None
+        if kind == REQ_KUBO_BASTIN and nump > 0:
+            if band_width is None:
+                raise ValueError("sigma needs the band_width H was rescaled with")
+            sig = np.zeros(3 * nump)
+            req.sigma_out = sig.ctypes.data_as(ctypes.POINTER(ctypes.c_double))
+            req.nump, req.band_width, req.band_center = nump, band_width, band_center
         t = ctypes.c_long()
         check(load().linqt_server_submit(self.h, ctypes.byref(req), ctypes.byref(t)))
-        self._keep[t.value] = (out, H, op, M, kind)
+        self._keep[t.value] = (out, H, op, M, kind, sig)
         return t.value
 
     def poll(self, ticket):
@@ -57,8 +67,21 @@ class Server:
         return st.value, lat.value
 
     def result(self, ticket):
-        out, _, _, M, kind = self._keep[ticket]
+        out, _, _, M, kind, _ = self._keep[ticket]
         return out if kind == REQ_DOS else out.reshape(M, M)
+
+    def result_sigma(self, ticket):
+        """(E, sigma, integrand) of a Kubo-Bastin request submitted with nump > 0."""
+        sig = self._keep[ticket][5]
+        n = len(sig) // 3
+        return sig[:n], sig[n:2 * n], sig[2 * n:]
+
+    def retries(self):
+        """(requests re-run on the device-wide lane after a co-residency timeout, requests
+        re-run alone after their workspaces did not fit next to the others)."""
+        a, b = ctypes.c_long(), ctypes.c_long()
+        check(load().linqt_server_stats(self.h, ctypes.byref(a), ctypes.byref(b)))
+        return a.value, b.value
 
     def cancel(self, ticket):
         """Withdraw a queued request (LinqtError if it already runs or has finished)."""
@@ -113,6 +136,7 @@ def request_stream(n_requests=200, seed=52, arrival_seed=51, n_min=1e4, n_max=2e
         if kind == REQ_KUBO_BASTIN and fam == "square":
             fam = "honeycomb"  # Kubo needs a velocity operator
         N = float(np.exp(np.log(n_min) + u[i, 2] * (np.log(n_max) - np.log(n_min))))
+        N = float(10 ** (np.round(np.log10(N) * 8) / 8))  # 8 sizes per decade: lattices are shared
         M = int(round((m_min + u[i, 3] * (m_max - m_min)) / 16) * 16)
         if kind == REQ_KUBO_BASTIN:
             M = max(m_min, M // 2)
@@ -124,9 +148,17 @@ def request_stream(n_requests=200, seed=52, arrival_seed=51, n_min=1e4, n_max=2e
     return reqs, gaps
 
 
+def sigma_points(M):
+    """Energies of a Kubo-Bastin request's sigma(E): the smallest 256 * 2^j >= 2 M."""
+    n = 256
+    while n < 2 * M:
+        n *= 2
+    return n
+
+
 def _prepare(reqs, session=None):
-    """Device-resident operators per request (lattices shared by family and size) and the
-    seed of each request's random-phase states."""
+    """Device-resident operators per request (lattices shared by family and size), the seed of
+    each request's random-phase states and H's rescaling (band width, centre)."""
     cache = {}
     prepared = []
     for i, r in enumerate(reqs):
@@ -136,9 +168,9 @@ def _prepare(reqs, session=None):
             Hg = Operator.from_csr(N, *H, session=session)
             Hg.rescale_to_chebyshev(hi - lo, (hi + lo) / 2)
             Vg = Operator.from_csr(N, *V, session=session) if V is not None else None
-            cache[key] = (N, Hg, Vg)
-        N, Hg, Vg = cache[key]
-        prepared.append((Hg, Vg, 1000 + i))
+            cache[key] = (N, Hg, Vg, hi - lo, (hi + lo) / 2)
+        N, Hg, Vg, bw, bc = cache[key]
+        prepared.append((Hg, Vg, 1000 + i, bw, bc))
     return prepared
 
 
@@ -150,7 +182,7 @@ def run_serial(reqs, prepared, fp64_only=True, session=None):
     sess = session or Session(stream=torch.cuda.current_stream().cuda_stream)  # ordered with torch's copies
     t0 = time.perf_counter()
     lat = []
-    for r, (Hg, Vg, seed) in zip(reqs, prepared):
+    for r, (Hg, Vg, seed, bw, bc) in zip(reqs, prepared):
         t = time.perf_counter()
         o = make_opts(precision=PREC_FP64 if fp64_only else r["precision"])
         N, R, M = Hg.n, r["R"], r["M"]
@@ -159,10 +191,14 @@ def run_serial(reqs, prepared, fp64_only=True, session=None):
         if r["kind"] == REQ_DOS:
             mu = torch.empty(2 * M, dtype=torch.float64, device="cuda")
             moments1d_dev(Hg, None, st, R, M, mu, opts=o, session=sess)
-        else:
+            mu.cpu()
+        else:  # the moment table and sigma(E) from one recursion, as the server runs it
+            nump = sigma_points(M)
             mu = torch.empty(2 * M * M, dtype=torch.float64, device="cuda")
-            moments2d_dev(Hg, Vg, Vg, st, R, M, mu, opts=o, session=sess)
-        mu.cpu()
+            out = torch.empty(3 * nump, dtype=torch.float64, device="cuda")
+            kubo_bastin_dev(Hg, Vg, Vg, st, R, M, nump, bw, bc, mu, out, opts=o, session=sess)
+            mu.cpu()
+            out.cpu()
         lat.append(1e3 * (time.perf_counter() - t))
     t_total = time.perf_counter() - t0
     if session is None:
@@ -177,12 +213,15 @@ def run_stream(reqs, prepared, gaps, mean_gap_s, max_active=4, hbm_budget_bytes=
     arrivals = np.cumsum(gaps) * mean_gap_s
     tickets = []
     t0 = time.perf_counter()
-    for i, (r, (Hg, Vg, seed)) in enumerate(zip(reqs, prepared)):
+    for i, (r, (Hg, Vg, seed, bw, bc)) in enumerate(zip(reqs, prepared)):
         now = time.perf_counter() - t0
         if arrivals[i] > now:
             time.sleep(arrivals[i] - now)
-        op = Vg if r["kind"] == REQ_KUBO_BASTIN else None
-        tickets.append(srv.submit(r["kind"], Hg, op, None, r["M"], r["precision"], R=r["R"], seed=seed))
+        if r["kind"] == REQ_KUBO_BASTIN:
+            tickets.append(srv.submit(r["kind"], Hg, Vg, None, r["M"], r["precision"], R=r["R"], seed=seed,
+                                      nump=sigma_points(r["M"]), band_width=bw, band_center=bc))
+        else:
+            tickets.append(srv.submit(r["kind"], Hg, None, None, r["M"], r["precision"], R=r["R"], seed=seed))
     srv.wait_all()
     makespan = time.perf_counter() - t0
     lat = []
@@ -208,17 +247,18 @@ def fifo_latencies(arrivals, service):
 
 def main(argv=None):
     """Serving benchmark: one JSON line with p50/p99 latency and throughput of the seeded stream
-    through the server, next to the same stream served one request at a time on the FP64 path."""
+    through the server (also per precision), next to the same stream served one request at a
+    time on the FP64 path.  Kubo-Bastin requests return their moment table and sigma(E)."""
     import argparse
     import json
     ap = argparse.ArgumentParser()
-    ap.add_argument("--requests", type=int, default=200)
+    ap.add_argument("--requests", type=int, default=400)
     ap.add_argument("--load", type=float, default=1.5,
                     help="offered load: arrival rate / serial FP64 service rate")
     ap.add_argument("--max-active", type=int, default=4)
-    ap.add_argument("--n-max", type=float, default=2e5)
-    ap.add_argument("--m-max", type=int, default=512)
-    ap.add_argument("--r-max", type=int, default=16)
+    ap.add_argument("--n-max", type=float, default=1e6)
+    ap.add_argument("--m-max", type=int, default=1024)
+    ap.add_argument("--r-max", type=int, default=32)
     a = ap.parse_args(argv)
     reqs, gaps = request_stream(a.requests, n_max=a.n_max, m_max=a.m_max, r_max=a.r_max)
     prepared = _prepare(reqs)
@@ -234,33 +274,54 @@ def main(argv=None):
                 warm_p.append(p)
     import torch
     sess = Session(stream=torch.cuda.current_stream().cuda_stream)
-    run_serial(warm_r, warm_p, fp64_only=False, session=sess)
+
+    def serial(rs, ps, fp64_only):
+        # the serial session returns its workspaces to the device pool after each pass, so
+        # that the server (same pool) finds the memory its HBM budget was set from
+        out = run_serial(rs, ps, fp64_only=fp64_only, session=sess)
+        torch.cuda.synchronize()
+        sess.trim()
+        return out
+
+    serial(warm_r, warm_p, False)
     # untimed passes of the whole stream: workspaces, pinned blocks and the device pool
     # reach their steady-state sizes before anything is timed
-    run_serial(reqs, prepared, fp64_only=True, session=sess)
-    run_serial(reqs, prepared, fp64_only=False, session=sess)
+    serial(reqs, prepared, True)
+    torch.cuda.empty_cache()
     srv = Server(0, 0, a.max_active)
     run_stream(reqs, prepared, np.zeros_like(gaps), 0.0, server=srv)
-    t_ser, svc = run_serial(reqs, prepared, fp64_only=True, session=sess)
-    t_mix, svc_mix = run_serial(reqs, prepared, fp64_only=False, session=sess)
+    t_ser, svc = serial(reqs, prepared, True)
+    t_mix, svc_mix = serial(reqs, prepared, False)
     sess.close()
     mean_gap = t_ser / len(reqs) / a.load
     arrivals = np.cumsum(gaps) * mean_gap
     lat_ser = 1e3 * fifo_latencies(arrivals, svc / 1e3)
     lat, makespan = run_stream(reqs, prepared, gaps, mean_gap, server=srv)
     lat_sat, makespan_sat = run_stream(reqs, prepared, np.zeros_like(gaps), 0.0, server=srv)
+    retried = srv.retries()
     srv.close()
-    q = lambda x, p: float(np.percentile(x, p))
+    q = lambda x, p: float(np.percentile(x, p)) if len(x) else None
+    mixed = np.array([r["precision"] == PREC_MIXED for r in reqs])
+    kubo = np.array([r["kind"] == REQ_KUBO_BASTIN for r in reqs])
+
+    def split(x):
+        return {"p50_ms": q(x, 50), "p99_ms": q(x, 99),
+                "mixed": {"requests": int(mixed.sum()), "p50_ms": q(x[mixed], 50), "p99_ms": q(x[mixed], 99)},
+                "fp64": {"requests": int((~mixed).sum()), "p50_ms": q(x[~mixed], 50), "p99_ms": q(x[~mixed], 99)},
+                "kubo_bastin": {"p50_ms": q(x[kubo], 50), "p99_ms": q(x[kubo], 99)},
+                "dos": {"p50_ms": q(x[~kubo], 50), "p99_ms": q(x[~kubo], 99)}}
+
     out = {
         "metric": "serving_stream", "requests": len(reqs), "offered_load": a.load,
         "mean_interarrival_ms": 1e3 * mean_gap, "max_active": a.max_active,
         "stream": {"n_range": [1e4, a.n_max], "m_range": [128, a.m_max], "r_max": a.r_max,
-                   "dos_fraction": sum(r["kind"] == REQ_DOS for r in reqs) / len(reqs)},
-        "server": {"p50_ms": q(lat, 50), "p99_ms": q(lat, 99), "requests_per_s": len(reqs) / makespan},
-        "serial_fp64": {"p50_ms": q(lat_ser, 50), "p99_ms": q(lat_ser, 99), "requests_per_s": len(reqs) / t_ser},
+                   "dos_fraction": float((~kubo).mean()), "mixed_fraction": float(mixed.mean()),
+                   "kubo_returns": "moment table and sigma(E) at the smallest 256*2^j >= 2M energies"},
+        "server": dict(split(lat), requests_per_s=len(reqs) / makespan),
+        "serial_fp64": dict(split(lat_ser), requests_per_s=len(reqs) / t_ser),
         "serial_request_precision_requests_per_s": len(reqs) / t_mix,
-        "server_saturated": {"p50_ms": q(lat_sat, 50), "p99_ms": q(lat_sat, 99),
-                             "requests_per_s": len(reqs) / makespan_sat},
+        "server_saturated": dict(split(lat_sat), requests_per_s=len(reqs) / makespan_sat),
+        "requests_rerun": {"on_the_cooperative_lane": retried[0], "alone_after_nomem": retried[1]},
     }
     print(json.dumps(out))
 

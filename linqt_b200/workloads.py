@@ -18,8 +18,9 @@ Kubo-Bastin graphene workload:
 Each line gives the device time per solve (CUDA events on the session stream, warm-up
 first), Chebyshev steps*nnz/s, the recursion's algorithmic bytes per second, and for the
 mixed-precision solve its error against FP64.  `spin` is the spin-transport case scaled
-from 512x512 cells, M = 1024, R = 32 (2.8e17 flop of contraction) to a size that runs in
-seconds; `cubic` is one disorder seed of the four.
+from 512x512 cells, M = 1024, R = 32 (2.8e14 flop of contraction, about 14 s per FP64 solve:
+`spin --cells 512 --moments 1024 --vectors 32 --reps 1` runs the full size) to a size that runs
+in a fraction of a second; `cubic` is one disorder seed of the four.
 """
 import argparse
 import json
@@ -27,7 +28,7 @@ import json
 import numpy as np
 
 from . import lattices
-from .core import PREC_FP64, PREC_MIXED, Operator, Session, make_opts, kubo_bastin_dev, moments1d_dev
+from .core import PREC_FP64, PREC_MIXED, PREC_MIXED_FAST, Operator, Session, make_opts, kubo_bastin_dev, moments1d_dev
 
 
 def _hbm_peak():
@@ -91,9 +92,11 @@ def run_1d(name, N, H, R, M, reps, phase_seed):
     }
 
 
-def run_spin(Lc, R, M, nump, reps):
+def run_spin(Lc, R, M, nump, reps, mixed_precisions=(PREC_MIXED,)):
     """Kane-Mele spin transport: the Kubo-Bastin solve (2D moments and the per-site FFT
-    reconstruction of sigma(E)) and the 2D moments alone, FP64 and mixed, layouts autotuned.
+    reconstruction of sigma(E)) and the 2D moments alone, FP64 and each of
+    `mixed_precisions` (LINQT_PREC_MIXED: 4-digit INT8 contraction; LINQT_PREC_MIXED_FAST:
+    3 digits, smaller digit planes and so wider vector chunks), layouts autotuned.
     sigma is also reconstructed from each precision's moment table by the Bastin energy sum
     (kuboBastinFromChebmom, all M moments kept), to state the error a moments-only mixed
     solve carries into sigma."""
@@ -103,7 +106,7 @@ def run_spin(Lc, R, M, nump, reps):
     st = lattices.random_phase_states(N, R, seed=32)
     st_dev = torch.from_numpy(st.view(np.float64).copy()).cuda()
     res = {}
-    for prec in (PREC_FP64, PREC_MIXED):
+    for prec in (PREC_FP64,) + tuple(mixed_precisions):
         # a session (and operators) of its own per precision, so that neither is timed next
         # to the other's cached workspaces
         sess, bw, bc, Hg, (Jg,) = _ops(N, H, [J])
@@ -129,7 +132,7 @@ def run_spin(Lc, R, M, nump, reps):
         del mu, out, mu2, Hg, Jg
         sess.close()
         torch.cuda.synchronize()
-    a, b = res[PREC_FP64], res[PREC_MIXED]
+    a = res[PREC_FP64]
     lo, hi = int(0.05 * nump), int(0.95 * nump)
     nd = len(a["s_mom"])
     lo2, hi2 = int(0.05 * nd), int(0.95 * nd)
@@ -140,15 +143,19 @@ def run_spin(Lc, R, M, nump, reps):
                 "moments2d_ms": r["ms2"], "moments2d_steps_nnz_per_s": work / (r["ms2"] * 1e-3)}
 
     out = {"workload": "spin_kane_mele_%dx%d" % (Lc, Lc), "N": N, "nnz_full": nnz, "R": R, "M": M, "nump": nump,
-           "operator": "{s_z, V_x}/2", "fp64": side(a), "mixed": side(b)}
+           "operator": "{s_z, V_x}/2", "fp64": side(a)}
     out["fp64"]["contraction_TFLOPs"] = 8.0 * M * M * N * R / (a["phases"][1] * 1e-3) / 1e12
-    out["mixed"].update({
-        "speedup_solve": a["ms"] / b["ms"], "speedup_moments2d": a["ms2"] / b["ms2"],
-        "err_mu_vs_fp64": float(np.abs(b["mu"] - a["mu"]).max() / np.abs(a["mu"]).max()),
-        "err_sigma_fft_vs_fp64_interior90": float(np.abs(b["s_fft"][lo:hi] - a["s_fft"][lo:hi]).max()
-                                                  / np.abs(a["s_fft"][lo:hi]).max()),
-        "err_sigma_from_moments_vs_fp64_interior90": float(np.abs(b["s_mom"][lo2:hi2] - a["s_mom"][lo2:hi2]).max()
-                                                           / np.abs(a["s_mom"][lo2:hi2]).max())})
+    for prec in mixed_precisions:
+        b = res[prec]
+        key = {PREC_MIXED: "mixed", PREC_MIXED_FAST: "mixed_fast"}.get(prec, "precision_%d" % prec)
+        out[key] = side(b)
+        out[key].update({
+            "speedup_solve": a["ms"] / b["ms"], "speedup_moments2d": a["ms2"] / b["ms2"],
+            "err_mu_vs_fp64": float(np.abs(b["mu"] - a["mu"]).max() / np.abs(a["mu"]).max()),
+            "err_sigma_fft_vs_fp64_interior90": float(np.abs(b["s_fft"][lo:hi] - a["s_fft"][lo:hi]).max()
+                                                      / np.abs(a["s_fft"][lo:hi]).max()),
+            "err_sigma_from_moments_vs_fp64_interior90": float(np.abs(b["s_mom"][lo2:hi2] - a["s_mom"][lo2:hi2]).max()
+                                                               / np.abs(a["s_mom"][lo2:hi2]).max())})
     return out
 
 
@@ -223,8 +230,10 @@ def run_cubic_full(L, S, Rs, M, mode=0):
     out = {"workload": "dos_cubic_%d_%dseeds_x_%d" % (L, S, Rs), "N": N, "nnz_full": nnz, "R_total": R,
            "M": M, "realisations": ["autotuned", "stacked", "separate"][mode], "host_setup_s": round(setup_s, 1)}
     mus = {}
-    for label, prec, esz in (("fp64", PREC_FP64, 16), ("mixed", PREC_MIXED, 8)):
-        o = make_opts(precision=prec, fmt=2, realisations=mode)
+    # complex128 operators with FP64 and FP32 blocks, and complex64 operators with FP32 blocks
+    for label, prec, esz, c64 in (("fp64", PREC_FP64, 16, 0), ("mixed", PREC_MIXED, 8, 0),
+                                  ("mixed_c64", PREC_MIXED, 8, 1)):
+        o = make_opts(precision=prec, fmt=2, realisations=mode, operator_precision=c64)
         mu = torch.zeros(2 * S * M, dtype=torch.float64, device="cuda")
         moments1d_realisations_dev(ops, st, R, 64, mu, opts=o, session=sess)  # warm-up
         torch.cuda.synchronize()
@@ -234,14 +243,15 @@ def run_cubic_full(L, S, Rs, M, mode=0):
         b.record()
         torch.cuda.synchronize()
         ms = a.elapsed_time(b)
-        bytes_step = S * (nnz * (16 + 4) + 4 * (N + 1)) + 3 * esz * N * R
+        bytes_step = S * (nnz * ((8 if c64 else 16) + 4) + 4 * (N + 1)) + 3 * esz * N * R
         gbs = steps * bytes_step / (ms * 1e-3) / 1e9
         mus[label] = mu.cpu().numpy().view(np.complex128).reshape(S, M)
         peak, src = _hbm_peak()
         out[label] = {"ms_per_solve": ms, "steps_nnz_per_s": M * R * nnz / (ms * 1e-3),
                       "recursion_GBps": gbs, "hbm_frac": gbs / peak, "hbm_peak_GBps": peak, "hbm_peak_source": src}
-    e = np.abs(mus["mixed"] - mus["fp64"]).max(axis=1) / np.abs(mus["fp64"]).max(axis=1)
-    out["mixed"]["err_mu_vs_fp64_per_seed"] = [float(x) for x in e]
+    for label in ("mixed", "mixed_c64"):
+        e = np.abs(mus[label] - mus["fp64"]).max(axis=1) / np.abs(mus["fp64"]).max(axis=1)
+        out[label]["err_mu_vs_fp64_per_seed"] = [float(x) for x in e]
     return out
 
 
@@ -401,6 +411,8 @@ def main(argv=None):
     ap.add_argument("--vectors", type=int, default=8, help="spin: R")
     ap.add_argument("--realisations", type=int, default=0, help="cubic_full: 0 autotuned, 1 stacked, 2 separate")
     ap.add_argument("--side", type=int, default=100, help="recur1d: cubic lattice side L")
+    ap.add_argument("--mixed", default="1", help="spin: comma-separated mixed precisions beside FP64 (1 = 4-digit "
+                                                 "INT8 contraction, 4 = 3-digit)")
     ap.add_argument("--format", type=int, default=0, help="recur1d: LINQT_FORMAT_* value")
     a = ap.parse_args(argv)
     if a.workload == "dos":
@@ -443,7 +455,8 @@ def main(argv=None):
             print(json.dumps(r))
         return
     else:
-        r = run_spin(a.cells, a.vectors, a.moments, max(1024, a.moments), a.reps)
+        r = run_spin(a.cells, a.vectors, a.moments, max(1024, a.moments), a.reps,
+                     tuple(int(x) for x in a.mixed.split(",")))
     print(json.dumps(r))
 
 

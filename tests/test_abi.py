@@ -22,7 +22,7 @@ def declared_symbols():
 def test_library_built_and_loads():
     assert os.path.exists(_lib.LIB_PATH)
     L = _lib.load()
-    assert L.linqt_abi_version() == 2
+    assert L.linqt_abi_version() == _lib.ABI_VERSION == 3
 
 
 def test_every_declared_symbol_is_exported():

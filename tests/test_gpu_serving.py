@@ -116,3 +116,65 @@ def test_cancel_a_queued_request():
     with pytest.raises(lq.LinqtError):
         srv.cancel(t1)
     srv.close()
+
+
+def test_kubo_bastin_request_returns_sigma():
+    """A Kubo-Bastin request with nump > 0 returns sigma_xx(E) from the same recursion as its
+    moment table: equal to linqt_kubo_bastin alone, and unchanged when served next to others."""
+    N, H, V, (lo, hi) = serve._family("honeycomb", 6000, seed=3)
+    bw, bc = hi - lo, (hi + lo) / 2
+    Hg = lq.Operator.from_csr(N, *H)
+    Hg.rescale_to_chebyshev(bw, bc)
+    Vg = lq.Operator.from_csr(N, *V)
+    st = lattices.random_phase_states(N, 3, seed=4)
+    M, nump = 96, 256
+    mu_ref, (E_ref, s_ref, i_ref) = lq.kubo_bastin(Hg, Vg, Vg, st, M, nump, bw, bc)
+    srv = serve.Server(0, 0, 3)
+    others = [srv.submit(serve.REQ_DOS, Hg, None, st, 200, lq.PREC_MIXED) for _ in range(3)]
+    t = srv.submit(serve.REQ_KUBO_BASTIN, Hg, Vg, st, M, lq.PREC_FP64, nump=nump, band_width=bw, band_center=bc)
+    srv.wait_all()
+    assert srv.poll(t)[0] == 2 and all(srv.poll(o)[0] == 2 for o in others)
+    E, s, integ = srv.result_sigma(t)
+    assert np.array_equal(E, E_ref)
+    assert np.abs(s - s_ref).max() <= 1e-12 * np.abs(s_ref).max()
+    assert np.abs(integ - i_ref).max() <= 1e-12 * np.abs(i_ref).max()
+    assert np.abs(srv.result(t) - mu_ref).max() <= 1e-12 * np.abs(mu_ref).max()
+    srv.close()
+
+
+def test_sessions_with_sm_shares_run_recursions_side_by_side():
+    """Two sessions with SM shares of 0.45 run their persistent recursions at the same time
+    from two host threads (grids sized to their share, launched on their own streams): the
+    results equal the whole-device solve up to the order of the partial sums."""
+    import threading
+    N, Hc = lattices.square_lattice(96, t=1.0, W=1.0, seed=11)
+    H = lq.Operator.from_csr(N, *Hc)
+    H.rescale_to_chebyshev(2 * 1.05 * 4.5, 0.0)
+    _, Hk, Jk, (lo, hi) = serve._family("kane_mele", 4000, seed=5)
+    Kg = lq.Operator.from_csr(len(Hk[0]) - 1, *Hk)
+    Kg.rescale_to_chebyshev(hi - lo, (hi + lo) / 2)
+    Jg = lq.Operator.from_csr(len(Jk[0]) - 1, *Jk)
+    st1 = lattices.random_phase_states(N, 4, seed=1)
+    st2 = lattices.random_phase_states(Kg.n, 3, seed=2)
+    ref1 = lq.moments1d(H, None, st1, 512)
+    ref2 = lq.moments2d(Kg, Jg, Jg, st2, 96)
+    out, errs = {}, []
+
+    def work(key, fn):
+        try:
+            s = lq.Session(0)
+            s.set_sm_share(0.45)
+            out[key] = [fn(s) for _ in range(4)]
+            s.close()
+        except Exception as e:  # reported below
+            errs.append(e)
+
+    t1 = threading.Thread(target=work, args=("1d", lambda s: lq.moments1d(H, None, st1, 512, session=s)))
+    t2 = threading.Thread(target=work, args=("2d", lambda s: lq.moments2d(Kg, Jg, Jg, st2, 96, session=s)))
+    t1.start(), t2.start()
+    t1.join(), t2.join()
+    assert not errs, errs
+    for got in out["1d"]:
+        assert np.abs(got - ref1).max() <= 1e-12 * np.abs(ref1).max()
+    for got in out["2d"]:
+        assert np.abs(got - ref2).max() <= 1e-12 * np.abs(ref2).max()
