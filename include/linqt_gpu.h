@@ -65,7 +65,7 @@ enum {
 
 enum { LINQT_KUBO_GREENWOOD = 0, LINQT_KUBO_BASTIN = 1 }; /* chebyshev::formula, include/Kubo_solver_FFT.hpp:17-21 */
 
-enum { LINQT_FORMAT_CSR = 0, LINQT_FORMAT_SELL = 1, LINQT_FORMAT_AUTO = 2 };
+enum { LINQT_FORMAT_CSR = 0, LINQT_FORMAT_SELL = 1, LINQT_FORMAT_AUTO = 2, LINQT_FORMAT_SELL_LOCAL = 3 };
 
 typedef struct linqt_op linqt_op;
 typedef struct linqt_session linqt_session;
@@ -74,11 +74,17 @@ typedef struct linqt_session linqt_session;
 typedef struct linqt_opts {
   int precision;    /* LINQT_PREC_* */
   int format;       /* sparse layout of H in the persistent recursions: LINQT_FORMAT_CSR (default),
-                       LINQT_FORMAT_SELL (SELL-C-sigma, C = 32, sigma = 8C) or LINQT_FORMAT_AUTO
+                       LINQT_FORMAT_SELL (SELL-C-sigma, C = 32, sigma = 8C), LINQT_FORMAT_SELL_LOCAL
+                       (the same with the rows visited in a locality order found by recursive
+                       bisection of the operator's graph, see linqt_locality_order: neighbour rows
+                       are read close together in time, for lattices such as 3D ones whose
+                       neighbours lie far apart in the row numbering) or LINQT_FORMAT_AUTO
                        (autotuned among CSR with and without its shared-memory row cache and SELL
-                       with C = 8, 32, times the thread shapes of the block (threads per row
-                       min(R, 32) >> s, s = 0..3), and for 1D moments without a fixed block_width
-                       the block width (R, R/2, R/4, R/8); cached per operator, width and precision) */
+                       with C = 8, 32, plus SELL_LOCAL when a block exceeds 64 MB, times the thread
+                       shapes of the block (threads per row min(R, 32) >> s, s = 0..3), and for 1D
+                       moments without a fixed block_width the block width (R, R/2, R/4, R/8);
+                       cached per operator, width and precision).  The layout changes only the
+                       order of the per-block dot-product sums. */
   int block_width;  /* vector columns per recursion block (0 = all R, or the autotuned chunk) */
   int doubling;     /* 1D: 0 = doubling identities when the operator is the identity, 1 = force them, 2 = direct <r|T_n r> */
   int use_graphs;   /* 1: *_dev solves replay an instantiated CUDA graph from the second call with the same
@@ -343,6 +349,13 @@ int linqt_kubo_from_moments(linqt_session *s, const double *mu, int M0, int M1, 
 /* Jackson kernels alone (in place on host arrays; returns the truncated sizes). */
 int linqt_jackson1d(double *mu, int M, double band_width, double broad_meV, int *M_out);
 int linqt_jackson2d(double *mu, int M0, int M1, double band_width, double b0, double b1, int *M0_out, int *M1_out);
+
+/* Locality order of the rows of a CSR pattern (host only; no LinQT counterpart: it is the
+ * traversal order behind LINQT_FORMAT_SELL_LOCAL).  The row graph is ordered breadth-first
+ * from a pseudo-peripheral row and cut into halves, recursively, until the parts have at most
+ * part_rows rows (>= 1); order[pos] = row, a permutation of 0..n-1.  The pattern must be
+ * structurally symmetric (a Hermitian operator's expanded rows are) with columns in [0, n). */
+int linqt_locality_order(int n, const int *rowptr, const int *col, int part_rows, int *order);
 
 /* ---- serving (continuous batching of DOS / Kubo-Bastin solves) ----------- */
 typedef struct linqt_server linqt_server;

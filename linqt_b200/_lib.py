@@ -107,6 +107,7 @@ SIGNATURES = {
                                         c_int, c_double, c_int, P_double, P_double, P_int]),
     "linqt_jackson1d": (c_int, [P_double, c_int, c_double, c_double, P_int]),
     "linqt_jackson2d": (c_int, [P_double, c_int, c_int, c_double, c_double, c_double, P_int, P_int]),
+    "linqt_locality_order": (c_int, [c_int, P_int, P_int, c_int, P_int]),
     "linqt_server_create": (c_int, [c_int, ctypes.c_size_t, c_int, ctypes.POINTER(c_void_p)]),
     "linqt_server_submit": (c_int, [c_void_p, ctypes.POINTER(Request), P_long]),
     "linqt_server_poll": (c_int, [c_void_p, c_long, P_int, P_double]),

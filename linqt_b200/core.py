@@ -24,6 +24,7 @@ PREC_FP64, PREC_MIXED, PREC_FP32, PREC_MIXED_TF32, PREC_MIXED_FAST = 0, 1, 2, 3,
 KUBO_GREENWOOD, KUBO_BASTIN = 0, 1
 STORAGE_HERMITIAN_UPPER, STORAGE_GENERAL = 0, 1
 OP_C128, OP_C64 = 0, 1  # opts.operator_precision: complex128 or complex64 operator values (1D recursions)
+FORMAT_CSR, FORMAT_SELL, FORMAT_AUTO, FORMAT_SELL_LOCAL = 0, 1, 2, 3  # opts.format
 
 
 def _dp(a):
@@ -469,6 +470,16 @@ def jackson2d(mu, band_width, b0, b1):
     check(load().linqt_jackson2d(_dp(m.view(np.float64)), M0, M1, band_width, b0, b1, ctypes.byref(a),
                                  ctypes.byref(b)))
     return m.reshape(-1)[: a.value * b.value].reshape(a.value, b.value)
+
+
+def locality_order(rowptr, col, part_rows=8192):
+    """The locality order behind FORMAT_SELL_LOCAL (host only): order[pos] = row."""
+    rp = np.ascontiguousarray(rowptr, dtype=np.int32)
+    ci = np.ascontiguousarray(col, dtype=np.int32)
+    n = len(rp) - 1
+    out = np.empty(max(n, 0), dtype=np.int32)
+    check(load().linqt_locality_order(n, _ip(rp), _ip(ci), part_rows, _ip(out)))
+    return out
 
 
 # --- operator builder (LinQT's utilities/wannier2sparse) ---------------------------------------

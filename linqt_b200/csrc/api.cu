@@ -54,6 +54,16 @@ void *Session::get(const std::string &name, size_t bytes) {
   }
   void *p = nullptr;
   cudaError_t e = cudaMallocAsync(&p, bytes, stream);
+  if (e == cudaErrorMemoryAllocation) {
+    // Blocks freed earlier stay cached in the pool, each in its own address range, so a
+    // larger buffer may not fit although the bytes are there: once this stream has reached
+    // its frees, hand the pool's unused memory back and try once more.
+    cudaGetLastError();
+    cudaMemPool_t pool = nullptr;
+    if (cudaStreamSynchronize(stream) == cudaSuccess && cudaDeviceGetDefaultMemPool(&pool, device) == cudaSuccess)
+      cudaMemPoolTrimTo(pool, 0);
+    e = cudaMallocAsync(&p, bytes, stream);
+  }
   if (e != cudaSuccess) {
     cudaGetLastError();
     fail(LINQT_ERR_NOMEM, "cudaMallocAsync(" + std::to_string(bytes) + ") for '" + name + "' failed: " +
@@ -235,6 +245,7 @@ void DeviceOp::upload() {
   }
   nnz = rowptr[n];
   free_device();
+  loc_order.clear();  // the pattern may have changed (a rescale can add diagonal entries)
   static std::atomic<unsigned long> next_uid{1};
   uid = next_uid++;
   LQ_CUDA(cudaSetDevice(device));
@@ -251,15 +262,22 @@ void DeviceOp::upload() {
 
 // SELL-C-sigma: rows sorted by decreasing length inside windows of sigma = 8C rows
 // (stable), slices of C rows, each slice stored column-major with width = its longest
-// row; padding entries point at the row itself with value zero.
-const DeviceOp::Sell &DeviceOp::ensure_sell(int C) {
-  LQ_REQUIRE(C > 0, "SELL slice height must be positive");
+// row; padding entries point at the row itself with value zero.  With kSellLocality in
+// the key the windows are cut from the locality order of the rows.
+const DeviceOp::Sell &DeviceOp::ensure_sell(int key) {
+  const int C = sell_height(key);
+  LQ_REQUIRE(C > 0 && (key & ~(kSellLocality | (kSellLocality - 1))) == 0, "bad SELL layout key");
   std::lock_guard<std::mutex> g(mu);
-  Sell &L = sell[C];
+  Sell &L = sell[key];
   if (!L.d_perm) {
     const int sigma = 8 * C;
     std::vector<int> order(n);
-    for (int i = 0; i < n; ++i) order[i] = i;
+    if (key & kSellLocality) {
+      if ((int)loc_order.size() != n) loc_order = locality_order(n, rowptr.data(), col.data(), kLocalityPart);
+      order = loc_order;
+    } else {
+      for (int i = 0; i < n; ++i) order[i] = i;
+    }
     auto len = [&](int r) { return rowptr[r + 1] - rowptr[r]; };
     for (int w0 = 0; w0 < n; w0 += sigma)
       std::stable_sort(order.begin() + w0, order.begin() + std::min(n, w0 + sigma),
@@ -326,7 +344,8 @@ static linqt_opts defaults(const linqt_opts *o) {
   linqt_opts d;
   std::memset(&d, 0, sizeof(d));
   if (o) d = *o;
-  LQ_REQUIRE(d.format == LINQT_FORMAT_CSR || d.format == LINQT_FORMAT_SELL || d.format == LINQT_FORMAT_AUTO,
+  LQ_REQUIRE(d.format == LINQT_FORMAT_CSR || d.format == LINQT_FORMAT_SELL || d.format == LINQT_FORMAT_AUTO ||
+                 d.format == LINQT_FORMAT_SELL_LOCAL,
              "opts.format: unknown sparse format");
   LQ_REQUIRE(d.operator_precision == 0 || d.operator_precision == 1, "opts.operator_precision must be 0 or 1");
   return d;
@@ -430,9 +449,9 @@ static RecCfg pick_layout(Session *s, const DeviceOp &H, const std::string &key,
                           bool csr_only = false) {
   if (best_ms) *best_ms = -1;
   if (format == LINQT_FORMAT_CSR) return RecCfg{0, 0};
-  if (format == LINQT_FORMAT_SELL) {
+  if (format == LINQT_FORMAT_SELL || format == LINQT_FORMAT_SELL_LOCAL) {
     if (csr_only) fail(LINQT_ERR_UNSUPPORTED, "complex64 operators: CSR layouts only");
-    return RecCfg{32, 0};
+    return RecCfg{format == LINQT_FORMAT_SELL ? 32 : 32 | kSellLocality, 0};
   }
   DeviceOp &Hm = const_cast<DeviceOp &>(H);
   {
@@ -447,10 +466,14 @@ static RecCfg pick_layout(Session *s, const DeviceOp &H, const std::string &key,
   RecCfg pick;
   bool first = true;
   // 0: CSR, its row slices cached in shared memory when they fit; -1: CSR without the
-  // cache (more resident CTAs per SM); 8, 32: SELL-C-sigma
-  for (int C : {0, -1, 8, 32})
+  // cache (more resident CTAs per SM); 8, 32: SELL-C-sigma; 32 | kSellLocality: SELL-C-sigma
+  // over the locality order, tried when one block of the lattice (8 bytes per value at
+  // least) exceeds 64 MB, i.e. when its neighbour rows can leave L2 between their reads
+  const bool big = (double)H.n * Rc * sizeof(float2) > 64e6;
+  for (int C : {0, -1, 8, 32, 32 | kSellLocality})
     for (int sh = 0; sh < recur_shapes(Rc); ++sh) {
       if (csr_only && C > 0) continue;
+      if ((C & kSellLocality) && !big) continue;
       trial(C, sh);
       LQ_CUDA(cudaEventRecord(a, s->stream));
       trial(C, sh);
@@ -826,7 +849,6 @@ struct Chunking {
 // and 6 on the R side per digit, i.e. 3 * digits bytes per complex entry of each store)
 static Chunking pick_chunks(Session *s, int N, int R, int M, size_t esz, const linqt_opts &o, size_t extra,
                             int digits = 0) {
-  esz += 3 * (size_t)digits;
   int Rc = o.block_width > 0 ? pow2_at_least(o.block_width) : pow2_at_least(R);
   Rc = std::min(Rc, 256);
   size_t avail;
@@ -836,16 +858,22 @@ static Chunking pick_chunks(Session *s, int N, int R, int M, size_t esz, const l
     avail = s->hbm_budget;
   } else {
     avail = free_device_bytes();
-    // keep what this session already caches for the same buffers
-    for (auto &kv : s->ws) avail += kv.second.second;
+    // plus what this session already holds in the buffers this solve reallocates (the L/R
+    // stores and the digit planes); its other cached workspaces stay allocated
+    for (auto &kv : s->ws)
+      if (kv.first.rfind("lr_", 0) == 0 || kv.first.rfind("mu_i8_", 0) == 0) avail += kv.second.second;
     avail = (size_t)(avail * 0.90);
   }
+  // the Chebyshev blocks (L and R stores, 4 scratch blocks) and, for the INT8 contraction,
+  // one K slab of digit planes
+  const auto need_at = [&](int rc) {
+    return esz * (size_t)N * rc * (2 * (size_t)M + 4) + extra + i8_digit_bytes(digits, M, (long)N * rc);
+  };
   while (Rc > 1) {
-    const size_t need = esz * (size_t)N * Rc * (2 * (size_t)M + 4) + extra;
-    if (need <= avail) break;
+    if (need_at(Rc) <= avail) break;
     Rc >>= 1;
   }
-  const size_t need = esz * (size_t)N * Rc * (2 * (size_t)M + 4) + extra;
+  const size_t need = need_at(Rc);
   if (need > avail)
     fail(LINQT_ERR_NOMEM, "2D moments: " + std::to_string(need >> 20) + " MiB of Chebyshev blocks exceed the " +
                               std::to_string(avail >> 20) + " MiB available");
@@ -1020,7 +1048,7 @@ static void moments_td_dev(Session *s, const DeviceOp &H, const DeviceOp *opl, c
   const std::vector<double2> c = td_coefficients(dt, band_width, band_center);
   double2 *coef = (double2 *)s->get("td_coef", sizeof(double2) * c.size());
   LQ_CUDA(cudaMemcpyAsync(coef, c.data(), sizeof(double2) * c.size(), cudaMemcpyHostToDevice, s->stream));
-  const int sellC = o.format == LINQT_FORMAT_SELL ? 32 : 0;
+  const int sellC = o.format == LINQT_FORMAT_SELL ? 32 : o.format == LINQT_FORMAT_SELL_LOCAL ? 32 | kSellLocality : 0;
   {
     PhaseScope ph(s, PH_RECURSION);
     for (int ch = 0; ch < nchunks; ++ch) {
@@ -1654,6 +1682,17 @@ int linqt_jackson1d(double *mu, int M, double band_width, double broad_meV, int 
       mu[2 * m + 1] *= g;
     }
     if (M_out) *M_out = Mt;
+  });
+}
+
+int linqt_locality_order(int n, const int *rowptr, const int *col, int part_rows, int *order) {
+  return guarded([&] {
+    LQ_REQUIRE(n >= 0 && rowptr && order && part_rows >= 1 && (col || n == 0), "bad argument");
+    LQ_REQUIRE(rowptr[0] == 0, "rowptr[0] must be 0");
+    for (int i = 0; i < n; ++i) LQ_REQUIRE(rowptr[i + 1] >= rowptr[i], "rowptr must be non-decreasing");
+    for (long k = 0; k < (long)rowptr[n]; ++k) LQ_REQUIRE(col[k] >= 0 && col[k] < n, "column index out of range");
+    const std::vector<int> o = locality_order(n, rowptr, col, part_rows);
+    std::copy(o.begin(), o.end(), order);
   });
 }
 

@@ -3,6 +3,7 @@
 
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <cstdint>
 #include <map>
 #include <mutex>
@@ -129,6 +130,16 @@ __device__ __forceinline__ float2 from_d2<float2>(double2 v) {
 // ---------------------------------------------------------------------------
 // device operator: Hermitian-expanded CSR (plus optional FP32 copy and SELL-C)
 // ---------------------------------------------------------------------------
+// SELL layout keys: slice height C in the low bits, kSellLocality when the slices are cut
+// from the locality order of the rows instead of their natural order
+constexpr int kSellLocality = 1 << 12;
+inline int sell_height(int key) { return key & (kSellLocality - 1); }
+// rows of the leaves of the recursive bisection behind the locality order
+constexpr int kLocalityPart = 8192;
+// Locality order of the rows of a CSR pattern (recursive graph bisection into parts of at
+// most `part` rows); order[pos] = row.
+std::vector<int> locality_order(int n, const int *rp, const int *ci, int part);
+
 struct SellView {
   int nslices = 0, C = 0;
   const long *slice_off = nullptr;  // [nslices+1], in entries
@@ -161,14 +172,16 @@ struct DeviceOp {
   double2 *d_val64 = nullptr;
   unsigned version = 0;  // bumped by rescale
   unsigned long uid = 0;  // distinct for every upload (keys the replayable graphs)
-  // SELL-C-sigma copies of the expanded operator, by slice height C (built on first use)
+  // SELL-C-sigma copies of the expanded operator, by layout key: the slice height C, plus
+  // kSellLocality when the slices follow the locality order of the rows (built on first use)
   struct Sell {
     int *d_perm = nullptr, *d_off = nullptr, *d_col = nullptr;
     double2 *d_val64 = nullptr;
     size_t len = 0;
   };
   std::map<int, Sell> sell;
-  const Sell &ensure_sell(int C);
+  const Sell &ensure_sell(int key);
+  std::vector<int> loc_order;  // locality order of the rows (made on first use)
   // format chosen by the autotuner, per (recursion kind, block width, precision, second operator)
   std::map<std::string, int> tuned;
   std::mutex mu;
@@ -289,6 +302,19 @@ void mu_contract_i8(Session *s, const void *L, const void *Rv, int M, long K, in
 inline int i8_digits(int precision) {
   return precision == LINQT_PREC_MIXED ? 4 : precision == LINQT_PREC_MIXED_FAST ? 3 : 0;
 }
+// The INT8 contraction splits K into slabs whose digit planes (6 * digits bytes per complex
+// entry of one moment's block, L and R sides together) fit kI8DigitBudget; the planes are
+// rewritten slab after slab.  i8_digit_bytes: the device bytes that takes for M moments of K.
+constexpr size_t kI8DigitBudget = 8ull << 30;
+inline long i8_slab(int digits, int M, long K) {
+  const long per = 6L * digits * M;                       // bytes per complex column of K
+  long slab = std::max(1024L, (long)(kI8DigitBudget / (size_t)per));
+  slab = slab / 1024 * 1024;                              // keeps slab starts 16-byte aligned
+  return std::min(K, slab);
+}
+inline size_t i8_digit_bytes(int digits, int M, long K) {
+  return digits ? (size_t)6 * digits * M * (size_t)(i8_slab(digits, M, K) + 1024) : 0;
+}
 
 // FFT path: accumulate p/w over all sites into acc[2*nump] (complex)
 // prefactors pf_m of Kubo_solver_FFT (kubo_fft.cu)
@@ -366,6 +392,10 @@ void coop_launch(Session *s, const void *f, int grid, void **args, size_t smem);
 
 // small utilities (util.cu)
 void sum_chunks_stream(cudaStream_t st, double2 *d, int len, int nchunks);
+// Raise a kernel's dynamic shared-memory limit on the current device to at least `bytes`,
+// never lowering it: the limit belongs to the function, and server slots on other threads
+// launch the same kernels with other sizes, so a lowered limit could fail their launches.
+void raise_smem_limit(const void *func, size_t bytes);
 void sum_chunks(Session *s, double2 *d, int len, int nchunks);       // d[0:len] += sum_{c>0} d[c*len : ...]
 void add_into(Session *s, double2 *dst, const double2 *src, int len); // dst += src
 void block_to_states(Session *s, const void *blk, double2 *states, int N, int R, int Rpad);  // N x Rpad -> R x N

@@ -490,12 +490,10 @@ void launch_fft(Session *s, const Tin *L, const Tin *Rv, long K, int M, const do
   // every output k < n is written by exactly one thread of each CTA (pairs cover 16 x 16,
   // halves cover the R3 outputs), so the partials need no clearing
   if (2 * M <= n) {
-    LQ_CUDA(cudaFuncSetAttribute(k_kubo_fft<R3, NSEQ, true, Tin>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                 (int)smem));
+    raise_smem_limit((const void *)k_kubo_fft<R3, NSEQ, true, Tin>, smem);
     k_kubo_fft<R3, NSEQ, true, Tin><<<nb, kFftThreads, smem, s->stream>>>(L, Rv, K, chunk, M, pf, part);
   } else {
-    LQ_CUDA(cudaFuncSetAttribute(k_kubo_fft<R3, NSEQ, false, Tin>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                 (int)smem));
+    raise_smem_limit((const void *)k_kubo_fft<R3, NSEQ, false, Tin>, smem);
     k_kubo_fft<R3, NSEQ, false, Tin><<<nb, kFftThreads, smem, s->stream>>>(L, Rv, K, chunk, M, pf, part);
   }
   LQ_LAUNCHED();
@@ -510,7 +508,7 @@ void launch_dft(Session *s, const Tin *L, const Tin *Rv, long K, int M, int nump
   LQ_LAUNCHED();
   const size_t smem = sizeof(double2) * 2 * (size_t)M;
   if (smem > 227 * 1024) fail(LINQT_ERR_UNSUPPORTED, "kubo_fft: M too large for the direct DFT");
-  LQ_CUDA(cudaFuncSetAttribute(k_kubo_dft<NSEQ, Tin>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  raise_smem_limit((const void *)k_kubo_dft<NSEQ, Tin>, smem);
   const int nb = (int)std::max(1L, std::min(K, (long)s->sm_count * 4));
   const long chunk = (K + nb - 1) / nb;
   double2 *part = (double2 *)s->get("kubo_part", sizeof(double2) * 2 * (size_t)nump * nb);

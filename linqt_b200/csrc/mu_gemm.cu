@@ -219,7 +219,7 @@ void zgemm_cn_t(Session *s, const Tc *A, int MA, const Tc *B, int MB, long K, do
   S = (K + kchunk - 1) / kchunk;
   double2 *part = (double2 *)s->get("zgemm_parts", sizeof(double2) * (size_t)S * MA * MB);
   const size_t smem = sizeof(Tc) * 2 * (BM + BN) * LDS;
-  LQ_CUDA(cudaFuncSetAttribute(k_zgemm_cn_f64<Tc>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  raise_smem_limit((const void *)k_zgemm_cn_f64<Tc>, smem);
   dim3 grid((MB + BN - 1) / BN, (MA + BM - 1) / BM, (unsigned)S);
   k_zgemm_cn_f64<Tc><<<grid, 256, smem, s->stream>>>(A, B, MA, MB, K, kchunk, part);
   LQ_LAUNCHED();

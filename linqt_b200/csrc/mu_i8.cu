@@ -256,7 +256,7 @@ __device__ __forceinline__ uint32_t pack4(int a, int b, int c, int d) {
 }
 
 // Digit planes of both sides: z = 0 the L side (ND planes), z = 1 the R side (ND planes of b,
-// then ND of b'' = (Bi, -Br)).  src: rows of kf floats; dig: [nchunk][planes][rows][kchunk]
+// then ND of b'' = (Bi, -Br)).  src: rows of kf floats, ld floats apart; dig: [nchunk][planes][rows][kchunk]
 // int8, chunk-major so that the rows one K chunk's CTAs read at the same time lie kchunk
 // bytes apart rather than the whole K apart (K padded with zeros to kfp; the part of the
 // last chunk past kfp is never read); expo[row][chunk]: the exponent e with max |x| over
@@ -268,7 +268,7 @@ constexpr int kDigitCluster = 4;
 
 template <int ND>
 __global__ void __cluster_dims__(kDigitCluster, 1, 1) __launch_bounds__(256)
-    k_digits(const float *__restrict__ srcA, const float *__restrict__ srcB, long kf, long kfp, long kchunk,
+    k_digits(const float *__restrict__ srcA, const float *__restrict__ srcB, long ld, long kf, long kfp, long kchunk,
              int rows, int nchunk, int8_t *__restrict__ digA, int8_t *__restrict__ digB, int *__restrict__ expA,
              int *__restrict__ expB) {
   extern __shared__ float4 stage_q[];
@@ -279,7 +279,7 @@ __global__ void __cluster_dims__(kDigitCluster, 1, 1) __launch_bounds__(256)
   const int row = blockIdx.y, c = blockIdx.x / kDigitCluster, quarter = blockIdx.x % kDigitCluster;
   const long q = kchunk / kDigitCluster;  // a multiple of 32 floats
   const long k0 = (long)c * kchunk + quarter * q, k1 = min(kfp, k0 + q), kd = min(k1, kf);
-  const float *x = (b_side ? srcB : srcA) + (size_t)row * kf;
+  const float *x = (b_side ? srcB : srcA) + (size_t)row * ld;  // rows ld floats apart, kf of them used
   // stage this quarter (kf is even: a pair (k, k+1) is all in or all out of [k0, kd))
   float mx = 0.f;
   const int nquad = (int)max(0L, (k1 - k0) / 4);
@@ -351,8 +351,9 @@ CUtensorMap make_map_i8(const void *base, int rows, long kchunk, int planes, int
   return m;
 }
 
+// One slab of K: columns [0, K) of rows ld complex apart.
 template <int ND>
-void contract_i8(Session *s, const void *L, const void *Rv, int M, long K, double2 *mu_raw) {
+void contract_i8_slab(Session *s, const void *L, const void *Rv, int M, long K, long ld, double2 *mu_raw) {
   using Cfg = I8Cfg<ND>;
   LQ_REQUIRE(((uintptr_t)L % 16) == 0 && ((uintptr_t)Rv % 16) == 0, "tensor-core operands must be 16-byte aligned");
   const long kf = 2 * K, kfp = (kf + I8_KPAD - 1) / I8_KPAD * I8_KPAD;
@@ -386,14 +387,14 @@ void contract_i8(Session *s, const void *L, const void *Rv, int M, long K, doubl
   int *err = (int *)s->get("mu_tc_err_barrier", sizeof(int) * 4);  // read by mu_tc_check_error
   s->barrier_used = true;
   const size_t qsmem = sizeof(float) * (size_t)(kchunk / kDigitCluster);
-  LQ_CUDA(cudaFuncSetAttribute(k_digits<ND>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)qsmem));
+  raise_smem_limit((const void *)k_digits<ND>, qsmem);
   k_digits<ND><<<dim3(kDigitCluster * nchunk, M, 2), 256, qsmem, s->stream>>>(
-      (const float *)L, (const float *)Rv, kf, kfp, kchunk, M, nchunk, dA, dB, eA, eB);
+      (const float *)L, (const float *)Rv, 2 * ld, kf, kfp, kchunk, M, nchunk, dA, dB, eA, eB);
   LQ_LAUNCHED();
   const CUtensorMap ta = make_map_i8(dA, M, kchunk, ND * nchunk, I8_BM, Cfg::BK),
                     tb = make_map_i8(dB, M, kchunk, 2 * ND * nchunk, I8_BN, Cfg::BK);
   const size_t smem = sizeof(I8Shared<ND>) + 1024;
-  LQ_CUDA(cudaFuncSetAttribute(k_mu_i8<ND>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  raise_smem_limit((const void *)k_mu_i8<ND>, smem);
   for (long koff = 0; koff < kfp; koff += S * kchunk) {
     const int Sp = (int)std::min(S, (kfp - koff + kchunk - 1) / kchunk);
     dim3 grid((M + I8_BN - 1) / I8_BN, (M + I8_BM - 1) / I8_BM, (unsigned)Sp);
@@ -401,6 +402,15 @@ void contract_i8(Session *s, const void *L, const void *Rv, int M, long K, doubl
     LQ_LAUNCHED();
     reduce_parts_into(s, part, Sp, (long)M * M, mu_raw);
   }
+}
+
+// K in slabs (i8_slab): each slab's digit planes overwrite the previous slab's, so the planes
+// take at most kI8DigitBudget however long K is; the slabs' sums add into mu_raw in FP64.
+template <int ND>
+void contract_i8(Session *s, const void *L, const void *Rv, int M, long K, double2 *mu_raw) {
+  const long slab = i8_slab(ND, M, K);
+  for (long kb = 0; kb < K; kb += slab)
+    contract_i8_slab<ND>(s, (const float2 *)L + kb, (const float2 *)Rv + kb, M, std::min(slab, K - kb), K, mu_raw);
 }
 
 }  // namespace

@@ -255,7 +255,7 @@ void mu_contract_tc(Session *s, const void *L, const void *Rv, int M, long K, do
   int *err = (int *)s->get("mu_tc_err_barrier", sizeof(int) * 4);
   s->barrier_used = true;
   const size_t smem = sizeof(TcShared) + 1024;
-  LQ_CUDA(cudaFuncSetAttribute(k_mu_tf32x3, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  raise_smem_limit((const void *)k_mu_tf32x3, smem);
   for (long koff = 0; koff < kf; koff += S * kchunk) {
     const int Sp = (int)std::min(S, (kf - koff + kchunk - 1) / kchunk);
     dim3 grid((M + TC_BN - 1) / TC_BN, (M + TC_BM - 1) / TC_BM, (unsigned)Sp);

@@ -498,8 +498,8 @@ int coop_setup(const void *func, int sm_count, const DeviceOp &H, const DeviceOp
   const auto cap = [&](int p) { return std::max(1L, (long)(p * (double)sm_count * share)); };
   const int grid0 = (int)std::max(1L, std::min(cap(per_sm), need));
   const size_t limit = 96 * 1024;
-  // the attribute is per function and shared by all threads: always the same value
-  LQ_CUDA(cudaFuncSetAttribute(func, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)limit));
+  // 96 KB for every launch of these kernels, whichever thread launches them
+  raise_smem_limit((const void *)func, limit);
   // Fewer CTAs fit with the cache, and fewer CTAs have larger slices: shrink the grid
   // until the slices of `grid` CTAs fit `grid` co-resident CTAs.
   int grid = grid0;
@@ -601,7 +601,7 @@ struct LRF {
     const int grid = coop_setup(f, s->sm_count, H, V, TPR, sizeof(double2), &smem, sellC == 0, s->coop_share);
     sellC = std::max(sellC, 0);  // -1: CSR without the shared-memory cache
     int cache = smem > 0;
-    int sc = sellC;
+    int sc = sell_height(sellC);
     void *args[] = {&n,    (void *)&H.d_rowptr, (void *)&hci, (void *)&hv, (void *)&vrp, (void *)&vci,
                     (void *)&vv, &L, &Rs, (void *)&ph, &tbuf, &M, &blk, &bar, &cache,
                     (void *)&sperm, (void *)&soff, &sc};
@@ -638,7 +638,7 @@ struct OneDF {
     sellC = std::max(sellC, 0);  // -1: CSR without the shared-memory cache
     if (stacked) grid = std::max(nreal, grid / nreal * nreal);  // equal CTA groups per realisation
     int cache = smem > 0;
-    int sc = sellC;
+    int sc = sell_height(sellC);
     int ldx = TPR * VPT * (stacked ? nreal : 1);
     double2 *partials = (double2 *)s->get("rec1d_part", sizeof(double2) * 2 * (size_t)steps * grid);
     int n = H.n;

@@ -67,8 +67,8 @@ size_t estimate_footprint(const linqt_request &r, int n, int sm_count, int Rc) {
     return io + esz * (size_t)n * Rc * 3 +
            sizeof(double2) * (2 * steps * ((size_t)sm_count * 32 + 1) + 2 * steps * chunks) + (1 << 20);
   }
-  // INT8 contraction planes: the solver's chunking counts 3 bytes per digit and stored value
-  const size_t digits = 3 * (size_t)i8_digits(r.precision) * n * Rc * (2 * (size_t)r.M + 4);
+  // INT8 contraction planes: one K slab of them, as the solver's chunking counts them
+  const size_t digits = i8_digit_bytes(i8_digits(r.precision), r.M, (long)n * Rc);
   // sigma(E): the per-site transforms' partial sums and the 3*nump outputs
   const size_t fft = r.sigma_out ? sizeof(double2) * 2 * (size_t)r.nump * 1024 + 3 * sizeof(double) * r.nump : 0;
   const size_t total = io + esz * (size_t)n * Rc * (2 * (size_t)r.M + 4) + digits +

@@ -35,6 +35,18 @@ void sum_chunks_stream(cudaStream_t st, double2 *d, int len, int nchunks) {
   LQ_LAUNCHED();
 }
 
+void raise_smem_limit(const void *func, size_t bytes) {
+  static std::mutex m;
+  static std::map<std::pair<int, const void *>, size_t> limits;
+  int dev = 0;
+  LQ_CUDA(cudaGetDevice(&dev));
+  std::lock_guard<std::mutex> g(m);
+  size_t &cur = limits[{dev, func}];
+  if (bytes <= cur) return;
+  LQ_CUDA(cudaFuncSetAttribute(func, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes));
+  cur = bytes;
+}
+
 void add_into(Session *s, double2 *dst, const double2 *src, int len) {
   k_add_into<<<(len + 255) / 256, 256, 0, s->stream>>>(dst, src, len);
   LQ_LAUNCHED();

@@ -66,6 +66,13 @@ class Server:
         check(load().linqt_server_poll(self.h, ticket, ctypes.byref(st), ctypes.byref(lat)))
         return st.value, lat.value
 
+    def error(self, ticket):
+        """The message of a failed request (empty for one that did not fail)."""
+        st, lat = ctypes.c_int(), ctypes.c_double()
+        check(load().linqt_server_poll(self.h, ticket, ctypes.byref(st), ctypes.byref(lat)))
+        msg = load().linqt_last_error() if st.value < 0 else b""
+        return msg.decode() if msg else ""
+
     def result(self, ticket):
         out, _, _, M, kind, _ = self._keep[ticket]
         return out if kind == REQ_DOS else out.reshape(M, M)
@@ -228,7 +235,8 @@ def run_stream(reqs, prepared, gaps, mean_gap_s, max_active=4, hbm_budget_bytes=
     for t in tickets:
         status, ms = srv.poll(t)
         if status != 2:
-            raise RuntimeError("request %d ended with status %d" % (t, status))
+            raise RuntimeError("request %d (%s) ended with status %d: %s"
+                               % (t, reqs[tickets.index(t)], status, srv.error(t)))
         lat.append(ms)
         srv.release(t)
     if server is None:

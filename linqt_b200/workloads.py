@@ -14,6 +14,7 @@ Kubo-Bastin graphene workload:
     python -m linqt_b200.workloads recur1d --side 100 --vectors 64 --moments 16 --precision 0  # one 1D recursion
     python -m linqt_b200.workloads time_corr     # <V(t)V> of graphene 128x128, R=16, M=512, 40 time steps
     python -m linqt_b200.workloads supercell     # supercell CSR assembly (wannier2sparse) of two Wannier models
+    python -m linqt_b200.workloads locality --side 200 --moments 128 --reps 3  # natural vs locality row order
 
 Each line gives the device time per solve (CUDA events on the session stream, warm-up
 first), Chebyshev steps*nnz/s, the recursion's algorithmic bytes per second, and for the
@@ -329,6 +330,47 @@ def run_recur1d_once(L, R, M, prec, fmt=0):
             "bytes_per_step": by}
 
 
+def run_locality(L, widths, M, reps):
+    """The 1D DOS recursion on the cubic Anderson lattice L^3 with the rows visited in their
+    natural order (CSR), in the locality order (SELL_LOCAL) and as autotuned, per block width and
+    precision of the blocks (one block of R vectors, CUDA events; the locality order is built
+    and the autotuner runs in the untimed first call)."""
+    import torch
+    from .core import FORMAT_AUTO, FORMAT_CSR, FORMAT_SELL_LOCAL, random_phase_states_dev
+    N, H = lattices.cubic_lattice(L, 1.0, 2.0, 41)
+    sess = Session()
+    sess.set_stream(torch.cuda.current_stream())
+    Hg = Operator.from_csr(N, *H, session=sess)
+    Hg.rescale_to_chebyshev(2 * 1.05 * 7.0, 0.0)
+    del H
+    peak, src = _hbm_peak()
+    rows = []
+    for R in widths:
+        st = torch.empty(2 * R * N, dtype=torch.float64, device="cuda")
+        random_phase_states_dev(N, R, 45, st, session=sess)
+        mu = torch.zeros(2 * M, dtype=torch.float64, device="cuda")
+        for prec in (PREC_FP64, PREC_MIXED):
+            esz = 16 if prec == PREC_FP64 else 8
+            by = Hg.nnz * 20 + 4 * (N + 1) + 3 * esz * N * R
+            res = {"R": R, "blocks": "fp64" if prec == PREC_FP64 else "fp32"}
+            ref = None
+            for name, fmt in (("csr", FORMAT_CSR), ("local", FORMAT_SELL_LOCAL), ("auto", FORMAT_AUTO)):
+                o = make_opts(precision=prec, fmt=fmt, block_width=R)
+                moments1d_dev(Hg, None, st, R, M, mu, opts=o, session=sess)
+                ms = _timed(lambda: moments1d_dev(Hg, None, st, R, M, mu, opts=o, session=sess), reps, torch)
+                gbs = (M + 1) // 2 * by / (ms * 1e-3) / 1e9
+                m = mu.cpu().numpy().view(np.complex128)
+                if ref is None:
+                    ref = m
+                res[name] = {"ms": round(ms, 3), "GBps": round(gbs, 1), "hbm_frac": round(gbs / peak, 3),
+                             "rel_diff_vs_csr": float(np.abs(m - ref).max() / np.abs(ref).max())}
+            rows.append(res)
+        del st
+        torch.cuda.empty_cache()
+    return {"workload": "locality_cubic_%d" % L, "N": N, "M": M, "bytes_per_step": "nnz*20 + 4(N+1) + 3*esz*N*R",
+            "hbm_peak_GBps": peak, "hbm_peak_source": src, "rows": rows}
+
+
 def run_moments2d_once(Lc, R, M, prec):
     """One warm-up and one timed Kane-Mele spin 2D-moment solve with per-phase times (the
     case the contraction kernels are profiled on)."""
@@ -403,7 +445,8 @@ def run_supercell(orbitals, reach, L, op, reps):
 def main(argv=None):
     ap = argparse.ArgumentParser()
     ap.add_argument("workload", choices=["dos", "cubic", "cubic_full", "spin", "layouts", "realisations",
-                                         "lr_layouts", "cubic_width", "moments2d", "recur1d", "time_corr", "supercell"])
+                                         "lr_layouts", "cubic_width", "moments2d", "recur1d", "time_corr", "supercell",
+                                         "locality"])
     ap.add_argument("--precision", type=int, default=PREC_MIXED, help="moments2d: LINQT_PREC_* value")
     ap.add_argument("--reps", type=int, default=5)
     ap.add_argument("--cells", type=int, default=64, help="spin: Kane-Mele cells per side")
@@ -435,6 +478,8 @@ def main(argv=None):
         r = run_supercell(4, 1, 2048, "HAM", a.reps)
     elif a.workload == "time_corr":
         r = run_time_corr(128, 16, 512, 40, 1.0, a.reps)
+    elif a.workload == "locality":
+        r = run_locality(a.side, (8, 64, 256), a.moments, a.reps)
     elif a.workload == "recur1d":
         r = run_recur1d_once(a.side, a.vectors, a.moments, a.precision, a.format)
     elif a.workload == "moments2d":
