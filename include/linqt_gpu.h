@@ -65,7 +65,7 @@ enum {
 
 enum { LINQT_KUBO_GREENWOOD = 0, LINQT_KUBO_BASTIN = 1 }; /* chebyshev::formula, include/Kubo_solver_FFT.hpp:17-21 */
 
-enum { LINQT_FORMAT_CSR = 0, LINQT_FORMAT_SELL = 1, LINQT_FORMAT_AUTO = 2, LINQT_FORMAT_SELL_LOCAL = 3 };
+enum { LINQT_FORMAT_CSR = 0, LINQT_FORMAT_SELL = 1, LINQT_FORMAT_AUTO = 2, LINQT_FORMAT_LOCAL = 3 };
 
 typedef struct linqt_op linqt_op;
 typedef struct linqt_session linqt_session;
@@ -74,13 +74,14 @@ typedef struct linqt_session linqt_session;
 typedef struct linqt_opts {
   int precision;    /* LINQT_PREC_* */
   int format;       /* sparse layout of H in the persistent recursions: LINQT_FORMAT_CSR (default),
-                       LINQT_FORMAT_SELL (SELL-C-sigma, C = 32, sigma = 8C), LINQT_FORMAT_SELL_LOCAL
-                       (the same with the rows visited in a locality order found by recursive
-                       bisection of the operator's graph, see linqt_locality_order: neighbour rows
-                       are read close together in time, for lattices such as 3D ones whose
-                       neighbours lie far apart in the row numbering) or LINQT_FORMAT_AUTO
+                       LINQT_FORMAT_SELL (SELL-C-sigma, C = 32, sigma = 8C), LINQT_FORMAT_LOCAL
+                       (the CSR rows copied in a locality order found by recursive bisection of the
+                       operator's graph and visited in that order, see linqt_locality_order:
+                       neighbour rows are read close together in time, for lattices such as 3D ones
+                       whose neighbours lie far apart in the row numbering) or LINQT_FORMAT_AUTO
                        (autotuned among CSR with and without its shared-memory row cache and SELL
-                       with C = 8, 32, plus SELL_LOCAL when a block exceeds 64 MB, times the thread
+                       with C = 8, 32, plus the CSR rows and SELL-32 in the locality order when a
+                       block exceeds 64 MB (linqt_op_tuned reports the choices), times the thread
                        shapes of the block (threads per row min(R, 32) >> s, s = 0..3), and for 1D
                        moments without a fixed block_width the block width (R, R/2, R/4, R/8);
                        cached per operator, width and precision).  The layout changes only the
@@ -95,7 +96,7 @@ typedef struct linqt_opts {
                        operator pattern, S, R/S and precision), 1 = stacked in one launch, 2 = one solve each */
   int operator_precision; /* values of H in the 1D recursions (linqt_moments1d[_dev],
                        linqt_moments1d_realisations[_dev]): 0 = complex128 (default), 1 = complex64 (each
-                       value rounded once to FP32, products accumulated in FP64; CSR layouts, persistent
+                       value rounded once to FP32, products accumulated in FP64; every layout, persistent
                        recursion); other solvers accept 0 only */
   int reserved[8];
 } linqt_opts;
@@ -143,6 +144,13 @@ int linqt_csr_create(linqt_session *s, int n, const int *rowptr, const int *col,
 int linqt_op_destroy(linqt_op *op);
 /* dimension and Hermitian-expanded non-zeros (diagonal included) */
 int linqt_op_info(const linqt_op *op, int *n, long *nnz);
+/* The autotuner's cached decisions for this operator (LINQT_FORMAT_AUTO and
+ * opts.realisations = 0), as text: one "key choice" line per tuned case, the key naming the
+ * recursion, block width, precision and second operator, the choice a layout and thread shape
+ * ("csr", "csr_nocache", "sell<C>", "sell<C>_local"; "shape <s>"), a block width or a
+ * realisations mode.  Writes at most cap bytes including the terminating NUL; *len = the full
+ * length without it (call with cap = 0 to size the buffer).  No LinQT counterpart. */
+int linqt_op_tuned(const linqt_op *op, char *buf, long cap, long *len);
 /* H <- a*H + b*I  -- SparseMatrixType::Rescale (src/mkl_sparse_matrix.cpp:73-97) */
 int linqt_op_rescale(linqt_op *op, const double a[2], const double b[2]);
 /* y <- a*op*x + b*y for ncols column-major vectors of length n (ld = n):
@@ -351,7 +359,7 @@ int linqt_jackson1d(double *mu, int M, double band_width, double broad_meV, int 
 int linqt_jackson2d(double *mu, int M0, int M1, double band_width, double b0, double b1, int *M0_out, int *M1_out);
 
 /* Locality order of the rows of a CSR pattern (host only; no LinQT counterpart: it is the
- * traversal order behind LINQT_FORMAT_SELL_LOCAL).  The row graph is ordered breadth-first
+ * traversal order behind LINQT_FORMAT_LOCAL).  The row graph is ordered breadth-first
  * from a pseudo-peripheral row and cut into halves, recursively, until the parts have at most
  * part_rows rows (>= 1); order[pos] = row, a permutation of 0..n-1.  The pattern must be
  * structurally symmetric (a Hermitian operator's expanded rows are) with columns in [0, n). */

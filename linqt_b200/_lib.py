@@ -61,6 +61,7 @@ SIGNATURES = {
     "linqt_csr_create": (c_int, [c_void_p, c_int, P_int, P_int, P_double, c_int, ctypes.POINTER(c_void_p)]),
     "linqt_op_destroy": (c_int, [c_void_p]),
     "linqt_op_info": (c_int, [c_void_p, P_int, P_long]),
+    "linqt_op_tuned": (c_int, [c_void_p, ctypes.c_char_p, c_long, P_long]),
     "linqt_op_rescale": (c_int, [c_void_p, P_double, P_double]),
     "linqt_op_multiply": (c_int, [c_void_p, c_void_p, P_double, P_double, P_double, P_double, c_int]),
     "linqt_spectral_bounds": (c_int, [c_void_p, c_void_p, P_double, P_double]),

@@ -24,7 +24,7 @@ PREC_FP64, PREC_MIXED, PREC_FP32, PREC_MIXED_TF32, PREC_MIXED_FAST = 0, 1, 2, 3,
 KUBO_GREENWOOD, KUBO_BASTIN = 0, 1
 STORAGE_HERMITIAN_UPPER, STORAGE_GENERAL = 0, 1
 OP_C128, OP_C64 = 0, 1  # opts.operator_precision: complex128 or complex64 operator values (1D recursions)
-FORMAT_CSR, FORMAT_SELL, FORMAT_AUTO, FORMAT_SELL_LOCAL = 0, 1, 2, 3  # opts.format
+FORMAT_CSR, FORMAT_SELL, FORMAT_AUTO, FORMAT_LOCAL = 0, 1, 2, 3  # opts.format
 
 
 def _dp(a):
@@ -172,6 +172,18 @@ class Operator:
         nnz = ctypes.c_long()
         check(load().linqt_op_info(self.h, ctypes.byref(n), ctypes.byref(nnz)))
         return n.value, nnz.value
+
+    def tuned(self):
+        """The autotuner's cached decisions for this operator: {key: choice}."""
+        ln = ctypes.c_long()
+        check(load().linqt_op_tuned(self.h, None, 0, ctypes.byref(ln)))
+        buf = ctypes.create_string_buffer(ln.value + 1)
+        check(load().linqt_op_tuned(self.h, buf, ln.value + 1, ctypes.byref(ln)))
+        out = {}
+        for line in buf.value.decode().splitlines():
+            k, _, v = line.partition(" ")
+            out[k] = v
+        return out
 
     @property
     def n(self):
@@ -473,7 +485,7 @@ def jackson2d(mu, band_width, b0, b1):
 
 
 def locality_order(rowptr, col, part_rows=8192):
-    """The locality order behind FORMAT_SELL_LOCAL (host only): order[pos] = row."""
+    """The locality order behind FORMAT_LOCAL (host only): order[pos] = row."""
     rp = np.ascontiguousarray(rowptr, dtype=np.int32)
     ci = np.ascontiguousarray(col, dtype=np.int32)
     n = len(rp) - 1

@@ -218,6 +218,7 @@ void DeviceOp::free_device() {
     cudaFree(kv.second.d_off);
     cudaFree(kv.second.d_col);
     cudaFree(kv.second.d_val64);
+    cudaFree(kv.second.d_val32);
   }
   sell.clear();
   tuned.clear();
@@ -264,7 +265,7 @@ void DeviceOp::upload() {
 // (stable), slices of C rows, each slice stored column-major with width = its longest
 // row; padding entries point at the row itself with value zero.  With kSellLocality in
 // the key the windows are cut from the locality order of the rows.
-const DeviceOp::Sell &DeviceOp::ensure_sell(int key) {
+const DeviceOp::Sell &DeviceOp::ensure_sell(int key, bool c64) {
   const int C = sell_height(key);
   LQ_REQUIRE(C > 0 && (key & ~(kSellLocality | (kSellLocality - 1))) == 0, "bad SELL layout key");
   std::lock_guard<std::mutex> g(mu);
@@ -316,6 +317,15 @@ const DeviceOp::Sell &DeviceOp::ensure_sell(int key) {
     LQ_CUDA(cudaMemcpy(L.d_col, sc.data(), sizeof(int) * L.len, cudaMemcpyHostToDevice));
     LQ_CUDA(cudaMemcpy(L.d_val64, sv.data(), sizeof(double2) * L.len, cudaMemcpyHostToDevice));
   }
+  if (c64 && !L.d_val32) {
+    std::vector<double2> sv(L.len);
+    LQ_CUDA(cudaSetDevice(device));
+    LQ_CUDA(cudaMemcpy(sv.data(), L.d_val64, sizeof(double2) * L.len, cudaMemcpyDeviceToHost));
+    std::vector<float2> s32(L.len);
+    for (size_t q = 0; q < L.len; ++q) s32[q] = make_float2((float)sv[q].x, (float)sv[q].y);
+    LQ_CUDA(cudaMalloc(&L.d_val32, sizeof(float2) * L.len));
+    LQ_CUDA(cudaMemcpy(L.d_val32, s32.data(), sizeof(float2) * L.len, cudaMemcpyHostToDevice));
+  }
   return L;
 }
 
@@ -345,7 +355,7 @@ static linqt_opts defaults(const linqt_opts *o) {
   std::memset(&d, 0, sizeof(d));
   if (o) d = *o;
   LQ_REQUIRE(d.format == LINQT_FORMAT_CSR || d.format == LINQT_FORMAT_SELL || d.format == LINQT_FORMAT_AUTO ||
-                 d.format == LINQT_FORMAT_SELL_LOCAL,
+                 d.format == LINQT_FORMAT_LOCAL,
              "opts.format: unknown sparse format");
   LQ_REQUIRE(d.operator_precision == 0 || d.operator_precision == 1, "opts.operator_precision must be 0 or 1");
   return d;
@@ -434,9 +444,11 @@ static void with_graph(Session *s, const linqt_opts &o, const std::string &key, 
 // ---------------------------------------------------------------------------
 // Sparse layout and thread shape of a persistent recursion.  LINQT_FORMAT_CSR: the
 // operator's CSR (whose per-CTA row slices the kernels keep in shared memory when they fit),
-// thread shape 0; LINQT_FORMAT_SELL: SELL-C-sigma with C = 32, shape 0; LINQT_FORMAT_AUTO:
-// the autotuner times a short run of the same recursion (trial(C, shape)) for every layout
-// (CSR cached, CSR uncached, SELL with C = 8 and 32) and thread shape, keeps the fastest per
+// thread shape 0; LINQT_FORMAT_SELL: SELL-C-sigma with C = 32, shape 0; LINQT_FORMAT_LOCAL:
+// the CSR rows in the locality order (SELL with C = 1 over that order), shape 0;
+// LINQT_FORMAT_AUTO: the autotuner times a short run of the same recursion (trial(C, shape))
+// for every layout (CSR cached, CSR uncached, SELL with C = 8 and 32, and on large blocks
+// the two locality layouts) and thread shape, keeps the fastest per
 // operator pair, block width and precision, and returns it.  Each candidate runs once
 // untimed (building its layout) and once timed.
 // ---------------------------------------------------------------------------
@@ -445,13 +457,11 @@ struct RecCfg {
 };
 
 static RecCfg pick_layout(Session *s, const DeviceOp &H, const std::string &key, int format, int Rc,
-                          const std::function<void(int, int)> &trial, float *best_ms = nullptr,
-                          bool csr_only = false) {
+                          const std::function<void(int, int)> &trial, float *best_ms = nullptr) {
   if (best_ms) *best_ms = -1;
   if (format == LINQT_FORMAT_CSR) return RecCfg{0, 0};
-  if (format == LINQT_FORMAT_SELL || format == LINQT_FORMAT_SELL_LOCAL) {
-    if (csr_only) fail(LINQT_ERR_UNSUPPORTED, "complex64 operators: CSR layouts only");
-    return RecCfg{format == LINQT_FORMAT_SELL ? 32 : 32 | kSellLocality, 0};
+  if (format == LINQT_FORMAT_SELL || format == LINQT_FORMAT_LOCAL) {
+    return RecCfg{format == LINQT_FORMAT_SELL ? 32 : 1 | kSellLocality, 0};
   }
   DeviceOp &Hm = const_cast<DeviceOp &>(H);
   {
@@ -466,13 +476,13 @@ static RecCfg pick_layout(Session *s, const DeviceOp &H, const std::string &key,
   RecCfg pick;
   bool first = true;
   // 0: CSR, its row slices cached in shared memory when they fit; -1: CSR without the
-  // cache (more resident CTAs per SM); 8, 32: SELL-C-sigma; 32 | kSellLocality: SELL-C-sigma
-  // over the locality order, tried when one block of the lattice (8 bytes per value at
-  // least) exceeds 64 MB, i.e. when its neighbour rows can leave L2 between their reads
+  // cache (more resident CTAs per SM); 8, 32: SELL-C-sigma; 1 | kSellLocality (the CSR rows
+  // copied in the locality order) and 32 | kSellLocality: tried when one block of the lattice
+  // (8 bytes per value at least) exceeds 64 MB, i.e. when its neighbour rows can leave L2
+  // between their reads
   const bool big = (double)H.n * Rc * sizeof(float2) > 64e6;
-  for (int C : {0, -1, 8, 32, 32 | kSellLocality})
+  for (int C : {0, -1, 8, 32, 1 | kSellLocality, 32 | kSellLocality})
     for (int sh = 0; sh < recur_shapes(Rc); ++sh) {
-      if (csr_only && C > 0) continue;
       if ((C & kSellLocality) && !big) continue;
       trial(C, sh);
       LQ_CUDA(cudaEventRecord(a, s->stream));
@@ -542,7 +552,7 @@ static void moments1d_dev(Session *s, const DeviceOp &H, const DeviceOp *op, con
           }
           recur_1d(s, H, b2, x0, b1, st, Mt, doubling ? 2 : 1, w, fp32, tdots, C, shape, nullptr, 1, c64);
         },
-        best_ms, c64);
+        best_ms);
   };
   // LINQT_FORMAT_AUTO without a fixed block width: also the block width, among Rc, Rc/2, Rc/4
   // and Rc/8, by trial time per vector (a narrower block streams fewer bytes per row, which
@@ -1048,7 +1058,7 @@ static void moments_td_dev(Session *s, const DeviceOp &H, const DeviceOp *opl, c
   const std::vector<double2> c = td_coefficients(dt, band_width, band_center);
   double2 *coef = (double2 *)s->get("td_coef", sizeof(double2) * c.size());
   LQ_CUDA(cudaMemcpyAsync(coef, c.data(), sizeof(double2) * c.size(), cudaMemcpyHostToDevice, s->stream));
-  const int sellC = o.format == LINQT_FORMAT_SELL ? 32 : o.format == LINQT_FORMAT_SELL_LOCAL ? 32 | kSellLocality : 0;
+  const int sellC = o.format == LINQT_FORMAT_SELL ? 32 : o.format == LINQT_FORMAT_LOCAL ? 1 | kSellLocality : 0;
   {
     PhaseScope ph(s, PH_RECURSION);
     for (int ch = 0; ch < nchunks; ++ch) {
@@ -1305,6 +1315,42 @@ int linqt_op_info(const linqt_op *op, int *n, long *nnz) {
     check_op(op, "op");
     if (n) *n = op->op.n;
     if (nnz) *nnz = op->op.nnz;
+  });
+}
+
+int linqt_op_tuned(const linqt_op *op, char *buf, long cap, long *len) {
+  return guarded([&] {
+    check_op(op, "op");
+    LQ_REQUIRE(cap >= 0 && (buf || cap == 0), "bad buffer");
+    std::string out;
+    {
+      DeviceOp &d = const_cast<DeviceOp &>(op->op);
+      std::lock_guard<std::mutex> g(d.mu);
+      for (const auto &kv : d.tuned) {
+        std::string v;
+        if (kv.first.rfind("1dw:", 0) == 0) {
+          v = "width " + std::to_string(kv.second);
+        } else if (kv.first.rfind("real:", 0) == 0) {
+          v = kv.second == 1 ? "stacked" : "separate";
+        } else {
+          const int key = kv.second / 16 - 1, shape = kv.second % 16;
+          if (key == 0)
+            v = "csr";
+          else if (key < 0)
+            v = "csr_nocache";
+          else
+            v = "sell" + std::to_string(sell_height(key)) + ((key & kSellLocality) ? "_local" : "");
+          v += " shape " + std::to_string(shape);
+        }
+        out += kv.first + " " + v + "\n";
+      }
+    }
+    if (len) *len = (long)out.size();
+    if (cap > 0) {
+      const size_t n = std::min((size_t)cap - 1, out.size());
+      std::memcpy(buf, out.data(), n);
+      buf[n] = 0;
+    }
   });
 }
 

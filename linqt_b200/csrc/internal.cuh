@@ -4,6 +4,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <condition_variable>
 #include <cstdint>
 #include <map>
 #include <mutex>
@@ -177,10 +178,11 @@ struct DeviceOp {
   struct Sell {
     int *d_perm = nullptr, *d_off = nullptr, *d_col = nullptr;
     double2 *d_val64 = nullptr;
+    float2 *d_val32 = nullptr;  // complex64 values (each rounded once), made on first use
     size_t len = 0;
   };
   std::map<int, Sell> sell;
-  const Sell &ensure_sell(int key);
+  const Sell &ensure_sell(int key, bool c64 = false);
   std::vector<int> loc_order;  // locality order of the rows (made on first use)
   // format chosen by the autotuner, per (recursion kind, block width, precision, second operator)
   std::map<std::string, int> tuned;
@@ -210,6 +212,18 @@ __host__ __device__ inline int rearranged_source(int j, int n) {
 
 enum Phase { PH_RECURSION = 0, PH_CONTRACT = 1, PH_FFT = 2, PH_OTHER = 3 };
 
+// Shares of a device's co-resident CTAs held by the persistent cooperative grids of the
+// sessions that use it (the server's slots).  A grid takes what it needs, up to what is free,
+// before its launch, and a host callback on its stream gives the share back when the kernel
+// has finished, so the grids that run side by side always fit on the device together.
+struct CoopLedger {
+  std::mutex mu;
+  std::condition_variable cv;
+  double free = 0.9;       // 10 % slack for how CTAs of different grids pack into SMs
+  double min_share = 0.2;  // a grid waits until this much (or all it needs) is free
+  long waits_expired = 0;  // waits that gave up (the grid then ran on what was free)
+};
+
 struct Session {
   int device = 0;
   cudaStream_t stream = nullptr;
@@ -226,6 +240,9 @@ struct Session {
   // fraction of the device's co-resident CTAs the session's persistent grids may use
   // (linqt_session_set_sm_share); below 1 they launch on the session stream, not the lane
   double coop_share = 1.0;
+  // with a ledger (server slots) and coop_share < 1, each grid's share comes from the ledger
+  CoopLedger *ledger = nullptr;
+  double held_share = 0;  // taken for the grid about to launch, not yet handed to a callback
   int inject_extra = 0;
   long long inject_limit = 0;
   bool barrier_cfg_dirty = false;
@@ -387,7 +404,11 @@ void moments1d_nonorth_dev(Session *s, const DeviceOp &H, const DeviceOp *op, co
 struct GridBarrier;
 GridBarrier *barrier_for(Session *s);
 // occupancy-sized cooperative grid and a launch through the device's cooperative lane (recur.cu)
-int coop_grid(const void *func, int sm_count, long max_blocks, size_t smem, double share = 1.0);
+int coop_grid(Session *s, const void *func, long max_blocks, size_t smem);
+// The fraction of the co-resident CTAs a persistent grid of `s` may use, `want` being what it
+// needs (at most 1): the session's fixed share, or with a ledger what it takes from it.
+double coop_share_take(Session *s, double want);
+void coop_share_return(Session *s);  // gives back a share taken for a grid that did not launch
 void coop_launch(Session *s, const void *f, int grid, void **args, size_t smem);
 
 // small utilities (util.cu)

@@ -373,8 +373,6 @@ void moments1d_nonorth_dev(Session *s, const DeviceOp &H, const DeviceOp *op, co
   LQ_CUDA(cudaMemcpyAsync(d_invd, invd.data(), sizeof(double2) * N, cudaMemcpyHostToDevice, s->stream));
   char *W = (char *)s->get("no_blocks", 11 * blk);
   const void *f = (const void *)k_nonorth_1d;
-  const int grid = coop_grid(f, s->sm_count, ((long)N * Rb + kT - 1) / kT, 0, s->coop_share);
-  double2 *part = (double2 *)s->get("no_part", sizeof(double2) * 3 * (size_t)grid * Rb);
   double2 *dots = (double2 *)s->get("no_dots", sizeof(double2) * (size_t)M * Rb);
   long long *its = (long long *)s->get("no_iters", sizeof(long long) * kMaxCols);
   std::vector<long long> h_its(kMaxCols);
@@ -404,11 +402,13 @@ void moments1d_nonorth_dev(Session *s, const DeviceOp &H, const DeviceOp *op, co
     a.V = b + 8 * (size_t)N * Rb;
     a.Sv = b + 9 * (size_t)N * Rb;
     a.Tv = b + 10 * (size_t)N * Rb;
-    a.part = part;
     a.dots = dots;
     a.iters = its;
     states_to_block_stream(s->stream, s->sm_count, states + (size_t)c0 * N, (void *)a.phi, N, w, Rb);
     a.bar = barrier_for(s);
+    // the grid (and its share of the device) is sized per launch
+    const int grid = coop_grid(s, f, ((long)N * Rb + kT - 1) / kT, 0);
+    a.part = (double2 *)s->get("no_part", sizeof(double2) * 3 * (size_t)grid * Rb);
     void *args[] = {&a};
     coop_launch(s, f, grid, args, 0);
     k_nonorth_mu<<<(M + 255) / 256, 256, 0, s->stream>>>(dots, M, Rb, w, R, c0 > 0, mu);

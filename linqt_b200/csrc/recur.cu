@@ -486,13 +486,14 @@ size_t max_slice_bytes(const DeviceOp &H, const DeviceOp *V, int grid, size_t es
 
 // Cooperative grid: as many co-resident CTAs as fit (at most one CTA's worth of rows per
 // group of TPR threads).  The operator slices are cached in shared memory when they fit.
-int coop_setup(const void *func, int sm_count, const DeviceOp &H, const DeviceOp *V, int tpr, size_t esz,
-               size_t *smem, bool allow_cache, double share) {
-  const int n = H.n;
+int coop_setup(Session *s, const void *func, const DeviceOp &H, const DeviceOp *V, int tpr, size_t esz,
+               size_t *smem, bool allow_cache) {
+  const int n = H.n, sm_count = s->sm_count;
   const long need = ((long)n * tpr + kThreads - 1) / kThreads;
   int per_sm = 0;
   LQ_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, func, kThreads, 0));
   if (per_sm <= 0) fail(LINQT_ERR_UNSUPPORTED, "persistent recursion: kernel does not fit on an SM");
+  const double share = coop_share_take(s, std::min(1.0, (double)need / ((double)per_sm * sm_count)));
   // a session with an SM share (linqt_session_set_sm_share) keeps its grid to that fraction
   // of the co-resident CTAs, so that grids of sessions whose shares add up to 1 fit together
   const auto cap = [&](int p) { return std::max(1L, (long)(p * (double)sm_count * share)); };
@@ -524,13 +525,54 @@ int coop_setup(const void *func, int sm_count, const DeviceOp &H, const DeviceOp
 
 // Co-resident CTAs of kThreads threads for func with smem bytes of dynamic shared memory,
 // at most max_blocks.
-int coop_grid(const void *func, int sm_count, long max_blocks, size_t smem, double share) {
+int coop_grid(Session *s, const void *func, long max_blocks, size_t smem) {
   int per_sm = 0;
   LQ_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, func, kThreads, smem));
   if (per_sm <= 0) fail(LINQT_ERR_UNSUPPORTED, "persistent kernel does not fit on an SM");
-  const long cap = std::max(1L, (long)(per_sm * (double)sm_count * share));
+  const double full = (double)per_sm * s->sm_count;
+  const double share = coop_share_take(s, std::min(1.0, (double)max_blocks / full));
+  const long cap = std::max(1L, (long)(full * share));
   return (int)std::max(1L, std::min(cap, max_blocks));
 }
+
+double coop_share_take(Session *s, double want) {
+  if (!s->ledger || s->coop_share >= 1.0 || s->capturing) return s->coop_share;
+  coop_share_return(s);  // a share left by a launch that failed before it was handed over
+  CoopLedger &L = *s->ledger;
+  std::unique_lock<std::mutex> g(L.mu);
+  const double floor = std::min(want, L.min_share);
+  // a share comes back when its kernel finishes; the wait is bounded in case a stream
+  // stopped running callbacks (a device error), and the grid then sizes itself to what is free
+  if (!L.cv.wait_for(g, std::chrono::seconds(120), [&] { return L.free >= floor - 1e-9; })) L.waits_expired++;
+  const double share = std::max(0.02, std::min(want, L.free));
+  L.free -= std::min(share, L.free);
+  s->held_share = share;
+  return share;
+}
+
+void coop_share_return(Session *s) {
+  if (!s->ledger || s->held_share <= 0) return;
+  std::lock_guard<std::mutex> g(s->ledger->mu);
+  s->ledger->free += s->held_share;
+  s->held_share = 0;
+  s->ledger->cv.notify_all();
+}
+
+namespace {
+struct ShareToken {
+  CoopLedger *ledger;
+  double share;
+};
+void CUDART_CB share_back(void *p) {  // host callback: no CUDA calls here
+  ShareToken *t = static_cast<ShareToken *>(p);
+  {
+    std::lock_guard<std::mutex> g(t->ledger->mu);
+    t->ledger->free += t->share;
+  }
+  t->ledger->cv.notify_all();
+  delete t;
+}
+}  // namespace
 
 // Cooperative kernels of all sessions on a device run one after another on one lane
 // stream.  A grid barrier needs every CTA of its grid resident; two persistent grids
@@ -547,7 +589,20 @@ void coop_launch(Session *s, const void *f, int grid, void **args, size_t smem) 
   // a graph capture of this session's stream (api.cu, with_graph), or a session whose grids
   // are sized to its SM share: launched on the session's own stream
   if (s->capturing || s->coop_share < 1.0) {
-    LQ_CUDA(cudaLaunchCooperativeKernel(f, dim3(grid), dim3(kThreads), args, smem, s->stream));
+    const cudaError_t e = cudaLaunchCooperativeKernel(f, dim3(grid), dim3(kThreads), args, smem, s->stream);
+    if (e != cudaSuccess) {
+      coop_share_return(s);
+      LQ_CUDA(e);
+    }
+    if (s->held_share > 0) {  // the ledger's share comes back once the kernel has finished
+      ShareToken *t = new ShareToken{s->ledger, s->held_share};
+      s->held_share = 0;
+      const cudaError_t h = cudaLaunchHostFunc(s->stream, share_back, t);
+      if (h != cudaSuccess) {
+        share_back(t);
+        LQ_CUDA(h);
+      }
+    }
     return;
   }
   static std::mutex table_mu;
@@ -598,7 +653,7 @@ struct LRF {
     const C *ph = (const C *)phi;
     const void *f = V ? (const void *)k_recur_lr<T, TPR, VPT, true> : (const void *)k_recur_lr<T, TPR, VPT, false>;
     size_t smem = 0;
-    const int grid = coop_setup(f, s->sm_count, H, V, TPR, sizeof(double2), &smem, sellC == 0, s->coop_share);
+    const int grid = coop_setup(s, f, H, V, TPR, sizeof(double2), &smem, sellC == 0);
     sellC = std::max(sellC, 0);  // -1: CSR without the shared-memory cache
     int cache = smem > 0;
     int sc = sell_height(sellC);
@@ -618,11 +673,10 @@ struct OneDF {
     const void *hv = stacked ? stacked : (c64 ? (const void *)const_cast<DeviceOp &>(H).val32() : H.d_val64);
     long vstride = stacked ? H.nnz : 0;
     LQ_REQUIRE(!stacked || (nreal >= 1 && sellC <= 0), "stacked realisations: CSR layout only");
-    LQ_REQUIRE(!c64 || sellC <= 0, "complex64 operators: CSR layout only");
     const int *hci = H.d_col, *sperm = nullptr, *soff = nullptr;
     if (sellC > 0) {
-      const DeviceOp::Sell &L = const_cast<DeviceOp &>(H).ensure_sell(sellC);
-      hv = L.d_val64;
+      const DeviceOp::Sell &L = const_cast<DeviceOp &>(H).ensure_sell(sellC, c64);
+      hv = c64 ? (const void *)L.d_val32 : (const void *)L.d_val64;
       hci = L.d_col;
       sperm = L.d_perm;
       soff = L.d_off;
@@ -633,8 +687,8 @@ struct OneDF {
                                    : (const void *)k_recur_1d<T, double2, TPR, VPT, false>);
     size_t smem = 0;
     // the shared-memory operator cache holds one value set: not with stacked realisations
-    int grid = coop_setup(f, s->sm_count, H, nullptr, TPR, c64 ? sizeof(float2) : sizeof(double2), &smem,
-                          sellC == 0 && !stacked, s->coop_share);
+    int grid = coop_setup(s, f, H, nullptr, TPR, c64 ? sizeof(float2) : sizeof(double2), &smem,
+                          sellC == 0 && !stacked);
     sellC = std::max(sellC, 0);  // -1: CSR without the shared-memory cache
     if (stacked) grid = std::max(nreal, grid / nreal * nreal);  // equal CTA groups per realisation
     int cache = smem > 0;
@@ -665,7 +719,7 @@ struct SeriesF {
   static void run(Session *s, const DeviceOp &H, void *X, void *a, void *b, const double2 *coef, int K, Barrier *bar) {
     const void *f = (const void *)k_cheb_series<TPR, VPT>;
     size_t smem = 0;
-    const int grid = coop_setup(f, s->sm_count, H, nullptr, TPR, sizeof(double2), &smem, true, s->coop_share);
+    const int grid = coop_setup(s, f, H, nullptr, TPR, sizeof(double2), &smem, true);
     int cache = smem > 0;
     int n = H.n;
     const double2 *hv = H.d_val64;

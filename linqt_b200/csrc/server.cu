@@ -39,7 +39,7 @@ namespace {
 
 typedef std::chrono::steady_clock clk;
 
-// Fraction of the device the slots' persistent grids share (each slot kSlotShare / slots):
+// Fraction of the device the slots' persistent grids share (through the server's ledger):
 // a little below 1 leaves room for CTAs of different kernels that do not pack evenly.
 constexpr double kSlotShare = 0.9;
 
@@ -107,6 +107,7 @@ struct linqt_server {
   std::vector<void *> pinned_all;
   cudaMemPool_t pool = nullptr;
   uint64_t old_threshold = 0;
+  CoopLedger ledger;  // the slots' persistent grids take their shares of the device from it
 
   void *pinned_get(size_t bytes, size_t *cap) {
     size_t c = 4096;
@@ -143,6 +144,7 @@ struct linqt_server {
       cudaStreamCreateWithFlags(&s.stream, cudaStreamNonBlocking);
       s.own_stream = true;
       cudaDeviceGetAttribute(&s.sm_count, cudaDevAttrMultiProcessorCount, device);
+      s.ledger = &ledger;
     }
     for (;;) {
       std::shared_ptr<Job> job;
@@ -157,7 +159,10 @@ struct linqt_server {
           const Job &f = *queue.front();
           return f.alone ? running == 0 : in_use + f.footprint <= budget;
         });
-        if (stop && queue.empty()) return;
+        if (stop && queue.empty()) {
+          cudaStreamSynchronize(sess->s.stream);  // its share callbacks have run
+          return;
+        }
         if (queue.empty()) continue;
         job = queue.front();
         queue.pop_front();
@@ -170,11 +175,15 @@ struct linqt_server {
       std::string err;
       void *res_host = nullptr;
       size_t res_cap = 0;
-      // Persistent recursions of the slots run side by side, each grid sized to its share of
-      // the device.  A grid that does not become co-resident in time ends its solve with
-      // LINQT_ERR_TIMEOUT; the request then runs again at once on the device-wide cooperative
-      // lane.  A request whose workspaces did not fit next to the others (LINQT_ERR_NOMEM: the
-      // footprint is an estimate) goes back to the head of the queue to run alone.
+      // Persistent recursions of the slots run side by side: each grid takes what it needs of
+      // the device from the server's ledger, up to what the other slots' running grids leave
+      // free (at least a 1 / max_active part of kSlotShare, or all it needs, waiting for it
+      // when less is free), and returns it when the kernel has finished; a request alone on
+      // the device so gets all of it.  A grid that does not become co-resident in time (CTAs
+      // of other kernels can hold SMs) ends its solve with LINQT_ERR_TIMEOUT; the request then
+      // runs again at once on the device-wide cooperative lane.  A request whose workspaces
+      // did not fit next to the others (LINQT_ERR_NOMEM: the footprint is an estimate) goes
+      // back to the head of the queue to run alone.
       for (int attempt = 0; attempt < 2; ++attempt) {
         sess->s.coop_share = (attempt == 0 && max_active > 1 && !job->alone) ? kSlotShare / max_active : 1.0;
         rc = 0;
@@ -214,10 +223,12 @@ struct linqt_server {
         } catch (const Error &e) {
           rc = e.code;
           err = e.what();
+          coop_share_return(&sess->s);
           sess->s.trim();
         } catch (const std::exception &e) {
           rc = LINQT_ERR_INTERNAL;
           err = e.what();
+          coop_share_return(&sess->s);
         }
         if (rc != LINQT_ERR_TIMEOUT || sess->s.coop_share >= 1.0) break;
         std::lock_guard<std::mutex> g(mu);
@@ -267,6 +278,8 @@ int linqt_server_create(int device, size_t hbm_budget_bytes, int max_active, lin
     s->device = device;
     s->budget = hbm_budget_bytes ? hbm_budget_bytes : (size_t)(fr * 0.8);
     s->max_active = max_active;
+    s->ledger.free = kSlotShare;
+    s->ledger.min_share = kSlotShare / max_active;
     LQ_CUDA(cudaDeviceGetAttribute(&s->sm_count, cudaDevAttrMultiProcessorCount, device));
     // keep up to the budget cached in the device pool between requests (restored at destroy)
     LQ_CUDA(cudaDeviceGetDefaultMemPool(&s->pool, device));

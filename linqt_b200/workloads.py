@@ -336,7 +336,7 @@ def run_locality(L, widths, M, reps):
     precision of the blocks (one block of R vectors, CUDA events; the locality order is built
     and the autotuner runs in the untimed first call)."""
     import torch
-    from .core import FORMAT_AUTO, FORMAT_CSR, FORMAT_SELL_LOCAL, random_phase_states_dev
+    from .core import FORMAT_AUTO, FORMAT_CSR, FORMAT_LOCAL, random_phase_states_dev
     N, H = lattices.cubic_lattice(L, 1.0, 2.0, 41)
     sess = Session()
     sess.set_stream(torch.cuda.current_stream())
@@ -354,7 +354,7 @@ def run_locality(L, widths, M, reps):
             by = Hg.nnz * 20 + 4 * (N + 1) + 3 * esz * N * R
             res = {"R": R, "blocks": "fp64" if prec == PREC_FP64 else "fp32"}
             ref = None
-            for name, fmt in (("csr", FORMAT_CSR), ("local", FORMAT_SELL_LOCAL), ("auto", FORMAT_AUTO)):
+            for name, fmt in (("csr", FORMAT_CSR), ("local", FORMAT_LOCAL), ("auto", FORMAT_AUTO)):
                 o = make_opts(precision=prec, fmt=fmt, block_width=R)
                 moments1d_dev(Hg, None, st, R, M, mu, opts=o, session=sess)
                 ms = _timed(lambda: moments1d_dev(Hg, None, st, R, M, mu, opts=o, session=sess), reps, torch)
@@ -364,6 +364,8 @@ def run_locality(L, widths, M, reps):
                     ref = m
                 res[name] = {"ms": round(ms, 3), "GBps": round(gbs, 1), "hbm_frac": round(gbs / peak, 3),
                              "rel_diff_vs_csr": float(np.abs(m - ref).max() / np.abs(ref).max())}
+            res["auto"]["choice"] = {k: v for k, v in Hg.tuned().items() if (":%d:" % R) in k and
+                                     (":f64:" if prec == PREC_FP64 else ":f32:") in k}
             rows.append(res)
         del st
         torch.cuda.empty_cache()

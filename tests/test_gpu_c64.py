@@ -41,7 +41,7 @@ def cubic(oracle_lib):
     return N, H, Hg, Ho, rounded_oracle_op(oracle_lib, Ho)
 
 
-@pytest.mark.parametrize("fmt", [0, 2])
+@pytest.mark.parametrize("fmt", [0, 1, 2, 3])  # CSR, SELL, autotuned, SELL over the locality order
 def test_c64_operator_matches_the_oracle_on_the_rounded_operator(oracle_lib, cubic, fmt):
     N, H, Hg, Ho, H32 = cubic
     st = lattices.random_phase_states(N, 8, seed=45)
@@ -84,5 +84,5 @@ def test_c64_operator_is_a_1d_option_only(cubic):
         lq.moments2d(Hg, Hg, Hg, st, 16, opts=lq.make_opts(operator_precision=lq.OP_C64))
     assert e.value.code == -4
     with pytest.raises(lq.LinqtError) as e:
-        lq.moments1d(Hg, None, st, 16, opts=lq.make_opts(operator_precision=lq.OP_C64, fmt=1))
+        lq.moments1d(Hg, None, st, 16, opts=lq.make_opts(operator_precision=lq.OP_C64, step_launches=1))
     assert e.value.code == -4

@@ -1,4 +1,4 @@
-"""LINQT_FORMAT_SELL_LOCAL: the persistent recursions visiting the rows of H in the locality
+"""LINQT_FORMAT_LOCAL: the persistent recursions visiting the rows of H in the locality
 order (recursive bisection of the operator's graph into parts of at most 8192 rows).
 
 Only the traversal changes: each row's gather keeps the order of its entries, so the 2D tables
@@ -6,6 +6,8 @@ Only the traversal changes: each row's gather keeps the order of its entries, so
 of their per-CTA dot-product sums.  Sizes are above 8192 rows so that the order is not the
 natural one.
 """
+import re
+
 import numpy as np
 import pytest
 
@@ -36,12 +38,12 @@ def test_cubic_dos_local_order(oracle_lib, R):
     Hg, Ho, _ = setup(oracle_lib, N, H)
     st = lattices.random_phase_states(N, R, seed=49)
     M = 200
-    loc = lq.moments1d(Hg, None, st, M, opts=lq.make_opts(fmt=lq.FORMAT_SELL_LOCAL))
+    loc = lq.moments1d(Hg, None, st, M, opts=lq.make_opts(fmt=lq.FORMAT_LOCAL))
     csr = lq.moments1d(Hg, None, st, M)
     assert rel(loc, csr) < 1e-13
     assert rel(loc, oracle_lib.moments1d(Ho, None, st, M)) < TOL
     # mixed precision: FP32 blocks, the same per-row rounding in both layouts
-    o = lq.make_opts(precision=lq.PREC_MIXED, fmt=lq.FORMAT_SELL_LOCAL)
+    o = lq.make_opts(precision=lq.PREC_MIXED, fmt=lq.FORMAT_LOCAL)
     mloc = lq.moments1d(Hg, None, st, M, opts=o)
     mcsr = lq.moments1d(Hg, None, st, M, opts=lq.make_opts(precision=lq.PREC_MIXED))
     assert rel(mloc, mcsr) < 1e-12
@@ -52,7 +54,7 @@ def test_kane_mele_2d_tables_bitwise(oracle_lib):
     Hg, Ho, ((Vg, Vo),) = setup(oracle_lib, N, H, [V])
     st = lattices.random_phase_states(N, 3, seed=35)
     M = 48
-    loc = lq.moments2d(Hg, Vg, Vg, st, M, opts=lq.make_opts(fmt=lq.FORMAT_SELL_LOCAL))
+    loc = lq.moments2d(Hg, Vg, Vg, st, M, opts=lq.make_opts(fmt=lq.FORMAT_LOCAL))
     csr = lq.moments2d(Hg, Vg, Vg, st, M)
     assert np.array_equal(loc, csr)
     assert rel(loc, oracle_lib.moments2d(Ho, Vo, Vo, st, M)) < TOL
@@ -65,7 +67,7 @@ def test_kubo_bastin_local_order(oracle_lib):
     M, nump = 64, 256
     lo, hi = lattices.gershgorin_bounds(N, *H)
     bw, bc = 1.05 * (hi - lo), (hi + lo) / 2
-    mu_a, fa = lq.kubo_bastin(Hg, Vg, Vg, st, M, nump, bw, bc, opts=lq.make_opts(fmt=lq.FORMAT_SELL_LOCAL))
+    mu_a, fa = lq.kubo_bastin(Hg, Vg, Vg, st, M, nump, bw, bc, opts=lq.make_opts(fmt=lq.FORMAT_LOCAL))
     mu_b, fb = lq.kubo_bastin(Hg, Vg, Vg, st, M, nump, bw, bc)
     assert np.array_equal(mu_a, mu_b)
     for x, y in zip(fa, fb):
@@ -80,3 +82,7 @@ def test_autotuner_considers_the_local_order(oracle_lib):
     st = lattices.random_phase_states(N, 64, seed=51)
     mu = lq.moments1d(Hg, None, st, 40, opts=lq.make_opts(fmt=lq.FORMAT_AUTO))
     assert rel(mu, oracle_lib.moments1d(Ho, None, st, 40)) < TOL
+    tuned = Hg.tuned()  # linqt_op_tuned: the cached layout and width decisions
+    layouts = [v for k, v in tuned.items() if k.startswith("1d:")]
+    assert layouts and all(re.fullmatch(r"(csr|csr_nocache|sell\d+(_local)?) shape \d", v) for v in layouts)
+    assert any(k.startswith("1dw:") and re.fullmatch(r"width \d+", v) for k, v in tuned.items())

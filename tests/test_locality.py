@@ -1,4 +1,4 @@
-"""The locality order behind LINQT_FORMAT_SELL_LOCAL (host-only entry point, no GPU).
+"""The locality order behind LINQT_FORMAT_LOCAL (host-only entry point, no GPU).
 
 The recursions visit the rows of H in this order; the vector blocks stay in the natural
 numbering.  On a periodic cubic lattice numbered x + L(y + Lz) a row's z neighbours are L^2
