@@ -15,6 +15,7 @@ Kubo-Bastin graphene workload:
     python -m linqt_b200.workloads time_corr     # <V(t)V> of graphene 128x128, R=16, M=512, 40 time steps
     python -m linqt_b200.workloads supercell     # supercell CSR assembly (wannier2sparse) of two Wannier models
     python -m linqt_b200.workloads locality --side 200 --moments 128 --reps 3  # natural vs locality row order
+    python -m linqt_b200.workloads lr_widths --cells 512 --vectors 16 --moments 64 --reps 2  # L/R recursion per width
 
 Each line gives the device time per solve (CUDA events on the session stream, warm-up
 first), Chebyshev steps*nnz/s, the recursion's algorithmic bytes per second, and for the
@@ -128,7 +129,8 @@ def run_spin(Lc, R, M, nump, reps, mixed_precisions=(PREC_MIXED,)):
         mu2 = torch.zeros(2 * M * M, dtype=torch.float64, device="cuda")
         ms2 = _timed(lambda: moments2d_dev(Hg, Jg, Jg, st_dev, R, M, mu2, opts=o, session=sess), reps, torch)
         E_m, s_mom = bastin_from_moments(mu_h, N, bw, bc, 1e-3, xbound=0.99, session=sess)
-        res[prec] = dict(ms=ms, phases=[round(x / reps, 3) for x in ph], mu=mu_h, s_fft=s_fft, ms2=ms2, s_mom=s_mom)
+        res[prec] = dict(ms=ms, phases=[round(x / reps, 3) for x in ph], mu=mu_h, s_fft=s_fft, ms2=ms2, s_mom=s_mom,
+                         tuned={":".join(k.split(":")[:3]): v for k, v in Hg.tuned().items()})
         nnz = Hg.nnz
         del mu, out, mu2, Hg, Jg
         sess.close()
@@ -141,7 +143,8 @@ def run_spin(Lc, R, M, nump, reps, mixed_precisions=(PREC_MIXED,)):
 
     def side(r):
         return {"ms_per_solve": r["ms"], "phases_ms": r["phases"], "steps_nnz_per_s": work / (r["ms"] * 1e-3),
-                "moments2d_ms": r["ms2"], "moments2d_steps_nnz_per_s": work / (r["ms2"] * 1e-3)}
+                "moments2d_ms": r["ms2"], "moments2d_steps_nnz_per_s": work / (r["ms2"] * 1e-3),
+                "autotuned": r["tuned"]}
 
     out = {"workload": "spin_kane_mele_%dx%d" % (Lc, Lc), "N": N, "nnz_full": nnz, "R": R, "M": M, "nump": nump,
            "operator": "{s_z, V_x}/2", "fp64": side(a)}
@@ -281,6 +284,39 @@ def run_lr_layouts(name, N, H, V, R, M, reps):
             sess.enable_timing(False)
             out[lab + "_" + fl + "_recursion_ms"] = ph[0] / reps
     return out
+
+
+def run_lr_widths(Lc, R, M, widths, reps):
+    """Recursion phase of the Kane-Mele spin 2D moments per precision and vector-block width
+    (opts.block_width), layout autotuned: ms per block step and vector, and the autotuner's
+    choice (the case the spin-transport workload's chunks run in)."""
+    import torch
+    from .core import moments2d_dev
+    N, H, J = lattices.kane_mele(Lc, Lc, seed=31)
+    sess, bw, bc, Hg, (Jg,) = _ops(N, H, [J])
+    st = torch.from_numpy(lattices.random_phase_states(N, R, seed=32).view(np.float64).copy()).cuda()
+    mu = torch.zeros(2 * M * M, dtype=torch.float64, device="cuda")
+    rows = []
+    for lab, prec in (("fp64", PREC_FP64), ("mixed", PREC_MIXED)):
+        for w in widths:
+            o = make_opts(precision=prec, fmt=2, block_width=w)
+            f = lambda: moments2d_dev(Hg, Jg, Jg, st, R, M, mu, opts=o, session=sess)
+            f()
+            f()
+            torch.cuda.synchronize()
+            sess.enable_timing(True)
+            sess.phase_times(reset=True)
+            for _ in range(reps):
+                f()
+            torch.cuda.synchronize()
+            ph, _ = sess.phase_times(reset=True)
+            sess.enable_timing(False)
+            rec = ph[0] / reps
+            choice = {k: v for k, v in Hg.tuned().items()
+                      if k.startswith("lr:%d:%s:" % (w, "f64" if prec == PREC_FP64 else "f32"))}
+            rows.append({"precision": lab, "block_width": w, "recursion_ms": round(rec, 3),
+                         "us_per_step_and_vector": round(1e3 * rec / (M * R), 3), "choice": choice})
+    return {"workload": "lr_widths_kane_mele_%dx%d" % (Lc, Lc), "N": N, "R": R, "M": M, "rows": rows}
 
 
 def run_cubic_width(L, R, M, reps):
@@ -448,7 +484,7 @@ def main(argv=None):
     ap = argparse.ArgumentParser()
     ap.add_argument("workload", choices=["dos", "cubic", "cubic_full", "spin", "layouts", "realisations",
                                          "lr_layouts", "cubic_width", "moments2d", "recur1d", "time_corr", "supercell",
-                                         "locality"])
+                                         "locality", "lr_widths"])
     ap.add_argument("--precision", type=int, default=PREC_MIXED, help="moments2d: LINQT_PREC_* value")
     ap.add_argument("--reps", type=int, default=5)
     ap.add_argument("--cells", type=int, default=64, help="spin: Kane-Mele cells per side")
@@ -480,6 +516,8 @@ def main(argv=None):
         r = run_supercell(4, 1, 2048, "HAM", a.reps)
     elif a.workload == "time_corr":
         r = run_time_corr(128, 16, 512, 40, 1.0, a.reps)
+    elif a.workload == "lr_widths":
+        r = run_lr_widths(a.cells, a.vectors, a.moments, (2, 4, 8, 16), a.reps)
     elif a.workload == "locality":
         r = run_locality(a.side, (8, 64, 256), a.moments, a.reps)
     elif a.workload == "recur1d":
