@@ -86,6 +86,12 @@ __device__ __forceinline__ void ld_row(const float2 *p, float2 (&o)[V]) {
   }
 }
 
+// Ask L2 for the line holding p (a hint: no register, no wait), so that a load of p issued
+// after other long-latency loads finds it there.
+__device__ __forceinline__ void prefetch_l2(const void *p) {
+  asm volatile("prefetch.global.L2 [%0];\n" ::"l"(p));
+}
+
 template <int V>
 __device__ __forceinline__ void st_row(double2 *p, const double2 (&v)[V]) {
 #pragma unroll
@@ -239,6 +245,10 @@ __global__ void __launch_bounds__(kThreads)
       double2 aL[VPT], aR[VPT];
 #pragma unroll
       for (int u = 0; u < VPT; ++u) aL[u] = aR[u] = make_double2(0, 0);
+      const size_t base = (size_t)row * R + c0;
+      // the previous vectors of this row, read after the gathers
+      if (doL && pL) prefetch_l2(pL + base);
+      if (yR && pR) prefetch_l2(pR + base);
 #pragma unroll 4
       for (int k = b; k < e; k += st) {
         const int j = ci[k];
@@ -247,7 +257,6 @@ __global__ void __launch_bounds__(kThreads)
         if (doL) gather_fma<C, VPT>(h, xL + off, aL);
         gather_fma<C, VPT>(h, xR + off, aR);
       }
-      const size_t base = (size_t)row * R + c0;
       if (HAS_V) {
         double2 aV[VPT];
 #pragma unroll
@@ -343,9 +352,10 @@ __global__ void __launch_bounds__(kThreads)
       double2 acc[VPT];
 #pragma unroll
       for (int u = 0; u < VPT; ++u) acc[u] = make_double2(0, 0);
+      const size_t base = (size_t)row * ldx + coff + c0;
+      if (prev) prefetch_l2(prev + base);  // T_{s-1} of this row, read after the gathers
 #pragma unroll 4
       for (int k = b; k < e; k += st) gather_fma<C, VPT>(to_d2(hv[k]), cur + (size_t)ci[k] * ldx + coff + c0, acc);
-      const size_t base = (size_t)row * ldx + coff + c0;
       C pv[VPT], yv[VPT], xv[VPT];
       if (prev) ld_row<VPT>(prev + base, pv);
 #pragma unroll
