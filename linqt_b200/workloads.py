@@ -368,9 +368,10 @@ def run_recur1d_once(L, R, M, prec, fmt=0):
 
 def run_locality(L, widths, M, reps):
     """The 1D DOS recursion on the cubic Anderson lattice L^3 with the rows visited in their
-    natural order (CSR), in the locality order (SELL_LOCAL) and as autotuned, per block width and
-    precision of the blocks (one block of R vectors, CUDA events; the locality order is built
-    and the autotuner runs in the untimed first call)."""
+    natural order (CSR), in the locality order (FORMAT_LOCAL) and as autotuned, per block width,
+    precision of the blocks and of the operator values (complex128, or complex64 with FP32
+    blocks), one block of R vectors, CUDA events; the locality order is built and the autotuner
+    runs in the untimed first call."""
     import torch
     from .core import FORMAT_AUTO, FORMAT_CSR, FORMAT_LOCAL, random_phase_states_dev
     N, H = lattices.cubic_lattice(L, 1.0, 2.0, 41)
@@ -385,13 +386,13 @@ def run_locality(L, widths, M, reps):
         st = torch.empty(2 * R * N, dtype=torch.float64, device="cuda")
         random_phase_states_dev(N, R, 45, st, session=sess)
         mu = torch.zeros(2 * M, dtype=torch.float64, device="cuda")
-        for prec in (PREC_FP64, PREC_MIXED):
+        for prec, c64 in ((PREC_FP64, 0), (PREC_MIXED, 0), (PREC_MIXED, 1)):
             esz = 16 if prec == PREC_FP64 else 8
-            by = Hg.nnz * 20 + 4 * (N + 1) + 3 * esz * N * R
-            res = {"R": R, "blocks": "fp64" if prec == PREC_FP64 else "fp32"}
+            by = Hg.nnz * (12 if c64 else 20) + 4 * (N + 1) + 3 * esz * N * R
+            res = {"R": R, "blocks": "fp64" if prec == PREC_FP64 else "fp32", "operator": "c64" if c64 else "c128"}
             ref = None
             for name, fmt in (("csr", FORMAT_CSR), ("local", FORMAT_LOCAL), ("auto", FORMAT_AUTO)):
-                o = make_opts(precision=prec, fmt=fmt, block_width=R)
+                o = make_opts(precision=prec, fmt=fmt, block_width=R, operator_precision=c64)
                 moments1d_dev(Hg, None, st, R, M, mu, opts=o, session=sess)
                 ms = _timed(lambda: moments1d_dev(Hg, None, st, R, M, mu, opts=o, session=sess), reps, torch)
                 gbs = (M + 1) // 2 * by / (ms * 1e-3) / 1e9
@@ -401,11 +402,13 @@ def run_locality(L, widths, M, reps):
                 res[name] = {"ms": round(ms, 3), "GBps": round(gbs, 1), "hbm_frac": round(gbs / peak, 3),
                              "rel_diff_vs_csr": float(np.abs(m - ref).max() / np.abs(ref).max())}
             res["auto"]["choice"] = {k: v for k, v in Hg.tuned().items() if (":%d:" % R) in k and
-                                     (":f64:" if prec == PREC_FP64 else ":f32:") in k}
+                                     (":f64:" if prec == PREC_FP64 else ":f32:") in k and
+                                     k.startswith("1d64:" if c64 else "1d:")}
             rows.append(res)
         del st
         torch.cuda.empty_cache()
-    return {"workload": "locality_cubic_%d" % L, "N": N, "M": M, "bytes_per_step": "nnz*20 + 4(N+1) + 3*esz*N*R",
+    return {"workload": "locality_cubic_%d" % L, "N": N, "M": M,
+            "bytes_per_step": "nnz*(20 or 12 with complex64 values) + 4(N+1) + 3*esz*N*R",
             "hbm_peak_GBps": peak, "hbm_peak_source": src, "rows": rows}
 
 
