@@ -498,6 +498,7 @@ def main(argv=None):
     ap.add_argument("--mixed", default="1", help="spin: comma-separated mixed precisions beside FP64 (1 = 4-digit "
                                                  "INT8 contraction, 4 = 3-digit)")
     ap.add_argument("--format", type=int, default=0, help="recur1d: LINQT_FORMAT_* value")
+    ap.add_argument("--widths", default="8,64,256", help="locality: comma-separated block widths")
     a = ap.parse_args(argv)
     if a.workload == "dos":
         N, H = lattices.square_lattice(256, 1.0, 1.0, 11)
@@ -522,7 +523,7 @@ def main(argv=None):
     elif a.workload == "lr_widths":
         r = run_lr_widths(a.cells, a.vectors, a.moments, (2, 4, 8, 16), a.reps)
     elif a.workload == "locality":
-        r = run_locality(a.side, (8, 64, 256), a.moments, a.reps)
+        r = run_locality(a.side, tuple(int(x) for x in a.widths.split(",")), a.moments, a.reps)
     elif a.workload == "recur1d":
         r = run_recur1d_once(a.side, a.vectors, a.moments, a.precision, a.format)
     elif a.workload == "moments2d":
