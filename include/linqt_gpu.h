@@ -98,7 +98,12 @@ typedef struct linqt_opts {
                        linqt_moments1d_realisations[_dev]): 0 = complex128 (default), 1 = complex64 (each
                        value rounded once to FP32, products accumulated in FP64; every layout, persistent
                        recursion); other solvers accept 0 only */
-  int reserved[8];
+  int thread_shape; /* 1D moments (linqt_moments1d[_dev]) in one persistent launch: 0 = the format's
+                       choice (shape 0, or autotuned with LINQT_FORMAT_AUTO); s + 1 = thread shape s,
+                       for tests and experiments (shape s of a block of R columns: min(R, 32) >> s
+                       threads per row, at most 8 columns per thread; an invalid s is
+                       LINQT_ERR_INVALID) */
+  int reserved[7];
 } linqt_opts;
 
 /* ---- library / sessions ------------------------------------------------ */

@@ -34,7 +34,7 @@ class LinqtError(RuntimeError):
 class Opts(ctypes.Structure):
     _fields_ = [("precision", c_int), ("format", c_int), ("block_width", c_int), ("doubling", c_int),
                 ("use_graphs", c_int), ("step_launches", c_int), ("realisations", c_int), ("operator_precision", c_int),
-                ("reserved", c_int * 8)]
+                ("thread_shape", c_int), ("reserved", c_int * 7)]
 
 
 class Request(ctypes.Structure):

@@ -49,7 +49,7 @@ def _ptr(x):
 
 
 def make_opts(precision=PREC_FP64, fmt=0, block_width=0, doubling=0, step_launches=0, use_graphs=0,
-              realisations=0, operator_precision=OP_C128):
+              realisations=0, operator_precision=OP_C128, thread_shape=0):
     """Solver options (linqt_opts).  doubling: 0 auto, 1 force, 2 off.  step_launches: 1 = one launch per
     recursion step instead of the persistent cooperative kernel.  use_graphs: 1 = *_dev solves replayed
     from CUDA graphs after their first call.  realisations: 0 autotuned, 1 stacked in one launch,
@@ -60,6 +60,7 @@ def make_opts(precision=PREC_FP64, fmt=0, block_width=0, doubling=0, step_launch
     o.use_graphs = use_graphs
     o.realisations = realisations
     o.operator_precision = operator_precision
+    o.thread_shape = thread_shape
     return o
 
 

@@ -358,6 +358,7 @@ static linqt_opts defaults(const linqt_opts *o) {
                  d.format == LINQT_FORMAT_LOCAL,
              "opts.format: unknown sparse format");
   LQ_REQUIRE(d.operator_precision == 0 || d.operator_precision == 1, "opts.operator_precision must be 0 or 1");
+  LQ_REQUIRE(d.thread_shape >= 0, "opts.thread_shape must be >= 0");
   return d;
 }
 
@@ -588,7 +589,13 @@ static void moments1d_dev(Session *s, const DeviceOp &H, const DeviceOp *op, con
   const size_t blk = esz * (size_t)N * Rc;
   double2 *dots = (double2 *)s->get("m1_dots", sizeof(double2) * 2 * (size_t)steps * nchunks);
   RecCfg cfg;
-  if (!o.step_launches) cfg = tune(Rc, nullptr);
+  if (!o.step_launches) {
+    cfg = tune(Rc, nullptr);
+    if (o.thread_shape > 0) {
+      LQ_REQUIRE(o.thread_shape - 1 < recur_shapes(Rc), "opts.thread_shape: no such shape at this block width");
+      cfg.shape = o.thread_shape - 1;
+    }
+  }
   LQ_CUDA(cudaMemsetAsync(dots, 0, sizeof(double2) * 2 * (size_t)steps * nchunks, s->stream));
   for (int c = 0; c < nchunks; ++c) {
     void *b0 = T, *b1 = T + blk, *b2 = T + 2 * blk;

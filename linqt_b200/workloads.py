@@ -252,7 +252,10 @@ def run_cubic_full(L, S, Rs, M, mode=0):
         mus[label] = mu.cpu().numpy().view(np.complex128).reshape(S, M)
         peak, src = _hbm_peak()
         out[label] = {"ms_per_solve": ms, "steps_nnz_per_s": M * R * nnz / (ms * 1e-3),
-                      "recursion_GBps": gbs, "hbm_frac": gbs / peak, "hbm_peak_GBps": peak, "hbm_peak_source": src}
+                      "recursion_GBps": gbs, "hbm_frac": gbs / peak, "hbm_peak_GBps": peak, "hbm_peak_source": src,
+                      "autotuned": {":".join(k.split(":")[:3]): v for k, v in ops[0].tuned().items()
+                                    if (":f64" if prec == PREC_FP64 else ":f32") in k
+                                    and ("c64" in k or k.startswith("1d64")) == bool(c64)}}
     for label in ("mixed", "mixed_c64"):
         e = np.abs(mus[label] - mus["fp64"]).max(axis=1) / np.abs(mus["fp64"]).max(axis=1)
         out[label]["err_mu_vs_fp64_per_seed"] = [float(x) for x in e]

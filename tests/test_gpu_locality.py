@@ -86,3 +86,25 @@ def test_autotuner_considers_the_local_order(oracle_lib):
     layouts = [v for k, v in tuned.items() if k.startswith("1d:")]
     assert layouts and all(re.fullmatch(r"(csr|csr_nocache|sell\d+(_local)?) shape \d", v) for v in layouts)
     assert any(k.startswith("1dw:") and re.fullmatch(r"width \d+", v) for k, v in tuned.items())
+
+
+@pytest.mark.parametrize("R", [1, 2, 8, 64])
+def test_every_1d_thread_shape(oracle_lib, R):
+    """Each thread shape of the 1D recursion (opts.thread_shape), in the natural and the
+    locality order, against the oracle, FP64 blocks at the FP64 tolerance and FP32 blocks at
+    the mixed path's."""
+    N, H = lattices.cubic_lattice(24, t=1.0, W=2.0, seed=52)  # 13,824 rows: two parts
+    Hg, Ho, _ = setup(oracle_lib, N, H)
+    st = lattices.random_phase_states(N, R, seed=53)
+    M = 96
+    ref = oracle_lib.moments1d(Ho, None, st, M)
+    shapes = {1: 1, 2: 2, 8: 4, 64: 3}[R]  # threads per row min(R, 32) >> s, <= 8 columns each
+    for fmt in (lq.FORMAT_CSR, lq.FORMAT_LOCAL):
+        for s in range(shapes):
+            mu = lq.moments1d(Hg, None, st, M, opts=lq.make_opts(fmt=fmt, block_width=R, thread_shape=s + 1))
+            assert rel(mu, ref) < TOL, (fmt, s)
+            mx = lq.moments1d(Hg, None, st, M, opts=lq.make_opts(precision=lq.PREC_MIXED, fmt=fmt, block_width=R,
+                                                                  thread_shape=s + 1))
+            assert rel(mx, ref) < 1e-7, (fmt, s)
+    with pytest.raises(lq.LinqtError):
+        lq.moments1d(Hg, None, st, M, opts=lq.make_opts(block_width=R, thread_shape=shapes + 1))
