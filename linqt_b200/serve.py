@@ -267,6 +267,9 @@ def main(argv=None):
     ap.add_argument("--n-max", type=float, default=1e6)
     ap.add_argument("--m-max", type=int, default=1024)
     ap.add_argument("--r-max", type=int, default=32)
+    ap.add_argument("--minimal", action="store_true",
+                    help="only the timed serial FP64 pass and the timed Poisson pass through the server (each "
+                         "warmed up on the short warm-up requests), for streams too long for the full set of passes")
     a = ap.parse_args(argv)
     reqs, gaps = request_stream(a.requests, n_max=a.n_max, m_max=a.m_max, r_max=a.r_max)
     prepared = _prepare(reqs)
@@ -292,20 +295,25 @@ def main(argv=None):
         return out
 
     serial(warm_r, warm_p, False)
-    # an untimed pass of the whole stream first (workspaces, the device pool); the serial
-    # passes run before the server exists, since its pool keeps up to its budget cached
-    serial(reqs, prepared, True)
+    if not a.minimal:
+        # an untimed pass of the whole stream first (workspaces, the device pool); the serial
+        # passes run before the server exists, since its pool keeps up to its budget cached
+        serial(reqs, prepared, True)
     t_ser, svc = serial(reqs, prepared, True)
-    t_mix, svc_mix = serial(reqs, prepared, False)
+    t_mix = serial(reqs, prepared, False)[0] if not a.minimal else None
     sess.close()
     torch.cuda.empty_cache()
     srv = Server(0, 0, a.max_active)
-    run_stream(reqs, prepared, np.zeros_like(gaps), 0.0, server=srv)  # untimed: pinned blocks, pool
+    if a.minimal:
+        run_stream(warm_r, warm_p, np.zeros(len(warm_r)), 0.0, server=srv)  # untimed: pinned blocks, pool
+    else:
+        run_stream(reqs, prepared, np.zeros_like(gaps), 0.0, server=srv)
     mean_gap = t_ser / len(reqs) / a.load
     arrivals = np.cumsum(gaps) * mean_gap
     lat_ser = 1e3 * fifo_latencies(arrivals, svc / 1e3)
     lat, makespan = run_stream(reqs, prepared, gaps, mean_gap, server=srv)
-    lat_sat, makespan_sat = run_stream(reqs, prepared, np.zeros_like(gaps), 0.0, server=srv)
+    if not a.minimal:
+        lat_sat, makespan_sat = run_stream(reqs, prepared, np.zeros_like(gaps), 0.0, server=srv)
     retried = srv.retries()
     srv.close()
     q = lambda x, p: float(np.percentile(x, p)) if len(x) else None
@@ -327,10 +335,11 @@ def main(argv=None):
                    "kubo_returns": "moment table and sigma(E) at the smallest 256*2^j >= 2M energies"},
         "server": dict(split(lat), requests_per_s=len(reqs) / makespan),
         "serial_fp64": dict(split(lat_ser), requests_per_s=len(reqs) / t_ser),
-        "serial_request_precision_requests_per_s": len(reqs) / t_mix,
-        "server_saturated": dict(split(lat_sat), requests_per_s=len(reqs) / makespan_sat),
         "requests_rerun": {"on_the_cooperative_lane": retried[0], "alone_after_nomem": retried[1]},
     }
+    if not a.minimal:
+        out["serial_request_precision_requests_per_s"] = len(reqs) / t_mix
+        out["server_saturated"] = dict(split(lat_sat), requests_per_s=len(reqs) / makespan_sat)
     print(json.dumps(out))
 
 
