@@ -554,10 +554,12 @@ double coop_share_take(Session *s, double want) {
   // a share comes back when its kernel finishes; the wait is bounded in case a stream
   // stopped running callbacks (a device error), and the grid then sizes itself to what is free
   if (!L.cv.wait_for(g, std::chrono::seconds(120), [&] { return L.free >= floor - 1e-9; })) L.waits_expired++;
-  const double share = std::max(0.02, std::min(want, L.free));
-  L.free -= std::min(share, L.free);
+  // what is given back later is exactly what is taken here; a grid sized from a share near
+  // zero (after an expired wait) still has one CTA
+  const double share = std::max(0.0, std::min(want, L.free));
+  L.free -= share;
   s->held_share = share;
-  return share;
+  return std::max(share, 1e-9);
 }
 
 void coop_share_return(Session *s) {
