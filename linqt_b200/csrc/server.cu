@@ -42,6 +42,8 @@ typedef std::chrono::steady_clock clk;
 // Fraction of the device the slots' persistent grids share (through the server's ledger):
 // a little below 1 leaves room for CTAs of different kernels that do not pack evenly.
 constexpr double kSlotShare = 0.9;
+// Times per slot that a queued request waiting for memory may be passed by later ones.
+constexpr int kMaxBypass = 4;
 
 struct Job {
   long ticket = 0;
@@ -52,6 +54,7 @@ struct Job {
   int block_width = 1;
   int status = 0;  // 0 pending, 1 running, 2 done, <0 error
   bool alone = false;  // ran out of memory next to other requests: runs again with none beside it
+  int bypassed = 0;    // requests admitted before it while it waited for memory
   double latency_ms = 0;
   std::string error;
   clk::time_point t_submit;
@@ -77,8 +80,9 @@ size_t estimate_footprint(const linqt_request &r, int n, int sm_count, int Rc) {
 }
 
 // Vector-block width of a request: the widest power of two up to R whose footprint fits in
-// `cap` (the server's budget shared by its slots), so that one large request cannot hold
-// the device alone; width 1 when none does.
+// `cap` (the server's budget), as a solve alone on the device would choose: a large request
+// then runs as efficiently as alone (and alone, when its footprint leaves no room), while
+// smaller ones that fit pass it in the queue; width 1 when none does.
 int pick_width(const linqt_request &r, int n, int sm_count, size_t cap) {
   int Rc = 1;
   while (Rc < r.R && Rc < 256) Rc <<= 1;
@@ -150,22 +154,29 @@ struct linqt_server {
       std::shared_ptr<Job> job;
       {
         std::unique_lock<std::mutex> g(mu);
-        // admission: the oldest queued job, once its footprint fits next to the running ones;
-        // a job marked `alone` (it ran out of memory next to others) waits until none runs,
-        // and nothing behind it is admitted meanwhile
-        cv.wait(g, [&] {
-          if (stop) return true;
-          if (queue.empty()) return false;
-          const Job &f = *queue.front();
-          return f.alone ? running == 0 : in_use + f.footprint <= budget;
-        });
-        if (stop && queue.empty()) {
+        // admission: the oldest queued job whose footprint fits next to the running ones.  A
+        // job that does not fit may be passed by later ones that do, at most kMaxBypass times
+        // a slot; after that nothing behind it is admitted until it runs.  A job marked `alone`
+        // (it ran out of memory next to others) waits at the head until none runs.
+        const int max_bypass = kMaxBypass * max_active;
+        auto pick = [&]() {
+          for (auto it = queue.begin(); it != queue.end(); ++it) {
+            const Job &f = **it;
+            if (f.alone) return (it == queue.begin() && running == 0) ? it : queue.end();
+            if (in_use + f.footprint <= budget) return it;
+            if (f.bypassed >= max_bypass) return queue.end();
+          }
+          return queue.end();
+        };
+        cv.wait(g, [&] { return (stop && queue.empty()) || pick() != queue.end(); });
+        if (queue.empty()) {  // stopping
           cudaStreamSynchronize(sess->s.stream);  // its share callbacks have run
           return;
         }
-        if (queue.empty()) continue;
-        job = queue.front();
-        queue.pop_front();
+        const auto it = pick();
+        for (auto p = queue.begin(); p != it; ++p) (*p)->bypassed++;
+        job = *it;
+        queue.erase(it);
         in_use += job->footprint;
         job->status = 1;
         running++;
@@ -306,7 +317,7 @@ int linqt_server_submit(linqt_server *srv, const linqt_request *req, long *ticke
     auto job = std::make_shared<Job>();
     job->req = *req;
     const int n = req->H->op.n;
-    job->block_width = pick_width(*req, n, srv->sm_count, srv->budget / srv->max_active);
+    job->block_width = pick_width(*req, n, srv->sm_count, srv->budget);
     job->footprint = estimate_footprint(*req, n, srv->sm_count, job->block_width);
     if (job->footprint > srv->budget)
       fail(LINQT_ERR_NOMEM, "server: request footprint " + std::to_string(job->footprint >> 20) +
