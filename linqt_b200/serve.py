@@ -263,7 +263,7 @@ def main(argv=None):
     ap.add_argument("--requests", type=int, default=400)
     ap.add_argument("--load", type=float, default=1.5,
                     help="offered load: arrival rate / serial FP64 service rate")
-    ap.add_argument("--max-active", type=int, default=4)
+    ap.add_argument("--max-active", type=int, default=2)
     ap.add_argument("--n-max", type=float, default=1e6)
     ap.add_argument("--m-max", type=int, default=1024)
     ap.add_argument("--r-max", type=int, default=32)
