@@ -52,6 +52,19 @@ def test_alone_equals_mixed():
         got, ref = srv.result(t), alone[j % len(work)]
         assert np.abs(got - ref).max() <= 1e-12 * np.abs(ref).max()
     srv.close()
+    # a budget that most requests nearly fill: they wait for memory, later ones that fit
+    # pass them (a bounded number of times), and every result is still the alone one
+    srv = serve.Server(0, 40 << 20, 4)
+    tickets = []
+    for _ in range(2):
+        for kind, Hg, Vg, st, M, prec in work:
+            tickets.append(srv.submit(kind, Hg, Vg if kind == serve.REQ_KUBO_BASTIN else None, st, M, prec))
+    srv.wait_all()
+    for j, t in enumerate(tickets):
+        assert srv.poll(t)[0] == 2
+        got, ref = srv.result(t), alone[j % len(work)]
+        assert np.abs(got - ref).max() <= 1e-12 * np.abs(ref).max()
+    srv.close()
     # and the FP64 requests agree with the regular entry points
     kind, Hg, Vg, st, M, prec = work[1]
     assert np.abs(alone[1] - lq.moments2d(Hg, Vg, Vg, st, M)).max() <= 1e-12 * np.abs(alone[1]).max()
