@@ -220,6 +220,7 @@ struct CoopLedger {
   std::mutex mu;
   std::condition_variable cv;
   double free = 0.9;       // 10 % slack for how CTAs of different grids pack into SMs
+  double capacity = 0.9;   // what `free` is when no grid holds a share
   double min_share = 0.2;  // a grid waits until this much (or all it needs) is free
   long waits_expired = 0;  // waits that gave up (the grid then ran on what was free)
 };
@@ -409,6 +410,13 @@ int coop_grid(Session *s, const void *func, long max_blocks, size_t smem);
 // needs (at most 1): the session's fixed share, or with a ledger what it takes from it.
 double coop_share_take(Session *s, double want);
 void coop_share_return(Session *s);  // gives back a share taken for a grid that did not launch
+// After a launch sized from coop_share_take: the share comes back (host callback on the
+// session stream) once the work enqueued so far has finished.
+void coop_share_hand_back(Session *s);
+// SMs for a persistent non-cooperative kernel that occupies whole SMs (the per-site FFT):
+// all of them, or with a ledger the share it takes (every SM when the ledger is all free),
+// to be given back with coop_share_hand_back after the launch.
+int sm_share_take(Session *s);
 void coop_launch(Session *s, const void *f, int grid, void **args, size_t smem);
 
 // small utilities (util.cu)

@@ -484,9 +484,12 @@ void launch_fft(Session *s, const Tin *L, const Tin *Rv, long K, int M, const do
   const size_t smem = sizeof(double2) * ((size_t)NSEQ * 16 * (16 * R3 + 1) + 16 * 16 * R3 + 16 * R3 + (size_t)M) +
                       sizeof(Tin) * 4 * (size_t)M;
   if (smem > 227 * 1024) fail(LINQT_ERR_UNSUPPORTED, "kubo_fft: nump too large for the shared-memory FFT");
-  const int nb = (int)std::max(1L, std::min(K, (long)s->sm_count));
+  // one CTA per SM (most of its shared memory), persistent over the sites; a server slot
+  // takes its SMs from the server's ledger, so that the slots' persistent grids and this one
+  // never wait for each other's SMs
+  double2 *part = (double2 *)s->get("kubo_part", sizeof(double2) * 2 * (size_t)n * s->sm_count);
+  const int nb = (int)std::max(1L, std::min(K, (long)sm_share_take(s)));
   const long chunk = (K + nb - 1) / nb;
-  double2 *part = (double2 *)s->get("kubo_part", sizeof(double2) * 2 * (size_t)n * nb);
   // every output k < n is written by exactly one thread of each CTA (pairs cover 16 x 16,
   // halves cover the R3 outputs), so the partials need no clearing
   if (2 * M <= n) {
@@ -496,7 +499,10 @@ void launch_fft(Session *s, const Tin *L, const Tin *Rv, long K, int M, const do
     raise_smem_limit((const void *)k_kubo_fft<R3, NSEQ, false, Tin>, smem);
     k_kubo_fft<R3, NSEQ, false, Tin><<<nb, kFftThreads, smem, s->stream>>>(L, Rv, K, chunk, M, pf, part);
   }
-  LQ_LAUNCHED();
+  const cudaError_t le = cudaGetLastError();
+  if (le != cudaSuccess) coop_share_return(s);
+  LQ_CUDA(le);
+  coop_share_hand_back(s);
   k_sum_parts<<<(2 * n + 255) / 256, 256, 0, s->stream>>>(part, nb, 2 * n, acc);
   LQ_LAUNCHED();
 }

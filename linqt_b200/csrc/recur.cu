@@ -586,6 +586,24 @@ void CUDART_CB share_back(void *p) {  // host callback: no CUDA calls here
 }
 }  // namespace
 
+void coop_share_hand_back(Session *s) {
+  if (!s->ledger || s->held_share <= 0) return;
+  ShareToken *t = new ShareToken{s->ledger, s->held_share};
+  s->held_share = 0;
+  const cudaError_t h = cudaLaunchHostFunc(s->stream, share_back, t);
+  if (h != cudaSuccess) {
+    share_back(t);
+    LQ_CUDA(h);
+  }
+}
+
+int sm_share_take(Session *s) {
+  if (!s->ledger || s->coop_share >= 1.0 || s->capturing) return s->sm_count;
+  const double share = coop_share_take(s, 1.0);
+  if (share >= s->ledger->capacity - 1e-9) return s->sm_count;  // nothing else holds a share
+  return std::max(1, (int)(share * s->sm_count));
+}
+
 // Cooperative kernels of all sessions on a device run one after another on one lane
 // stream.  A grid barrier needs every CTA of its grid resident; two persistent grids
 // that each fill the device, launched from two sessions' streams, could hold half the
@@ -606,15 +624,7 @@ void coop_launch(Session *s, const void *f, int grid, void **args, size_t smem) 
       coop_share_return(s);
       LQ_CUDA(e);
     }
-    if (s->held_share > 0) {  // the ledger's share comes back once the kernel has finished
-      ShareToken *t = new ShareToken{s->ledger, s->held_share};
-      s->held_share = 0;
-      const cudaError_t h = cudaLaunchHostFunc(s->stream, share_back, t);
-      if (h != cudaSuccess) {
-        share_back(t);
-        LQ_CUDA(h);
-      }
-    }
+    coop_share_hand_back(s);  // the ledger's share comes back once the kernel has finished
     return;
   }
   static std::mutex table_mu;

@@ -289,7 +289,7 @@ int linqt_server_create(int device, size_t hbm_budget_bytes, int max_active, lin
     s->device = device;
     s->budget = hbm_budget_bytes ? hbm_budget_bytes : (size_t)(fr * 0.8);
     s->max_active = max_active;
-    s->ledger.free = kSlotShare;
+    s->ledger.free = s->ledger.capacity = kSlotShare;
     s->ledger.min_share = kSlotShare / max_active;
     LQ_CUDA(cudaDeviceGetAttribute(&s->sm_count, cudaDevAttrMultiProcessorCount, device));
     // keep up to the budget cached in the device pool between requests (restored at destroy)
