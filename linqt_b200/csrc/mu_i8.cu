@@ -31,7 +31,7 @@
 // (M = 128, N = 128, K = 32), warps 2-5 run the epilogue.  ND = 3: 128-byte K blocks
 // (128-byte swizzle), 2 stages of 96 KB; ND = 4: 64-byte K blocks (64-byte swizzle),
 // 3 stages of 64 KB.  Every mbarrier wait is bounded; on expiry the kernel raises the error
-// flag, stops issuing, drains what it issued, frees TMEM and returns.  No TMA multicast.
+// flag, stops issuing, drains what it issued, frees TMEM and returns.  Every TMA load is issued by and for one CTA.
 #include <cuda.h>
 
 #include <cooperative_groups.h>

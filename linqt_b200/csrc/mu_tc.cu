@@ -22,7 +22,7 @@
 // Two pipeline stages of 96 KB (A hi/lo, B = [B'; B''] hi/lo).  Every mbarrier wait is
 // bounded.  On expiry the kernel raises the error flag, stops issuing work, waits for its
 // own copies and MMAs, frees TMEM and returns.
-// No TMA multicast is used.
+// Every TMA load fills the shared memory of the CTA that issues it.
 #include <cuda.h>
 
 #include <cstdint>

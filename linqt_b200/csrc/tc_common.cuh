@@ -1,5 +1,5 @@
 // Device helpers shared by the tcgen05 kernels (mu_tc.cu, mu_i8.cu): mbarriers with
-// bounded waits, TMA tile loads (no cluster multicast), shared-memory matrix descriptors,
+// bounded waits, TMA tile loads into the issuing CTA only, shared-memory matrix descriptors,
 // MMA completion commits and TMEM loads; on the host, cuTensorMapEncodeTiled through the
 // driver entry point (the runtime is linked statically).
 #pragma once
